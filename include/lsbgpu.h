@@ -1,0 +1,146 @@
+/* lsbgpu.h -- C ABI of the B200 (sm_100a) implementation of LSBFLOW's per-time-step
+ * hot path.  It is the drop-in boundary a Fortran driver binds through iso_c_binding
+ * (bind(C) interfaces with the same argument order as the subroutines they replace)
+ * or a Python/C host binds through ctypes / dlopen.
+ *
+ * Conventions
+ *  - Every function returns an int status: 0 = LSB_OK, negative = error; the message
+ *    of the last error of the calling thread is returned by lsb_last_error().
+ *  - Arrays are FP64 in the reference's Fortran storage order (first index fastest):
+ *      spectral  (nx, ny, nzp)     : nx reals = nx/2 complex kx modes interleaved Re/Im,
+ *                                    ky in FFT order, k = 1 the ceiling, k = nzp the wall
+ *      physical  (nx+2, ny, nzp)   : two pad columns per x row (written as 0, never read)
+ *    nx, ny, nz are the reference's &dimen values, nzp = nz + 1, nzm = nz - 1.
+ *  - Caller-owned host arrays are never retained.  Device state belongs to the handle.
+ *  - A handle is one CUDA stream; it is not thread-safe, distinct handles are.
+ *  - Temperature is not carried: the reference's set-up keeps T and its mean at exactly
+ *    zero (src/init.f90:353-355,429), which makes every temperature term vanish.
+ */
+#ifndef LSBGPU_H
+#define LSBGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LSB_OK 0
+#define LSB_ERR_ARG (-1)
+#define LSB_ERR_CUDA (-2)
+#define LSB_ERR_UNSUPPORTED (-3)
+#define LSB_ERR_STATE (-4)
+#define LSB_ERR_NONFINITE (-5)
+
+typedef struct lsb_handle lsb_handle;
+
+/* Run switches; the reference's namelists &dimen, &run, &param, &sgsin
+ * (src/common.f90:20,78,92,107) restricted to what the time step reads. */
+typedef struct {
+    int nx, ny, nz;
+    int dealiasflag;       /* 0 none, 1 3/2-rule products, 2 (3) exponential spectral filter  */
+    int dealias_layout;    /* 0 = the reference's spanwise padding (src/dealiasing.f90:329,435),
+                              1 = the textbook 3/2 layout                                        */
+    int sgsflag, sgsmodel; /* sgsmodel 0 Smagorinsky, 1 dynamic, 2 sigma, 3 interscale, 4 TNS */
+    int forcing;           /* 1: fringe forcing of src/navierstokes.f90:92-211                 */
+    int bctype;            /* 0 homogeneous, 1 Spalart suction/blowing, 2 H-type strip,
+                              3 ceiling dipole w = A (x-xc)/s exp(-((x-xc)/s)^2)                */
+    int ifrz;
+    int nstart;            /* 0: Euler/BDF2 start-up as src/navierstokes.f90:1500-1590       */
+    int mapping;
+    double xnu, u0, x0, xlen, ylen, zlen;
+    double a, b, cs;       /* 3-point filter weights and the Smagorinsky constant             */
+    double kc, filt_order, filt_amp;
+    double istartbound, samp;
+    double bc3_amp, bc3_xc, bc3_s;
+    double fsize;          /* fringe fraction (bounds the z-CFL region in the diagnostics) */
+} lsb_config;
+
+/* Host set-up arrays (inputs, as the reference passes diag/smat/simat): see
+ * src/init.f90:130-293 and src/helmholtz.f90:13-126.  Matrices are row-major [row][col]. */
+typedef struct {
+    const double* xpts;    /* [nx]  */
+    const double* ypts;    /* [ny]  */
+    const double* zpts;    /* [nzp] */
+    const double* wavx;    /* [nx]  interleaved (wavx[2i] = wavx[2i+1] = i*alpha) */
+    const double* wavy;    /* [ny]  FFT order */
+    double dx, dy;
+    const double* dz1;     /* [nzp][nzp] matrix applied by dfdz  */
+    const double* dz2;     /* [nzp][nzp] matrix applied by d2fdz2 */
+    const double* lam;     /* [nzm] eigenvalues of D2(2:nz,2:nz)   */
+    const double* e;       /* [nzm][nzm] eigenvectors (columns)   */
+    const double* ei;      /* [nzm][nzm] inverse                  */
+    const double* ubar; const double* ubarp; const double* ubarpp;   /* [nzp] */
+    const double* hbot; const double* htop; const double* d2hbot; const double* d2htop; /* [nzp] */
+    const double* lamx;    /* [nx] fringe lambda(x) */
+} lsb_setup;
+
+typedef struct {
+    double divergence;     /* mean |div u|, divcheck (src/derivatives.f90:348-392)    */
+    double umax, umin, vmax, vmin, wmax, wmin;
+    double cflx, cfly, cflz;
+    double energy_total, energy_pert;  /* ener (src/orrsomm.f90:625-666) */
+    double t, dt;
+    int istep;
+    int nonfinite;         /* 1 if any NaN/Inf was found in u, v, w */
+} lsb_diagnostics;
+
+const char* lsb_last_error(void);
+int lsb_version(void);
+
+/* ---------------- Tier 2: resident state --------------------------------------------- */
+/* replaces initialize()'s device-side part (src/init.f90:7-127) */
+int lsb_create(const lsb_config* cfg, const lsb_setup* setup, lsb_handle** out);
+int lsb_destroy(lsb_handle* h);
+/* run on a caller stream (cudaStream_t passed as void*); NULL restores the handle's own */
+int lsb_set_stream(lsb_handle* h, void* stream);
+/* the module ``core`` state (src/common.f90:162-175) and the ``time`` scalars */
+int lsb_upload_state(lsb_handle* h, const double* uf, const double* vf, const double* wf,
+                     const double* pf, const double* pnf,
+                     const double* unif, const double* unmif, const double* nlnif, const double* nlnmif,
+                     double t, double dt, double dt2, double dt3, int istep);
+int lsb_download_state(lsb_handle* h, double* uf, double* vf, double* wf, double* pf, double* pnf,
+                       double* unif, double* unmif, double* nlnif, double* nlnmif,
+                       double* t, double* dt, double* dt2, double* dt3, int* istep);
+/* device-resident variants: pointers are device addresses of the same layouts */
+int lsb_upload_state_device(lsb_handle* h, const double* uf, const double* vf, const double* wf);
+int lsb_download_velocity_device(lsb_handle* h, double* uf, double* vf, double* wf);
+/* nsteps calls of timestep() (src/navierstokes.f90:10-90) on the device */
+int lsb_step(lsb_handle* h, int nsteps);
+int lsb_diag(lsb_handle* h, lsb_diagnostics* out);
+int lsb_synchronize(lsb_handle* h);
+/* asynchronous host<->device copies of u, v, w only (the histories stay resident);
+ * host buffers should be pinned for the copies to overlap */
+int lsb_upload_velocity(lsb_handle* h, const double* uf, const double* vf, const double* wf);
+int lsb_download_velocity(lsb_handle* h, double* uf, double* vf, double* wf);
+/* CUDA-event timers per kernel group: enable=1 clears and starts, 0 stops;
+ * the report has one "group launches total_ms" line per group */
+int lsb_timers(lsb_handle* h, int enable);
+int lsb_timer_report(lsb_handle* h, char* buf, int buflen);
+
+/* ---------------- Tier 1: the reference's subroutine interfaces (host arrays) --------- */
+/* horfft(ain, ainf, is)             src/horfft.f90:61      is = -1 phys->spec, +1 spec->phys */
+int lsb_horfft(lsb_handle* h, double* ain, double* ainf, int is);
+/* dealiasing_2d_fftw(a, b, ab)      src/dealiasing.f90:262 (physical in/out)   */
+int lsb_dealias_product(lsb_handle* h, const double* a, const double* b, double* ab);
+/* dfdx / dfdy / dfdz / d2fdz2 / lapl src/derivatives.f90:261,283,112,161,306 */
+int lsb_dfdx(lsb_handle* h, const double* uf, double* out);
+int lsb_dfdy(lsb_handle* h, const double* uf, double* out);
+int lsb_dfdz(lsb_handle* h, const double* uf, double* out);
+int lsb_d2fdz2(lsb_handle* h, const double* uf, double* out);
+int lsb_lapl(lsb_handle* h, const double* uf, double* out);
+/* divuv(uf, vf, divf)               src/derivatives.f90:394 */
+int lsb_divuv(lsb_handle* h, const double* uf, const double* vf, double* out);
+/* solve_helmholtz(rhs, dtnui, n, diag, smat, simat)   src/helmholtz.f90:130 (n = nzm;
+ * the eigenbasis given at lsb_create is used) */
+int lsb_solve_helmholtz(lsb_handle* h, double* rhs, double dtnui);
+/* solve_nhom_helmholtz(rhs, bc, dtnui, diag, smat, simat)   src/helmholtz.f90:211 */
+int lsb_solve_nhom_helmholtz(lsb_handle* h, double* rhs, const double* bc, double dtnui);
+/* nlterm_skewsym(uif, tempf, nltermif, nltempf, sgsflag)  src/navierstokes.f90:658
+ * velocity part: uif = 3 spectral fields, nltermif = 3 spectral fields */
+int lsb_nlterm(lsb_handle* h, const double* uif, double* nltermif);
+/* tau_sgs(ui, uiuj, duidxj, tauij)  src/sgsterm.f90:10  (physical (nx+2,ny,nzp,3[,3]) arrays) */
+int lsb_tau_sgs(lsb_handle* h, const double* ui, const double* uiuj, const double* duidxj, double* tauij);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LSBGPU_H */

@@ -1,0 +1,177 @@
+// FP64 z contractions on the tensor cores: out = A . in over every (kx, ky) column.
+//
+// These are the Chebyshev derivatives dfdz / d2fdz2 (src/derivatives.f90:112-188, the
+// DCT-I path of src/chebyshev.f90:204-270 written as its dense matrix) and the two
+// eigenbasis products of solve_helmholtz (src/helmholtz.f90:130-208), with the
+// lifting-function prologue / epilogue of solve_nhom_helmholtz (src/helmholtz.f90:
+// 324-353) and the pressure / Poisson right-hand sides of navierstokes_update
+// (src/navierstokes.f90:1411-1476) fused in.
+//
+// tcgen05 has no FP64 kind, so the FP64 form uses the FP64 tensor-core MMA
+// (mma.sync m8n8k4 f64).  One CTA owns all Mp rows of a 64-column block: 8 warps x
+// 8 columns, Mp/8 row tiles per warp, A and B staged through shared memory in
+// k-chunks of 16 with conflict-free strides.
+#include "lsb_internal.cuh"
+
+namespace lsb {
+
+constexpr int GBN = 64;
+constexpr int GBK = 16;
+constexpr int LDA_S = 20;  // doubles; 8r mod 32 distinct for r = 0..3 -> no bank conflicts
+constexpr int LDB_S = 68;
+
+__device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(c[0]), "+d"(c[1])
+                 : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ double w2_of(const GemmArgs& g, long long c) {
+    const int i = (int)(c % g.nx);
+    const int j = (int)(c / g.nx);
+    const double wx = g.wavx[i], wy = g.wavy[j];
+    return wx * wx + wy * wy;
+}
+
+__device__ __forceinline__ void cp_async8(void* smem_ptr, const void* gptr, int src_bytes) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem_ptr);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gptr), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+template <int MT>
+__global__ void __launch_bounds__(256) k_gemm(GemmArgs g) {
+    extern __shared__ double gsm[];
+    double (*As)[MT * 8][LDA_S] = reinterpret_cast<double (*)[MT * 8][LDA_S]>(gsm);
+    double (*Bs)[GBK][LDB_S] = reinterpret_cast<double (*)[GBK][LDB_S]>(gsm + 2 * MT * 8 * LDA_S);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int f = blockIdx.y;
+    const long long c0 = (long long)blockIdx.x * GBN;
+    const double* in = g.in + f * g.in_fstride;
+    const double* bcb = g.bcb ? g.bcb + f * g.bc_fstride : nullptr;
+    const double* bct = g.bct ? g.bct + f * g.bc_fstride : nullptr;
+    const bool lift = (g.epi != 5) && (bcb != nullptr);
+    double acc[MT][2];
+#pragma unroll
+    for (int t = 0; t < MT; ++t) acc[t][0] = acc[t][1] = 0.0;
+
+    auto load_chunk = [&](int buf, int kc) {
+        for (int idx = tid; idx < MT * 8 * GBK; idx += 256) {
+            const int r = idx / GBK, cc = idx % GBK;
+            cp_async8(&As[buf][r][cc], &g.A[(long long)r * g.Kp + kc + cc], 8);
+        }
+        for (int idx = tid; idx < GBK * GBN; idx += 256) {
+            const int kk = idx / GBN, n = idx % GBN;
+            const int k = kc + kk;
+            const long long c = c0 + n;
+            const bool ok = (k < g.K && c < g.C);
+            const int kin = k + g.koff;
+            if (!lift) {
+                cp_async8(&Bs[buf][kk][n], ok ? (const void*)&in[(long long)kin * g.C + c] : (const void*)in, ok ? 8 : 0);
+            } else {
+                double v = 0.0;
+                if (ok) {
+                    v = in[(long long)kin * g.C + c];
+                    const double w2 = w2_of(g, c);
+                    const double fac = (-w2) - g.lift_sigma;
+                    const double abot = g.d2hb[kin] + fac * g.hb[kin];
+                    v = v - abot * bcb[c];
+                    const double atop = g.d2ht[kin] + fac * g.ht[kin];
+                    v = v - atop * bct[c];
+                }
+                Bs[buf][kk][n] = v;
+            }
+        }
+        cp_async_commit();
+    };
+
+    const int nchunks = g.Kp / GBK;
+    load_chunk(0, 0);
+    for (int ch = 0; ch < nchunks; ++ch) {
+        const int buf = ch & 1;
+        if (ch + 1 < nchunks) {
+            load_chunk(buf ^ 1, (ch + 1) * GBK);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k4 = 0; k4 < GBK / 4; ++k4) {
+            const double b = Bs[buf][k4 * 4 + (lane & 3)][warp * 8 + (lane >> 2)];
+#pragma unroll
+            for (int t = 0; t < MT; ++t) {
+                const double a = As[buf][t * 8 + (lane >> 2)][k4 * 4 + (lane & 3)];
+                dmma(acc[t], a, b);
+            }
+        }
+        __syncthreads();
+    }
+
+    double* out = g.out + f * g.out_fstride;
+    const double* aux = g.aux ? g.aux + f * g.out_fstride : nullptr;
+#pragma unroll
+    for (int t = 0; t < MT; ++t) {
+        const int r = t * 8 + (lane >> 2);
+        if (r >= g.M) continue;
+        const long long cb = c0 + warp * 8 + (lane & 3) * 2;
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const long long c = cb + e;
+            if (c >= g.C) continue;
+            const long long o = (long long)(r + g.roff) * g.C + c;
+            double v = acc[t][e];
+            switch (g.epi) {
+                case EPI_STORE: break;
+                case EPI_AXPBY: v = g.alpha * v + (g.beta != 0.0 ? g.beta * out[o] : 0.0); break;
+                case EPI_HELM_SCALE: {
+                    const double w2 = w2_of(g, c);
+                    const double dfac = (-w2) - g.sigma;
+                    v = v / (g.lam[r] + dfac);
+                    break;
+                }
+                case EPI_PRESSURE: {
+                    const double w2 = w2_of(g, c);
+                    v = (w2 == 0.0) ? 0.0 : -(v + aux[o]) / (w2 * g.alpha * g.beta);
+                    break;
+                }
+                case EPI_POISSON_RHS: {
+                    const double w2 = w2_of(g, c);
+                    v = -v - w2 * aux[o];
+                    break;
+                }
+                default: {  // EPI_LIFT_ADD (5): acc + hb*bcb + ht*bct
+                    if (bcb != nullptr) v = v + g.hb[r + g.roff] * bcb[c] + g.ht[r + g.roff] * bct[c];
+                    break;
+                }
+            }
+            out[o] = v;
+        }
+    }
+}
+
+void launch_gemm(const GemmArgs& g, cudaStream_t s) {
+    dim3 grid((unsigned)((g.C + GBN - 1) / GBN), g.nfields);
+    const int mt = g.Mp / 8;
+    switch (mt) {
+#define LSB_MT(n)                                                                                       \
+    case n: {                                                                                           \
+        const size_t sm = (size_t)(2 * n * 8 * LDA_S + 2 * GBK * LDB_S) * sizeof(double);               \
+        static bool attr = false;                                                                       \
+        if (!attr) {                                                                                    \
+            cudaFuncSetAttribute(k_gemm<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);      \
+            attr = true;                                                                                \
+        }                                                                                               \
+        k_gemm<n><<<grid, 256, sm, s>>>(g);                                                             \
+        break;                                                                                          \
+    }
+        LSB_MT(1) LSB_MT(2) LSB_MT(3) LSB_MT(4) LSB_MT(5) LSB_MT(6) LSB_MT(7) LSB_MT(8) LSB_MT(9)
+        LSB_MT(10) LSB_MT(11) LSB_MT(12) LSB_MT(13) LSB_MT(14) LSB_MT(15) LSB_MT(16) LSB_MT(17)
+#undef LSB_MT
+        default: break;
+    }
+}
+
+}  // namespace lsb

@@ -1,0 +1,141 @@
+// The library handle (shared by lsbgpu.cu and sgs_kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "lsb_internal.cuh"
+#include "lsbgpu.h"
+
+namespace lsb {
+
+struct LsbError {
+    int code;
+    std::string msg;
+};
+
+#define CK(x)                                                                                    \
+    do {                                                                                         \
+        cudaError_t e_ = (x);                                                                    \
+        if (e_ != cudaSuccess)                                                                   \
+            throw ::lsb::LsbError{LSB_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)}; \
+    } while (0)
+
+struct Mat {
+    double* p = nullptr;
+    int M = 0, K = 0, Mp = 0, Kp = 0;
+};
+
+// SGS working set (physical fields on the unpadded grid, [nzp][ny][nx] each)
+struct SgsWork {
+    bool nonsym = false;        // interscale model: tau is not symmetric
+    double* tau = nullptr;      // 9 fields, index 3*l + m
+    double* H9 = nullptr;       // 9 spectral fields h(l,m) when tau is not symmetric
+    double* w = nullptr;        // model work fields
+    int nw = 0;
+    double* zf = nullptr;       // z filter coefficients: az, bz, cz for (a, b) and for (1, 1): 6*nzp
+    double* delta = nullptr;    // [nzp] (dx dy dz)^(1/3) of dynamic/sigma
+    double* sdelta = nullptr;   // [nzp] static-Smagorinsky delta (its own quirks)
+    double* scal = nullptr;     // device scalars (u_tau average)
+};
+
+}  // namespace lsb
+
+struct lsb_handle {
+    lsb_config cfg{};
+    lsb::Dims d;
+    cudaStream_t own = nullptr, stream = nullptr;
+    std::vector<void*> allocs;
+
+    // set-up arrays
+    double *wavx = nullptr, *wavy = nullptr, *zpts = nullptr, *ubar = nullptr, *ubarp = nullptr, *ubarpp = nullptr;
+    double *hb = nullptr, *ht = nullptr, *d2hb = nullptr, *d2ht = nullptr, *lam = nullptr, *lamx = nullptr;
+    std::vector<double> h_xpts, h_ypts, h_zpts, h_ubar;
+    double dx = 0, dy = 0;
+    lsb::Mat m_dz1, m_dz2, m_dz2rows, m_ei, m_eext;
+    // FFT plans: y (ny), y padded (nyl), x real (nx), x real padded (nxl)
+    lsb::FftPlan py, pyl;
+    lsb::RealPlan rx, rxl;
+    // state
+    double *vel = nullptr, *veln = nullptr, *velnm = nullptr;  // 3S each
+    double *nlc = nullptr, *nln = nullptr, *nlnm = nullptr;   // 3S each
+    double *p = nullptr, *pn = nullptr;                       // S each
+    // scratch
+    double *filt = nullptr, *dz = nullptr, *H = nullptr, *rhs = nullptr, *T = nullptr, *divf = nullptr;
+    double *Y = nullptr;     // 18 y-intermediates on the (padded) transform grid
+    double *Yu = nullptr;    // 12 y-intermediates on the unpadded grid
+    double *phys = nullptr;  // physical scratch (unpadded grid), kPhys fields
+    double *bc = nullptr, *bcp = nullptr, *d2w = nullptr, *bshape = nullptr;
+    double *io = nullptr;    // host-transfer staging, 12 S
+    double *red = nullptr;   // reduction scratch
+    lsb::SgsWork sgs;
+    int* sgs_wall = nullptr;
+    int sgs_nwall = 0;
+    // per kernel-group CUDA-event timers (lsb_timers / lsb_timer_report)
+    bool timing = false;
+    std::map<std::string, std::vector<std::pair<cudaEvent_t, cudaEvent_t>>> timers;
+    static constexpr int kPhys = 24;
+    long long Yl = 0, Yu1 = 0, P = 0;
+    // scalars
+    double t = 0, dt = 0, dt2 = 0, dt3 = 0;
+    int istep = 0;
+    double abfac[3] = {0, 0, 0}, bdf[3] = {0, 0, 0}, bdfv = 0;
+    double bshape_norm = 0.0;  // bctype 1: S_top(0,0) / S_wall(0,0) helper
+
+    double* alloc(size_t n) {
+        void* q = nullptr;
+        CK(cudaMalloc(&q, n * sizeof(double) > 0 ? n * sizeof(double) : 8));
+        CK(cudaMemsetAsync(q, 0, n * sizeof(double), stream));
+        allocs.push_back(q);
+        return (double*)q;
+    }
+    double* upload(const double* h, size_t n) {
+        double* q = alloc(n);
+        CK(cudaMemcpyAsync(q, h, n * sizeof(double), cudaMemcpyHostToDevice, stream));
+        return q;
+    }
+    ~lsb_handle() {
+        if (stream) cudaStreamSynchronize(stream);
+        for (void* q : allocs) cudaFree(q);
+        if (own) cudaStreamDestroy(own);
+    }
+};
+
+
+namespace lsb {
+// records CUDA events around the launches of one kernel group when timing is on
+struct TimerScope {
+    lsb_handle* h;
+    const char* name;
+    cudaEvent_t a = nullptr, b = nullptr;
+    TimerScope(lsb_handle* h_, const char* n) : h(h_), name(n) {
+        if (h->timing) {
+            cudaEventCreate(&a);
+            cudaEventCreate(&b);
+            cudaEventRecord(a, h->stream);
+        }
+    }
+    ~TimerScope() {
+        if (h->timing) {
+            cudaEventRecord(b, h->stream);
+            h->timers[name].emplace_back(a, b);
+        }
+    }
+};
+// sgs_kernels.cu
+void sgs_init(lsb_handle* h);
+void sgs_add_tau(lsb_handle* h, double* const* ph, bool dealias);
+void sgs_tau_phys(lsb_handle* h, const double* ui, const double* g, const double* uiuj, double* tau);
+void sgs_mul(double* y, const double* x, long long n, cudaStream_t s);
+void diag_compute(lsb_handle* h, lsb_diagnostics* out);
+// lsbgpu.cu helpers used by sgs_kernels.cu
+void phys_to_spec(lsb_handle* h, const double* const* phys, double* const* spec, int nf, int nzp, double alpha,
+                  double beta, double* const* ybuf);
+void spec_to_phys(lsb_handle* h, const double* const* spec, double* const* phys, int nf, int nzp,
+                  const double* const* means, const int* modes);
+void zgemm(lsb_handle* h, const Mat& m, const double* in, double* out, int nf, int epi, double alpha, double beta,
+           const double* aux);
+}  // namespace lsb

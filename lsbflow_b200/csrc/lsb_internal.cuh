@@ -1,0 +1,146 @@
+// Internal declarations of the LSBFLOW B200 time-step library.
+//
+// Device data layout (all FP64, reference ordering, i fastest):
+//   spectral field  : [nzp][ny][nx]       nx reals = nx/2 complex kx modes (Re, Im interleaved),
+//                                          ky in FFT order, k = 0 the ceiling, k = nzp-1 the wall
+//   y-intermediate  : [nzp][nyl][nx]      after the spanwise transform: kx modes per physical y row
+//   physical field  : [nzp][ny][nx]       no pad columns on the device (the reference's two pad
+//                                          columns hold nothing any result depends on)
+// nyl / nxl are the 3/2-rule padded sizes when dealiasflag == 1, else ny / nx.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+namespace lsb {
+
+constexpr int kMaxStages = 16;
+
+// One complex FFT length: radix schedule + twiddle table tw[m] = exp(-2 pi i m / n).
+struct FftPlan {
+    int n = 0;
+    int nst = 0;
+    int radix[kMaxStages] = {0};
+    const double2* tw = nullptr;   // device, n entries
+};
+
+// A real transform of length nr (even) done through a complex FFT of length nr/2.
+struct RealPlan {
+    int nr = 0;                    // real length
+    FftPlan half;                  // complex plan of length nr/2
+    const double2* twr = nullptr;  // device, nr entries: exp(-2 pi i m / nr)
+};
+
+struct Dims {
+    int nx = 0, ny = 0, nz = 0, nzp = 0, nzm = 0;
+    int kx = 0;            // nx/2 stored complex kx modes
+    int nxl = 0, nyl = 0;  // transform grid (padded when dealiasing)
+    long long S() const { return (long long)nx * ny * nzp; }
+    long long C() const { return (long long)nx * ny; }
+};
+
+// ---------------------------------------------------------------- FFT passes (fft_kernels.cu)
+// multiplier applied to a spectral column before the y inverse transform
+enum YMode { YM_COPY = 0, YM_IKY = 1, YM_IKX = 2 };
+
+struct YInvJob {
+    const double* in;   // spectral [nzp][ny][nx]
+    double* out;        // y-intermediate [nzp][nyl][nx]
+    int mode;
+};
+struct YFwdJob {
+    const double* in;   // y-intermediate [nzp][nyl][nx]
+    double* out;        // spectral [nzp][ny][nx]
+    double alpha;       // out = alpha * T(in) + beta * out
+    double beta;
+    int sym;            // apply the kx = 0 Hermitian symmetrisation of the horfft round trip
+};
+
+struct YPassArgs {
+    int ny, nyl, kxc, nzp, nx;  // kxc = number of complex kx columns
+    int layout;                 // 0 = reference layout, 1 = correct 3/2 layout
+    double scale;               // forward only: 1/(nxl*nyl)
+    const double* wavy;         // [ny] device
+    const double* wavx;         // [nx] device
+    FftPlan plan;               // length nyl
+};
+
+constexpr int kMaxJobs = 12;
+struct YInvJobList { int n; YInvJob j[kMaxJobs]; };
+struct YFwdJobList { int n; YFwdJob j[kMaxJobs]; };
+void launch_yinv(const YInvJobList& jobs, const YPassArgs& a, cudaStream_t s);
+void launch_yfwd(const YFwdJobList& jobs, const YPassArgs& a, cudaStream_t s);
+
+// row transforms between y-intermediate rows (kxc complex modes) and physical rows (nxl reals)
+struct RowIO {
+    const double* yin;  // y-intermediate source (c2r) or physical source (r2c)
+    double* out;
+    int mode;           // YM_COPY or YM_IKX (c2r only)
+    double add_mean;    // c2r only: 0 or 1 -> add mean[k] to the physical row (u + ubar)
+    const double* mean; // [nzp] or nullptr
+};
+struct RowArgs {
+    int kxc, nxl, nyl, nzp;
+    long long row_pitch;        // physical row pitch in doubles (nxl)
+    const double* wavx;
+    RealPlan rp;
+};
+struct RowJobList { int n; RowIO j[kMaxJobs]; };
+void launch_row_c2r(const RowJobList& jobs, const RowArgs& a, cudaStream_t s);
+void launch_row_r2c(const RowJobList& jobs, const RowArgs& a, cudaStream_t s);
+
+// the fused nonlinear-product row kernel
+struct NlRowArgs {
+    RowArgs r;
+    const double* U[3];   // y-intermediate velocities
+    const double* DY[3];  // y-intermediate d/dy
+    const double* DZ[3];  // y-intermediate d/dz
+    double* N[3];         // y-intermediate outputs: -0.5 u_m d_m u_l (+ forcing)
+    double* H[6];         // y-intermediate outputs: 0.5 u_l u_m for (11,12,13,22,23,33)
+    const double* ubar;   // [nzp]
+    const double* ubarp;  // [nzp]
+    const double* lamx;   // [nxl] fringe lambda(x) or nullptr (only on the unpadded grid)
+};
+void launch_row_nl(const NlRowArgs& a, cudaStream_t s);
+
+// ---------------------------------------------------------------- z contractions (gemm_kernels.cu)
+// out[f][r][c] = epi( sum_k A[r][k] * in[f][k + koff][c] ) for r < M (rows written at r + roff)
+enum GemmEpi {
+    EPI_STORE = 0,          // out = acc
+    EPI_AXPBY = 1,          // out = alpha*acc + beta*out
+    EPI_HELM_SCALE = 2,     // out = acc / (lam[r] - w2(c) - sigma)
+    EPI_PRESSURE = 3,       // out = -(acc + aux)/(w2(c)*coef), 0 where w2 == 0
+    EPI_POISSON_RHS = 4,    // out = -acc - w2(c)*aux
+    EPI_LIFT_ADD = 5,       // out = acc + hb[row]*bcb(c) + ht[row]*bct(c)   (bcb may be null)
+};
+struct GemmArgs {
+    const double* A;        // device, [Mp][Kp] zero padded
+    int M, K, Mp, Kp;
+    const double* in;       // field base
+    long long in_fstride;
+    int koff;               // first input row
+    double* out;
+    long long out_fstride;
+    int roff;               // first output row
+    long long C;            // columns per plane (nx*ny)
+    int nfields;
+    int epi;
+    double alpha, beta, sigma, coef;
+    const double* lam;      // EPI_HELM_SCALE
+    const double* aux;      // EPI_PRESSURE / EPI_POISSON_RHS: aux field (same layout as out)
+    const double* wavx;     // [nx]
+    const double* wavy;     // [ny]
+    int nx;
+    // lift prologue (solve_nhom_helmholtz): in' = in - abot(k,c)*bcb(c) - atop(k,c)*bct(c)
+    const double* bcb;      // wall plane of the boundary field, or nullptr
+    const double* bct;      // ceiling plane
+    long long bc_fstride;
+    const double* hb; const double* ht; const double* d2hb; const double* d2ht;
+    double lift_sigma;
+};
+void launch_gemm(const GemmArgs& g, cudaStream_t s);
+
+}  // namespace lsb

@@ -1,0 +1,1095 @@
+// C ABI and step orchestration of the LSBFLOW B200 library (include/lsbgpu.h).
+//
+// lsb_step() is timestep() / navierstokes_update() (src/navierstokes.f90:10-90, 1157-1496)
+// as a fixed sequence of kernels on one stream, with the histories (u^{n-1}, u^{n-2},
+// N^{n-1}, N^{n-2}, p^{n-1}) kept resident as rotating buffers: no copies between steps.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "lsb_internal.cuh"
+#include "lsb_spectral.cuh"
+#include "lsb_handle.cuh"
+
+using namespace lsb;
+
+namespace {
+
+thread_local std::string g_err;
+
+template <class F>
+int guard(F&& f) {
+    try {
+        f();
+        return LSB_OK;
+    } catch (const LsbError& e) {
+        g_err = e.msg;
+        return e.code;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return LSB_ERR_STATE;
+    }
+}
+
+void fail(int code, const std::string& m) { throw LsbError{code, m}; }
+
+bool factor(int n, std::vector<int>& rad) {
+    rad.clear();
+    while (n % 4 == 0 && n > 1) { rad.push_back(4); n /= 4; }
+    while (n % 2 == 0 && n > 1) { rad.push_back(2); n /= 2; }
+    for (int r : {3, 5, 7}) while (n % r == 0 && n > 1) { rad.push_back(r); n /= r; }
+    return n == 1;
+}
+
+}  // namespace
+
+namespace {
+
+void make_plan(lsb_handle* h, int n, FftPlan& P) {
+    std::vector<int> rad;
+    if (!factor(n, rad) || (int)rad.size() > kMaxStages)
+        fail(LSB_ERR_UNSUPPORTED, "FFT length " + std::to_string(n) + " is not a product of 2,3,5,7");
+    P.n = n;
+    P.nst = (int)rad.size();
+    for (int i = 0; i < P.nst; ++i) P.radix[i] = rad[i];
+    std::vector<double> tw(2 * (size_t)n);
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int m = 0; m < n; ++m) {
+        const long double a = 2.0L * pi * (long double)m / (long double)n;
+        tw[2 * m] = (double)cosl(a);
+        tw[2 * m + 1] = (double)-sinl(a);
+    }
+    P.tw = (const double2*)h->upload(tw.data(), tw.size());
+}
+
+void make_real_plan(lsb_handle* h, int nr, RealPlan& R) {
+    if (nr % 2) fail(LSB_ERR_UNSUPPORTED, "real transform length must be even");
+    R.nr = nr;
+    make_plan(h, nr / 2, R.half);
+    std::vector<double> tw(2 * (size_t)nr);
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int m = 0; m < nr; ++m) {
+        const long double a = 2.0L * pi * (long double)m / (long double)nr;
+        tw[2 * m] = (double)cosl(a);
+        tw[2 * m + 1] = (double)-sinl(a);
+    }
+    R.twr = (const double2*)h->upload(tw.data(), tw.size());
+}
+
+Mat make_mat(lsb_handle* h, const double* A, int M, int K, int row0 = 0, int nrows = -1, int zero_pad_rows_top = 0,
+             int total_rows = -1) {
+    // builds a zero-padded [Mp][Kp] copy of rows row0..row0+nrows-1 of A (M x K, row-major),
+    // optionally placed starting at output row zero_pad_rows_top inside total_rows rows
+    if (nrows < 0) nrows = M;
+    if (total_rows < 0) total_rows = nrows;
+    Mat m;
+    m.M = total_rows;
+    m.K = K;
+    m.Mp = ((total_rows + 7) / 8) * 8;
+    m.Kp = ((K + 15) / 16) * 16;
+    if (m.Mp > 136) fail(LSB_ERR_UNSUPPORTED, "nz too large (nzp <= 136 supported)");
+    std::vector<double> buf((size_t)m.Mp * m.Kp, 0.0);
+    for (int r = 0; r < nrows; ++r)
+        for (int k = 0; k < K; ++k) buf[(size_t)(r + zero_pad_rows_top) * m.Kp + k] = A[(size_t)(row0 + r) * K + k];
+    m.p = h->upload(buf.data(), buf.size());
+    return m;
+}
+
+GemmArgs gemm_base(lsb_handle* h, const Mat& m) {
+    GemmArgs g{};
+    g.A = m.p;
+    g.M = m.M;
+    g.K = m.K;
+    g.Mp = m.Mp;
+    g.Kp = m.Kp;
+    g.C = h->d.C();
+    g.nfields = 1;
+    g.wavx = h->wavx;
+    g.wavy = h->wavy;
+    g.nx = h->d.nx;
+    g.in_fstride = g.out_fstride = h->d.S();
+    g.alpha = 1.0;
+    g.hb = h->hb;
+    g.ht = h->ht;
+    g.d2hb = h->d2hb;
+    g.d2ht = h->d2ht;
+    return g;
+}
+
+}  // namespace
+
+namespace lsb {
+// out = Mz . in   (dfdz when mz = dz1, d2fdz2 when dz2), nf fields of stride S
+void zgemm(lsb_handle* h, const Mat& m, const double* in, double* out, int nf, int epi, double alpha, double beta,
+           const double* aux) {
+    GemmArgs g = gemm_base(h, m);
+    g.in = in;
+    g.out = out;
+    g.nfields = nf;
+    g.epi = epi;
+    g.alpha = alpha;
+    g.beta = beta;
+    g.aux = aux;
+    launch_gemm(g, h->stream);
+}
+}  // namespace lsb
+
+namespace {
+void zgemm1(lsb_handle* h, const Mat& m, const double* in, double* out, int nf) {
+    zgemm(h, m, in, out, nf, EPI_STORE, 1.0, 0.0, nullptr);
+}
+
+// Helmholtz / Poisson solve of nf fields (stride S): out = solve(rhs, sigma) with the
+// lifting functions of solve_nhom_helmholtz when bc != null (bc: [nf][2][C], ceiling first)
+void helmholtz(lsb_handle* h, const double* rhs, double* out, int nf, double sigma, const double* bc) {
+    const long long C = h->d.C();
+    GemmArgs g1 = gemm_base(h, h->m_ei);
+    g1.in = rhs;
+    g1.koff = 1;
+    g1.out = h->T;
+    g1.nfields = nf;
+    g1.epi = EPI_HELM_SCALE;
+    g1.sigma = sigma;
+    g1.lam = h->lam;
+    if (bc) {
+        g1.bcb = bc + C;
+        g1.bct = bc;
+        g1.bc_fstride = 2 * C;
+        g1.lift_sigma = sigma;
+    }
+    launch_gemm(g1, h->stream);
+    GemmArgs g2 = gemm_base(h, h->m_eext);
+    g2.in = h->T;
+    g2.out = out;
+    g2.nfields = nf;
+    g2.epi = EPI_LIFT_ADD;
+    if (bc) {
+        g2.bcb = bc + C;
+        g2.bct = bc;
+        g2.bc_fstride = 2 * C;
+    }
+    launch_gemm(g2, h->stream);
+}
+
+YPassArgs ypass(lsb_handle* h, bool padded, int nzp) {
+    YPassArgs a{};
+    a.ny = h->d.ny;
+    a.nyl = padded ? h->d.nyl : h->d.ny;
+    a.kxc = h->d.kx;
+    a.nzp = nzp;
+    a.nx = h->d.nx;
+    a.layout = h->cfg.dealias_layout;
+    a.scale = 1.0 / ((double)(padded ? h->d.nxl : h->d.nx) * (double)(padded ? h->d.nyl : h->d.ny));
+    a.wavy = h->wavy;
+    a.wavx = h->wavx;
+    a.plan = padded ? h->pyl : h->py;
+    return a;
+}
+
+RowArgs rowargs(lsb_handle* h, bool padded, int nzp) {
+    RowArgs r{};
+    r.kxc = h->d.kx;
+    r.nxl = padded ? h->d.nxl : h->d.nx;
+    r.nyl = padded ? h->d.nyl : h->d.ny;
+    r.nzp = nzp;
+    r.row_pitch = r.nxl;
+    r.wavx = h->wavx;
+    r.rp = padded ? h->rxl : h->rx;
+    return r;
+}
+
+}  // namespace
+
+namespace lsb {
+// horfft(-1): physical (unpadded, [nzp][ny][nx]) -> spectral, nf fields
+void phys_to_spec(lsb_handle* h, const double* const* phys, double* const* spec, int nf, int nzp, double alpha,
+                  double beta, double* const* ybuf) {
+    for (int f0 = 0; f0 < nf; f0 += kMaxJobs) {
+        const int n = std::min(kMaxJobs, nf - f0);
+        RowJobList rj{};
+        YFwdJobList yj{};
+        rj.n = yj.n = n;
+        for (int i = 0; i < n; ++i) {
+            double* y = ybuf ? ybuf[f0 + i] : h->Yu + (long long)i * h->Yu1;
+            rj.j[i] = RowIO{phys[f0 + i], y, YM_COPY, 0.0, nullptr};
+            yj.j[i] = YFwdJob{y, spec[f0 + i], alpha, beta, 0};
+        }
+        launch_row_r2c(rj, rowargs(h, false, nzp), h->stream);
+        launch_yfwd(yj, ypass(h, false, nzp), h->stream);
+    }
+}
+
+// horfft(+1): spectral -> physical (unpadded), optional mean added to field 0
+void spec_to_phys(lsb_handle* h, const double* const* spec, double* const* phys, int nf, int nzp,
+                  const double* const* means, const int* modes) {
+    for (int f0 = 0; f0 < nf; f0 += kMaxJobs) {
+        const int n = std::min(kMaxJobs, nf - f0);
+        YInvJobList yj{};
+        RowJobList rj{};
+        yj.n = rj.n = n;
+        for (int i = 0; i < n; ++i) {
+            double* y = h->Yu + (long long)i * h->Yu1;
+            const int mode = modes ? modes[f0 + i] : YM_COPY;
+            yj.j[i] = YInvJob{spec[f0 + i], y, mode == YM_IKY ? YM_IKY : YM_COPY};
+            const double* mean = means ? means[f0 + i] : nullptr;
+            rj.j[i] = RowIO{y, phys[f0 + i], mode == YM_IKX ? YM_IKX : YM_COPY, mean ? 1.0 : 0.0, mean};
+        }
+        launch_yinv(yj, ypass(h, false, nzp), h->stream);
+        launch_row_c2r(rj, rowargs(h, false, nzp), h->stream);
+    }
+}
+
+}  // namespace lsb
+
+namespace {
+double* Hsym(lsb_handle* h, int l, int m) {
+    static const int idx[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+    return h->H + (long long)idx[l][m] * h->d.S();
+}
+
+// nlterm_skewsym (src/navierstokes.f90:658-855), velocity part: uin (3S) -> Nout (3S)
+void nlterm(lsb_handle* h, const double* uin, double* Nout) {
+    const Dims& d = h->d;
+    const long long S = d.S();
+    const bool dealias = h->cfg.dealiasflag == 1;
+    // du_l/dz
+    { TimerScope ts(h, "gemm_dz"); zgemm1(h, h->m_dz1, uin, h->dz, 3); }
+    // spanwise inverse: u_l, du_l/dy, du_l/dz  -> Y[0..8]
+    YInvJobList yj{};
+    yj.n = 9;
+    for (int l = 0; l < 3; ++l) {
+        yj.j[l] = YInvJob{uin + l * S, h->Y + (long long)l * h->Yl, YM_COPY};
+        yj.j[3 + l] = YInvJob{uin + l * S, h->Y + (long long)(3 + l) * h->Yl, YM_IKY};
+        yj.j[6 + l] = YInvJob{h->dz + l * S, h->Y + (long long)(6 + l) * h->Yl, YM_COPY};
+    }
+    { TimerScope ts(h, "yinv_nl"); launch_yinv(yj, ypass(h, dealias, d.nzp), h->stream); }
+    NlRowArgs na{};
+    na.r = rowargs(h, dealias, d.nzp);
+    for (int l = 0; l < 3; ++l) {
+        na.U[l] = h->Y + (long long)l * h->Yl;
+        na.DY[l] = h->Y + (long long)(3 + l) * h->Yl;
+        na.DZ[l] = h->Y + (long long)(6 + l) * h->Yl;
+        na.N[l] = h->Y + (long long)(9 + l) * h->Yl;
+    }
+    for (int m = 0; m < 6; ++m) na.H[m] = h->Y + (long long)(12 + m) * h->Yl;
+    na.ubar = h->ubar;
+    na.ubarp = h->ubarp;
+    na.lamx = (!dealias && h->cfg.forcing == 1) ? h->lamx : nullptr;
+    { TimerScope ts(h, "row_nl"); launch_row_nl(na, h->stream); }
+    YFwdJobList yf{};
+    yf.n = 9;
+    for (int l = 0; l < 3; ++l) yf.j[l] = YFwdJob{na.N[l], Nout + l * S, 1.0, 0.0, dealias ? 1 : 0};
+    for (int m = 0; m < 6; ++m) yf.j[3 + m] = YFwdJob{na.H[m], h->H + m * S, 1.0, 0.0, dealias ? 1 : 0};
+    { TimerScope ts(h, "yfwd_nl"); launch_yfwd(yf, ypass(h, dealias, d.nzp), h->stream); }
+
+    const bool need_phys = (dealias && h->cfg.forcing == 1) || h->cfg.sgsflag == 1;
+    if (need_phys) {
+        // unpadded physical u_l (+ubar), du_l/dx_m (+ubarp on du/dz)
+        const long long P = h->P;
+        double* ph[12];
+        for (int i = 0; i < 12; ++i) ph[i] = h->phys + i * P;
+        const double* spec[12];
+        int modes[12];
+        const double* means[12] = {nullptr};
+        for (int l = 0; l < 3; ++l) {
+            spec[l] = uin + l * S;  // u_l
+            modes[l] = YM_COPY;
+            spec[3 + 3 * l + 0] = uin + l * S;  // du_l/dx
+            modes[3 + 3 * l + 0] = YM_IKX;
+            spec[3 + 3 * l + 1] = uin + l * S;  // du_l/dy
+            modes[3 + 3 * l + 1] = YM_IKY;
+            spec[3 + 3 * l + 2] = h->dz + l * S;  // du_l/dz
+            modes[3 + 3 * l + 2] = YM_COPY;
+        }
+        means[0] = h->ubar;
+        means[3 + 2] = h->ubarp;
+        const int nphys = (h->cfg.sgsflag == 1) ? 12 : 3;
+        { TimerScope ts(h, "phys_fields"); spec_to_phys(h, spec, ph, nphys, d.nzp, means, modes); }
+        if (dealias && h->cfg.forcing == 1) {
+            TimerScope ts(h, "forcing");
+            double* fo[3] = {h->phys + 12 * P, h->phys + 13 * P, h->phys + 14 * P};
+            launch_force_phys(ph[0], ph[1], ph[2], fo[0], fo[1], fo[2], h->lamx, h->ubar, d.nx, d.ny, P, h->stream);
+            double* no[3] = {Nout, Nout + S, Nout + 2 * S};
+            phys_to_spec(h, fo, no, 3, d.nzp, 1.0, 1.0, nullptr);
+        }
+        if (h->cfg.sgsflag == 1) { TimerScope ts(h, "sgs_total"); sgs_add_tau(h, ph, dealias); }
+    }
+    // N_l -= d h_l1/dx + d h_l2/dy + d h_l3/dz
+    NlDivArgs nd{};
+    const bool full9 = h->cfg.sgsflag == 1 && h->sgs.nonsym;
+    for (int l = 0; l < 3; ++l) {
+        nd.N[l] = Nout + l * S;
+        nd.hx[l] = full9 ? h->sgs.H9 + (l * 3 + 0) * S : Hsym(h, l, 0);
+        nd.hy[l] = full9 ? h->sgs.H9 + (l * 3 + 1) * S : Hsym(h, l, 1);
+    }
+    nd.wavx = h->wavx;
+    nd.wavy = h->wavy;
+    nd.nx = d.nx;
+    nd.S = S;
+    nd.C = d.C();
+    TimerScope ts(h, "nl_divergence");
+    launch_nl_div_xy(nd, h->stream);
+    for (int l = 0; l < 3; ++l) {
+        const double* hz = full9 ? h->sgs.H9 + (l * 3 + 2) * S : Hsym(h, l, 2);
+        zgemm(h, h->m_dz1, hz, Nout + l * S, 1, EPI_AXPBY, -1.0, 1.0, nullptr);
+    }
+}
+
+void coefficients(lsb_handle* h) {
+    const int istep = h->istep;
+    const int nstart = h->cfg.nstart;
+    if (istep <= 3 || h->dt != h->dt2 || h->dt2 != h->dt3) {
+        if (nstart == 0 && istep == 1) { h->abfac[0] = 1; h->abfac[1] = 0; h->abfac[2] = 0; }
+        else if (nstart == 0 && istep == 2) { h->abfac[0] = 2; h->abfac[1] = -1; h->abfac[2] = 0; }
+        else { h->abfac[0] = 3; h->abfac[1] = -3; h->abfac[2] = 1; }
+        const double dt1 = h->dt, dt2 = h->dt2, dt3 = h->dt3;
+        if (nstart == 0 && istep == 1) {
+            h->bdfv = 1.0; h->bdf[0] = 1.0; h->bdf[1] = 0.0; h->bdf[2] = 0.0;
+        } else if (nstart == 0 && istep == 2) {
+            h->bdfv = 2. / 3.; h->bdf[0] = 2.0; h->bdf[1] = -0.5; h->bdf[2] = 0.0;
+        } else if (dt1 != dt2 || dt2 != dt3) {
+            const double d12 = dt1 + dt2, d23 = dt2 + dt3, d123 = dt1 + dt2 + dt3;
+            const double v = 1. + dt1 / d12 + dt1 / d123;
+            h->bdfv = 1. / v;
+            h->bdf[0] = -(-1. - dt1 / dt2 - dt1 / d123 - dt1 * dt1 / (d123 * dt2) - dt1 * dt1 * d12 / (d123 * d23 * dt2));
+            h->bdf[1] = -(dt1 * dt1 / (d12 * dt2) + dt1 * dt1 / (dt2 * d123) + dt1 * dt1 * d12 / (dt2 * d23 * d123) +
+                          dt1 * dt1 * d12 / (dt3 * d23 * d123));
+            h->bdf[2] = -(-dt1 * dt1 * d12 / (dt3 * d23 * d123));
+        } else {
+            h->bdfv = 6. / 11.; h->bdf[0] = 3.0; h->bdf[1] = -1.5; h->bdf[2] = 1. / 3.;
+        }
+    }
+}
+
+// time coefficients of bound(): ceiling shape, wall shapes a and b (src/navierstokes.f90:214-355)
+void bound_coeffs(lsb_handle* h, double t, double& ctop, double& cwa, double& cwb) {
+    const lsb_config& c = h->cfg;
+    const double pi = 4.0 * std::atan(1.0);
+    ctop = cwa = cwb = 0.0;
+    if (c.bctype == 1) {
+        double amp = c.samp * c.u0 / (0.24 * std::sqrt(pi));
+        double bamp = c.samp / 2.25;
+        const double ref_time = c.xlen / c.u0;
+        if (t - c.istartbound <= ref_time) {
+            const double s = std::pow(std::sin(0.5 * pi * (t - c.istartbound) / ref_time), 2.0);
+            amp *= s;
+            bamp *= s;
+        } else if (!(t - c.istartbound > ref_time)) {
+            amp = bamp = 0.0;
+        }
+        ctop = amp;
+        // bfac = bcf(1,1,1)/bcf(1,1,nzp) makes the wall flux balance the ceiling flux
+        const double b00 = bamp * h->bshape_norm;  // bamp * S_wall(0,0) relative to S_top(0,0)
+        cwa = (b00 != 0.0) ? amp / h->bshape_norm : 0.0;
+        (void)b00;
+    } else if (c.bctype == 2) {
+        const double A = 0.002 * c.u0, A_half = 0.0001 * c.u0, phi = 0.0;
+        const double omega = 1.24e-4 * (c.x0 / c.u0);
+        const double theta = t - c.istartbound;
+        cwa = A * std::sin(omega * theta);
+        cwb = A_half * std::cos(omega / 2.0 * theta + phi);
+    } else if (c.bctype == 3) {
+        ctop = 1.0;
+    }
+}
+
+void build_bound_shapes(lsb_handle* h) {
+    const lsb_config& c = h->cfg;
+    const Dims& d = h->d;
+    if (c.bctype == 0) return;
+    const double pi = 4.0 * std::atan(1.0);
+    const int nx = d.nx, ny = d.ny;
+    std::vector<double> top((size_t)nx * ny, 0.0), wa((size_t)nx * ny, 0.0), wb((size_t)nx * ny, 0.0);
+    const std::vector<double>& x = h->h_xpts;
+    if (c.bctype == 1) {
+        const double hh = h->h_zpts[0];
+        double xloc = 1.0e5 * c.xnu / c.u0;
+        if (x[nx / 2 - 1] < xloc) xloc = c.x0 + 3. / 7. * c.xlen;
+        const double xwidth = 0.24 * hh;
+        const double bwidth = xwidth * 2.25;
+        const double x1 = x[nx - 1] - 2. * bwidth;
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                const double eta = (x[i] - xloc) / xwidth;
+                top[(size_t)j * nx + i] = std::exp(-std::pow(eta, 2.0));
+                const double eta0 = (x[i] - x1) / bwidth;
+                wa[(size_t)j * nx + i] = std::exp(-std::pow(eta0, 4.0));
+            }
+    } else if (c.bctype == 2) {
+        const double x1 = 1.655e5 * c.xnu / c.u0, x2 = 1.81e5 * c.xnu / c.u0, xm = (x1 + x2) / 2.0;
+        const double lambda_y = 0.151367188 * c.x0;
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                double eta = 0.0;
+                if (x[i] >= x1 && x[i] <= xm) eta = (x[i] - x1) / (xm - x1);
+                if (x[i] >= xm && x[i] <= x2) eta = (x2 - x[i]) / (x2 - xm);
+                if (x[i] >= x1 && x[i] <= x2) {
+                    double f = 15.1875 * std::pow(eta, 5) - 35.4375 * std::pow(eta, 4) + 20.25 * std::pow(eta, 3);
+                    if (x[i] > xm) f = -f;
+                    const double g = std::cos(2.0 * pi * h->h_ypts[j] / lambda_y);
+                    wa[(size_t)j * nx + i] = f;
+                    wb[(size_t)j * nx + i] = f * g;
+                }
+            }
+    } else if (c.bctype == 3) {
+        const double xc = x[0] + c.bc3_xc;
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                const double e = (x[i] - xc) / c.bc3_s;
+                top[(size_t)j * nx + i] = c.bc3_amp * e * std::exp(-e * e);
+            }
+    } else {
+        fail(LSB_ERR_UNSUPPORTED, "bctype must be 0..3");
+    }
+    const long long C = d.C();
+    double* tmp = h->phys;
+    CK(cudaMemcpyAsync(tmp, top.data(), C * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(tmp + C, wa.data(), C * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(tmp + 2 * C, wb.data(), C * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    const double* ph[3] = {tmp, tmp + C, tmp + 2 * C};
+    double* sp[3] = {h->bshape, h->bshape + C, h->bshape + 2 * C};
+    phys_to_spec(h, ph, sp, 3, 1, 1.0, 0.0, nullptr);
+    if (c.bctype == 1) {
+        double s00[2];
+        CK(cudaMemcpyAsync(&s00[0], h->bshape, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(&s00[1], h->bshape + C, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        // wall coefficient = bfac*bamp = amp*S_top00/S_wall00 (0 when S_wall00 = 0)
+        h->bshape_norm = (s00[1] != 0.0) ? s00[1] / s00[0] : 0.0;
+    }
+}
+
+void step_one(lsb_handle* h) {
+    const Dims& d = h->d;
+    const lsb_config& c = h->cfg;
+    const long long S = d.S(), C = d.C();
+    cudaStream_t st = h->stream;
+    h->istep += 1;
+    coefficients(h);
+    const double dt = h->dt;
+    // 1-2. nonlinear term (from spectrally filtered velocities when dealiasflag >= 2)
+    const double* uin = h->vel;
+    if (c.dealiasflag >= 2) {
+        const double pi = 4.0 * std::atan(1.0);
+        const double alpha = 2.0 * pi / c.xlen, beta = 2.0 * pi / c.ylen;
+        SpecFilterArgs fa{};
+        for (int l = 0; l < 3; ++l) {
+            fa.in[l] = h->vel + l * S;
+            fa.out[l] = h->filt + l * S;
+        }
+        fa.S = S;
+        fa.C = C;
+        fa.nx = d.nx;
+        fa.wavx = h->wavx;
+        fa.wavy = h->wavy;
+        fa.akmax = std::sqrt(std::pow((d.nx / 2) * alpha, 2) + std::pow((d.ny / 2) * beta, 2));
+        fa.akc = fa.akmax * c.kc;
+        fa.amp = c.filt_amp;
+        fa.order = c.filt_order;
+        { TimerScope ts(h, "specfilter"); launch_specfilter(fa, st); }
+        uin = h->filt;
+    }
+    nlterm(h, uin, h->nlc);
+    const double* uif = (c.dealiasflag >= 3) ? h->filt : h->vel;
+    // 3. velocity right-hand sides
+    const double dtnui = 1.0 / (c.xnu * dt);
+    RhsArgs ra{};
+    for (int l = 0; l < 3; ++l) {
+        ra.rhs[l] = h->rhs + l * S;
+        ra.N[l] = h->nlc + l * S;
+        ra.nln[l] = h->nln + l * S;
+        ra.nlnm[l] = h->nlnm + l * S;
+        ra.u[l] = uif + l * S;
+        ra.un[l] = h->veln + l * S;
+        ra.unm[l] = h->velnm + l * S;
+        ra.ab[l] = h->abfac[l];
+        ra.bdf[l] = h->bdf[l];
+    }
+    ra.dt = dt;
+    ra.dtnui = dtnui;
+    ra.ubarpp = h->ubarpp;
+    ra.S = S;
+    ra.C = C;
+    { TimerScope ts(h, "rhs"); launch_rhs(ra, st); }
+    // 4. rotate the histories: N^{n-2} <- N^{n-1} <- N^n, u^{n-2} <- u^{n-1} <- u^n
+    {
+        double* t1 = h->nlnm;
+        h->nlnm = h->nln;
+        h->nln = h->nlc;
+        h->nlc = t1;
+        double* t2 = h->velnm;
+        h->velnm = h->veln;
+        h->veln = h->vel;
+        h->vel = t2;
+        if (c.dealiasflag >= 3) CK(cudaMemcpyAsync(h->veln, h->filt, 3 * S * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    }
+    // 5. boundary planes (Zang-Hussaini)
+    double pfac0 = 2.0, pfac1 = -1.0;
+    if (h->istep == 1) { pfac0 = 0.0; pfac1 = 0.0; }
+    else if (h->istep == 2) { pfac0 = 1.0; pfac1 = 0.0; }
+    {
+        TimerScope ts(h, "bc_planes");
+        GemmArgs g = gemm_base(h, h->m_dz2rows);  // rows 1 and nzp of d2fdz2(w^n)
+        g.in = h->veln + 2 * S;
+        g.out = h->d2w;
+        launch_gemm(g, st);
+    }
+    const bool active = c.bctype > 0 && h->t >= c.istartbound;
+    BcArgs ba{};
+    for (int l = 0; l < 3; ++l) {
+        ba.bc[l] = h->bc + l * 2 * C;
+        ba.rtop[l] = h->rhs + l * S;
+    }
+    ba.bcp = h->bcp;
+    ba.pwall = h->p + (long long)(d.nzp - 1) * C;
+    ba.pnwall = h->pn + (long long)(d.nzp - 1) * C;
+    ba.d2w = h->d2w;
+    ba.btop = h->bshape;
+    ba.bwa = h->bshape + C;
+    ba.bwb = h->bshape + 2 * C;
+    bound_coeffs(h, h->t, ba.ctop, ba.cwa, ba.cwb);
+    ba.pfac0 = pfac0;
+    ba.pfac1 = pfac1;
+    ba.dt = dt;
+    ba.bdfv = h->bdfv;
+    ba.dtnui = dtnui;
+    ba.xnu = c.xnu;
+    ba.active = active ? 1 : 0;
+    ba.wavx = h->wavx;
+    ba.wavy = h->wavy;
+    ba.nx = d.nx;
+    ba.C = C;
+    { TimerScope ts(h, "bc_planes"); launch_bc_planes(ba, st); }
+    // 6. three Helmholtz solves (non-homogeneous when bctype>0 or forcing, src/navierstokes.f90:1388-1394)
+    const bool nhom = active || c.forcing == 1;
+    { TimerScope ts(h, "helmholtz_uvw"); helmholtz(h, h->rhs, h->vel, 3, dtnui / h->bdfv, nhom ? h->bc : nullptr); }
+    // 7. Poisson right-hand side: -D(ikx u + iky v) - k^2 w
+    {
+        TimerScope ts(h, "poisson");
+        launch_divuv(h->vel, h->vel + S, h->divf, h->wavx, h->wavy, d.nx, S, C, st);
+        zgemm(h, h->m_dz1, h->divf, h->rhs, 1, EPI_POISSON_RHS, 1.0, 0.0, h->vel + 2 * S);
+        // 8-9. Poisson solve for w^{n+1}
+        helmholtz(h, h->rhs, h->vel + 2 * S, 1, 0.0, h->bcp);
+    }
+    // 10. pressure phi = -(Dw + div)/(k^2 dt bdfv) into pn, then swap
+    {
+        TimerScope ts(h, "pressure");
+        GemmArgs g = gemm_base(h, h->m_dz1);
+        g.in = h->vel + 2 * S;
+        g.out = h->pn;
+        g.epi = EPI_PRESSURE;
+        g.aux = h->divf;
+        g.alpha = dt;
+        g.beta = h->bdfv;
+        launch_gemm(g, st);
+        std::swap(h->p, h->pn);
+    }
+    // 11. projection of u, v; norm; ifrz
+    TimerScope ts(h, "projection_norm");
+    launch_pressure_update(h->vel, h->vel + S, h->p, h->wavx, h->wavy, d.nx, S, C, dt * h->bdfv, st);
+    launch_norm(h->vel, h->vel + S, h->vel + 2 * S, d.nx, d.ny, d.nzp, c.ifrz, st);
+    // 12. time
+    h->t = h->t + dt;
+    h->dt3 = h->dt2;
+    h->dt2 = dt;
+}
+
+void check_launch() {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) fail(LSB_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+}
+
+}  // namespace
+
+// ====================================================================================== C ABI
+extern "C" {
+
+const char* lsb_last_error(void) { return g_err.c_str(); }
+int lsb_version(void) { return 1; }
+
+int lsb_create(const lsb_config* cfg, const lsb_setup* su, lsb_handle** out) {
+    return guard([&] {
+        if (!cfg || !su || !out) fail(LSB_ERR_ARG, "null argument");
+        *out = nullptr;
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) fail(LSB_ERR_CUDA, "no CUDA device");
+        std::unique_ptr<lsb_handle> h(new lsb_handle());
+        h->cfg = *cfg;
+        Dims& d = h->d;
+        d.nx = cfg->nx;
+        d.ny = cfg->ny;
+        d.nz = cfg->nz;
+        d.nzp = cfg->nz + 1;
+        d.nzm = cfg->nz - 1;
+        d.kx = cfg->nx / 2;
+        if (d.nx < 4 || d.nx % 2 || d.ny < 1 || d.nz < 3) fail(LSB_ERR_ARG, "bad grid size");
+        if (cfg->dealiasflag == 1) {
+            // setup_dealiasing, nproch = 1 (src/dealiasing.f90:133-154)
+            if (d.nx % 2 == 0 && d.nx % 4 == 0) d.nxl = 3 * d.nx / 2;
+            else if (d.nx % 3 == 0) d.nxl = 5 * d.nx / 3;
+            else if (d.nx % 5 == 0) d.nxl = 8 * d.nx / 5;
+            else d.nxl = 2 * d.nx;
+            if (d.ny % 2 == 0) d.nyl = 3 * d.ny / 2;
+            else if (d.ny % 3 == 0) d.nyl = 5 * d.ny / 3;
+            else if (d.ny % 5 == 0) d.nyl = 8 * d.ny / 5;
+            else d.nyl = 2 * d.ny;
+        } else {
+            d.nxl = d.nx;
+            d.nyl = d.ny;
+        }
+        if (cfg->sgsflag == 1 && (cfg->sgsmodel < 0 || cfg->sgsmodel > 4)) fail(LSB_ERR_ARG, "sgsmodel must be 0..4");
+        CK(cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking));
+        h->stream = h->own;
+        const int nx = d.nx, ny = d.ny, nzp = d.nzp, nzm = d.nzm;
+        h->h_xpts.assign(su->xpts, su->xpts + nx);
+        h->h_ypts.assign(su->ypts, su->ypts + ny);
+        h->h_zpts.assign(su->zpts, su->zpts + nzp);
+        h->h_ubar.assign(su->ubar, su->ubar + nzp);
+        h->dx = su->dx;
+        h->dy = su->dy;
+        h->wavx = h->upload(su->wavx, nx);
+        h->wavy = h->upload(su->wavy, ny);
+        h->zpts = h->upload(su->zpts, nzp);
+        h->ubar = h->upload(su->ubar, nzp);
+        h->ubarp = h->upload(su->ubarp, nzp);
+        h->ubarpp = h->upload(su->ubarpp, nzp);
+        h->hb = h->upload(su->hbot, nzp);
+        h->ht = h->upload(su->htop, nzp);
+        h->d2hb = h->upload(su->d2hbot, nzp);
+        h->d2ht = h->upload(su->d2htop, nzp);
+        h->lam = h->upload(su->lam, nzm);
+        h->lamx = h->upload(su->lamx, nx);
+        h->m_dz1 = make_mat(h.get(), su->dz1, nzp, nzp);
+        h->m_dz2 = make_mat(h.get(), su->dz2, nzp, nzp);
+        {
+            std::vector<double> rows(2 * (size_t)nzp);
+            for (int k = 0; k < nzp; ++k) {
+                rows[k] = su->dz2[k];
+                rows[nzp + k] = su->dz2[(size_t)(nzp - 1) * nzp + k];
+            }
+            h->m_dz2rows = make_mat(h.get(), rows.data(), 2, nzp);
+        }
+        h->m_ei = make_mat(h.get(), su->ei, nzm, nzm);
+        h->m_eext = make_mat(h.get(), su->e, nzm, nzm, 0, nzm, 1, nzp);  // zero ceiling / wall rows
+        make_plan(h.get(), ny, h->py);
+        make_plan(h.get(), d.nyl, h->pyl);
+        make_real_plan(h.get(), nx, h->rx);
+        make_real_plan(h.get(), d.nxl, h->rxl);
+        const long long S = d.S(), C = d.C();
+        h->Yl = (long long)nzp * d.nyl * nx;
+        h->Yu1 = (long long)nzp * ny * nx;
+        h->P = (long long)nzp * ny * nx;
+        h->vel = h->alloc(3 * S);
+        h->veln = h->alloc(3 * S);
+        h->velnm = h->alloc(3 * S);
+        h->nlc = h->alloc(3 * S);
+        h->nln = h->alloc(3 * S);
+        h->nlnm = h->alloc(3 * S);
+        h->p = h->alloc(S);
+        h->pn = h->alloc(S);
+        h->filt = h->alloc(3 * S);
+        h->dz = h->alloc(3 * S);
+        h->H = h->alloc(6 * S);
+        h->rhs = h->alloc(3 * S);
+        h->T = h->alloc(3 * S);
+        h->divf = h->alloc(S);
+        h->Y = h->alloc(18 * h->Yl);
+        h->Yu = h->alloc(kMaxJobs * h->Yu1);
+        h->phys = h->alloc((long long)lsb_handle::kPhys * h->P);
+        h->bc = h->alloc(6 * C);
+        h->bcp = h->alloc(2 * C);
+        h->d2w = h->alloc(2 * C);
+        h->bshape = h->alloc(3 * C);
+        h->io = h->alloc(12 * S);
+        h->red = h->alloc(512);
+        if (cfg->sgsflag == 1) sgs_init(h.get());
+        build_bound_shapes(h.get());
+        CK(cudaStreamSynchronize(h->stream));
+        check_launch();
+        *out = h.release();
+    });
+}
+
+int lsb_destroy(lsb_handle* h) {
+    return guard([&] { delete h; });
+}
+
+int lsb_set_stream(lsb_handle* h, void* stream) {
+    return guard([&] {
+        if (!h) fail(LSB_ERR_ARG, "null handle");
+        CK(cudaStreamSynchronize(h->stream));
+        h->stream = stream ? (cudaStream_t)stream : h->own;
+    });
+}
+
+int lsb_synchronize(lsb_handle* h) {
+    return guard([&] {
+        if (!h) fail(LSB_ERR_ARG, "null handle");
+        CK(cudaStreamSynchronize(h->stream));
+        check_launch();
+    });
+}
+
+int lsb_upload_state(lsb_handle* h, const double* uf, const double* vf, const double* wf, const double* pf,
+                     const double* pnf, const double* unif, const double* unmif, const double* nlnif,
+                     const double* nlnmif, double t, double dt, double dt2, double dt3, int istep) {
+    return guard([&] {
+        if (!h || !uf || !vf || !wf) fail(LSB_ERR_ARG, "null argument");
+        const long long S = h->d.S();
+        const size_t B = S * sizeof(double);
+        auto up = [&](double* dst, const double* src, size_t bytes) {
+            if (src) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->stream));
+            else CK(cudaMemsetAsync(dst, 0, bytes, h->stream));
+        };
+        up(h->vel, uf, B);
+        up(h->vel + S, vf, B);
+        up(h->vel + 2 * S, wf, B);
+        up(h->p, pf, B);
+        up(h->pn, pnf, B);
+        up(h->veln, unif, 3 * B);
+        up(h->velnm, unmif, 3 * B);
+        up(h->nln, nlnif, 3 * B);
+        up(h->nlnm, nlnmif, 3 * B);
+        h->t = t;
+        h->dt = dt;
+        h->dt2 = dt2;
+        h->dt3 = dt3;
+        h->istep = istep;
+        CK(cudaStreamSynchronize(h->stream));
+    });
+}
+
+int lsb_download_state(lsb_handle* h, double* uf, double* vf, double* wf, double* pf, double* pnf, double* unif,
+                       double* unmif, double* nlnif, double* nlnmif, double* t, double* dt, double* dt2, double* dt3,
+                       int* istep) {
+    return guard([&] {
+        if (!h) fail(LSB_ERR_ARG, "null handle");
+        const long long S = h->d.S();
+        const size_t B = S * sizeof(double);
+        auto dn = [&](double* dst, const double* src, size_t bytes) {
+            if (dst) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, h->stream));
+        };
+        dn(uf, h->vel, B);
+        dn(vf, h->vel + S, B);
+        dn(wf, h->vel + 2 * S, B);
+        dn(pf, h->p, B);
+        dn(pnf, h->pn, B);
+        dn(unif, h->veln, 3 * B);
+        dn(unmif, h->velnm, 3 * B);
+        dn(nlnif, h->nln, 3 * B);
+        dn(nlnmif, h->nlnm, 3 * B);
+        CK(cudaStreamSynchronize(h->stream));
+        if (t) *t = h->t;
+        if (dt) *dt = h->dt;
+        if (dt2) *dt2 = h->dt2;
+        if (dt3) *dt3 = h->dt3;
+        if (istep) *istep = h->istep;
+    });
+}
+
+int lsb_upload_state_device(lsb_handle* h, const double* uf, const double* vf, const double* wf) {
+    return guard([&] {
+        if (!h || !uf || !vf || !wf) fail(LSB_ERR_ARG, "null argument");
+        const long long S = h->d.S();
+        CK(cudaMemcpyAsync(h->vel, uf, S * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->vel + S, vf, S * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->vel + 2 * S, wf, S * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    });
+}
+
+int lsb_download_velocity_device(lsb_handle* h, double* uf, double* vf, double* wf) {
+    return guard([&] {
+        if (!h || !uf || !vf || !wf) fail(LSB_ERR_ARG, "null argument");
+        const long long S = h->d.S();
+        CK(cudaMemcpyAsync(uf, h->vel, S * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        CK(cudaMemcpyAsync(vf, h->vel + S, S * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        CK(cudaMemcpyAsync(wf, h->vel + 2 * S, S * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    });
+}
+
+int lsb_step(lsb_handle* h, int nsteps) {
+    return guard([&] {
+        if (!h) fail(LSB_ERR_ARG, "null handle");
+        if (nsteps < 0) fail(LSB_ERR_ARG, "nsteps < 0");
+        if (!(h->dt > 0.0) || !std::isfinite(h->dt)) fail(LSB_ERR_STATE, "dt must be finite and > 0");
+        for (int i = 0; i < nsteps; ++i) {
+            step_one(h);
+            check_launch();
+        }
+    });
+}
+
+// ---------------------------------------------------------------- tier 1
+namespace {
+void to_dev_phys(lsb_handle* h, const double* src, double* dst, int nf) {
+    // host (nx+2, ny, nzp) -> device [nzp][ny][nx]
+    const Dims& d = h->d;
+    const size_t rows = (size_t)d.ny * d.nzp;
+    for (int f = 0; f < nf; ++f)
+        CK(cudaMemcpy2DAsync(dst + f * h->P, d.nx * sizeof(double), src + f * rows * (d.nx + 2),
+                             (d.nx + 2) * sizeof(double), d.nx * sizeof(double), rows, cudaMemcpyHostToDevice,
+                             h->stream));
+}
+void from_dev_phys(lsb_handle* h, const double* src, double* dst, int nf) {
+    const Dims& d = h->d;
+    const size_t rows = (size_t)d.ny * d.nzp;
+    for (int f = 0; f < nf; ++f) {
+        std::memset(dst + f * rows * (d.nx + 2), 0, rows * (d.nx + 2) * sizeof(double));
+        CK(cudaMemcpy2DAsync(dst + f * rows * (d.nx + 2), (d.nx + 2) * sizeof(double), src + f * h->P,
+                             d.nx * sizeof(double), d.nx * sizeof(double), rows, cudaMemcpyDeviceToHost, h->stream));
+    }
+}
+void to_dev(lsb_handle* h, const double* src, double* dst, long long n) {
+    CK(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+}
+void from_dev(lsb_handle* h, const double* src, double* dst, long long n) {
+    CK(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    check_launch();
+}
+}  // namespace
+
+int lsb_horfft(lsb_handle* h, double* ain, double* ainf, int is) {
+    return guard([&] {
+        if (!h || !ain || !ainf) fail(LSB_ERR_ARG, "null argument");
+        const long long S = h->d.S();
+        double* ph = h->phys;
+        double* sp = h->io;
+        if (is == -1) {
+            to_dev_phys(h, ain, ph, 1);
+            const double* pp[1] = {ph};
+            double* ss[1] = {sp};
+            phys_to_spec(h, pp, ss, 1, h->d.nzp, 1.0, 0.0, nullptr);
+            from_dev(h, sp, ainf, S);
+        } else if (is == 1) {
+            to_dev(h, ainf, sp, S);
+            const double* ss[1] = {sp};
+            double* pp[1] = {ph};
+            spec_to_phys(h, ss, pp, 1, h->d.nzp, nullptr, nullptr);
+            from_dev_phys(h, ph, ain, 1);
+            CK(cudaStreamSynchronize(h->stream));
+            check_launch();
+        } else {
+            fail(LSB_ERR_ARG, "is must be -1 or +1");
+        }
+    });
+}
+
+int lsb_dfdx(lsb_handle* h, const double* uf, double* out) {
+    return guard([&] {
+        const long long S = h->d.S();
+        to_dev(h, uf, h->io, S);
+        launch_dxy(h->io, h->io + S, h->wavx, h->wavy, h->d.nx, S, h->d.C(), 0, h->stream);
+        from_dev(h, h->io + S, out, S);
+    });
+}
+
+int lsb_dfdy(lsb_handle* h, const double* uf, double* out) {
+    return guard([&] {
+        const long long S = h->d.S();
+        to_dev(h, uf, h->io, S);
+        launch_dxy(h->io, h->io + S, h->wavx, h->wavy, h->d.nx, S, h->d.C(), 1, h->stream);
+        from_dev(h, h->io + S, out, S);
+    });
+}
+
+int lsb_dfdz(lsb_handle* h, const double* uf, double* out) {
+    return guard([&] {
+        const long long S = h->d.S();
+        to_dev(h, uf, h->io, S);
+        zgemm1(h, h->m_dz1, h->io, h->io + S, 1);
+        from_dev(h, h->io + S, out, S);
+    });
+}
+
+int lsb_d2fdz2(lsb_handle* h, const double* uf, double* out) {
+    return guard([&] {
+        const long long S = h->d.S();
+        to_dev(h, uf, h->io, S);
+        zgemm1(h, h->m_dz2, h->io, h->io + S, 1);
+        from_dev(h, h->io + S, out, S);
+    });
+}
+
+int lsb_lapl(lsb_handle* h, const double* uf, double* out) {
+    return guard([&] {
+        const long long S = h->d.S();
+        to_dev(h, uf, h->io, S);
+        zgemm1(h, h->m_dz2, h->io, h->io + S, 1);
+        launch_lapl_xy(h->io, h->io + S, h->wavx, h->wavy, h->d.nx, S, h->d.C(), h->stream);
+        from_dev(h, h->io + S, out, S);
+    });
+}
+
+int lsb_divuv(lsb_handle* h, const double* uf, const double* vf, double* out) {
+    return guard([&] {
+        const long long S = h->d.S();
+        to_dev(h, uf, h->io, S);
+        to_dev(h, vf, h->io + S, S);
+        launch_divuv(h->io, h->io + S, h->io + 2 * S, h->wavx, h->wavy, h->d.nx, S, h->d.C(), h->stream);
+        from_dev(h, h->io + 2 * S, out, S);
+    });
+}
+
+int lsb_solve_helmholtz(lsb_handle* h, double* rhs, double dtnui) {
+    return guard([&] {
+        const long long S = h->d.S();
+        to_dev(h, rhs, h->io, S);
+        helmholtz(h, h->io, h->io + S, 1, dtnui, nullptr);
+        from_dev(h, h->io + S, rhs, S);
+    });
+}
+
+int lsb_solve_nhom_helmholtz(lsb_handle* h, double* rhs, const double* bc, double dtnui) {
+    return guard([&] {
+        const Dims& d = h->d;
+        const long long S = d.S(), C = d.C();
+        to_dev(h, rhs, h->io, S);
+        // boundary field: only its planes k = 1 (ceiling) and k = nzp (wall) are read
+        to_dev(h, bc, h->io + 2 * S, C);
+        to_dev(h, bc + (long long)(d.nzp - 1) * C, h->io + 2 * S + C, C);
+        helmholtz(h, h->io, h->io + S, 1, dtnui, h->io + 2 * S);
+        from_dev(h, h->io + S, rhs, S);
+    });
+}
+
+int lsb_dealias_product(lsb_handle* h, const double* a, const double* b, double* ab) {
+    return guard([&] {
+        const Dims& d = h->d;
+        if (h->cfg.dealiasflag != 1) fail(LSB_ERR_STATE, "handle was created without dealiasflag = 1");
+        const long long S = d.S();
+        to_dev_phys(h, a, h->phys, 1);
+        to_dev_phys(h, b, h->phys + h->P, 1);
+        const double* pp[2] = {h->phys, h->phys + h->P};
+        double* ss[2] = {h->io, h->io + S};
+        phys_to_spec(h, pp, ss, 2, d.nzp, 1.0, 0.0, nullptr);
+        // pad, inverse, product, forward, truncate: reuse the spanwise / row passes on the padded grid
+        YInvJobList yj{};
+        yj.n = 2;
+        yj.j[0] = YInvJob{h->io, h->Y, YM_COPY};
+        yj.j[1] = YInvJob{h->io + S, h->Y + h->Yl, YM_COPY};
+        launch_yinv(yj, ypass(h, true, d.nzp), h->stream);
+        RowJobList rj{};
+        rj.n = 2;
+        const long long PL = (long long)d.nxl * d.nyl * d.nzp;
+        double* pl = h->Y + 2 * h->Yl;  // padded physical rows live after the two y-intermediates
+        if (2 * h->Yl + 3 * PL > 18 * h->Yl) fail(LSB_ERR_STATE, "scratch too small");
+        rj.j[0] = RowIO{h->Y, pl, YM_COPY, 0.0, nullptr};
+        rj.j[1] = RowIO{h->Y + h->Yl, pl + PL, YM_COPY, 0.0, nullptr};
+        launch_row_c2r(rj, rowargs(h, true, d.nzp), h->stream);
+        launch_axpby(pl + 2 * PL, pl, 1.0, 0.0, PL, h->stream);
+        sgs_mul(pl + 2 * PL, pl + PL, PL, h->stream);
+        RowJobList rf{};
+        rf.n = 1;
+        rf.j[0] = RowIO{pl + 2 * PL, h->Y, YM_COPY, 0.0, nullptr};
+        launch_row_r2c(rf, rowargs(h, true, d.nzp), h->stream);
+        YFwdJobList yf{};
+        yf.n = 1;
+        yf.j[0] = YFwdJob{h->Y, h->io + 2 * S, 1.0, 0.0, 0};
+        launch_yfwd(yf, ypass(h, true, d.nzp), h->stream);
+        const double* ss2[1] = {h->io + 2 * S};
+        double* pp2[1] = {h->phys + 2 * h->P};
+        spec_to_phys(h, ss2, pp2, 1, d.nzp, nullptr, nullptr);
+        from_dev_phys(h, h->phys + 2 * h->P, ab, 1);
+        CK(cudaStreamSynchronize(h->stream));
+        check_launch();
+    });
+}
+
+int lsb_nlterm(lsb_handle* h, const double* uif, double* nltermif) {
+    return guard([&] {
+        const long long S = h->d.S();
+        to_dev(h, uif, h->io, 3 * S);
+        nlterm(h, h->io, h->io + 3 * S);
+        from_dev(h, h->io + 3 * S, nltermif, 3 * S);
+    });
+}
+
+int lsb_tau_sgs(lsb_handle* h, const double* ui, const double* uiuj, const double* duidxj, double* tauij) {
+    return guard([&] {
+        if (h->cfg.sgsflag != 1) fail(LSB_ERR_STATE, "handle was created without sgsflag = 1");
+        const long long P = h->P;
+        const size_t F = (size_t)(h->d.nx + 2) * h->d.ny * h->d.nzp;  // host field size
+        // ui: 3 fields; uiuj, duidxj, tauij: 9 fields in Fortran order (..., l, m), l fastest;
+        // on the device tensor component (l, m) is field 3*l + m
+        to_dev_phys(h, ui, h->phys, 3);
+        for (int l = 0; l < 3; ++l)
+            for (int m = 0; m < 3; ++m) {
+                to_dev_phys(h, duidxj + (l + 3 * m) * F, h->phys + (3 + 3 * l + m) * P, 1);
+                to_dev_phys(h, uiuj + (l + 3 * m) * F, h->phys + (12 + 3 * l + m) * P, 1);
+            }
+        sgs_tau_phys(h, h->phys, h->phys + 3 * P, h->phys + 12 * P, h->sgs.tau);
+        for (int l = 0; l < 3; ++l)
+            for (int m = 0; m < 3; ++m) from_dev_phys(h, h->sgs.tau + (3 * l + m) * P, tauij + (l + 3 * m) * F, 1);
+        CK(cudaStreamSynchronize(h->stream));
+        check_launch();
+    });
+}
+
+int lsb_timers(lsb_handle* h, int enable) {
+    return guard([&] {
+        if (!h) fail(LSB_ERR_ARG, "null handle");
+        CK(cudaStreamSynchronize(h->stream));
+        if (enable) {
+            for (auto& kv : h->timers)
+                for (auto& ev : kv.second) {
+                    cudaEventDestroy(ev.first);
+                    cudaEventDestroy(ev.second);
+                }
+            h->timers.clear();
+        }
+        h->timing = enable != 0;
+    });
+}
+
+int lsb_timer_report(lsb_handle* h, char* buf, int buflen) {
+    return guard([&] {
+        if (!h || !buf || buflen <= 0) fail(LSB_ERR_ARG, "null argument");
+        CK(cudaStreamSynchronize(h->stream));
+        std::string s;
+        for (auto& kv : h->timers) {
+            double tot = 0.0;
+            for (auto& ev : kv.second) {
+                float ms = 0.f;
+                CK(cudaEventElapsedTime(&ms, ev.first, ev.second));
+                tot += ms;
+            }
+            s += kv.first + " " + std::to_string(kv.second.size()) + " " + std::to_string(tot) + "\n";
+        }
+        std::strncpy(buf, s.c_str(), (size_t)buflen - 1);
+        buf[buflen - 1] = 0;
+    });
+}
+
+int lsb_upload_velocity(lsb_handle* h, const double* uf, const double* vf, const double* wf) {
+    return guard([&] {
+        if (!h || !uf || !vf || !wf) fail(LSB_ERR_ARG, "null argument");
+        const long long S = h->d.S();
+        CK(cudaMemcpyAsync(h->vel, uf, S * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->vel + S, vf, S * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->vel + 2 * S, wf, S * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    });
+}
+
+int lsb_download_velocity(lsb_handle* h, double* uf, double* vf, double* wf) {
+    return guard([&] {
+        if (!h || !uf || !vf || !wf) fail(LSB_ERR_ARG, "null argument");
+        const long long S = h->d.S();
+        CK(cudaMemcpyAsync(uf, h->vel, S * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(vf, h->vel + S, S * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(wf, h->vel + 2 * S, S * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    });
+}
+
+int lsb_diag(lsb_handle* h, lsb_diagnostics* out) {
+    return guard([&] {
+        if (!h || !out) fail(LSB_ERR_ARG, "null argument");
+        diag_compute(h, out);
+    });
+}
+
+}  // extern "C"

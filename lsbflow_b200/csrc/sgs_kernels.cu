@@ -1,0 +1,662 @@
+// Subgrid-scale stresses in physical space (src/sgsterm.f90:10-467) with the
+// 3-point x/y/z test filter of filter_q_3pt (src/filters.f90:363-613), and the
+// reductions of the diagnostics (maxcalc, divcheck, ener).
+//
+// Fields live on the unpadded physical grid [nzp][ny][nx] (one GPU: the spanwise
+// halo exchange of filtery_q_3pt becomes a periodic wrap).  Tensor fields are stored
+// as 9 components with index 3*l + m (du_l/dx_m), symmetric ones as 6 components
+// (11, 12, 13, 22, 23, 33).  Floating-point expressions keep the reference's order.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "lsb_handle.cuh"
+#include "lsb_spectral.cuh"
+
+namespace lsb {
+
+namespace {
+void sfail(int code, const std::string& m) { throw LsbError{code, m}; }
+
+__host__ __device__ __forceinline__ int sym6(int l, int m) {
+    // (1,1)=0 (1,2)=1 (1,3)=2 (2,2)=3 (2,3)=4 (3,3)=5
+    const int a = l < m ? l : m, b = l < m ? m : l;
+    return a == 0 ? b : (a == 1 ? 2 + b : 5);
+}
+
+inline int nblk(long long n) {
+    long long b = (n + 255) / 256;
+    if (b > 148LL * 16) b = 148LL * 16;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+struct FieldList {
+    const double* in[9];
+    double* out[9];
+    int n;
+};
+struct P9 {
+    const double* p[9];
+};
+struct W9 {
+    double* p[9];
+};
+
+// filter_q_3pt: x (periodic) then y (periodic) then z (interior planes, non-uniform weights)
+__global__ void k_filter3(FieldList fl, int nx, int ny, int nzp, double a, double b, const double* __restrict__ az,
+                          const double* __restrict__ bz, const double* __restrict__ cz) {
+    const long long P = (long long)nx * ny * nzp;
+    const double s = 2.0 * a + b;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < P * fl.n;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int f = (int)(e / P);
+        const long long x = e % P;
+        const int i = (int)(x % nx);
+        const int j = (int)((x / nx) % ny);
+        const int k = (int)(x / ((long long)nx * ny));
+        const double* q = fl.in[f];
+        const int im = (i == 0) ? nx - 1 : i - 1, ip = (i == nx - 1) ? 0 : i + 1;
+        const int jm = (j == 0) ? ny - 1 : j - 1, jp = (j == ny - 1) ? 0 : j + 1;
+        auto xf = [&](int kk, int jj) {
+            const double* r = q + ((long long)kk * ny + jj) * nx;
+            return (a * r[im] + b * r[i] + a * r[ip]) / s;
+        };
+        auto yf = [&](int kk) { return (a * xf(kk, jm) + b * xf(kk, j) + a * xf(kk, jp)) / s; };
+        double v;
+        if (k == 0 || k == nzp - 1) {
+            v = yf(k);
+        } else {
+            v = (az[k] * yf(k - 1) + bz[k] * yf(k) + cz[k] * yf(k + 1)) / s;
+        }
+        fl.out[f][x] = v;
+    }
+}
+
+void filter3(lsb_handle* h, const double* const* in, double* const* out, int n, double a, double b, int which) {
+    const Dims& d = h->d;
+    for (int f0 = 0; f0 < n; f0 += 9) {
+        FieldList fl{};
+        fl.n = std::min(9, n - f0);
+        for (int i = 0; i < fl.n; ++i) {
+            fl.in[i] = in[f0 + i];
+            fl.out[i] = out[f0 + i];
+        }
+        const double* zf = h->sgs.zf + (long long)which * 3 * d.nzp;
+        TimerScope ts(h, "sgs_filter3");
+        k_filter3<<<nblk(h->P * fl.n), 256, 0, h->stream>>>(fl, d.nx, d.ny, d.nzp, a, b, zf, zf + d.nzp,
+                                                           zf + 2 * d.nzp);
+    }
+}
+
+// ---------------------------------------------------------------- dynamic Smagorinsky
+struct DynArgs {
+    const double* g[9];     // du_l/dx_m
+    double* sij[6];
+    double* sijhat[6];
+    double* lij[6];
+    double* mij[6];
+    const double* uihat[3];
+    double* lf[6];          // filtered u_i u_j
+    double* snorm;
+    double* numc;
+    double* denomc;
+    const double* ctot;
+    const double* cdd;
+    double* tau[9];
+    const double* delta;    // [nzp]
+    long long P;
+    int nxy;
+};
+
+__global__ void k_dyn1(DynArgs a) {  // S_ij, |S|
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < a.P; e += (long long)gridDim.x * blockDim.x) {
+        double s6[6];
+        for (int l = 0; l < 3; ++l)
+            for (int m = l; m < 3; ++m) s6[sym6(l, m)] = 0.5 * (a.g[3 * l + m][e] + a.g[3 * m + l][e]);
+        double sn = 0.0;
+        for (int m = 0; m < 3; ++m)
+            for (int l = 0; l < 3; ++l) {
+                const double v = s6[sym6(l, m)];
+                sn = sn + 2. * v * v;
+            }
+        for (int q = 0; q < 6; ++q) a.sij[q][e] = s6[q];
+        a.snorm[e] = sqrt(sn);
+    }
+}
+
+__global__ void k_dyn2(DynArgs a) {  // |[S]|, L' = delta^2 |S| S_ij, [delta]^2 |[S]| [S_ij]
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < a.P; e += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(e / a.nxy);
+        const double dl = a.delta[k], cd = 2.0 * dl;
+        double sh = 0.0;
+        for (int m = 0; m < 3; ++m)
+            for (int l = 0; l < 3; ++l) {
+                const double v = a.sijhat[sym6(l, m)][e];
+                sh = sh + 2. * v * v;
+            }
+        sh = sqrt(sh);
+        const double sn = a.snorm[e];
+        for (int q = 0; q < 6; ++q) {
+            a.lij[q][e] = dl * dl * sn * a.sij[q][e];
+            a.sijhat[q][e] = cd * cd * sh * a.sijhat[q][e];
+        }
+    }
+}
+
+__global__ void k_dyn3(DynArgs a) {  // M_ij, L_ij, <M L>, <M M> integrands
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < a.P; e += (long long)gridDim.x * blockDim.x) {
+        double m6[6], l6[6];
+        for (int q = 0; q < 6; ++q) m6[q] = 2.0 * (a.mij[q][e] - a.sijhat[q][e]);
+        for (int l = 0; l < 3; ++l)
+            for (int m = l; m < 3; ++m) l6[sym6(l, m)] = a.lf[sym6(l, m)][e] - a.uihat[l][e] * a.uihat[m][e];
+        double num = 0.0, den = 0.0;
+        for (int m = 0; m < 3; ++m)
+            for (int l = 0; l < 3; ++l) {
+                const int q = sym6(l, m);
+                num = num + m6[q] * l6[q];
+                den = den + m6[q] * m6[q];
+            }
+        a.numc[e] = num;
+        a.denomc[e] = den;
+    }
+}
+
+__global__ void k_dyn4(DynArgs a) {  // C clip, nu_sgs, tau = -2 nu S_ij
+    const double cmax = 0.2 * 0.2;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < a.P; e += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(e / a.nxy);
+        const double dl = a.delta[k];
+        double c = a.ctot[e] / a.cdd[e];
+        if (c < 0.0 || isnan(c)) c = 0.0;
+        if (c > cmax) c = cmax;
+        const double nu = c * dl * dl * a.snorm[e];
+        for (int l = 0; l < 3; ++l)
+            for (int m = 0; m < 3; ++m) a.tau[3 * l + m][e] = -2.0 * nu * a.sij[sym6(l, m)][e];
+    }
+}
+
+// ---------------------------------------------------------------- static Smagorinsky
+__global__ void k_utau(const double* __restrict__ dudz, const int* __restrict__ wall, int nwall, long long C,
+                       double xnu, int nxy, double* out) {
+    __shared__ double red[256];
+    double acc = 0.0;
+    for (long long c = threadIdx.x; c < C; c += blockDim.x) {
+        double u = 0.0;
+        for (int w = 0; w < nwall; ++w) u = u + xnu * dudz[(long long)wall[w] * C + c];
+        acc += u / nwall;
+    }
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[0] = sqrt(fabs(red[0] / (double)nxy));
+}
+
+__global__ void k_static(P9 g, W9 tau, const double* __restrict__ sdelta,
+                         const double* __restrict__ zpts, const double* __restrict__ utau, double cs, double xnu,
+                         long long P, int nxy) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < P; e += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(e / nxy);
+        double sn = 0.0;
+        for (int j = 0; j < 3; ++j)
+            for (int i = 0; i < 3; ++i) {
+                const double v = 0.5 * (g.p[3 * i + j][e] + g.p[3 * j + i][e]);
+                sn = sn + v * v;
+            }
+        sn = sqrt(2. * sn);
+        const double zplus = zpts[k] * utau[0] / xnu;
+        const double f = cs * sdelta[k] * (1. - exp(-zplus / 25.));
+        const double nu = -(f * f) * sn;
+        for (int j = 0; j < 3; ++j)
+            for (int i = 0; i < 3; ++i) tau.p[3 * i + j][e] = nu * 0.5 * (g.p[3 * i + j][e] + g.p[3 * j + i][e]);
+    }
+}
+
+// ---------------------------------------------------------------- sigma model
+__global__ void k_sigma(P9 g, W9 tau, const double* __restrict__ delta, long long P,
+                        int nxy) {
+    const double pi = 4. * atan(1.);
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < P; e += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(e / nxy);
+        double gij[3][3], G[3][3], G2[3][3];
+        for (int l = 0; l < 3; ++l)
+            for (int m = 0; m < 3; ++m) gij[l][m] = g.p[3 * l + m][e];
+        for (int l = 0; l < 3; ++l)
+            for (int m = 0; m < 3; ++m) {
+                double s = 0.0;
+                for (int q = 0; q < 3; ++q) s += gij[q][l] * gij[q][m];  // (g^T g)(l,m)
+                G[l][m] = s;
+            }
+        for (int l = 0; l < 3; ++l)
+            for (int m = 0; m < 3; ++m) {
+                double s = 0.0;
+                for (int q = 0; q < 3; ++q) s += G[l][q] * G[q][m];
+                G2[l][m] = s;
+            }
+        const double i1 = G[0][0] + G[1][1] + G[2][2];
+        const double i2 = 0.5 * (i1 * i1 - (G2[0][0] + G2[1][1] + G2[2][2]));
+        const double i3 = G[0][0] * (G[1][1] * G[2][2] - G[1][2] * G[2][1]) -
+                          G[0][1] * (G[1][0] * G[2][2] - G[1][2] * G[2][0]) +
+                          G[0][2] * (G[1][0] * G[2][1] - G[1][1] * G[2][0]);
+        double a1 = i1 * i1 / 9. - i2 / 3.;
+        const double a2 = i1 * i1 * i1 / 27. - i1 * i2 / 6. + 0.5 * i3;
+        if (a1 < 0.0) a1 = fabs(a1);
+        const double sq = sqrt(a1);
+        const double pre = a2 / pow(sq, 3.0);
+        double a3;
+        if (pre >= 1. || isnan(pre)) a3 = 0.0;
+        else if (pre <= -1.) a3 = pi / 3.;
+        else a3 = acos(pre) / 3.;
+        const double s1 = sqrt(fabs(i1 / 3. + 2. * sq * cos(a3)));
+        const double s2 = sqrt(fabs(i1 / 3. - 2. * sq * cos(pi / 3. + a3)));
+        const double s3 = sqrt(fabs(i1 / 3. - 2. * sq * cos(pi / 3. - a3)));
+        double ds = s3 * (s1 - s2) * (s2 - s3);
+        if (s1 != 0.) ds = ds / (s1 * s1);
+        if (ds < 0.0 || isnan(ds)) ds = 0.0;
+        const double cd = 1.35 * delta[k];
+        const double nu = -(cd * cd) * ds;
+        for (int l = 0; l < 3; ++l)
+            for (int m = 0; m < 3; ++m) tau.p[3 * l + m][e] = 2.0 * nu * 0.5 * (gij[l][m] + gij[m][l]);
+    }
+}
+
+// ---------------------------------------------------------------- interscale
+__global__ void k_prod9(P9 a, P9 b, W9 out, long long P) {
+    // out[3l+m] = a[l] * b[m]
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < P; e += (long long)gridDim.x * blockDim.x)
+        for (int l = 0; l < 3; ++l)
+            for (int m = 0; m < 3; ++m) out.p[3 * l + m][e] = a.p[l][e] * b.p[m][e];
+}
+
+__global__ void k_interscale(P9 u, P9 ub, P9 ub2, P9 uibujbar, W9 tau, long long P) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < P; e += (long long)gridDim.x * blockDim.x)
+        for (int l = 0; l < 3; ++l)
+            for (int m = 0; m < 3; ++m)
+                tau.p[3 * l + m][e] = uibujbar.p[3 * l + m][e] - ub2.p[l][e] * ub2.p[m][e] -
+                                      ub.p[l][e] * (u.p[m][e] - ub.p[m][e]);
+}
+
+__global__ void k_uiuj(P9 u, W9 out, long long P) {
+    // out[sym(l,m)] = u_l u_m   (src/navierstokes.f90:744)
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < P; e += (long long)gridDim.x * blockDim.x)
+        for (int l = 0; l < 3; ++l)
+            for (int m = l; m < 3; ++m) out.p[sym6(l, m)][e] = u.p[m][e] * u.p[l][e];
+}
+
+__global__ void k_mul(double* y, const double* x, long long n) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+        y[e] = y[e] * x[e];
+}
+
+
+}  // namespace
+
+void sgs_mul(double* y, const double* x, long long n, cudaStream_t s) { k_mul<<<nblk(n), 256, 0, s>>>(y, x, n); }
+
+static void zfilter_coeffs(const std::vector<double>& zp, int mapping, double a, double b, double* az, double* bz,
+                           double* cz) {
+    const int n = (int)zp.size();
+    for (int k = 0; k < n; ++k) az[k] = bz[k] = cz[k] = 0.0;
+    if (mapping == 1 || mapping == 2) {
+        for (int k = 1; k < n - 1; ++k) {
+            const double dltm = zp[k] - zp[k - 1], dltp = zp[k + 1] - zp[k];
+            az[k] = a * 2.0 * dltm / (dltp + dltm);
+            bz[k] = a * 2.0 * (1. - dltm / dltp) + b;
+            cz[k] = a * 2.0 * dltm * dltm / (dltp * (dltp + dltm));
+        }
+        if (mapping == 1) { az[1] = 0.0; bz[1] = 2.0 * a + b; cz[1] = 0.0; }
+    } else {
+        const int m = (n + 1) / 2;
+        for (int k = 2; k <= m - 1; ++k) {
+            const double dltm = zp[k - 1] - zp[k - 2], dltp = zp[k] - zp[k - 1];
+            az[k - 1] = a * 2.0 * dltm / (dltp + dltm);
+            bz[k - 1] = a * 2.0 * (1. - dltm / dltp) + b;
+            cz[k - 1] = a * 2.0 * dltm * dltm / (dltp * (dltp + dltm));
+        }
+        for (int k = m + 1; k <= n - 1; ++k) {
+            const double dltm = zp[k - 1] - zp[k - 2], dltp = zp[k] - zp[k - 1];
+            az[k - 1] = a * 2.0 * dltp * dltp / (dltm * (dltm + dltp));
+            bz[k - 1] = a * 2.0 * (1. - dltp / dltm) + b;
+            cz[k - 1] = a * 2.0 * dltp / (dltm + dltp);
+        }
+        az[m - 1] = a; bz[m - 1] = b; cz[m - 1] = a;
+    }
+}
+
+void sgs_init(lsb_handle* h) {
+    const Dims& d = h->d;
+    const lsb_config& c = h->cfg;
+    SgsWork& s = h->sgs;
+    s.nonsym = (c.sgsmodel == 3);
+    s.tau = h->alloc(9 * h->P);
+    if (s.nonsym) s.H9 = h->alloc(9 * d.S());
+    s.nw = 40;
+    s.w = h->alloc((size_t)s.nw * h->P);
+    std::vector<double> zf(6 * (size_t)d.nzp);
+    zfilter_coeffs(h->h_zpts, c.mapping, c.a, c.b, &zf[0], &zf[d.nzp], &zf[2 * d.nzp]);
+    zfilter_coeffs(h->h_zpts, c.mapping, 1.0, 1.0, &zf[3 * d.nzp], &zf[4 * d.nzp], &zf[5 * d.nzp]);
+    s.zf = h->upload(zf.data(), zf.size());
+    // delta of the dynamic and sigma models (src/sgsterm.f90:159-164, 367-376)
+    const std::vector<double>& zp = h->h_zpts;
+    const int n = d.nzp;
+    std::vector<double> dl(n), sd(n, 0.0);
+    for (int k = 0; k < n; ++k) {
+        double dz;
+        if (k == 0) dz = zp[0] - zp[1];
+        else if (k == n - 1) dz = zp[n - 2] - zp[n - 1];
+        else dz = 0.5 * (zp[k - 1] - zp[k + 1]);
+        dl[k] = std::pow(h->dx * h->dy * dz, 1. / 3.);
+    }
+    // static Smagorinsky (src/sgsterm.f90:96-103): delta(1) overwritten, delta(nzp) unset
+    for (int k = 1; k < n - 1; ++k) sd[k] = std::pow(h->dx * h->dy * ((zp[k - 1] - zp[k + 1]) / 2.), 1. / 3.);
+    sd[0] = std::pow(h->dx * h->dy * std::fabs(zp[n - 1] - zp[n - 2]), 1. / 3.);
+    sd[n - 1] = 0.0;
+    s.delta = h->upload(dl.data(), n);
+    s.sdelta = h->upload(sd.data(), n);
+    s.scal = h->alloc(16);
+    // wall planes for u_tau: zpts == 0 or |zpts| == 0.5 (src/sgsterm.f90:62-67)
+    std::vector<int> wall;
+    for (int k = 0; k < n; ++k)
+        if (zp[k] == 0.0 || std::fabs(zp[k]) == 0.5) wall.push_back(k);
+    if (c.sgsmodel == 0 && wall.empty()) sfail(LSB_ERR_UNSUPPORTED, "static Smagorinsky needs a wall plane");
+    double* wbuf = h->alloc(8);
+    std::vector<int> wi(16, 0);
+    for (size_t i = 0; i < wall.size() && i < 16; ++i) wi[i] = wall[i];
+    CK(cudaMemcpyAsync(wbuf, wi.data(), 16 * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    h->sgs_wall = (int*)wbuf;
+    h->sgs_nwall = (int)wall.size();
+}
+
+// tau (9 components, index 3l+m) from physical u_l, g = du_l/dx_m (9), uiuj (9, index 3l+m or sym)
+static void model_tau(lsb_handle* h, const double* const* u, const double* const* g, const double* const* uu6,
+                      double* tau) {
+    const Dims& d = h->d;
+    const lsb_config& c = h->cfg;
+    const long long P = h->P;
+    const int nxy = d.nx * d.ny;
+    SgsWork& s = h->sgs;
+    cudaStream_t st = h->stream;
+    double* w = s.w;
+    auto W = [&](int i) { return w + (long long)i * P; };
+    double* T[9];
+    for (int q = 0; q < 9; ++q) T[q] = tau + (long long)q * P;
+    if (c.sgsmodel == 1) {
+        DynArgs a{};
+        for (int q = 0; q < 9; ++q) a.g[q] = g[q];
+        for (int q = 0; q < 6; ++q) {
+            a.sij[q] = W(q);
+            a.sijhat[q] = W(6 + q);
+            a.lij[q] = W(12 + q);
+            a.mij[q] = W(18 + q);
+            a.lf[q] = W(24 + q);
+        }
+        for (int l = 0; l < 3; ++l) a.uihat[l] = W(30 + l);
+        a.snorm = W(33);
+        a.numc = W(34);
+        a.denomc = W(35);
+        a.ctot = W(36);
+        a.cdd = W(37);
+        for (int q = 0; q < 9; ++q) a.tau[q] = T[q];
+        a.delta = s.delta;
+        a.P = P;
+        a.nxy = nxy;
+        k_dyn1<<<nblk(P), 256, 0, st>>>(a);
+        filter3(h, (const double* const*)a.sij, a.sijhat, 6, c.a, c.b, 0);
+        k_dyn2<<<nblk(P), 256, 0, st>>>(a);
+        filter3(h, (const double* const*)a.lij, a.mij, 6, c.a, c.b, 0);
+        double* uh[3] = {W(30), W(31), W(32)};
+        filter3(h, u, uh, 3, c.a, c.b, 0);
+        filter3(h, uu6, a.lf, 6, c.a, c.b, 0);
+        k_dyn3<<<nblk(P), 256, 0, st>>>(a);
+        const double* nd[2] = {a.numc, a.denomc};
+        double* cc[2] = {W(36), W(37)};
+        filter3(h, nd, cc, 2, 1.0, 1.0, 1);
+        k_dyn4<<<nblk(P), 256, 0, st>>>(a);
+    } else if (c.sgsmodel == 0) {
+        P9 gt{};
+        W9 tt{};
+        for (int q = 0; q < 9; ++q) {
+            gt.p[q] = g[q];
+            tt.p[q] = T[q];
+        }
+        k_utau<<<1, 256, 0, st>>>(g[2], h->sgs_wall, h->sgs_nwall, d.C(), c.xnu, nxy, s.scal);
+        k_static<<<nblk(P), 256, 0, st>>>(gt, tt, s.sdelta, h->zpts, s.scal, c.cs, c.xnu, P, nxy);
+    } else if (c.sgsmodel == 2) {
+        P9 gt{};
+        W9 tt{};
+        for (int q = 0; q < 9; ++q) {
+            gt.p[q] = g[q];
+            tt.p[q] = T[q];
+        }
+        k_sigma<<<nblk(P), 256, 0, st>>>(gt, tt, s.delta, P, nxy);
+    } else if (c.sgsmodel == 3) {
+        double* ub[3] = {W(0), W(1), W(2)};
+        double* ub2[3] = {W(3), W(4), W(5)};
+        double* pr[9];
+        double* pb[9];
+        for (int q = 0; q < 9; ++q) {
+            pr[q] = W(6 + q);
+            pb[q] = W(15 + q);
+        }
+        filter3(h, u, ub, 3, c.a, c.b, 0);
+        filter3(h, (const double* const*)ub, ub2, 3, c.a, c.b, 0);
+        P9 ubt{}, ut{}, ub2t{}, pbt{};
+        W9 prt{}, tt{};
+        for (int l = 0; l < 3; ++l) {
+            ubt.p[l] = ub[l];
+            ut.p[l] = u[l];
+            ub2t.p[l] = ub2[l];
+        }
+        for (int q = 0; q < 9; ++q) {
+            prt.p[q] = pr[q];
+            pbt.p[q] = pb[q];
+            tt.p[q] = T[q];
+        }
+        k_prod9<<<nblk(P), 256, 0, st>>>(ubt, ut, prt, P);
+        filter3(h, (const double* const*)pr, pb, 9, c.a, c.b, 0);
+        k_interscale<<<nblk(P), 256, 0, st>>>(ut, ubt, ub2t, pbt, tt, P);
+    } else {
+        CK(cudaMemsetAsync(tau, 0, 9 * P * sizeof(double), st));
+    }
+}
+
+// nlterm hook: ph[0..2] = u_l (+ubar), ph[3+3l+m] = du_l/dx_m; adds the forward transform of
+// tau into the spectral h fields.
+void sgs_add_tau(lsb_handle* h, double* const* ph, bool dealias) {
+    const Dims& d = h->d;
+    const long long P = h->P, S = d.S();
+    SgsWork& s = h->sgs;
+    cudaStream_t st = h->stream;
+    // u_i u_j on the unpadded grid: the dealiased products (2 * horfft(+1) of h) or plain products
+    double* uu6[6];
+    for (int q = 0; q < 6; ++q) uu6[q] = h->phys + (12 + q) * P;
+    const double* u3[3] = {ph[0], ph[1], ph[2]};
+    if (dealias) {
+        const double* hs[6];
+        for (int q = 0; q < 6; ++q) hs[q] = h->H + q * S;
+        spec_to_phys(h, hs, uu6, 6, d.nzp, nullptr, nullptr);
+        for (int q = 0; q < 6; ++q) launch_axpby(uu6[q], uu6[q], 2.0, 0.0, P, st);
+    } else {
+        P9 ut{};
+        W9 ot{};
+        for (int l = 0; l < 3; ++l) ut.p[l] = ph[l];
+        for (int q = 0; q < 6; ++q) ot.p[q] = uu6[q];
+        k_uiuj<<<nblk(P), 256, 0, st>>>(ut, ot, P);
+    }
+    const double* g[9];
+    for (int q = 0; q < 9; ++q) g[q] = ph[3 + q];
+    model_tau(h, u3, g, (const double* const*)uu6, s.tau);
+    if (!s.nonsym) {
+        // symmetric: add T(tau_lm) to h_lm for the 6 independent components
+        const double* tp[6];
+        double* hp[6];
+        for (int l = 0; l < 3; ++l)
+            for (int m = l; m < 3; ++m) {
+                tp[sym6(l, m)] = s.tau + (3 * l + m) * P;
+                hp[sym6(l, m)] = h->H + sym6(l, m) * S;
+            }
+        phys_to_spec(h, tp, hp, 6, d.nzp, 1.0, 1.0, nullptr);
+    } else {
+        const double* tp[9];
+        double* hp[9];
+        for (int l = 0; l < 3; ++l)
+            for (int m = 0; m < 3; ++m) {
+                CK(cudaMemcpyAsync(s.H9 + (3 * l + m) * S, h->H + sym6(l, m) * S, S * sizeof(double),
+                                   cudaMemcpyDeviceToDevice, st));
+                tp[3 * l + m] = s.tau + (3 * l + m) * P;
+                hp[3 * l + m] = s.H9 + (3 * l + m) * S;
+            }
+        phys_to_spec(h, tp, hp, 9, d.nzp, 1.0, 1.0, nullptr);
+    }
+}
+
+void sgs_tau_phys(lsb_handle* h, const double* ui, const double* g, const double* uiuj, double* tau) {
+    const long long P = h->P;
+    const double* u3[3] = {ui, ui + P, ui + 2 * P};
+    const double* g9[9];
+    for (int q = 0; q < 9; ++q) g9[q] = g + q * P;
+    const double* uu6[6];
+    for (int l = 0; l < 3; ++l)
+        for (int m = l; m < 3; ++m) uu6[sym6(l, m)] = uiuj + (3 * l + m) * P;
+    model_tau(h, u3, g9, uu6, tau);
+}
+
+// ---------------------------------------------------------------- diagnostics
+namespace {
+struct PlaneStats {
+    double e_tot, e_pert, umax, umin, vmax, vmin, wmax, wmin, uabs, vabs, wcfl, divabs, nonfinite;
+};
+constexpr int kStats = 13;
+
+__global__ void k_plane_stats(const double* __restrict__ u, const double* __restrict__ v,
+                              const double* __restrict__ w, const double* __restrict__ up,
+                              const double* __restrict__ vp, const double* __restrict__ wp,
+                              const double* __restrict__ div, const double* __restrict__ wscale, int findex, int nx,
+                              int ny, double* out) {
+    const int k = blockIdx.x;
+    const long long base = (long long)k * nx * ny;
+    __shared__ double red[kStats][256];
+    double et = 0, ep = 0, umax = -INFINITY, umin = INFINITY, vmax = -INFINITY, vmin = INFINITY, wmax = -INFINITY,
+           wmin = INFINITY, ua = 0, va = 0, wc = 0, da = 0, nf = 0;
+    for (int e = threadIdx.x; e < nx * ny; e += blockDim.x) {
+        const double a = u[base + e], b = v[base + e], c = w[base + e];
+        et += 0.5 * (a * a + b * b + c * c);
+        const double pa = up[base + e], pb = vp[base + e], pc = wp[base + e];
+        ep += 0.5 * (pa * pa + pb * pb + pc * pc);
+        umax = fmax(umax, a); umin = fmin(umin, a);
+        vmax = fmax(vmax, b); vmin = fmin(vmin, b);
+        wmax = fmax(wmax, c); wmin = fmin(wmin, c);
+        ua = fmax(ua, fabs(a)); va = fmax(va, fabs(b));
+        const int i = e % nx;
+        if (i < findex) wc = fmax(wc, fabs(c * wscale[k]));
+        da += fabs(div[base + e]);
+        if (!isfinite(a) || !isfinite(b) || !isfinite(c)) nf = 1;
+    }
+    const double vals[kStats] = {et, ep, umax, umin, vmax, vmin, wmax, wmin, ua, va, wc, da, nf};
+    for (int q = 0; q < kStats; ++q) red[q][threadIdx.x] = vals[q];
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            for (int q = 0; q < kStats; ++q) {
+                const double x = red[q][threadIdx.x], y = red[q][threadIdx.x + s];
+                double r;
+                if (q == 0 || q == 1 || q == 11) r = x + y;
+                else if (q == 3 || q == 5 || q == 7) r = fmin(x, y);
+                else r = fmax(x, y);
+                red[q][threadIdx.x] = r;
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < kStats) out[(long long)k * kStats + threadIdx.x] = red[threadIdx.x][0];
+}
+
+__global__ void k_zero_mean(double* f, long long S, long long C, int nzp) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < nzp) {
+        f[(long long)k * C] = 0.0;
+        f[(long long)k * C + 1] = 0.0;
+    }
+}
+}  // namespace
+
+void diag_compute(lsb_handle* h, lsb_diagnostics* out) {
+    const Dims& d = h->d;
+    const long long S = d.S(), C = d.C(), P = h->P;
+    cudaStream_t st = h->stream;
+    // physical u (+ubar), v, w; perturbation copies (mean mode removed); divergence
+    double* io = h->io;
+    CK(cudaMemcpyAsync(io, h->vel, 3 * S * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    for (int l = 0; l < 3; ++l) k_zero_mean<<<(d.nzp + 127) / 128, 128, 0, st>>>(io + l * S, S, C, d.nzp);
+    // divergence = dfdx(u) + dfdy(v) + dfdz(w)
+    double* dv = io + 3 * S;
+    zgemm(h, h->m_dz1, h->vel + 2 * S, dv, 1, EPI_STORE, 1.0, 0.0, nullptr);
+    launch_dxy(h->vel, io + 4 * S, h->wavx, h->wavy, d.nx, S, C, 0, st);
+    launch_dxy(h->vel + S, io + 5 * S, h->wavx, h->wavy, d.nx, S, C, 1, st);
+    launch_axpby(dv, io + 4 * S, 1.0, 1.0, S, st);
+    launch_axpby(dv, io + 5 * S, 1.0, 1.0, S, st);
+    double* ph[7];
+    for (int i = 0; i < 7; ++i) ph[i] = h->phys + i * P;
+    const double* sp[7] = {h->vel, h->vel + S, h->vel + 2 * S, io, io + S, io + 2 * S, dv};
+    const double* means[7] = {h->ubar, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    spec_to_phys(h, sp, ph, 7, d.nzp, means, nullptr);
+    // w CFL scale per plane (maxcalc, src/navierstokes.f90:430-437)
+    const std::vector<double>& zp = h->h_zpts;
+    const int nz = d.nz;
+    std::vector<double> ws(d.nzp);
+    for (int k = 0; k < nz; ++k) ws[k] = h->dt / (zp[k] - zp[k + 1]);
+    ws[0] = ws[0] * h->dt / (zp[0] - zp[1]);
+    ws[nz] = h->dt / (zp[nz - 1] - zp[nz]);
+    double* wsd = h->red;
+    CK(cudaMemcpyAsync(wsd, ws.data(), d.nzp * sizeof(double), cudaMemcpyHostToDevice, st));
+    const double fsz = h->cfg.fsize;
+    int findex = d.nx;
+    if (h->t > h->cfg.istartbound) findex = (int)((1. - 0.8 * fsz) * d.nx);
+    double* stats = h->T;
+    k_plane_stats<<<d.nzp, 256, 0, st>>>(ph[0], ph[1], ph[2], ph[3], ph[4], ph[5], ph[6], wsd, findex, d.nx, d.ny,
+                                         stats);
+    std::vector<double> hs((size_t)d.nzp * kStats);
+    CK(cudaMemcpyAsync(hs.data(), stats, hs.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    std::memset(out, 0, sizeof(*out));
+    double umax = -INFINITY, umin = INFINITY, vmax = 0.0, vmin = 0.0, wmax = 0.0, wmin = 0.0, ua = 0, va = 0, wc = 0,
+           da = 0, nf = 0;
+    for (int k = 0; k < d.nzp; ++k) {
+        const double* r = &hs[(size_t)k * kStats];
+        umax = std::fmax(umax, r[2]); umin = std::fmin(umin, r[3]);
+        vmax = std::fmax(vmax, r[4]); vmin = std::fmin(vmin, r[5]);
+        wmax = std::fmax(wmax, r[6]); wmin = std::fmin(wmin, r[7]);
+        ua = std::fmax(ua, r[8]); va = std::fmax(va, r[9]);
+        wc = std::fmax(wc, r[10]);
+        da += r[11];
+        nf = std::fmax(nf, r[12]);
+    }
+    // the reference's maxima include the two pad columns: 0 + ubar(k) for u, 0 for v and w
+    for (double ub : h->h_ubar) {
+        umax = std::fmax(umax, ub);
+        umin = std::fmin(umin, ub);
+        ua = std::fmax(ua, std::fabs(ub));
+    }
+    // ener (src/orrsomm.f90:660-664): trapezoid from k = nz down to 2, ceiling plane excluded
+    double et = 0.0, ep = 0.0;
+    for (int k = nz - 1; k >= 1; --k) {
+        et = et + 0.5 * (hs[(size_t)(k + 1) * kStats + 0] + hs[(size_t)k * kStats + 0]) * (zp[k] - zp[k + 1]);
+        ep = ep + 0.5 * (hs[(size_t)(k + 1) * kStats + 1] + hs[(size_t)k * kStats + 1]) * (zp[k] - zp[k + 1]);
+    }
+    out->divergence = da / (double)(d.nx * d.ny * d.nzp);
+    out->umax = umax; out->umin = umin; out->vmax = vmax; out->vmin = vmin; out->wmax = wmax; out->wmin = wmin;
+    out->cflx = ua * h->dt / h->dx;
+    out->cfly = va * h->dt / h->dy;
+    out->cflz = wc;
+    out->energy_total = et;
+    out->energy_pert = ep;
+    out->t = h->t;
+    out->dt = h->dt;
+    out->istep = h->istep;
+    out->nonfinite = nf != 0.0 ? 1 : 0;
+}
+
+}  // namespace lsb

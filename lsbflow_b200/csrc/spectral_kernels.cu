@@ -1,0 +1,286 @@
+// Elementwise spectral / physical kernels of navierstokes_update and timestep
+// (src/navierstokes.f90:10-90, 1157-1496), the spectral filter of filterqspec
+// (src/filters.f90:164-192, 281-360) and norm (src/horfft.f90:153-224).
+// Floating-point expressions keep the reference's evaluation order.
+#include "lsb_spectral.cuh"
+
+namespace lsb {
+
+__device__ __forceinline__ void ij_of(long long c2, int nx, int& i, int& j) {
+    // c2 = complex index within a plane: (j, ic) with ic < nx/2
+    const int kxc = nx / 2;
+    j = (int)(c2 / kxc);
+    i = 2 * (int)(c2 % kxc);
+}
+
+// ---------------------------------------------------------------- spectral filter
+__global__ void k_specfilter(SpecFilterArgs a) {
+    const long long n2 = a.S / 2;  // complex elements per field
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < 3 * n2; e += (long long)gridDim.x * blockDim.x) {
+        const int f = (int)(e / n2);
+        const long long ce = e % n2;
+        const long long cplane = ce % (a.C / 2);
+        int i, j;
+        ij_of(cplane, a.nx, i, j);
+        const double fr = a.in[f][2 * ce], fi = a.in[f][2 * ce + 1];
+        const double fmag = sqrt(fr * fr + fi * fi);
+        double orr = 0.0, oi = 0.0;
+        if (fmag != 0.0) {
+            double cosc = fr / fmag;
+            const double sinc = fi / fmag;
+            cosc = fmin(1.0, fmax(-1.0, cosc));
+            const double phase = (sinc >= 0.0) ? acos(cosc) : -acos(cosc);
+            const double wx = a.wavx[i], wy = a.wavy[j];
+            const double ak = sqrt(wx * wx + wy * wy);
+            double filt = 1.0;
+            if (fabs(ak) >= a.akc) {
+                const double theta = (fabs(ak) - a.akc) / (a.akmax - a.akc);
+                filt = exp(-a.amp * pow(theta, 2.0 * a.order));
+            }
+            const double fmagf = fmag * filt;
+            orr = fmagf * cos(phase);
+            oi = fmagf * sin(phase);
+        }
+        a.out[f][2 * ce] = orr;
+        a.out[f][2 * ce + 1] = oi;
+    }
+}
+
+// ---------------------------------------------------------------- velocity RHS
+// rhs_l = -dtnui*(dt*(ab0 N + ab1 nln + ab2 nlnm) + bdf0 u + bdf1 un + bdf2 unm) ;
+// rhs_1 -= horfft(ubarpp) (the (0,0) mode)      src/navierstokes.f90:1239,1282-1296
+__global__ void k_rhs(RhsArgs a) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < 3 * a.S; e += (long long)gridDim.x * blockDim.x) {
+        const int l = (int)(e / a.S);
+        const long long x = e % a.S;
+        const double nlt = a.ab[0] * a.N[l][x] + a.ab[1] * a.nln[l][x] + a.ab[2] * a.nlnm[l][x];
+        double r = -a.dtnui * (a.dt * nlt + a.bdf[0] * a.u[l][x] + a.bdf[1] * a.un[l][x] + a.bdf[2] * a.unm[l][x]);
+        if (l == 0 && (x % a.C) == 0) r = r - a.ubarpp[x / a.C];
+        a.rhs[l][x] = r;
+    }
+}
+
+// ---------------------------------------------------------------- boundary planes
+// Zang-Hussaini BCs of src/navierstokes.f90:1320-1373; bc[f][0] = ceiling (k=1),
+// bc[f][1] = wall (k=nzp).  Bound planes = c_top*btop, c_wa*bwa + c_wb*bwb.
+__global__ void k_bc_planes(BcArgs a) {
+    const long long n2 = a.C / 2;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n2; e += (long long)gridDim.x * blockDim.x) {
+        int i, j;
+        ij_of(e, a.nx, i, j);
+        const double wx = a.wavx[i], wy = a.wavy[j];
+        const double w2 = wx * wx + wy * wy;
+        const long long re = 2 * e, im = 2 * e + 1;
+        const double den = w2 + a.dtnui / a.bdfv;
+        const double psr = a.pfac0 * a.pwall[re] + a.pfac1 * a.pnwall[re];
+        const double psi = a.pfac0 * a.pwall[im] + a.pfac1 * a.pnwall[im];
+        const double dtb = a.dt * a.bdfv;
+        // u
+        a.bc[0][re] = -a.rtop[0][re] / den;
+        a.bc[0][im] = -a.rtop[0][im] / den;
+        a.bc[0][a.C + re] = dtb * (-wx * psi);
+        a.bc[0][a.C + im] = dtb * (wx * psr);
+        // v
+        a.bc[1][re] = -a.rtop[1][re] / den;
+        a.bc[1][im] = -a.rtop[1][im] / den;
+        a.bc[1][a.C + re] = dtb * (-wy * psi);
+        a.bc[1][a.C + im] = dtb * (wy * psr);
+        // w
+        const double zh = a.xnu * a.dt * a.bdfv;
+        if (a.active) {
+            double tr = 0.0, ti = 0.0, wr = 0.0, wi = 0.0;
+            if (a.btop) { tr = a.ctop * a.btop[re]; ti = a.ctop * a.btop[im]; }
+            if (a.bwa) { wr = a.cwa * a.bwa[re]; wi = a.cwa * a.bwa[im]; }
+            if (a.bwb) { wr += a.cwb * a.bwb[re]; wi += a.cwb * a.bwb[im]; }
+            a.bc[2][re] = tr + zh * a.d2w[re];
+            a.bc[2][im] = ti + zh * a.d2w[im];
+            a.bc[2][a.C + re] = wr;
+            a.bc[2][a.C + im] = wi;
+            // the pressure step's w BC (bound() again, src/navierstokes.f90:1432-1433)
+            a.bcp[re] = tr;
+            a.bcp[im] = ti;
+            a.bcp[a.C + re] = wr;
+            a.bcp[a.C + im] = wi;
+        } else {
+            a.bc[2][re] = zh * a.d2w[re];
+            a.bc[2][im] = zh * a.d2w[im];
+            a.bc[2][a.C + re] = zh * a.d2w[a.C + re];
+            a.bc[2][a.C + im] = zh * a.d2w[a.C + im];
+            a.bcp[re] = 0.0;
+            a.bcp[im] = 0.0;
+            a.bcp[a.C + re] = 0.0;
+            a.bcp[a.C + im] = 0.0;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- small spectral ops
+__global__ void k_divuv(const double* __restrict__ u, const double* __restrict__ v, double* __restrict__ out,
+                        const double* __restrict__ wavx, const double* __restrict__ wavy, int nx, long long S,
+                        long long C) {
+    const long long n2 = S / 2;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n2; e += (long long)gridDim.x * blockDim.x) {
+        int i, j;
+        ij_of(e % (C / 2), nx, i, j);
+        const double wx = wavx[i], wy = wavy[j];
+        const double ur = u[2 * e], ui = u[2 * e + 1], vr = v[2 * e], vi = v[2 * e + 1];
+        out[2 * e] = -wx * ui - wy * vi;
+        out[2 * e + 1] = wx * ur + wy * vr;
+    }
+}
+
+// out = d/dx (mode 0), d/dy (mode 1) of in; lapl uses k_lapl_xy
+__global__ void k_dxy(const double* __restrict__ in, double* __restrict__ out, const double* __restrict__ wavx,
+                      const double* __restrict__ wavy, int nx, long long S, long long C, int mode) {
+    const long long n2 = S / 2;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n2; e += (long long)gridDim.x * blockDim.x) {
+        int i, j;
+        ij_of(e % (C / 2), nx, i, j);
+        const double w = (mode == 0) ? wavx[i] : wavy[j];
+        const double r = in[2 * e], im = in[2 * e + 1];
+        out[2 * e] = -w * im;
+        out[2 * e + 1] = w * r;
+    }
+}
+
+// lapl: out = d2 - (wavxx + wavyy)*u  (src/derivatives.f90:319-323)
+__global__ void k_lapl_xy(const double* __restrict__ u, double* __restrict__ d2, const double* __restrict__ wavx,
+                          const double* __restrict__ wavy, int nx, long long S, long long C) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < S; e += (long long)gridDim.x * blockDim.x) {
+        const long long c = e % C;
+        const int i = (int)(c % nx), j = (int)(c / nx);
+        const double wx = wavx[i], wy = wavy[j];
+        d2[e] = d2[e] - (wx * wx + wy * wy) * u[e];
+    }
+}
+
+// N_l = (N_l - dfdx(h_l1)) - dfdy(h_l2)   (src/navierstokes.f90:789-795, x and y parts)
+__global__ void k_nl_div_xy(NlDivArgs a) {
+    const long long n2 = a.S / 2;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < 3 * n2; e += (long long)gridDim.x * blockDim.x) {
+        const int l = (int)(e / n2);
+        const long long ce = e % n2;
+        int i, j;
+        ij_of(ce % (a.C / 2), a.nx, i, j);
+        const double wx = a.wavx[i], wy = a.wavy[j];
+        const double* hx = a.hx[l];
+        const double* hy = a.hy[l];
+        double nr = a.N[l][2 * ce], ni = a.N[l][2 * ce + 1];
+        nr = nr - (-wx * hx[2 * ce + 1]);
+        ni = ni - (wx * hx[2 * ce]);
+        nr = nr - (-wy * hy[2 * ce + 1]);
+        ni = ni - (wy * hy[2 * ce]);
+        a.N[l][2 * ce] = nr;
+        a.N[l][2 * ce + 1] = ni;
+    }
+}
+
+// u -= dt*bdfv*dfdx(p), v -= dt*bdfv*dfdy(p)   (src/navierstokes.f90:1478-1488)
+__global__ void k_pressure_update(double* __restrict__ u, double* __restrict__ v, const double* __restrict__ p,
+                                  const double* __restrict__ wavx, const double* __restrict__ wavy, int nx,
+                                  long long S, long long C, double dtb) {
+    const long long n2 = S / 2;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n2; e += (long long)gridDim.x * blockDim.x) {
+        int i, j;
+        ij_of(e % (C / 2), nx, i, j);
+        const double wx = wavx[i], wy = wavy[j];
+        const double pr = p[2 * e], pi = p[2 * e + 1];
+        u[2 * e] = u[2 * e] - dtb * (-wx * pi);
+        u[2 * e + 1] = u[2 * e + 1] - dtb * (wx * pr);
+        v[2 * e] = v[2 * e] - dtb * (-wy * pi);
+        v[2 * e + 1] = v[2 * e + 1] - dtb * (wy * pr);
+    }
+}
+
+// norm (src/horfft.f90:153-224) on 3 fields + the ifrz mean removal (src/navierstokes.f90:53-59)
+__global__ void k_norm(double* f0, double* f1, double* f2, int nx, int ny, int nzp, int ifrz) {
+    const int k = blockIdx.x;
+    double* f = (blockIdx.y == 0) ? f0 : (blockIdx.y == 1 ? f1 : f2);
+    double* pl = f + (long long)k * nx * ny;
+    const int nyh = ny / 2;
+    if (threadIdx.x == 0) {
+        pl[1] = 0.0;
+        if (ny > 2) {
+            for (int jj = 1; jj <= nyh - 1; ++jj) {
+                const int jp = ny - jj;
+                pl[jj * nx + 0] = 0.5 * (pl[jj * nx + 0] + pl[jp * nx + 0]);
+                pl[jj * nx + 1] = 0.5 * (pl[jj * nx + 1] - pl[jp * nx + 1]);
+            }
+            for (int jj = 1; jj <= nyh - 1; ++jj) {
+                const int jp = ny - jj;
+                pl[jp * nx + 0] = pl[jj * nx + 0];
+                pl[jp * nx + 1] = -pl[jj * nx + 1];
+            }
+        }
+    }
+    __syncthreads();
+    if (ny > 2) {
+        for (int i = threadIdx.x; i < nx; i += blockDim.x) pl[nyh * nx + i] = 0.0;
+    }
+    __syncthreads();
+    if (ifrz && threadIdx.x == 0) {
+        pl[0] = 0.0;
+        pl[1] = 0.0;
+    }
+}
+
+// fringe forcing on the unpadded physical grid (src/navierstokes.f90:191-204); u0 holds u + ubar
+__global__ void k_force_phys(const double* __restrict__ u0, const double* __restrict__ u1,
+                             const double* __restrict__ u2, double* __restrict__ f0, double* __restrict__ f1,
+                             double* __restrict__ f2, const double* __restrict__ lamx,
+                             const double* __restrict__ ubar, int nx, int ny, long long P) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < P; e += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(e % nx);
+        const int k = (int)(e / ((long long)nx * ny));
+        const double l = lamx[x];
+        f0[e] = l * (ubar[k] - u0[e]);
+        f1[e] = l * (0.0 - u1[e]);
+        f2[e] = l * (0.0 - u2[e]);
+    }
+}
+
+__global__ void k_axpby(double* __restrict__ y, const double* __restrict__ x, double a, double b, long long n) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+        y[e] = a * x[e] + (b != 0.0 ? b * y[e] : 0.0);
+}
+
+// ---------------------------------------------------------------- launchers
+static inline int nblk(long long n) {
+    long long b = (n + 255) / 256;
+    if (b > 148LL * 16) b = 148LL * 16;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+void launch_specfilter(const SpecFilterArgs& a, cudaStream_t s) { k_specfilter<<<nblk(3 * a.S / 2), 256, 0, s>>>(a); }
+void launch_rhs(const RhsArgs& a, cudaStream_t s) { k_rhs<<<nblk(3 * a.S), 256, 0, s>>>(a); }
+void launch_bc_planes(const BcArgs& a, cudaStream_t s) { k_bc_planes<<<nblk(a.C / 2), 256, 0, s>>>(a); }
+void launch_divuv(const double* u, const double* v, double* out, const double* wavx, const double* wavy, int nx,
+                  long long S, long long C, cudaStream_t s) {
+    k_divuv<<<nblk(S / 2), 256, 0, s>>>(u, v, out, wavx, wavy, nx, S, C);
+}
+void launch_dxy(const double* in, double* out, const double* wavx, const double* wavy, int nx, long long S,
+                long long C, int mode, cudaStream_t s) {
+    k_dxy<<<nblk(S / 2), 256, 0, s>>>(in, out, wavx, wavy, nx, S, C, mode);
+}
+void launch_lapl_xy(const double* u, double* d2, const double* wavx, const double* wavy, int nx, long long S,
+                    long long C, cudaStream_t s) {
+    k_lapl_xy<<<nblk(S), 256, 0, s>>>(u, d2, wavx, wavy, nx, S, C);
+}
+void launch_nl_div_xy(const NlDivArgs& a, cudaStream_t s) { k_nl_div_xy<<<nblk(3 * a.S / 2), 256, 0, s>>>(a); }
+void launch_pressure_update(double* u, double* v, const double* p, const double* wavx, const double* wavy, int nx,
+                            long long S, long long C, double dtb, cudaStream_t s) {
+    k_pressure_update<<<nblk(S / 2), 256, 0, s>>>(u, v, p, wavx, wavy, nx, S, C, dtb);
+}
+void launch_norm(double* f0, double* f1, double* f2, int nx, int ny, int nzp, int ifrz, cudaStream_t s) {
+    k_norm<<<dim3(nzp, 3), 128, 0, s>>>(f0, f1, f2, nx, ny, nzp, ifrz);
+}
+void launch_force_phys(const double* u0, const double* u1, const double* u2, double* f0, double* f1, double* f2,
+                       const double* lamx, const double* ubar, int nx, int ny, long long P, cudaStream_t s) {
+    k_force_phys<<<nblk(P), 256, 0, s>>>(u0, u1, u2, f0, f1, f2, lamx, ubar, nx, ny, P);
+}
+void launch_axpby(double* y, const double* x, double a, double b, long long n, cudaStream_t s) {
+    k_axpby<<<nblk(n), 256, 0, s>>>(y, x, a, b, n);
+}
+
+}  // namespace lsb

@@ -29,6 +29,35 @@ from lsbflow_b200.hostsetup import Setup
 
 PI = 4.0 * math.atan(1.0)
 
+# z-derivative algorithm for nz > 31: "dct" follows the reference (dct_diff, FFTW
+# REDFT00); "dense" applies the same operator as its dense matrix (what the device
+# contraction does).  Both are the same linear map; they differ only in rounding.
+ZDER = "dct"
+# threads used by scipy.fft (the timed CPU baseline sets this to the host's cores)
+WORKERS = 1
+
+
+def _fft(x, axis):
+    return scipy.fft.fft(x, axis=axis, workers=WORKERS)
+
+
+def _ifft(x, axis):
+    return scipy.fft.ifft(x, axis=axis, workers=WORKERS)
+
+
+def _rfft(x, axis):
+    return scipy.fft.rfft(x, axis=axis, workers=WORKERS)
+
+
+def _irfft(x, n, axis):
+    return scipy.fft.irfft(x, n=n, axis=axis, workers=WORKERS)
+
+
+def _zmat(m, f):
+    """m (nzp x nzp) applied along axis 0 of f (z, ...)."""
+    sh = f.shape
+    return (m @ f.reshape(sh[0], -1)).reshape((m.shape[0],) + sh[1:])
+
 
 # ----------------------------------------------------------------------------- FFTs
 def to_complex(af: np.ndarray) -> np.ndarray:
@@ -44,8 +73,8 @@ def to_real(cf: np.ndarray) -> np.ndarray:
 
 def horfft_fwd(a: np.ndarray, nx: int, ny: int) -> np.ndarray:
     """horfft(is=-1) (src/horfft.f90:94-119): x r2c, drop the kx Nyquist, y c2c, /(nx ny)."""
-    xh = np.fft.rfft(a[..., :nx], axis=-1)[..., : nx // 2]
-    c = np.fft.fft(xh, axis=-2) * (1.0 / float(nx * ny))
+    xh = _rfft(a[..., :nx], axis=-1)[..., : nx // 2]
+    c = _fft(xh, axis=-2) * (1.0 / float(nx * ny))
     return to_real(c)
 
 
@@ -55,12 +84,12 @@ def c2r(X: np.ndarray, n: int) -> np.ndarray:
     X[..., 0] = X[..., 0].real
     if X.shape[-1] > n // 2:
         X[..., n // 2] = X[..., n // 2].real
-    return np.fft.irfft(X, n=n, axis=-1) * n
+    return _irfft(X, n=n, axis=-1) * n
 
 
 def horfft_inv(af: np.ndarray, nx: int, ny: int) -> np.ndarray:
     """horfft(is=+1) (src/horfft.f90:121-144): y c2c backward, x c2r; pad columns 0."""
-    c = np.fft.ifft(to_complex(af), axis=-2) * ny
+    c = _ifft(to_complex(af), axis=-2) * ny
     full = np.zeros(c.shape[:-1] + (nx // 2 + 1,), dtype=np.complex128)
     full[..., : nx // 2] = c
     out = np.zeros(af.shape[:-1] + (nx + 2,))
@@ -124,13 +153,13 @@ def _dct_diff_z(st: Setup, y, p):
     shape = (n,) + (1,) * (y.ndim - 1)
     gf = g.gf.reshape(shape)
     for _ in range(p):
-        alpha = scipy.fft.dct(beta, type=1, axis=0)
+        alpha = scipy.fft.dct(beta, type=1, axis=0, workers=WORKERS)
         alpha[1:n - 1] = alpha[1:n - 1] / half
         beta = np.zeros_like(alpha)
         beta[n - 2] = 2.0 * (n - 1.0) * alpha[n - 1]
         for k in range(n - 1, 1, -1):
             beta[k - 2] = beta[k] + 2.0 * (k - 1.0) * alpha[k - 1]
-        alpha = scipy.fft.dct(beta, type=1, axis=0)
+        alpha = scipy.fft.dct(beta, type=1, axis=0, workers=WORKERS)
         beta = alpha * gf / nlog
     return beta
 
@@ -138,15 +167,15 @@ def _dct_diff_z(st: Setup, y, p):
 def dfdz(st: Setup, uf):
     """dfdz (src/derivatives.f90:112-132): DCT path for nz > 31, else matmul(d, .)."""
     if st.cfg.nz > 31:
-        return _dct_diff_z(st, uf, 1)
-    return np.einsum("km,mji->kji", st.d, uf)
+        return _dct_diff_z(st, uf, 1) if ZDER == "dct" else _zmat(st.dz1, uf)
+    return _zmat(st.d, uf)
 
 
 def d2fdz2(st: Setup, uf):
     """d2fdz2 (src/derivatives.f90:161-188)."""
     if st.cfg.nz > 31:
-        return _dct_diff_z(st, uf, 2)
-    return np.einsum("km,mji->kji", st.d2, uf)
+        return _dct_diff_z(st, uf, 2) if ZDER == "dct" else _zmat(st.dz2, uf)
+    return _zmat(st.d2, uf)
 
 
 def wav2(st: Setup):
@@ -161,9 +190,9 @@ def solve_helmholtz(st: Setup, rhs, dtnui):
     nz = st.cfg.nz
     q = rhs[1:nz]                                       # (nzm, ny, nx)
     dfac = -wav2(st) - dtnui                             # (ny, nx)
-    trhs = np.einsum("km,mji->kji", st.Ei, q)
+    trhs = _zmat(st.Ei, q)
     trhs = trhs / (st.lam[:, None, None] + dfac[None])
-    q = np.einsum("km,mji->kji", st.E, trhs)
+    q = _zmat(st.E, trhs)
     rhs[1:nz] = q
     rhs[0] = 0.0
     rhs[nz] = 0.0
@@ -207,12 +236,12 @@ def dealias_product(st: Setup, a, b, layout: str):
             h = ny // 2
             out[..., :h, : nx // 2] = cf[..., :h, :]
             out[..., nyl - h:, : nx // 2] = cf[..., h:, :]
-        out = np.fft.ifft(out, axis=-2) * nyl
+        out = _ifft(out, axis=-2) * nyl
         return c2r(out, nxl)
 
     prod = pad(af) * pad(bf)
-    xh = np.fft.rfft(prod, axis=-1)
-    c = np.fft.fft(xh, axis=-2) * (1.0 / (float(nxl) * float(nyl)))
+    xh = _rfft(prod, axis=-1)
+    c = _fft(xh, axis=-2) * (1.0 / (float(nxl) * float(nyl)))
     if layout == "ref":
         t = c[..., :ny, : nx // 2]
     else:

@@ -1,0 +1,230 @@
+"""Parity of the CUDA library (through the C ABI) with the FP64 oracle.
+
+Tolerances (relative L2 over the whole field): single operators 1e-12 (transforms
+and contractions in FP64 differ from numpy/scipy only by rounding order); whole time
+steps 1e-10 after the stated number of steps.
+"""
+import numpy as np
+import pytest
+
+from lsbflow_b200 import hostsetup as hs
+from lsbflow_b200 import ic
+from lsbflow_b200.config import workload
+from oracle import lsb_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL_OP = 1e-12
+TOL_STEP = 1e-10
+
+
+def rel(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)
+
+
+def solver(cfg):
+    from lsbflow_b200 import lib
+    st = hs.make_setup(cfg)
+    return st, lib.Solver(st)
+
+
+GRIDS = [(16, 8, 16), (24, 6, 12), (64, 16, 32), (40, 10, 8), (224, 24, 32)]
+
+
+def rand_spec(st, seed):
+    rng = np.random.default_rng(seed)
+    c = st.cfg
+    f = rng.standard_normal((c.nzp, c.ny, c.nx))
+    O.norm([f], c.ny)
+    return f
+
+
+def rand_phys(st, seed):
+    rng = np.random.default_rng(seed)
+    c = st.cfg
+    a = np.zeros((c.nzp, c.ny, c.nx + 2))
+    a[..., : c.nx] = rng.standard_normal((c.nzp, c.ny, c.nx))
+    return a
+
+
+@pytest.mark.parametrize("nx,ny,nz", GRIDS)
+def test_horfft(nx, ny, nz):
+    st, s = solver(workload("dns64", nx=nx, ny=ny, nz=nz, dealiasflag=0))
+    a = rand_phys(st, 1)
+    f = s.horfft(a, None, -1)
+    assert rel(f, O.horfft_fwd(a, nx, ny)) < TOL_OP
+    g = rng_f = np.random.default_rng(2).standard_normal((nz + 1, ny, nx))
+    p = s.horfft(None, g, 1)
+    ref = O.horfft_inv(g, nx, ny)
+    assert rel(p, ref) < TOL_OP
+    assert np.all(p[..., nx:] == 0.0)
+
+
+@pytest.mark.parametrize("nx,ny,nz", GRIDS)
+def test_derivatives(nx, ny, nz):
+    st, s = solver(workload("dns64", nx=nx, ny=ny, nz=nz, dealiasflag=0))
+    u = rand_spec(st, 3)
+    v = rand_spec(st, 4)
+    assert rel(s.dfdx(u), O.dfdx(st, u)) < TOL_OP
+    assert rel(s.dfdy(u), O.dfdy(st, u)) < TOL_OP
+    assert rel(s.dfdz(u), O.dfdz(st, u)) < TOL_OP
+    assert rel(s.d2fdz2(u), O.d2fdz2(st, u)) < TOL_OP
+    assert rel(s.divuv(u, v), O.divuv(st, u, v)) < TOL_OP
+    lap = O.d2fdz2(st, u) - O.wav2(st)[None] * u
+    assert rel(s.lapl(u), lap) < TOL_OP
+
+
+@pytest.mark.parametrize("nx,ny,nz", GRIDS)
+def test_helmholtz(nx, ny, nz):
+    st, s = solver(workload("dns64", nx=nx, ny=ny, nz=nz, dealiasflag=0))
+    r = rand_spec(st, 5)
+    bc = rand_spec(st, 6)
+    for dtnui in (0.0, 1.0 / (st.cfg.xnu * st.dt) / (6.0 / 11.0)):
+        ref = O.solve_helmholtz(st, r.copy(), dtnui)
+        assert rel(s.solve_helmholtz(r, dtnui), ref) < TOL_OP
+        ref = O.solve_nhom_helmholtz(st, r.copy(), bc, dtnui)
+        assert rel(s.solve_nhom_helmholtz(r, bc, dtnui), ref) < TOL_OP
+
+
+@pytest.mark.parametrize("layout", ["ref", "correct"])
+@pytest.mark.parametrize("nx,ny,nz", [(16, 8, 8), (64, 16, 16), (40, 10, 8)])
+def test_dealias_product(layout, nx, ny, nz):
+    st, s = solver(workload("dns64", nx=nx, ny=ny, nz=nz, dealiasflag=1, dealias_layout=layout))
+    a = rand_phys(st, 7)
+    b = rand_phys(st, 8)
+    ref = O.dealias_product(st, a, b, layout)
+    assert rel(s.dealias_product(a, b), ref) < TOL_OP
+
+
+NL_CASES = [
+    dict(dealiasflag=0, forcing=0), dict(dealiasflag=0, forcing=1), dict(dealiasflag=2, forcing=1),
+    dict(dealiasflag=1, dealias_layout="ref", forcing=1), dict(dealiasflag=1, dealias_layout="correct", forcing=1),
+]
+
+
+@pytest.mark.parametrize("over", NL_CASES)
+def test_nlterm(over):
+    st, s = solver(workload("dns64", nx=32, ny=8, nz=16, **over))
+    u, v, w = ic.seeded_noise(st, 11, 1e-2)
+    ref = O.nlterm_skewsym(st, [u, v, w])
+    got = s.nlterm(np.array([u, v, w]))
+    for l in range(3):
+        assert rel(got[l], ref[l]) < TOL_OP, l
+
+
+def run_both(cfg, nsteps, seed=3, amp=1e-3, zder="dct"):
+    st, s = solver(cfg)
+    u, v, w = ic.seeded_noise(st, seed, amp)
+    ost = O.State.zeros_like(st, u, v, w, st.dt)
+    s.upload(u, v, w, dt=st.dt)
+    old = O.ZDER
+    O.ZDER = zder
+    try:
+        for _ in range(nsteps):
+            O.timestep(st, ost)
+    finally:
+        O.ZDER = old
+    s.step(nsteps)
+    got = s.download()
+    return st, ost, got
+
+
+STEP_CASES = [
+    ("dns-nodealias", dict(dealiasflag=0)),
+    ("dns-specfilter", dict(dealiasflag=2)),
+    ("dns-ref32", dict(dealiasflag=1, dealias_layout="ref")),
+    ("dns-correct32", dict(dealiasflag=1, dealias_layout="correct")),
+    ("bctype0-hom", dict(dealiasflag=0, bctype=0, forcing=0)),
+    ("bctype1", dict(dealiasflag=2, bctype=1, samp=0.3)),
+    ("bctype2", dict(dealiasflag=2, bctype=2)),
+]
+
+
+# The pressure phi = -(Dw + div)/(k^2 dt bdfv) is a near-cancellation: replacing the
+# oracle's own DCT-I z derivative (the reference's dct_diff) by the identical dense
+# matrix moves p by 1.6e-10 relative after 20 steps at this grid while u moves by
+# 2e-12.  Against the DCT oracle p is therefore held to TOL_P_DCT; against the
+# dense-matrix oracle (same linear map as the device) every field is held to 1e-10.
+TOL_P_DCT = 5e-10
+
+
+@pytest.mark.parametrize("name,over", STEP_CASES, ids=[c[0] for c in STEP_CASES])
+def test_steps_match_oracle(name, over):
+    cfg = workload("dns64", nx=32, ny=8, nz=32, **over)
+    st, ost, got = run_both(cfg, 20)
+    for key, ref in (("uf", ost.uf), ("vf", ost.vf), ("wf", ost.wf)):
+        assert rel(got[key], ref) < TOL_STEP, (key, rel(got[key], ref))
+    assert rel(got["pf"], ost.pf) < TOL_P_DCT, rel(got["pf"], ost.pf)
+    assert got["istep"] == 20 and abs(got["t"] - ost.t) < 1e-12
+
+
+@pytest.mark.parametrize("name,over", STEP_CASES[:4], ids=[c[0] for c in STEP_CASES[:4]])
+def test_steps_match_dense_oracle(name, over):
+    cfg = workload("dns64", nx=32, ny=8, nz=32, **over)
+    st, ost, got = run_both(cfg, 20, zder="dense")
+    for key, ref in (("uf", ost.uf), ("vf", ost.vf), ("wf", ost.wf), ("pf", ost.pf)):
+        assert rel(got[key], ref) < TOL_STEP, (key, rel(got[key], ref))
+
+
+# The sigma model's singular values come from a trigonometric solution of the
+# characteristic cubic (src/sgsterm.f90:334-364); a 1e-16 relative perturbation of
+# the velocity gradient moves its tau by 8e-8 relative on this field, so the sigma
+# model is held to a tolerance 25x that conditioning.
+TOL_SIGMA_TAU = 2e-6
+TOL_SIGMA_STEP = 2e-6
+
+
+@pytest.mark.parametrize("model", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("dealias", [0, 1])
+def test_sgs_steps_match_oracle(model, dealias):
+    cfg = workload("dns64", nx=32, ny=8, nz=32, sgsflag=1, sgsmodel=model, dealiasflag=dealias,
+                   dealias_layout="correct")
+    st, ost, got = run_both(cfg, 5, amp=2e-2, zder="dense")
+    tol = TOL_SIGMA_STEP if model == 2 else TOL_STEP
+    for key, ref in (("uf", ost.uf), ("vf", ost.vf), ("wf", ost.wf), ("pf", ost.pf)):
+        assert rel(got[key], ref) < tol, (key, rel(got[key], ref))
+
+
+@pytest.mark.parametrize("model", [0, 1, 2, 3])
+def test_tau_sgs(model):
+    cfg = workload("dns64", nx=32, ny=8, nz=32, sgsflag=1, sgsmodel=model, dealiasflag=0)
+    st, s = solver(cfg)
+    u, v, w = ic.seeded_noise(st, 5, 5e-2)
+    _, parts = O.nlterm_skewsym(st, [u, v, w], return_parts=True)
+    ui, g, uu = parts["ui"], parts["duidxj"], parts["uiuj"]
+    ref = O.tau_sgs(st, ui, uu, g)
+    # Fortran storage (..., l, m): numpy index [m][l]
+    gF = np.array([[g[l][m] for l in range(3)] for m in range(3)])
+    uuF = np.array([[uu[l][m] for l in range(3)] for m in range(3)])
+    tau = s.tau_sgs(np.array(ui), uuF, gF)
+    nx = cfg.nx
+    if model == 2:
+        # small off-diagonal components of the sigma model respond at 6e-6 to a 1e-16
+        # input perturbation, so the check is on the whole tensor
+        r = np.array([[ref[l][m][..., :nx] for m in range(3)] for l in range(3)])
+        t = np.array([[tau[m][l][..., :nx] for m in range(3)] for l in range(3)])
+        assert rel(t, r) < TOL_SIGMA_TAU, rel(t, r)
+        return
+    for l in range(3):
+        for m in range(3):
+            r = ref[l][m][..., :nx]
+            t = tau[m][l][..., :nx]
+            assert rel(t, r) < 1e-11 or np.abs(t - r).max() < 1e-14, (l, m, rel(t, r))
+
+
+def test_diag_divergence_and_energy():
+    cfg = workload("dns64", nx=32, ny=8, nz=32, dealiasflag=1)
+    st, ost, got = run_both(cfg, 5)
+    from lsbflow_b200 import lib
+    s = lib.Solver(st)
+    s.upload(got["uf"], got["vf"], got["wf"], dt=st.dt)
+    d = s.diag()
+    div = O.divcheck(st, ost.uf, ost.vf, ost.wf)
+    assert abs(d["divergence"] - div) <= 1e-9 * max(div, 1e-30) + 1e-18
+    e1, e2 = O.lintest(st, ost)
+    assert abs(d["energy_total"] - e1) <= 1e-11 * abs(e1)
+    assert abs(d["energy_pert"] - e2) <= 1e-9 * abs(e2) + 1e-30
+    assert d["nonfinite"] == 0
