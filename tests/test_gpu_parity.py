@@ -171,9 +171,8 @@ def test_steps_match_dense_oracle(name, over):
 
 # The sigma model's singular values come from a trigonometric solution of the
 # characteristic cubic (src/sgsterm.f90:334-364); a 1e-16 relative perturbation of
-# the velocity gradient moves its tau by 8e-8 relative on this field, so the sigma
-# model is held to a tolerance 25x that conditioning.
-TOL_SIGMA_TAU = 2e-6
+# the velocity gradient moves its tau by 1e-7 (diagonal) to 1e-5 (small off-diagonal
+# components) relative on these fields, so whole sigma-model steps are held to 2e-6.
 TOL_SIGMA_STEP = 2e-6
 
 
@@ -202,11 +201,16 @@ def test_tau_sgs(model):
     tau = s.tau_sgs(np.array(ui), uuF, gF)
     nx = cfg.nx
     if model == 2:
-        # small off-diagonal components of the sigma model respond at 6e-6 to a 1e-16
-        # input perturbation, so the check is on the whole tensor
+        # The sigma model is ill-conditioned: its small off-diagonal components respond
+        # at ~6e-6 to a 1e-16 relative perturbation of the gradient.  The tolerance is
+        # calibrated on the oracle itself: 10x its response to a 1e-15 perturbation.
         r = np.array([[ref[l][m][..., :nx] for m in range(3)] for l in range(3)])
         t = np.array([[tau[m][l][..., :nx] for m in range(3)] for l in range(3)])
-        assert rel(t, r) < TOL_SIGMA_TAU, rel(t, r)
+        rng = np.random.default_rng(1)
+        gp = [[x * (1.0 + 1e-15 * rng.standard_normal(x.shape)) for x in row] for row in g]
+        tp = O.sigma_model(st, gp)
+        cond = rel(np.array([[tp[l][m][..., :nx] for m in range(3)] for l in range(3)]), r)
+        assert rel(t, r) < max(10.0 * cond, 1e-10), (rel(t, r), cond)
         return
     for l in range(3):
         for m in range(3):
