@@ -140,6 +140,24 @@ int lsb_nlterm(lsb_handle* h, const double* uif, double* nltermif);
 /* tau_sgs(ui, uiuj, duidxj, tauij)  src/sgsterm.f90:10  (physical (nx+2,ny,nzp,3[,3]) arrays) */
 int lsb_tau_sgs(lsb_handle* h, const double* ui, const double* uiuj, const double* duidxj, double* tauij);
 
+/* ---------------- Allocation-free Helmholtz solve ------------------------------------ */
+/* No counterpart in the reference.  solve_helmholtz (homogeneous Dirichlet BCs) for
+ * callers that may not allocate GPU memory: programs whose device memory belongs to a
+ * pool allocator or framework that forbids direct cudaMalloc, or time-stepping loops
+ * that cannot pay for cudaMalloc/cudaFree's device-wide synchronisation.  No handle is
+ * needed and nothing is allocated: every pointer is a device address the caller owns
+ * (rhs, out: spectral (nx, ny, nzp); lam: nzm; e, ei: nzm x nzm row-major; wavx: nx;
+ * wavy: ny), and the work memory is a static device array of LSB_NOALLOC_SCRATCH_BYTES
+ * that every GPU loading the library keeps until exit.  Limit: nzp <= 129 (any nx*ny;
+ * columns are processed in chunks that fit the array); larger nz returns
+ * LSB_ERR_UNSUPPORTED.  The first call on a device looks up the array's address, so make
+ * it before any stream capture.  Calls share the array: calls that overlap on the GPU
+ * race and must be serialised by the caller.  stream is a cudaStream_t (NULL = default). */
+#define LSB_NOALLOC_SCRATCH_BYTES (8u << 20)
+int lsb_solve_helmholtz_noalloc(int nx, int ny, int nz, const double* rhs, double* out, const double* lam,
+                                const double* e, const double* ei, const double* wavx, const double* wavy,
+                                double dtnui, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

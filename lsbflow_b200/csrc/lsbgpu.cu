@@ -605,6 +605,10 @@ void check_launch() {
 
 }  // namespace
 
+namespace lsb {
+void set_last_error(const std::string& m) { g_err = m; }
+}  // namespace lsb
+
 // ====================================================================================== C ABI
 extern "C" {
 

@@ -27,6 +27,7 @@ EXPORTS = [
     "lsb_synchronize", "lsb_horfft", "lsb_dealias_product", "lsb_dfdx", "lsb_dfdy", "lsb_dfdz", "lsb_d2fdz2",
     "lsb_lapl", "lsb_divuv", "lsb_solve_helmholtz", "lsb_solve_nhom_helmholtz", "lsb_nlterm", "lsb_tau_sgs",
     "lsb_upload_velocity", "lsb_download_velocity", "lsb_timers", "lsb_timer_report",
+    "lsb_solve_helmholtz_noalloc",
 ]
 
 
@@ -106,6 +107,16 @@ def config_struct(cfg: LsbConfig) -> LsbConfigC:
         cfg.kc, cfg.filt_order, cfg.filt_amp, cfg.istartbound, cfg.samp,
         cfg.bc3_amp, cfg.bc3_xc, cfg.bc3_s, cfg.fsize,
     )
+
+
+def solve_helmholtz_noalloc(nx, ny, nz, rhs_ptr, out_ptr, lam_ptr, e_ptr, ei_ptr, wavx_ptr, wavy_ptr, dtnui,
+                            stream_ptr=0):
+    """Allocation-free Helmholtz solve on device pointers (raw addresses)."""
+    lib = load()
+    _ck(lib.lsb_solve_helmholtz_noalloc(C.c_int(nx), C.c_int(ny), C.c_int(nz), C.c_void_p(rhs_ptr),
+                                        C.c_void_p(out_ptr), C.c_void_p(lam_ptr), C.c_void_p(e_ptr),
+                                        C.c_void_p(ei_ptr), C.c_void_p(wavx_ptr), C.c_void_p(wavy_ptr),
+                                        C.c_double(dtnui), C.c_void_p(stream_ptr)))
 
 
 class Solver:
