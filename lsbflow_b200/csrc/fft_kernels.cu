@@ -11,8 +11,8 @@
 //             kx = 0 Hermitian symmetrisation of the reference's horfft(+1)/horfft(-1)
 //             round trip, accumulated into the output as alpha*T + beta*out.
 //
-// The complex FFT of a line is a mixed-radix (2,3,4,5,7,8) Stockham autosort transform in
-// shared memory owned by one warp.  FFTW's c2r semantics are kept: the imaginary parts of
+// The complex FFTs are mixed-radix (2,3,4,5,7) Stockham autosort transforms in shared
+// memory; every stage runs over all lines a block holds, with all its threads.  FFTW's c2r semantics are kept: the imaginary parts of
 // the DC and Nyquist inputs are ignored and the kx Nyquist mode is dropped / zero.
 #include "lsb_internal.cuh"
 
@@ -63,16 +63,28 @@ __device__ __forceinline__ void dft_small(double2 (&u)[R], const double2* __rest
     }
 }
 
+__device__ __forceinline__ uint32_t fdiv(uint32_t n, const FastDiv& f) {
+    return f.d == 1 ? n : ((__umulhi(n, f.m) + n) >> f.s);
+}
+
+// One radix-R Stockham stage over nlines lines (line stride ls) done by the whole block.
 template <int R, int SIGN>
-__device__ __forceinline__ void fft_stage(const double2* __restrict__ src, double2* __restrict__ dst, int n, int p,
-                                          const double2* __restrict__ tw, int lane) {
+__device__ __forceinline__ void bstage(const double2* __restrict__ src, double2* __restrict__ dst, int nlines, int ls,
+                                       int n, int p, const FastDiv& fdT, const FastDiv& fdP,
+                                       const double2* __restrict__ tw, int tid, int nthr) {
     const int T = n / R;
     const int stride = n / (p * R);
-    for (int i = lane; i < T; i += 32) {
-        const int k = i % p;
+    const int total = nlines * T;
+    for (int idx = tid; idx < total; idx += nthr) {
+        const int line = (int)fdiv((uint32_t)idx, fdT);
+        const int i = idx - line * T;
+        const int mq = (int)fdiv((uint32_t)i, fdP);
+        const int k = i - mq * p;
+        const double2* sl = src + line * ls;
+        double2* dl = dst + line * ls;
         double2 u[R];
 #pragma unroll
-        for (int q = 0; q < R; ++q) u[q] = src[i + q * T];
+        for (int q = 0; q < R; ++q) u[q] = sl[i + q * T];
         if (k != 0) {
 #pragma unroll
             for (int q = 1; q < R; ++q) {
@@ -82,36 +94,40 @@ __device__ __forceinline__ void fft_stage(const double2* __restrict__ src, doubl
             }
         }
         dft_small<R, SIGN>(u, tw, n);
-        const int j = (i - k) * R + k;
+        const int j = mq * p * R + k;
 #pragma unroll
-        for (int q = 0; q < R; ++q) dst[j + q * p] = u[q];
+        for (int q = 0; q < R; ++q) dl[j + q * p] = u[q];
     }
 }
 
-// Complex FFT of one line a[0..n) by one warp; b is scratch of the same size.
-// Returns the buffer holding the result (a if the stage count is even, else b).
-template <int SIGN>
-__device__ double2* fft_line(double2* a, double2* b, const FftPlan& P, int lane) {
-    double2* src = a;
-    double2* dst = b;
-    int p = 1;
+// Complex FFT of nlines lines held in A (stride ls) by the whole block; B is scratch of
+// the same shape.  Returns true when the result is in A (even number of stages).
+// WIDE kernels also carry the radix-5 and radix-7 stages (lengths with factors 5 or 7);
+// the others only 2, 3, 4, which keeps their register footprint small.
+template <int SIGN, bool WIDE>
+__device__ bool fft_batch(double2* A, double2* B, int nlines, int ls, const FftPlan& P, int tid, int nthr) {
+    double2* src = A;
+    double2* dst = B;
     for (int s = 0; s < P.nst; ++s) {
-        const int R = P.radix[s];
-        switch (R) {
-            case 2: fft_stage<2, SIGN>(src, dst, P.n, p, P.tw, lane); break;
-            case 3: fft_stage<3, SIGN>(src, dst, P.n, p, P.tw, lane); break;
-            case 4: fft_stage<4, SIGN>(src, dst, P.n, p, P.tw, lane); break;
-            case 5: fft_stage<5, SIGN>(src, dst, P.n, p, P.tw, lane); break;
-            case 7: fft_stage<7, SIGN>(src, dst, P.n, p, P.tw, lane); break;
-            default: fft_stage<8, SIGN>(src, dst, P.n, p, P.tw, lane); break;
+        switch (P.radix[s]) {
+            case 2: bstage<2, SIGN>(src, dst, nlines, ls, P.n, P.p[s], P.fdT[s], P.fdP[s], P.tw, tid, nthr); break;
+            case 3: bstage<3, SIGN>(src, dst, nlines, ls, P.n, P.p[s], P.fdT[s], P.fdP[s], P.tw, tid, nthr); break;
+            case 4: bstage<4, SIGN>(src, dst, nlines, ls, P.n, P.p[s], P.fdT[s], P.fdP[s], P.tw, tid, nthr); break;
+            default:
+                if constexpr (WIDE) {
+                    if (P.radix[s] == 5)
+                        bstage<5, SIGN>(src, dst, nlines, ls, P.n, P.p[s], P.fdT[s], P.fdP[s], P.tw, tid, nthr);
+                    else
+                        bstage<7, SIGN>(src, dst, nlines, ls, P.n, P.p[s], P.fdT[s], P.fdP[s], P.tw, tid, nthr);
+                }
+                break;
         }
-        __syncwarp();
+        __syncthreads();
         double2* t = src;
         src = dst;
         dst = t;
-        p *= R;
     }
-    return src;
+    return src == A;
 }
 
 __device__ __forceinline__ int pad_row(int j, int ny, int nyl, int layout) {
@@ -122,16 +138,18 @@ __device__ __forceinline__ int pad_row(int j, int ny, int nyl, int layout) {
 constexpr int KC = 16;  // kx columns per spanwise block
 
 // ----------------------------------------------------------------------------- k_yinv
-__global__ void __launch_bounds__(256) k_yinv(YInvJobList jobs, YPassArgs a) {
+template <bool WIDE>
+__global__ void __launch_bounds__(256, WIDE ? 2 : 3) k_yinv(YInvJobList jobs, YPassArgs a) {
     extern __shared__ double2 smem[];
     const YInvJob job = jobs.j[blockIdx.z];
     const int z = blockIdx.y;
     const int c0 = blockIdx.x * KC;
     const int nyl = a.nyl, ny = a.ny;
+    const int LS = nyl + 1;  // odd line stride: conflict-free column writes
     double2* A = smem;
-    double2* B = smem + KC * nyl;
+    double2* B = smem + KC * LS;
     const int tid = threadIdx.x;
-    for (int i = tid; i < KC * nyl; i += blockDim.x) A[i] = make_double2(0.0, 0.0);
+    for (int i = tid; i < KC * LS; i += blockDim.x) A[i] = make_double2(0.0, 0.0);
     __syncthreads();
     for (int idx = tid; idx < ny * KC; idx += blockDim.x) {
         const int j = idx / KC, cc = idx % KC, c = c0 + cc;
@@ -145,50 +163,46 @@ __global__ void __launch_bounds__(256) k_yinv(YInvJobList jobs, YPassArgs a) {
             const double k = a.wavx[2 * c];
             r = make_double2(-k * v.y, k * v.x);
         }
-        A[cc * nyl + pad_row(j, ny, nyl, a.layout)] = r;
+        A[cc * LS + pad_row(j, ny, nyl, a.layout)] = r;
     }
     __syncthreads();
-    const int warp = tid >> 5, lane = tid & 31;
-    for (int cc = warp; cc < KC; cc += blockDim.x >> 5) fft_line<+1>(A + cc * nyl, B + cc * nyl, a.plan, lane);
-    const bool inA = (a.plan.nst % 2) == 0;
-    __syncthreads();
+    const bool inA = fft_batch<+1, WIDE>(A, B, KC, LS, a.plan, tid, blockDim.x);
     const double2* R = inA ? A : B;
     for (int idx = tid; idx < nyl * KC; idx += blockDim.x) {
         const int jl = idx / KC, cc = idx % KC, c = c0 + cc;
         if (c >= a.kxc) continue;
-        *reinterpret_cast<double2*>(job.out + ((long long)z * nyl + jl) * a.nx + 2 * c) = R[cc * nyl + jl];
+        *reinterpret_cast<double2*>(job.out + ((long long)z * nyl + jl) * a.nx + 2 * c) = R[cc * LS + jl];
     }
 }
 
 // ----------------------------------------------------------------------------- k_yfwd
-__global__ void __launch_bounds__(256) k_yfwd(YFwdJobList jobs, YPassArgs a) {
+template <bool WIDE>
+__global__ void __launch_bounds__(256, WIDE ? 2 : 3) k_yfwd(YFwdJobList jobs, YPassArgs a) {
     extern __shared__ double2 smem[];
     const YFwdJob job = jobs.j[blockIdx.z];
     const int z = blockIdx.y;
     const int c0 = blockIdx.x * KC;
     const int nyl = a.nyl, ny = a.ny;
+    const int LS = nyl + 1;
     double2* A = smem;
-    double2* B = smem + KC * nyl;
+    double2* B = smem + KC * LS;
     const int tid = threadIdx.x;
     for (int idx = tid; idx < nyl * KC; idx += blockDim.x) {
         const int jl = idx / KC, cc = idx % KC, c = c0 + cc;
         double2 v = make_double2(0.0, 0.0);
         if (c < a.kxc) v = *reinterpret_cast<const double2*>(job.in + ((long long)z * nyl + jl) * a.nx + 2 * c);
-        A[cc * nyl + jl] = v;
+        A[cc * LS + jl] = v;
     }
     __syncthreads();
-    const int warp = tid >> 5, lane = tid & 31;
-    for (int cc = warp; cc < KC; cc += blockDim.x >> 5) fft_line<-1>(A + cc * nyl, B + cc * nyl, a.plan, lane);
-    const bool inA = (a.plan.nst % 2) == 0;
-    __syncthreads();
+    const bool inA = fft_batch<-1, WIDE>(A, B, KC, LS, a.plan, tid, blockDim.x);
     const double2* R = inA ? A : B;
     for (int idx = tid; idx < ny * KC; idx += blockDim.x) {
         const int j = idx / KC, cc = idx % KC, c = c0 + cc;
         if (c >= a.kxc) continue;
-        double2 v = R[cc * nyl + pad_row(j, ny, nyl, a.layout)];
+        double2 v = R[cc * LS + pad_row(j, ny, nyl, a.layout)];
         if (job.sym && c == 0) {
             const int jm = (ny - j) % ny;
-            const double2 w = R[cc * nyl + pad_row(jm, ny, nyl, a.layout)];
+            const double2 w = R[cc * LS + pad_row(jm, ny, nyl, a.layout)];
             v = make_double2(0.5 * (v.x + w.x), 0.5 * (v.y - w.y));
         }
         v.x *= a.scale;
@@ -205,7 +219,18 @@ __global__ void __launch_bounds__(256) k_yfwd(YFwdJobList jobs, YPassArgs a) {
     }
 }
 
-static size_t ypass_smem(const YPassArgs& a) { return (size_t)2 * KC * a.nyl * sizeof(double2); }
+static size_t ypass_smem(const YPassArgs& a) { return (size_t)2 * KC * (a.nyl + 1) * sizeof(double2); }
+
+static bool wide(const FftPlan& P) {
+    for (int i = 0; i < P.nst; ++i)
+        if (P.radix[i] > 4) return true;
+    return false;
+}
+
+template <class K>
+static void smem_attr(K kern) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+}
 
 void launch_yinv(const YInvJobList& jobs, const YPassArgs& a, cudaStream_t s) {
     if (jobs.n <= 0) return;
@@ -213,10 +238,12 @@ void launch_yinv(const YInvJobList& jobs, const YPassArgs& a, cudaStream_t s) {
     size_t sm = ypass_smem(a);
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_yinv, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        smem_attr(k_yinv<true>);
+        smem_attr(k_yinv<false>);
         attr = true;
     }
-    k_yinv<<<grid, 256, sm, s>>>(jobs, a);
+    if (wide(a.plan)) k_yinv<true><<<grid, 256, sm, s>>>(jobs, a);
+    else k_yinv<false><<<grid, 256, sm, s>>>(jobs, a);
 }
 
 void launch_yfwd(const YFwdJobList& jobs, const YPassArgs& a, cudaStream_t s) {
@@ -225,166 +252,195 @@ void launch_yfwd(const YFwdJobList& jobs, const YPassArgs& a, cudaStream_t s) {
     size_t sm = ypass_smem(a);
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_yfwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        smem_attr(k_yfwd<true>);
+        smem_attr(k_yfwd<false>);
         attr = true;
     }
-    k_yfwd<<<grid, 256, sm, s>>>(jobs, a);
+    if (wide(a.plan)) k_yfwd<true><<<grid, 256, sm, s>>>(jobs, a);
+    else k_yfwd<false><<<grid, 256, sm, s>>>(jobs, a);
 }
 
 // ----------------------------------------------------------------------------- rows
-// c2r of one y-intermediate row into Z (N = nxl/2 double2 = the nxl physical reals).
-// X is scratch of N+1 entries (it doubles as the FFT ping-pong buffer).
-__device__ void row_c2r_warp(const double* __restrict__ yrow, int mode, const double* __restrict__ wavx, int kxc,
-                             double meanv, const RealPlan& rp, double2* X, double2* Z, int lane) {
+// Batched c2r of L lines.  On entry X[l][0..N] holds the kx modes (zero beyond kxc, DC
+// imaginary part already dropped); Z is scratch.  Returns the buffer holding the N double2
+// (= 2N physical reals) of each line (stride N+1).
+template <bool WIDE>
+__device__ double2* rows_c2r(double2* X, double2* Z, int L, const RealPlan& rp, int tid, int nthr) {
+    const int N = rp.nr / 2, LS = N + 1;
+    for (int idx = tid; idx < L * N; idx += nthr) {
+        const int l = idx / N, k = idx - l * N;
+        const double2* xl = X + l * LS;
+        const double2 xa = xl[k];
+        const double2 xb = cconj(xl[N - k]);
+        const double2 e = cadd(xa, xb);
+        const double2 o = cmul(csub(xa, xb), cconj(__ldg(&rp.twr[k])));
+        Z[l * LS + k] = make_double2(e.x - o.y, e.y + o.x);
+    }
+    __syncthreads();
+    const bool inZ = fft_batch<+1, WIDE>(Z, X, L, LS, rp.half, tid, nthr);
+    return inZ ? Z : X;
+}
+
+// Batched r2c of L physical lines held in Z (N double2 each, stride N+1; destroyed); X is
+// scratch.  Returns the buffer holding the half-length spectra; the kx mode k < kxc of
+// line l is then made by r2c_mode().
+template <bool WIDE>
+__device__ double2* rows_r2c(double2* Z, double2* X, int L, const RealPlan& rp, int tid, int nthr) {
     const int N = rp.nr / 2;
-    for (int k = lane; k <= N; k += 32) {
+    const bool inZ = fft_batch<-1, WIDE>(Z, X, L, N + 1, rp.half, tid, nthr);
+    return inZ ? Z : X;
+}
+
+__device__ __forceinline__ double2 r2c_mode(const double2* Rl, int k, int N, const double2* __restrict__ twr) {
+    const double2 za = Rl[k];
+    const double2 zb = cconj(Rl[(N - k) % N]);
+    const double2 e = make_double2(0.5 * (za.x + zb.x), 0.5 * (za.y + zb.y));
+    const double2 o = make_double2(0.5 * (za.x - zb.x), 0.5 * (za.y - zb.y));
+    const double2 t = cmul(__ldg(&twr[k]), o);
+    return make_double2(e.x + t.y, e.y - t.x);
+}
+
+constexpr int RB = 8;  // rows per block of the generic row kernels
+
+template <bool WIDE>
+__global__ void __launch_bounds__(256, WIDE ? 2 : 3) k_row_c2r(RowJobList jobs, RowArgs a) {
+    extern __shared__ double2 smem[];
+    const RowIO job = jobs.j[blockIdx.y];
+    const int N = a.nxl / 2, LS = N + 1;
+    const int nrows = a.nyl * a.nzp;
+    const int row0 = blockIdx.x * RB;
+    const int L = min(RB, nrows - row0);
+    double2* X = smem;
+    double2* Z = smem + RB * LS;
+    const int tid = threadIdx.x;
+    for (int idx = tid; idx < L * LS; idx += blockDim.x) {
+        const int l = idx / LS, k = idx - l * LS;
         double2 v = make_double2(0.0, 0.0);
-        if (k < kxc) {
-            v = *reinterpret_cast<const double2*>(yrow + 2 * k);
-            if (mode == YM_IKX) {
-                const double kk = wavx[2 * k];
+        if (k < a.kxc) {
+            v = *reinterpret_cast<const double2*>(job.yin + (long long)(row0 + l) * 2 * a.kxc + 2 * k);
+            if (job.mode == YM_IKX) {
+                const double kk = a.wavx[2 * k];
                 v = make_double2(-kk * v.y, kk * v.x);
             }
         }
-        if (k == 0) v = make_double2(v.x, 0.0);  // FFTW c2r ignores Im of the DC input
-        X[k] = v;
+        if (k == 0) v.y = 0.0;  // FFTW c2r ignores Im of the DC input
+        X[idx] = v;
     }
-    __syncwarp();
-    for (int k = lane; k < N; k += 32) {
-        const double2 xa = X[k];
-        const double2 xb = cconj(X[N - k]);
-        const double2 e = cadd(xa, xb);
-        const double2 o = cmul(csub(xa, xb), cconj(__ldg(&rp.twr[k])));
-        Z[k] = make_double2(e.x - o.y, e.y + o.x);
-    }
-    __syncwarp();
-    double2* r = fft_line<+1>(Z, X, rp.half, lane);
-    if (r != Z) {
-        for (int k = lane; k < N; k += 32) Z[k] = r[k];
-        __syncwarp();
-    }
-    if (meanv != 0.0) {
-        for (int k = lane; k < N; k += 32) {
-            Z[k].x += meanv;
-            Z[k].y += meanv;
+    __syncthreads();
+    const double2* R = rows_c2r<WIDE>(X, Z, L, a.rp, tid, blockDim.x);
+    for (int idx = tid; idx < L * N; idx += blockDim.x) {
+        const int l = idx / N, k = idx - l * N;
+        double2 v = R[l * LS + k];
+        if (job.mean != nullptr && job.add_mean != 0.0) {
+            const double m = job.mean[(row0 + l) / a.nyl] * job.add_mean;
+            v.x += m;
+            v.y += m;
         }
-        __syncwarp();
+        reinterpret_cast<double2*>(job.out + (long long)(row0 + l) * a.row_pitch)[k] = v;
     }
 }
 
-// r2c of the physical row held in Z (destroyed); writes kx modes 0..kxc-1 to yrow.
-__device__ void row_r2c_warp(double2* Z, double2* X, const RealPlan& rp, int kxc, double* __restrict__ yrow,
-                             int lane) {
-    const int N = rp.nr / 2;
-    const double2* r = fft_line<-1>(Z, X, rp.half, lane);
-    for (int k = lane; k < kxc; k += 32) {
-        const double2 za = r[k];
-        const double2 zb = cconj(r[(N - k) % N]);
-        const double2 e = make_double2(0.5 * (za.x + zb.x), 0.5 * (za.y + zb.y));
-        const double2 o = make_double2(0.5 * (za.x - zb.x), 0.5 * (za.y - zb.y));
-        const double2 t = cmul(__ldg(&rp.twr[k]), o);
-        *reinterpret_cast<double2*>(yrow + 2 * k) = make_double2(e.x + t.y, e.y - t.x);
+template <bool WIDE>
+__global__ void __launch_bounds__(256, WIDE ? 2 : 3) k_row_r2c(RowJobList jobs, RowArgs a) {
+    extern __shared__ double2 smem[];
+    const RowIO job = jobs.j[blockIdx.y];
+    const int N = a.nxl / 2, LS = N + 1;
+    const int nrows = a.nyl * a.nzp;
+    const int row0 = blockIdx.x * RB;
+    const int L = min(RB, nrows - row0);
+    double2* Z = smem;
+    double2* X = smem + RB * LS;
+    const int tid = threadIdx.x;
+    for (int idx = tid; idx < L * N; idx += blockDim.x) {
+        const int l = idx / N, k = idx - l * N;
+        Z[l * LS + k] = reinterpret_cast<const double2*>(job.yin + (long long)(row0 + l) * a.row_pitch)[k];
     }
-    __syncwarp();
+    __syncthreads();
+    const double2* R = rows_r2c<WIDE>(Z, X, L, a.rp, tid, blockDim.x);
+    for (int idx = tid; idx < L * a.kxc; idx += blockDim.x) {
+        const int l = idx / a.kxc, k = idx - l * a.kxc;
+        *reinterpret_cast<double2*>(job.out + (long long)(row0 + l) * 2 * a.kxc + 2 * k) =
+            r2c_mode(R + l * LS, k, N, a.rp.twr);
+    }
 }
 
-constexpr int ROW_WARPS = 4;
-
-__global__ void __launch_bounds__(ROW_WARPS * 32) k_row_c2r(RowJobList jobs, RowArgs a) {
-    extern __shared__ double2 smem[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int row = blockIdx.x * ROW_WARPS + warp;
-    if (row >= a.nyl * a.nzp) return;
-    const RowIO job = jobs.j[blockIdx.y];
-    const int N = a.nxl / 2;
-    double2* X = smem + warp * (2 * N + 1);
-    double2* Z = X + N + 1;
-    const int z = row / a.nyl;
-    const double meanv = (job.mean != nullptr && job.add_mean != 0.0) ? job.mean[z] * job.add_mean : 0.0;
-    row_c2r_warp(job.yin + (long long)row * 2 * a.kxc, job.mode, a.wavx, a.kxc, meanv, a.rp, X, Z, lane);
-    double2* o = reinterpret_cast<double2*>(job.out + (long long)row * a.row_pitch);
-    for (int k = lane; k < N; k += 32) o[k] = Z[k];
-}
-
-__global__ void __launch_bounds__(ROW_WARPS * 32) k_row_r2c(RowJobList jobs, RowArgs a) {
-    extern __shared__ double2 smem[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int row = blockIdx.x * ROW_WARPS + warp;
-    if (row >= a.nyl * a.nzp) return;
-    const RowIO job = jobs.j[blockIdx.y];
-    const int N = a.nxl / 2;
-    double2* X = smem + warp * (2 * N + 1);
-    double2* Z = X + N + 1;
-    const double2* in = reinterpret_cast<const double2*>(job.yin + (long long)row * a.row_pitch);
-    for (int k = lane; k < N; k += 32) Z[k] = in[k];
-    __syncwarp();
-    row_r2c_warp(Z, X, a.rp, a.kxc, job.out + (long long)row * 2 * a.kxc, lane);
-}
+static size_t rows_smem(int nxl) { return (size_t)2 * RB * (nxl / 2 + 1) * sizeof(double2); }
 
 void launch_row_c2r(const RowJobList& jobs, const RowArgs& a, cudaStream_t s) {
     if (jobs.n <= 0) return;
     const int rows = a.nyl * a.nzp;
-    dim3 grid((rows + ROW_WARPS - 1) / ROW_WARPS, jobs.n);
-    size_t sm = (size_t)ROW_WARPS * (a.nxl + 1) * sizeof(double2);
-    k_row_c2r<<<grid, ROW_WARPS * 32, sm, s>>>(jobs, a);
+    dim3 grid((rows + RB - 1) / RB, jobs.n);
+    static bool attr = false;
+    if (!attr) {
+        smem_attr(k_row_c2r<true>);
+        smem_attr(k_row_c2r<false>);
+        attr = true;
+    }
+    if (wide(a.rp.half)) k_row_c2r<true><<<grid, 256, rows_smem(a.nxl), s>>>(jobs, a);
+    else k_row_c2r<false><<<grid, 256, rows_smem(a.nxl), s>>>(jobs, a);
 }
 
 void launch_row_r2c(const RowJobList& jobs, const RowArgs& a, cudaStream_t s) {
     if (jobs.n <= 0) return;
     const int rows = a.nyl * a.nzp;
-    dim3 grid((rows + ROW_WARPS - 1) / ROW_WARPS, jobs.n);
-    size_t sm = (size_t)ROW_WARPS * (a.nxl + 1) * sizeof(double2);
-    k_row_r2c<<<grid, ROW_WARPS * 32, sm, s>>>(jobs, a);
+    dim3 grid((rows + RB - 1) / RB, jobs.n);
+    static bool attr = false;
+    if (!attr) {
+        smem_attr(k_row_r2c<true>);
+        smem_attr(k_row_r2c<false>);
+        attr = true;
+    }
+    if (wide(a.rp.half)) k_row_r2c<true><<<grid, 256, rows_smem(a.nxl), s>>>(jobs, a);
+    else k_row_r2c<false><<<grid, 256, rows_smem(a.nxl), s>>>(jobs, a);
 }
 
 // ----------------------------------------------------------------------------- NL row
 // One (z, y) row per block: 12 c2r (u, du/dx, du/dy, du/dz for 3 components), the
 // skew-symmetric products of nlterm_skewsym (src/navierstokes.f90:725-769), and 9 r2c.
-constexpr int NL_WARPS = 8;
-
-__global__ void __launch_bounds__(NL_WARPS * 32) k_row_nl(NlRowArgs a) {
+template <bool WIDE>
+__global__ void __launch_bounds__(256, WIDE ? 2 : 3) k_row_nl(NlRowArgs a) {
     extern __shared__ double2 smem[];
     const RowArgs& r = a.r;
-    const int N = r.nxl / 2;
+    const int N = r.nxl / 2, LS = N + 1;
     const int yl = blockIdx.x, z = blockIdx.y;
     const long long row = (long long)z * r.nyl + yl;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double2* P = smem;                          // 12 rows of N double2
-    double2* X = smem + 12 * N + warp * (N + 1);
+    const int tid = threadIdx.x;
+    double2* X = smem;            // 12 lines
+    double2* Z = smem + 12 * LS;  // 12 lines
     // inputs: 0..2 u_l, 3..5 du_l/dx, 6..8 du_l/dy, 9..11 du_l/dz
-    for (int f = warp; f < 12; f += NL_WARPS) {
+    for (int idx = tid; idx < 12 * LS; idx += blockDim.x) {
+        const int f = idx / LS, k = idx - f * LS;
         const int l = f % 3, kind = f / 3;
-        const double* src;
-        int mode = YM_COPY;
-        double meanv = 0.0;
-        if (kind == 0) {
-            src = a.U[l];
-            if (l == 0) meanv = a.ubar[z];
-        } else if (kind == 1) {
-            src = a.U[l];
-            mode = YM_IKX;
-        } else if (kind == 2) {
-            src = a.DY[l];
-        } else {
-            src = a.DZ[l];
-            if (l == 0) meanv = a.ubarp[z];
+        double2 v = make_double2(0.0, 0.0);
+        if (k < r.kxc) {
+            const double* src = (kind == 0 || kind == 1) ? a.U[l] : (kind == 2 ? a.DY[l] : a.DZ[l]);
+            v = *reinterpret_cast<const double2*>(src + row * 2 * r.kxc + 2 * k);
+            if (kind == 1) {
+                const double kk = r.wavx[2 * k];
+                v = make_double2(-kk * v.y, kk * v.x);
+            }
         }
-        row_c2r_warp(src + row * 2 * r.kxc, mode, r.wavx, r.kxc, meanv, r.rp, X, P + f * N, lane);
+        if (k == 0) v.y = 0.0;
+        X[idx] = v;
     }
     __syncthreads();
-    const double* p = reinterpret_cast<const double*>(P);
-    double* q = reinterpret_cast<double*>(P);
-    const int n = r.nxl;
-    const double ub = a.ubar[z];
-    for (int x = threadIdx.x; x < n; x += blockDim.x) {
+    double2* R = rows_c2r<WIDE>(X, Z, 12, r.rp, tid, blockDim.x);
+    double2* O = (R == Z) ? X : Z;
+    const double* p = reinterpret_cast<const double*>(R);
+    double* q = reinterpret_cast<double*>(O);
+    const int n = r.nxl, L2 = 2 * LS;
+    const double ub = a.ubar[z], ubp = a.ubarp[z];
+    for (int x = tid; x < n; x += blockDim.x) {
         double u[3], g[3][3];
 #pragma unroll
         for (int l = 0; l < 3; ++l) {
-            u[l] = p[(0 + l) * 2 * N + x];
-            g[l][0] = p[(3 + l) * 2 * N + x];
-            g[l][1] = p[(6 + l) * 2 * N + x];
-            g[l][2] = p[(9 + l) * 2 * N + x];
+            u[l] = p[(0 + l) * L2 + x];
+            g[l][0] = p[(3 + l) * L2 + x];
+            g[l][1] = p[(6 + l) * L2 + x];
+            g[l][2] = p[(9 + l) * L2 + x];
         }
+        u[0] += ub;
+        g[0][2] += ubp;
         double nl[3];
 #pragma unroll
         for (int l = 0; l < 3; ++l) {
@@ -400,35 +456,37 @@ __global__ void __launch_bounds__(NL_WARPS * 32) k_row_nl(NlRowArgs a) {
             nl[1] = nl[1] + lx * (0.0 - u[1]);
             nl[2] = nl[2] + lx * (0.0 - u[2]);
         }
-        const double h11 = 0.5 * (u[0] * u[0]), h12 = 0.5 * (u[0] * u[1]), h13 = 0.5 * (u[0] * u[2]);
-        const double h22 = 0.5 * (u[1] * u[1]), h23 = 0.5 * (u[1] * u[2]), h33 = 0.5 * (u[2] * u[2]);
-        q[0 * 2 * N + x] = nl[0];
-        q[1 * 2 * N + x] = nl[1];
-        q[2 * 2 * N + x] = nl[2];
-        q[3 * 2 * N + x] = h11;
-        q[4 * 2 * N + x] = h12;
-        q[5 * 2 * N + x] = h13;
-        q[6 * 2 * N + x] = h22;
-        q[7 * 2 * N + x] = h23;
-        q[8 * 2 * N + x] = h33;
+        q[0 * L2 + x] = nl[0];
+        q[1 * L2 + x] = nl[1];
+        q[2 * L2 + x] = nl[2];
+        q[3 * L2 + x] = 0.5 * (u[0] * u[0]);
+        q[4 * L2 + x] = 0.5 * (u[0] * u[1]);
+        q[5 * L2 + x] = 0.5 * (u[0] * u[2]);
+        q[6 * L2 + x] = 0.5 * (u[1] * u[1]);
+        q[7 * L2 + x] = 0.5 * (u[1] * u[2]);
+        q[8 * L2 + x] = 0.5 * (u[2] * u[2]);
     }
     __syncthreads();
-    for (int f = warp; f < 9; f += NL_WARPS) {
+    const double2* R2 = rows_r2c<WIDE>(O, R, 9, r.rp, tid, blockDim.x);
+    for (int idx = tid; idx < 9 * r.kxc; idx += blockDim.x) {
+        const int f = idx / r.kxc, k = idx - f * r.kxc;
         double* dst = (f < 3) ? a.N[f] : a.H[f - 3];
-        row_r2c_warp(P + f * N, X, r.rp, r.kxc, dst + row * 2 * r.kxc, lane);
+        *reinterpret_cast<double2*>(dst + row * 2 * r.kxc + 2 * k) = r2c_mode(R2 + f * LS, k, N, r.rp.twr);
     }
 }
 
 void launch_row_nl(const NlRowArgs& a, cudaStream_t s) {
     const int N = a.r.nxl / 2;
-    size_t sm = (size_t)(12 * N + NL_WARPS * (N + 1)) * sizeof(double2);
+    size_t sm = (size_t)24 * (N + 1) * sizeof(double2);
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_row_nl, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        smem_attr(k_row_nl<true>);
+        smem_attr(k_row_nl<false>);
         attr = true;
     }
     dim3 grid(a.r.nyl, a.r.nzp);
-    k_row_nl<<<grid, NL_WARPS * 32, sm, s>>>(a);
+    if (wide(a.r.rp.half)) k_row_nl<true><<<grid, 256, sm, s>>>(a);
+    else k_row_nl<false><<<grid, 256, sm, s>>>(a);
 }
 
 }  // namespace lsb

@@ -19,11 +19,21 @@ namespace lsb {
 
 constexpr int kMaxStages = 16;
 
+// exact unsigned division by a constant: q = (umulhi(n, m) + n) >> s  (d > 1), valid for
+// the n < 2^31 used here
+struct FastDiv {
+    uint32_t d = 1, m = 0, s = 0;
+};
+
 // One complex FFT length: radix schedule + twiddle table tw[m] = exp(-2 pi i m / n).
+// Per stage st: p = product of the radices before it, T = n / R, stride = n / (p R).
 struct FftPlan {
     int n = 0;
     int nst = 0;
     int radix[kMaxStages] = {0};
+    int p[kMaxStages] = {0};
+    FastDiv fdT[kMaxStages];
+    FastDiv fdP[kMaxStages];
     const double2* tw = nullptr;   // device, n entries
 };
 

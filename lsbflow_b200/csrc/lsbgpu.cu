@@ -55,7 +55,25 @@ void make_plan(lsb_handle* h, int n, FftPlan& P) {
         fail(LSB_ERR_UNSUPPORTED, "FFT length " + std::to_string(n) + " is not a product of 2,3,5,7");
     P.n = n;
     P.nst = (int)rad.size();
-    for (int i = 0; i < P.nst; ++i) P.radix[i] = rad[i];
+    auto fd = [](uint32_t d) {
+        FastDiv f;
+        f.d = d;
+        if (d > 1) {
+            uint32_t s = 0;
+            while ((1ull << s) < d) ++s;
+            f.s = s;
+            f.m = (uint32_t)((((1ull << s) - d) << 32) / d + 1);
+        }
+        return f;
+    };
+    int pp = 1;
+    for (int i = 0; i < P.nst; ++i) {
+        P.radix[i] = rad[i];
+        P.p[i] = pp;
+        P.fdT[i] = fd((uint32_t)(n / rad[i]));
+        P.fdP[i] = fd((uint32_t)pp);
+        pp *= rad[i];
+    }
     std::vector<double> tw(2 * (size_t)n);
     const long double pi = 3.141592653589793238462643383279502884L;
     for (int m = 0; m < n; ++m) {

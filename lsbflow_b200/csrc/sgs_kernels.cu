@@ -43,38 +43,66 @@ struct W9 {
     double* p[9];
 };
 
-// filter_q_3pt: x (periodic) then y (periodic) then z (interior planes, non-uniform weights)
-__global__ void k_filter3(FieldList fl, int nx, int ny, int nzp, double a, double b, const double* __restrict__ az,
-                          const double* __restrict__ bz, const double* __restrict__ cz) {
-    const long long P = (long long)nx * ny * nzp;
+// filter_q_3pt: x (periodic) then y (periodic) then z (interior planes, non-uniform
+// weights; the ceiling and wall planes are xy-filtered only, src/filters.f90:450).
+// A block owns a JB x IB tile of (y, x) columns and marches a chunk of ZC planes in z:
+// each plane is read once into shared memory with a one-point periodic halo, filtered in
+// x and y, and the last three y-filtered planes are kept in registers for the z stencil.
+constexpr int FIB = 32, FJB = 8, FZC = 16;
+
+__global__ void __launch_bounds__(256) k_filter3(FieldList fl, int nx, int ny, int nzp, double a, double b,
+                                                 const double* __restrict__ az, const double* __restrict__ bz,
+                                                 const double* __restrict__ cz, int nzc) {
+    __shared__ double tile[FJB + 2][FIB + 2];
+    __shared__ double X[FJB + 2][FIB];
+    const int f = blockIdx.z / nzc, zc = blockIdx.z % nzc;
+    const double* q = fl.in[f];
+    double* out = fl.out[f];
+    const int i0 = blockIdx.x * FIB, j0 = blockIdx.y * FJB;
+    const int k0 = zc * FZC, k1 = min(nzp, k0 + FZC);  // output planes [k0, k1)
+    const int ks = max(0, k0 - 1), ke = min(nzp - 1, k1);
     const double s = 2.0 * a + b;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < P * fl.n;
-         e += (long long)gridDim.x * blockDim.x) {
-        const int f = (int)(e / P);
-        const long long x = e % P;
-        const int i = (int)(x % nx);
-        const int j = (int)((x / nx) % ny);
-        const int k = (int)(x / ((long long)nx * ny));
-        const double* q = fl.in[f];
-        const int im = (i == 0) ? nx - 1 : i - 1, ip = (i == nx - 1) ? 0 : i + 1;
-        const int jm = (j == 0) ? ny - 1 : j - 1, jp = (j == ny - 1) ? 0 : j + 1;
-        auto xf = [&](int kk, int jj) {
-            const double* r = q + ((long long)kk * ny + jj) * nx;
-            return (a * r[im] + b * r[i] + a * r[ip]) / s;
-        };
-        auto yf = [&](int kk) { return (a * xf(kk, jm) + b * xf(kk, j) + a * xf(kk, jp)) / s; };
-        double v;
-        if (k == 0 || k == nzp - 1) {
-            v = yf(k);
-        } else {
-            v = (az[k] * yf(k - 1) + bz[k] * yf(k) + cz[k] * yf(k + 1)) / s;
+    const int tid = threadIdx.x;
+    const int jj = tid / FIB, ii = tid % FIB;  // this thread's output column (256 = FJB * FIB)
+    const int jo = j0 + jj, io = i0 + ii;
+    const bool mine = (jo < ny) && (io < nx);
+    double y0 = 0.0, y1 = 0.0, y2 = 0.0;  // y-filtered planes kk-2, kk-1, kk
+    for (int kk = ks; kk <= ke; ++kk) {
+        const double* pl = q + (long long)kk * ny * nx;
+        for (int idx = tid; idx < (FJB + 2) * (FIB + 2); idx += 256) {
+            const int jr = idx / (FIB + 2), ir = idx % (FIB + 2);
+            int j = j0 + jr - 1, i = i0 + ir - 1;
+            j = (j % ny + ny) % ny;
+            i = (i % nx + nx) % nx;
+            tile[jr][ir] = pl[(long long)j * nx + i];
         }
-        fl.out[f][x] = v;
+        __syncthreads();
+        for (int idx = tid; idx < (FJB + 2) * FIB; idx += 256) {
+            const int jr = idx / FIB, ir = idx % FIB;
+            X[jr][ir] = (a * tile[jr][ir] + b * tile[jr][ir + 1] + a * tile[jr][ir + 2]) / s;
+        }
+        __syncthreads();
+        const double yn = (a * X[jj][ii] + b * X[jj + 1][ii] + a * X[jj + 2][ii]) / s;
+        y0 = y1;
+        y1 = y2;
+        y2 = yn;
+        if (mine) {
+            const int ko = kk - 1;  // plane whose z stencil is now complete
+            if (ko >= k0 && ko < k1) {
+                double v;
+                if (ko == 0) v = y1;
+                else v = (az[ko] * y0 + bz[ko] * y1 + cz[ko] * y2) / s;
+                out[((long long)ko * ny + jo) * nx + io] = v;
+            }
+            if (kk == nzp - 1 && kk >= k0 && kk < k1) out[((long long)kk * ny + jo) * nx + io] = yn;
+        }
+        __syncthreads();
     }
 }
 
 void filter3(lsb_handle* h, const double* const* in, double* const* out, int n, double a, double b, int which) {
     const Dims& d = h->d;
+    const int nzc = (d.nzp + FZC - 1) / FZC;
     for (int f0 = 0; f0 < n; f0 += 9) {
         FieldList fl{};
         fl.n = std::min(9, n - f0);
@@ -84,8 +112,8 @@ void filter3(lsb_handle* h, const double* const* in, double* const* out, int n, 
         }
         const double* zf = h->sgs.zf + (long long)which * 3 * d.nzp;
         TimerScope ts(h, "sgs_filter3");
-        k_filter3<<<nblk(h->P * fl.n), 256, 0, h->stream>>>(fl, d.nx, d.ny, d.nzp, a, b, zf, zf + d.nzp,
-                                                           zf + 2 * d.nzp);
+        dim3 grid((d.nx + FIB - 1) / FIB, (d.ny + FJB - 1) / FJB, nzc * fl.n);
+        k_filter3<<<grid, 256, 0, h->stream>>>(fl, d.nx, d.ny, d.nzp, a, b, zf, zf + d.nzp, zf + 2 * d.nzp, nzc);
     }
 }
 
