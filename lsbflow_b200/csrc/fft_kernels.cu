@@ -15,15 +15,9 @@
 // memory; every stage runs over all lines a block holds, with all its threads.  FFTW's c2r semantics are kept: the imaginary parts of
 // the DC and Nyquist inputs are ignored and the kx Nyquist mode is dropped / zero.
 #include "lsb_internal.cuh"
+#include "lsb_fftdev.cuh"
 
 namespace lsb {
-
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-    return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
-}
-__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
 
 // R-point DFT of u in registers, U[s] = sum_q u[q] exp(SIGN 2 pi i q s / R)
 template <int R, int SIGN>
@@ -61,6 +55,77 @@ __device__ __forceinline__ void dft_small(double2 (&u)[R], const double2* __rest
 #pragma unroll
         for (int s = 0; s < R; ++s) u[s] = U[s];
     }
+}
+
+// Complex FFT of L lines (stride ls) of length N = N1*N2 by the whole block, result in A:
+// pass 1 does the N1-point DFTs of the stride-N2 subsequences in registers and the
+// twiddles exp(SIGN 2 pi i n2 k1 / N) (table tw), into B with padded rows; pass 2 the
+// N2-point DFTs, back into A in natural order.
+template <int N1, int N2, int SIGN>
+__device__ void fft2p(double2* A, double2* B, int L, int ls, const double2* __restrict__ tw, int tid, int nthr) {
+    if constexpr (N2 == 1) {
+        for (int line = tid; line < L; line += nthr) {
+            double2* a = A + line * ls;
+            double2 v[N1];
+#pragma unroll
+            for (int k = 0; k < N1; ++k) v[k] = a[k];
+            dft_reg<N1, SIGN>(v);
+#pragma unroll
+            for (int k = 0; k < N1; ++k) a[k] = v[k];
+        }
+        __syncthreads();
+    } else {
+        constexpr int PB = (N2 % 2 == 0) ? N2 + 1 : N2;
+        for (int idx = tid; idx < L * N2; idx += nthr) {
+            const int line = idx / N2, n2 = idx - line * N2;
+            const double2* a = A + line * ls;
+            double2 v[N1];
+#pragma unroll
+            for (int n1 = 0; n1 < N1; ++n1) v[n1] = a[N2 * n1 + n2];
+            dft_reg<N1, SIGN>(v);
+            if (n2 != 0) {
+#pragma unroll
+                for (int k1 = 1; k1 < N1; ++k1) {
+                    double2 w = __ldg(&tw[n2 * k1]);
+                    if (SIGN > 0) w.y = -w.y;
+                    v[k1] = cmul(v[k1], w);
+                }
+            }
+            double2* b = B + line * ls;
+#pragma unroll
+            for (int k1 = 0; k1 < N1; ++k1) b[k1 * PB + n2] = v[k1];
+        }
+        __syncthreads();
+        for (int idx = tid; idx < L * N1; idx += nthr) {
+            const int line = idx / N1, k1 = idx - line * N1;
+            const double2* b = B + line * ls;
+            double2 v[N2];
+#pragma unroll
+            for (int n2 = 0; n2 < N2; ++n2) v[n2] = b[k1 * PB + n2];
+            dft_reg<N2, SIGN>(v);
+            double2* a = A + line * ls;
+#pragma unroll
+            for (int k2 = 0; k2 < N2; ++k2) a[k1 + N1 * k2] = v[k2];
+        }
+        __syncthreads();
+    }
+}
+
+// returns true (result in A) when the plan has a register two-pass split
+template <int SIGN>
+__device__ __forceinline__ bool fft_twopass(double2* A, double2* B, int L, int ls, const FftPlan& P, int tid,
+                                            int nthr) {
+#define LSB_2P(a_, b_)                                                   \
+    if (P.n1 == a_ && P.n2 == b_) {                                     \
+        fft2p<a_, b_, SIGN>(A, B, L, ls, P.tw, tid, nthr);              \
+        return true;                                                    \
+    }
+    LSB_2P(2, 1) LSB_2P(3, 1) LSB_2P(4, 1) LSB_2P(6, 1) LSB_2P(8, 1) LSB_2P(12, 1) LSB_2P(16, 1)
+    LSB_2P(3, 3) LSB_2P(6, 3) LSB_2P(8, 3) LSB_2P(8, 4) LSB_2P(12, 3) LSB_2P(8, 6) LSB_2P(16, 3)
+    LSB_2P(8, 8) LSB_2P(12, 6) LSB_2P(12, 8) LSB_2P(16, 6) LSB_2P(12, 12) LSB_2P(16, 8) LSB_2P(16, 12)
+    LSB_2P(16, 16)
+#undef LSB_2P
+    return false;
 }
 
 __device__ __forceinline__ uint32_t fdiv(uint32_t n, const FastDiv& f) {
@@ -106,6 +171,9 @@ __device__ __forceinline__ void bstage(const double2* __restrict__ src, double2*
 // the others only 2, 3, 4, which keeps their register footprint small.
 template <int SIGN, bool WIDE>
 __device__ bool fft_batch(double2* A, double2* B, int nlines, int ls, const FftPlan& P, int tid, int nthr) {
+    if constexpr (!WIDE) {
+        if (fft_twopass<SIGN>(A, B, nlines, ls, P, tid, nthr)) return true;
+    }
     double2* src = A;
     double2* dst = B;
     for (int s = 0; s < P.nst; ++s) {
@@ -135,91 +203,142 @@ __device__ __forceinline__ int pad_row(int j, int ny, int nyl, int layout) {
     return (j < ny / 2) ? j : j + (nyl - ny);
 }
 
-constexpr int KC = 16;  // kx columns per spanwise block
+constexpr int KC = 16;  // kx columns per spanwise work item
+constexpr int RB = 8;   // rows per work item of the generic row kernels
+
+// ---------------------------------------------------------------- pipelining helpers
+// Every FFT kernel below is persistent: a block loops over work items and stages the
+// next item's input with cp.async while it transforms the current one (two input
+// buffers used alternately, one scratch buffer for the FFT ping-pong).
+__device__ __forceinline__ void cpa16(void* sdst, const void* gsrc) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc));
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cpa_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
 
 // ----------------------------------------------------------------------------- k_yinv
+// item = (job, z, kx chunk); input rows go straight into line layout (pad rows zeroed)
 template <bool WIDE>
-__global__ void __launch_bounds__(256, WIDE ? 2 : 3) k_yinv(YInvJobList jobs, YPassArgs a) {
+__global__ void __launch_bounds__(256, 2) k_yinv(YInvJobList jobs, YPassArgs a, int nch) {
     extern __shared__ double2 smem[];
-    const YInvJob job = jobs.j[blockIdx.z];
-    const int z = blockIdx.y;
-    const int c0 = blockIdx.x * KC;
-    const int nyl = a.nyl, ny = a.ny;
-    const int LS = nyl + 1;  // odd line stride: conflict-free column writes
-    double2* A = smem;
-    double2* B = smem + KC * LS;
+    const int ny = a.ny, nyl = a.nyl, LS = a.plan.ls;
+    double2* Buf[2] = {smem, smem + KC * LS};
+    double2* Scr = smem + 2 * KC * LS;
     const int tid = threadIdx.x;
-    for (int i = tid; i < KC * LS; i += blockDim.x) A[i] = make_double2(0.0, 0.0);
-    __syncthreads();
-    for (int idx = tid; idx < ny * KC; idx += blockDim.x) {
-        const int j = idx / KC, cc = idx % KC, c = c0 + cc;
-        if (c >= a.kxc) continue;
-        const double2 v = *reinterpret_cast<const double2*>(job.in + ((long long)z * ny + j) * a.nx + 2 * c);
-        double2 r = v;
-        if (job.mode == YM_IKY) {
-            const double k = a.wavy[j];
-            r = make_double2(-k * v.y, k * v.x);
-        } else if (job.mode == YM_IKX) {
-            const double k = a.wavx[2 * c];
-            r = make_double2(-k * v.y, k * v.x);
+    const int nitems = jobs.n * a.nzp * nch;
+    const int npad = nyl - ny;
+    auto issue = [&](int item, double2* A) {
+        const int ch = item % nch, rest = item / nch, z = rest % a.nzp, jb = rest / a.nzp;
+        const double* in = jobs.j[jb].in;
+        const int c0 = ch * KC;
+        for (int idx = tid; idx < ny * KC; idx += 256) {
+            const int j = idx / KC, cc = idx - j * KC, c = c0 + cc;
+            double2* d = &A[cc * LS + pad_row(j, ny, nyl, a.layout)];
+            if (c < a.kxc) cpa16(d, in + ((long long)z * ny + j) * a.nx + 2 * c);
+            else *d = make_double2(0.0, 0.0);
         }
-        A[cc * LS + pad_row(j, ny, nyl, a.layout)] = r;
-    }
-    __syncthreads();
-    const bool inA = fft_batch<+1, WIDE>(A, B, KC, LS, a.plan, tid, blockDim.x);
-    const double2* R = inA ? A : B;
-    for (int idx = tid; idx < nyl * KC; idx += blockDim.x) {
-        const int jl = idx / KC, cc = idx % KC, c = c0 + cc;
-        if (c >= a.kxc) continue;
-        *reinterpret_cast<double2*>(job.out + ((long long)z * nyl + jl) * a.nx + 2 * c) = R[cc * LS + jl];
+        for (int idx = tid; idx < npad * KC; idx += 256) {
+            const int r = idx / KC, cc = idx - r * KC;
+            const int jl = (a.layout == 0) ? ny + r : ny / 2 + r;
+            A[cc * LS + jl] = make_double2(0.0, 0.0);
+        }
+        cpa_commit();
+    };
+    int cur = 0;
+    int item = blockIdx.x;
+    if (item < nitems) issue(item, Buf[0]);
+    for (; item < nitems; item += gridDim.x) {
+        const int ch = item % nch, rest = item / nch, z = rest % a.nzp, jb = rest / a.nzp;
+        const YInvJob job = jobs.j[jb];
+        const int c0 = ch * KC;
+        double2* A = Buf[cur];
+        cpa_wait_all();
+        __syncthreads();
+        if (job.mode != YM_COPY) {
+            for (int idx = tid; idx < ny * KC; idx += 256) {
+                const int j = idx / KC, cc = idx - j * KC, c = c0 + cc;
+                double2* d = &A[cc * LS + pad_row(j, ny, nyl, a.layout)];
+                const double k = (job.mode == YM_IKY) ? a.wavy[j] : a.wavx[2 * min(c, a.kxc - 1)];
+                const double2 v = *d;
+                *d = make_double2(-k * v.y, k * v.x);
+            }
+            __syncthreads();
+        }
+        const int next = item + gridDim.x;
+        if (next < nitems) issue(next, Buf[cur ^ 1]);
+        const bool inA = fft_batch<+1, WIDE>(A, Scr, KC, LS, a.plan, tid, 256);
+        const double2* R = inA ? A : Scr;
+        for (int idx = tid; idx < nyl * KC; idx += 256) {
+            const int jl = idx / KC, cc = idx - jl * KC, c = c0 + cc;
+            if (c >= a.kxc) continue;
+            *reinterpret_cast<double2*>(job.out + ((long long)z * nyl + jl) * a.nx + 2 * c) = R[cc * LS + jl];
+        }
+        __syncthreads();
+        cur ^= 1;
     }
 }
 
 // ----------------------------------------------------------------------------- k_yfwd
 template <bool WIDE>
-__global__ void __launch_bounds__(256, WIDE ? 2 : 3) k_yfwd(YFwdJobList jobs, YPassArgs a) {
+__global__ void __launch_bounds__(256, 2) k_yfwd(YFwdJobList jobs, YPassArgs a, int nch) {
     extern __shared__ double2 smem[];
-    const YFwdJob job = jobs.j[blockIdx.z];
-    const int z = blockIdx.y;
-    const int c0 = blockIdx.x * KC;
-    const int nyl = a.nyl, ny = a.ny;
-    const int LS = nyl + 1;
-    double2* A = smem;
-    double2* B = smem + KC * LS;
+    const int ny = a.ny, nyl = a.nyl, LS = a.plan.ls;
+    double2* Buf[2] = {smem, smem + KC * LS};
+    double2* Scr = smem + 2 * KC * LS;
     const int tid = threadIdx.x;
-    for (int idx = tid; idx < nyl * KC; idx += blockDim.x) {
-        const int jl = idx / KC, cc = idx % KC, c = c0 + cc;
-        double2 v = make_double2(0.0, 0.0);
-        if (c < a.kxc) v = *reinterpret_cast<const double2*>(job.in + ((long long)z * nyl + jl) * a.nx + 2 * c);
-        A[cc * LS + jl] = v;
-    }
-    __syncthreads();
-    const bool inA = fft_batch<-1, WIDE>(A, B, KC, LS, a.plan, tid, blockDim.x);
-    const double2* R = inA ? A : B;
-    for (int idx = tid; idx < ny * KC; idx += blockDim.x) {
-        const int j = idx / KC, cc = idx % KC, c = c0 + cc;
-        if (c >= a.kxc) continue;
-        double2 v = R[cc * LS + pad_row(j, ny, nyl, a.layout)];
-        if (job.sym && c == 0) {
-            const int jm = (ny - j) % ny;
-            const double2 w = R[cc * LS + pad_row(jm, ny, nyl, a.layout)];
-            v = make_double2(0.5 * (v.x + w.x), 0.5 * (v.y - w.y));
+    const int nitems = jobs.n * a.nzp * nch;
+    auto issue = [&](int item, double2* A) {
+        const int ch = item % nch, rest = item / nch, z = rest % a.nzp, jb = rest / a.nzp;
+        const double* in = jobs.j[jb].in;
+        const int c0 = ch * KC;
+        for (int idx = tid; idx < nyl * KC; idx += 256) {
+            const int jl = idx / KC, cc = idx - jl * KC, c = c0 + cc;
+            double2* d = &A[cc * LS + jl];
+            if (c < a.kxc) cpa16(d, in + ((long long)z * nyl + jl) * a.nx + 2 * c);
+            else *d = make_double2(0.0, 0.0);
         }
-        v.x *= a.scale;
-        v.y *= a.scale;
-        double2* o = reinterpret_cast<double2*>(job.out + ((long long)z * ny + j) * a.nx + 2 * c);
-        double2 r;
-        if (job.beta != 0.0) {
-            const double2 old = *o;
-            r = make_double2(fma(job.alpha, v.x, job.beta * old.x), fma(job.alpha, v.y, job.beta * old.y));
-        } else {
-            r = make_double2(job.alpha * v.x, job.alpha * v.y);
+        cpa_commit();
+    };
+    int cur = 0;
+    int item = blockIdx.x;
+    if (item < nitems) issue(item, Buf[0]);
+    for (; item < nitems; item += gridDim.x) {
+        const int ch = item % nch, rest = item / nch, z = rest % a.nzp, jb = rest / a.nzp;
+        const YFwdJob job = jobs.j[jb];
+        const int c0 = ch * KC;
+        double2* A = Buf[cur];
+        cpa_wait_all();
+        __syncthreads();
+        const int next = item + gridDim.x;
+        if (next < nitems) issue(next, Buf[cur ^ 1]);
+        const bool inA = fft_batch<-1, WIDE>(A, Scr, KC, LS, a.plan, tid, 256);
+        const double2* R = inA ? A : Scr;
+        for (int idx = tid; idx < ny * KC; idx += 256) {
+            const int j = idx / KC, cc = idx - j * KC, c = c0 + cc;
+            if (c >= a.kxc) continue;
+            double2 v = R[cc * LS + pad_row(j, ny, nyl, a.layout)];
+            if (job.sym && c == 0) {
+                const int jm = (ny - j) % ny;
+                const double2 w = R[cc * LS + pad_row(jm, ny, nyl, a.layout)];
+                v = make_double2(0.5 * (v.x + w.x), 0.5 * (v.y - w.y));
+            }
+            v.x *= a.scale;
+            v.y *= a.scale;
+            double2* o = reinterpret_cast<double2*>(job.out + ((long long)z * ny + j) * a.nx + 2 * c);
+            double2 r;
+            if (job.beta != 0.0) {
+                const double2 old = *o;
+                r = make_double2(fma(job.alpha, v.x, job.beta * old.x), fma(job.alpha, v.y, job.beta * old.y));
+            } else {
+                r = make_double2(job.alpha * v.x, job.alpha * v.y);
+            }
+            *o = r;
         }
-        *o = r;
+        __syncthreads();
+        cur ^= 1;
     }
 }
-
-static size_t ypass_smem(const YPassArgs& a) { return (size_t)2 * KC * (a.nyl + 1) * sizeof(double2); }
 
 static bool wide(const FftPlan& P) {
     for (int i = 0; i < P.nst; ++i)
@@ -227,37 +346,42 @@ static bool wide(const FftPlan& P) {
     return false;
 }
 
+// persistent grid: resident blocks per SM x SMs, capped by the number of work items
 template <class K>
-static void smem_attr(K kern) {
+static int persistent_grid(K kern, size_t smem, int nitems) {
+    static int nsm = 0;
+    if (nsm == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        if (nsm <= 0) nsm = 148;
+    }
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 256, smem);
+    if (occ < 1) occ = 1;
+    const int g = occ * nsm;
+    return g < nitems ? g : nitems;
 }
 
 void launch_yinv(const YInvJobList& jobs, const YPassArgs& a, cudaStream_t s) {
     if (jobs.n <= 0) return;
-    dim3 grid((a.kxc + KC - 1) / KC, a.nzp, jobs.n);
-    size_t sm = ypass_smem(a);
-    static bool attr = false;
-    if (!attr) {
-        smem_attr(k_yinv<true>);
-        smem_attr(k_yinv<false>);
-        attr = true;
-    }
-    if (wide(a.plan)) k_yinv<true><<<grid, 256, sm, s>>>(jobs, a);
-    else k_yinv<false><<<grid, 256, sm, s>>>(jobs, a);
+    if (launch_yinv_warp(jobs, a, s)) return;
+    const int nch = (a.kxc + KC - 1) / KC;
+    const int nitems = jobs.n * a.nzp * nch;
+    const size_t sm = (size_t)3 * KC * a.plan.ls * sizeof(double2);
+    if (wide(a.plan)) k_yinv<true><<<persistent_grid(k_yinv<true>, sm, nitems), 256, sm, s>>>(jobs, a, nch);
+    else k_yinv<false><<<persistent_grid(k_yinv<false>, sm, nitems), 256, sm, s>>>(jobs, a, nch);
 }
 
 void launch_yfwd(const YFwdJobList& jobs, const YPassArgs& a, cudaStream_t s) {
     if (jobs.n <= 0) return;
-    dim3 grid((a.kxc + KC - 1) / KC, a.nzp, jobs.n);
-    size_t sm = ypass_smem(a);
-    static bool attr = false;
-    if (!attr) {
-        smem_attr(k_yfwd<true>);
-        smem_attr(k_yfwd<false>);
-        attr = true;
-    }
-    if (wide(a.plan)) k_yfwd<true><<<grid, 256, sm, s>>>(jobs, a);
-    else k_yfwd<false><<<grid, 256, sm, s>>>(jobs, a);
+    if (launch_yfwd_warp(jobs, a, s)) return;
+    const int nch = (a.kxc + KC - 1) / KC;
+    const int nitems = jobs.n * a.nzp * nch;
+    const size_t sm = (size_t)3 * KC * a.plan.ls * sizeof(double2);
+    if (wide(a.plan)) k_yfwd<true><<<persistent_grid(k_yfwd<true>, sm, nitems), 256, sm, s>>>(jobs, a, nch);
+    else k_yfwd<false><<<persistent_grid(k_yfwd<false>, sm, nitems), 256, sm, s>>>(jobs, a, nch);
 }
 
 // ----------------------------------------------------------------------------- rows
@@ -266,7 +390,7 @@ void launch_yfwd(const YFwdJobList& jobs, const YPassArgs& a, cudaStream_t s) {
 // (= 2N physical reals) of each line (stride N+1).
 template <bool WIDE>
 __device__ double2* rows_c2r(double2* X, double2* Z, int L, const RealPlan& rp, int tid, int nthr) {
-    const int N = rp.nr / 2, LS = N + 1;
+    const int N = rp.nr / 2, LS = rp.half.ls;
     for (int idx = tid; idx < L * N; idx += nthr) {
         const int l = idx / N, k = idx - l * N;
         const double2* xl = X + l * LS;
@@ -287,7 +411,7 @@ __device__ double2* rows_c2r(double2* X, double2* Z, int L, const RealPlan& rp, 
 template <bool WIDE>
 __device__ double2* rows_r2c(double2* Z, double2* X, int L, const RealPlan& rp, int tid, int nthr) {
     const int N = rp.nr / 2;
-    const bool inZ = fft_batch<-1, WIDE>(Z, X, L, N + 1, rp.half, tid, nthr);
+    const bool inZ = fft_batch<-1, WIDE>(Z, X, L, rp.half.ls, rp.half, tid, nthr);
     return inZ ? Z : X;
 }
 
@@ -300,193 +424,239 @@ __device__ __forceinline__ double2 r2c_mode(const double2* Rl, int k, int N, con
     return make_double2(e.x + t.y, e.y - t.x);
 }
 
-constexpr int RB = 8;  // rows per block of the generic row kernels
 
+// item = (job, chunk of RB rows)
 template <bool WIDE>
-__global__ void __launch_bounds__(256, WIDE ? 2 : 3) k_row_c2r(RowJobList jobs, RowArgs a) {
+__global__ void __launch_bounds__(256, 2) k_row_c2r(RowJobList jobs, RowArgs a) {
     extern __shared__ double2 smem[];
-    const RowIO job = jobs.j[blockIdx.y];
-    const int N = a.nxl / 2, LS = N + 1;
+    const int N = a.nxl / 2, LS = a.rp.half.ls;
     const int nrows = a.nyl * a.nzp;
-    const int row0 = blockIdx.x * RB;
-    const int L = min(RB, nrows - row0);
-    double2* X = smem;
-    double2* Z = smem + RB * LS;
+    const int nrc = (nrows + RB - 1) / RB;
+    const int nitems = jobs.n * nrc;
+    double2* Buf[2] = {smem, smem + RB * LS};
+    double2* Z = smem + 2 * RB * LS;
     const int tid = threadIdx.x;
-    for (int idx = tid; idx < L * LS; idx += blockDim.x) {
-        const int l = idx / LS, k = idx - l * LS;
-        double2 v = make_double2(0.0, 0.0);
-        if (k < a.kxc) {
-            v = *reinterpret_cast<const double2*>(job.yin + (long long)(row0 + l) * 2 * a.kxc + 2 * k);
+    auto issue = [&](int item, double2* X) {
+        const int rc = item % nrc, jb = item / nrc;
+        const int row0 = rc * RB, L = min(RB, nrows - row0);
+        const double* yin = jobs.j[jb].yin;
+        for (int idx = tid; idx < L * (N + 1); idx += 256) {
+            const int l = idx / (N + 1), k = idx - l * (N + 1);
+            double2* d = &X[l * LS + k];
+            if (k < a.kxc) cpa16(d, yin + (long long)(row0 + l) * 2 * a.kxc + 2 * k);
+            else *d = make_double2(0.0, 0.0);
+        }
+        cpa_commit();
+    };
+    int cur = 0;
+    int item = blockIdx.x;
+    if (item < nitems) issue(item, Buf[0]);
+    for (; item < nitems; item += gridDim.x) {
+        const int rc = item % nrc, jb = item / nrc;
+        const RowIO job = jobs.j[jb];
+        const int row0 = rc * RB, L = min(RB, nrows - row0);
+        double2* X = Buf[cur];
+        cpa_wait_all();
+        __syncthreads();
+        for (int idx = tid; idx < L * a.kxc; idx += 256) {
+            const int l = idx / a.kxc, k = idx - l * a.kxc;
+            double2 v = X[l * LS + k];
             if (job.mode == YM_IKX) {
                 const double kk = a.wavx[2 * k];
                 v = make_double2(-kk * v.y, kk * v.x);
             }
+            if (k == 0) v.y = 0.0;  // FFTW c2r ignores Im of the DC input
+            X[l * LS + k] = v;
         }
-        if (k == 0) v.y = 0.0;  // FFTW c2r ignores Im of the DC input
-        X[idx] = v;
-    }
-    __syncthreads();
-    const double2* R = rows_c2r<WIDE>(X, Z, L, a.rp, tid, blockDim.x);
-    for (int idx = tid; idx < L * N; idx += blockDim.x) {
-        const int l = idx / N, k = idx - l * N;
-        double2 v = R[l * LS + k];
-        if (job.mean != nullptr && job.add_mean != 0.0) {
-            const double m = job.mean[(row0 + l) / a.nyl] * job.add_mean;
-            v.x += m;
-            v.y += m;
+        __syncthreads();
+        const int next = item + gridDim.x;
+        if (next < nitems) issue(next, Buf[cur ^ 1]);
+        const double2* R = rows_c2r<WIDE>(X, Z, L, a.rp, tid, 256);
+        for (int idx = tid; idx < L * N; idx += 256) {
+            const int l = idx / N, k = idx - l * N;
+            double2 v = R[l * LS + k];
+            if (job.mean != nullptr && job.add_mean != 0.0) {
+                const double m = job.mean[(row0 + l) / a.nyl] * job.add_mean;
+                v.x += m;
+                v.y += m;
+            }
+            reinterpret_cast<double2*>(job.out + (long long)(row0 + l) * a.row_pitch)[k] = v;
         }
-        reinterpret_cast<double2*>(job.out + (long long)(row0 + l) * a.row_pitch)[k] = v;
+        __syncthreads();
+        cur ^= 1;
     }
 }
 
 template <bool WIDE>
-__global__ void __launch_bounds__(256, WIDE ? 2 : 3) k_row_r2c(RowJobList jobs, RowArgs a) {
+__global__ void __launch_bounds__(256, 2) k_row_r2c(RowJobList jobs, RowArgs a) {
     extern __shared__ double2 smem[];
-    const RowIO job = jobs.j[blockIdx.y];
-    const int N = a.nxl / 2, LS = N + 1;
+    const int N = a.nxl / 2, LS = a.rp.half.ls;
     const int nrows = a.nyl * a.nzp;
-    const int row0 = blockIdx.x * RB;
-    const int L = min(RB, nrows - row0);
-    double2* Z = smem;
-    double2* X = smem + RB * LS;
+    const int nrc = (nrows + RB - 1) / RB;
+    const int nitems = jobs.n * nrc;
+    double2* Buf[2] = {smem, smem + RB * LS};
+    double2* X = smem + 2 * RB * LS;
     const int tid = threadIdx.x;
-    for (int idx = tid; idx < L * N; idx += blockDim.x) {
-        const int l = idx / N, k = idx - l * N;
-        Z[l * LS + k] = reinterpret_cast<const double2*>(job.yin + (long long)(row0 + l) * a.row_pitch)[k];
-    }
-    __syncthreads();
-    const double2* R = rows_r2c<WIDE>(Z, X, L, a.rp, tid, blockDim.x);
-    for (int idx = tid; idx < L * a.kxc; idx += blockDim.x) {
-        const int l = idx / a.kxc, k = idx - l * a.kxc;
-        *reinterpret_cast<double2*>(job.out + (long long)(row0 + l) * 2 * a.kxc + 2 * k) =
-            r2c_mode(R + l * LS, k, N, a.rp.twr);
+    auto issue = [&](int item, double2* Z) {
+        const int rc = item % nrc, jb = item / nrc;
+        const int row0 = rc * RB, L = min(RB, nrows - row0);
+        const double* in = jobs.j[jb].yin;
+        for (int idx = tid; idx < L * N; idx += 256) {
+            const int l = idx / N, k = idx - l * N;
+            cpa16(&Z[l * LS + k], in + (long long)(row0 + l) * a.row_pitch + 2 * k);
+        }
+        cpa_commit();
+    };
+    int cur = 0;
+    int item = blockIdx.x;
+    if (item < nitems) issue(item, Buf[0]);
+    for (; item < nitems; item += gridDim.x) {
+        const int rc = item % nrc, jb = item / nrc;
+        const RowIO job = jobs.j[jb];
+        const int row0 = rc * RB, L = min(RB, nrows - row0);
+        double2* Z = Buf[cur];
+        cpa_wait_all();
+        __syncthreads();
+        const int next = item + gridDim.x;
+        if (next < nitems) issue(next, Buf[cur ^ 1]);
+        const double2* R = rows_r2c<WIDE>(Z, X, L, a.rp, tid, 256);
+        for (int idx = tid; idx < L * a.kxc; idx += 256) {
+            const int l = idx / a.kxc, k = idx - l * a.kxc;
+            *reinterpret_cast<double2*>(job.out + (long long)(row0 + l) * 2 * a.kxc + 2 * k) =
+                r2c_mode(R + l * LS, k, N, a.rp.twr);
+        }
+        __syncthreads();
+        cur ^= 1;
     }
 }
 
-static size_t rows_smem(int nxl) { return (size_t)2 * RB * (nxl / 2 + 1) * sizeof(double2); }
-
 void launch_row_c2r(const RowJobList& jobs, const RowArgs& a, cudaStream_t s) {
     if (jobs.n <= 0) return;
-    const int rows = a.nyl * a.nzp;
-    dim3 grid((rows + RB - 1) / RB, jobs.n);
-    static bool attr = false;
-    if (!attr) {
-        smem_attr(k_row_c2r<true>);
-        smem_attr(k_row_c2r<false>);
-        attr = true;
-    }
-    if (wide(a.rp.half)) k_row_c2r<true><<<grid, 256, rows_smem(a.nxl), s>>>(jobs, a);
-    else k_row_c2r<false><<<grid, 256, rows_smem(a.nxl), s>>>(jobs, a);
+    if (launch_row_c2r_warp(jobs, a, s)) return;
+    const int nitems = jobs.n * ((a.nyl * a.nzp + RB - 1) / RB);
+    const size_t sm = (size_t)3 * RB * a.rp.half.ls * sizeof(double2);
+    if (wide(a.rp.half)) k_row_c2r<true><<<persistent_grid(k_row_c2r<true>, sm, nitems), 256, sm, s>>>(jobs, a);
+    else k_row_c2r<false><<<persistent_grid(k_row_c2r<false>, sm, nitems), 256, sm, s>>>(jobs, a);
 }
 
 void launch_row_r2c(const RowJobList& jobs, const RowArgs& a, cudaStream_t s) {
     if (jobs.n <= 0) return;
-    const int rows = a.nyl * a.nzp;
-    dim3 grid((rows + RB - 1) / RB, jobs.n);
-    static bool attr = false;
-    if (!attr) {
-        smem_attr(k_row_r2c<true>);
-        smem_attr(k_row_r2c<false>);
-        attr = true;
-    }
-    if (wide(a.rp.half)) k_row_r2c<true><<<grid, 256, rows_smem(a.nxl), s>>>(jobs, a);
-    else k_row_r2c<false><<<grid, 256, rows_smem(a.nxl), s>>>(jobs, a);
+    if (launch_row_r2c_warp(jobs, a, s)) return;
+    const int nitems = jobs.n * ((a.nyl * a.nzp + RB - 1) / RB);
+    const size_t sm = (size_t)3 * RB * a.rp.half.ls * sizeof(double2);
+    if (wide(a.rp.half)) k_row_r2c<true><<<persistent_grid(k_row_r2c<true>, sm, nitems), 256, sm, s>>>(jobs, a);
+    else k_row_r2c<false><<<persistent_grid(k_row_r2c<false>, sm, nitems), 256, sm, s>>>(jobs, a);
 }
 
 // ----------------------------------------------------------------------------- NL row
-// One (z, y) row per block: 12 c2r (u, du/dx, du/dy, du/dz for 3 components), the
+// One (z, y) row per work item: 12 c2r (u, du/dx, du/dy, du/dz for 3 components), the
 // skew-symmetric products of nlterm_skewsym (src/navierstokes.f90:725-769), and 9 r2c.
 template <bool WIDE>
-__global__ void __launch_bounds__(256, WIDE ? 2 : 3) k_row_nl(NlRowArgs a) {
+__global__ void __launch_bounds__(256, 2) k_row_nl(NlRowArgs a) {
     extern __shared__ double2 smem[];
     const RowArgs& r = a.r;
-    const int N = r.nxl / 2, LS = N + 1;
-    const int yl = blockIdx.x, z = blockIdx.y;
-    const long long row = (long long)z * r.nyl + yl;
+    const int N = r.nxl / 2, LS = r.rp.half.ls;
+    const int nitems = r.nyl * r.nzp;
+    double2* Buf[2] = {smem, smem + 12 * LS};
+    double2* Z = smem + 24 * LS;
     const int tid = threadIdx.x;
-    double2* X = smem;            // 12 lines
-    double2* Z = smem + 12 * LS;  // 12 lines
-    // inputs: 0..2 u_l, 3..5 du_l/dx, 6..8 du_l/dy, 9..11 du_l/dz
-    for (int idx = tid; idx < 12 * LS; idx += blockDim.x) {
-        const int f = idx / LS, k = idx - f * LS;
-        const int l = f % 3, kind = f / 3;
-        double2 v = make_double2(0.0, 0.0);
-        if (k < r.kxc) {
-            const double* src = (kind == 0 || kind == 1) ? a.U[l] : (kind == 2 ? a.DY[l] : a.DZ[l]);
-            v = *reinterpret_cast<const double2*>(src + row * 2 * r.kxc + 2 * k);
-            if (kind == 1) {
+    // lines: 0..2 u_l, 3..5 u_l (-> du_l/dx), 6..8 du_l/dy, 9..11 du_l/dz
+    auto issue = [&](int row, double2* X) {
+        for (int idx = tid; idx < 12 * (N + 1); idx += 256) {
+            const int f = idx / (N + 1), k = idx - f * (N + 1);
+            const int l = f % 3, kind = f / 3;
+            double2* d = &X[f * LS + k];
+            if (k < r.kxc) {
+                const double* src = (kind <= 1) ? a.U[l] : (kind == 2 ? a.DY[l] : a.DZ[l]);
+                cpa16(d, src + (long long)row * 2 * r.kxc + 2 * k);
+            } else {
+                *d = make_double2(0.0, 0.0);
+            }
+        }
+        cpa_commit();
+    };
+    int cur = 0;
+    int row = blockIdx.x;
+    if (row < nitems) issue(row, Buf[0]);
+    for (; row < nitems; row += gridDim.x) {
+        const int z = row / r.nyl;
+        double2* X = Buf[cur];
+        cpa_wait_all();
+        __syncthreads();
+        for (int idx = tid; idx < 12 * r.kxc; idx += 256) {
+            const int f = idx / r.kxc, k = idx - f * r.kxc;
+            double2 v = X[f * LS + k];
+            if (f >= 3 && f < 6) {
                 const double kk = r.wavx[2 * k];
                 v = make_double2(-kk * v.y, kk * v.x);
             }
+            if (k == 0) v.y = 0.0;
+            X[f * LS + k] = v;
         }
-        if (k == 0) v.y = 0.0;
-        X[idx] = v;
-    }
-    __syncthreads();
-    double2* R = rows_c2r<WIDE>(X, Z, 12, r.rp, tid, blockDim.x);
-    double2* O = (R == Z) ? X : Z;
-    const double* p = reinterpret_cast<const double*>(R);
-    double* q = reinterpret_cast<double*>(O);
-    const int n = r.nxl, L2 = 2 * LS;
-    const double ub = a.ubar[z], ubp = a.ubarp[z];
-    for (int x = tid; x < n; x += blockDim.x) {
-        double u[3], g[3][3];
+        __syncthreads();
+        const int next = row + gridDim.x;
+        if (next < nitems) issue(next, Buf[cur ^ 1]);
+        double2* R = rows_c2r<WIDE>(X, Z, 12, r.rp, tid, 256);
+        double2* O = (R == Z) ? X : Z;
+        const double* p = reinterpret_cast<const double*>(R);
+        double* q = reinterpret_cast<double*>(O);
+        const int n = r.nxl, L2 = 2 * LS;
+        const double ub = a.ubar[z], ubp = a.ubarp[z];
+        for (int x = tid; x < n; x += 256) {
+            double u[3], g[3][3];
 #pragma unroll
-        for (int l = 0; l < 3; ++l) {
-            u[l] = p[(0 + l) * L2 + x];
-            g[l][0] = p[(3 + l) * L2 + x];
-            g[l][1] = p[(6 + l) * L2 + x];
-            g[l][2] = p[(9 + l) * L2 + x];
-        }
-        u[0] += ub;
-        g[0][2] += ubp;
-        double nl[3];
+            for (int l = 0; l < 3; ++l) {
+                u[l] = p[(0 + l) * L2 + x];
+                g[l][0] = p[(3 + l) * L2 + x];
+                g[l][1] = p[(6 + l) * L2 + x];
+                g[l][2] = p[(9 + l) * L2 + x];
+            }
+            u[0] += ub;
+            g[0][2] += ubp;
+            double nl[3];
 #pragma unroll
-        for (int l = 0; l < 3; ++l) {
-            double acc = 0.0;
-            acc = acc - 0.5 * (u[0] * g[l][0]);
-            acc = acc - 0.5 * (u[1] * g[l][1]);
-            acc = acc - 0.5 * (u[2] * g[l][2]);
-            nl[l] = acc;
+            for (int l = 0; l < 3; ++l) {
+                double acc = 0.0;
+                acc = acc - 0.5 * (u[0] * g[l][0]);
+                acc = acc - 0.5 * (u[1] * g[l][1]);
+                acc = acc - 0.5 * (u[2] * g[l][2]);
+                nl[l] = acc;
+            }
+            if (a.lamx != nullptr) {
+                const double lx = a.lamx[x];
+                nl[0] = nl[0] + lx * (ub - u[0]);
+                nl[1] = nl[1] + lx * (0.0 - u[1]);
+                nl[2] = nl[2] + lx * (0.0 - u[2]);
+            }
+            q[0 * L2 + x] = nl[0];
+            q[1 * L2 + x] = nl[1];
+            q[2 * L2 + x] = nl[2];
+            q[3 * L2 + x] = 0.5 * (u[0] * u[0]);
+            q[4 * L2 + x] = 0.5 * (u[0] * u[1]);
+            q[5 * L2 + x] = 0.5 * (u[0] * u[2]);
+            q[6 * L2 + x] = 0.5 * (u[1] * u[1]);
+            q[7 * L2 + x] = 0.5 * (u[1] * u[2]);
+            q[8 * L2 + x] = 0.5 * (u[2] * u[2]);
         }
-        if (a.lamx != nullptr) {
-            const double lx = a.lamx[x];
-            nl[0] = nl[0] + lx * (ub - u[0]);
-            nl[1] = nl[1] + lx * (0.0 - u[1]);
-            nl[2] = nl[2] + lx * (0.0 - u[2]);
+        __syncthreads();
+        const double2* R2 = rows_r2c<WIDE>(O, R, 9, r.rp, tid, 256);
+        for (int idx = tid; idx < 9 * r.kxc; idx += 256) {
+            const int f = idx / r.kxc, k = idx - f * r.kxc;
+            double* dst = (f < 3) ? a.N[f] : a.H[f - 3];
+            *reinterpret_cast<double2*>(dst + (long long)row * 2 * r.kxc + 2 * k) =
+                r2c_mode(R2 + f * LS, k, N, r.rp.twr);
         }
-        q[0 * L2 + x] = nl[0];
-        q[1 * L2 + x] = nl[1];
-        q[2 * L2 + x] = nl[2];
-        q[3 * L2 + x] = 0.5 * (u[0] * u[0]);
-        q[4 * L2 + x] = 0.5 * (u[0] * u[1]);
-        q[5 * L2 + x] = 0.5 * (u[0] * u[2]);
-        q[6 * L2 + x] = 0.5 * (u[1] * u[1]);
-        q[7 * L2 + x] = 0.5 * (u[1] * u[2]);
-        q[8 * L2 + x] = 0.5 * (u[2] * u[2]);
-    }
-    __syncthreads();
-    const double2* R2 = rows_r2c<WIDE>(O, R, 9, r.rp, tid, blockDim.x);
-    for (int idx = tid; idx < 9 * r.kxc; idx += blockDim.x) {
-        const int f = idx / r.kxc, k = idx - f * r.kxc;
-        double* dst = (f < 3) ? a.N[f] : a.H[f - 3];
-        *reinterpret_cast<double2*>(dst + row * 2 * r.kxc + 2 * k) = r2c_mode(R2 + f * LS, k, N, r.rp.twr);
+        __syncthreads();
+        cur ^= 1;
     }
 }
 
 void launch_row_nl(const NlRowArgs& a, cudaStream_t s) {
-    const int N = a.r.nxl / 2;
-    size_t sm = (size_t)24 * (N + 1) * sizeof(double2);
-    static bool attr = false;
-    if (!attr) {
-        smem_attr(k_row_nl<true>);
-        smem_attr(k_row_nl<false>);
-        attr = true;
-    }
-    dim3 grid(a.r.nyl, a.r.nzp);
-    if (wide(a.r.rp.half)) k_row_nl<true><<<grid, 256, sm, s>>>(a);
-    else k_row_nl<false><<<grid, 256, sm, s>>>(a);
+    if (launch_row_nl_warp(a, s)) return;
+    const size_t sm = (size_t)36 * a.r.rp.half.ls * sizeof(double2);
+    const int nitems = a.r.nyl * a.r.nzp;
+    if (wide(a.r.rp.half)) k_row_nl<true><<<persistent_grid(k_row_nl<true>, sm, nitems), 256, sm, s>>>(a);
+    else k_row_nl<false><<<persistent_grid(k_row_nl<false>, sm, nitems), 256, sm, s>>>(a);
 }
 
 }  // namespace lsb

@@ -1,0 +1,591 @@
+// Warp-group register FFTs for the horizontal transforms (horfft, src/horfft.f90:61-150,
+// and the padded passes of dealiasing_2d_fftw, src/dealiasing.f90:262-447).
+//
+// A line of N = G*R complex values is held by a group of G lanes (G a power of two <= 32),
+// lane g holding the R elements n = g + G*r.  The transform is the four-step split
+// N = R x G: an R-point DFT in registers, the twiddles exp(-+2 pi i g k1 / N), then a
+// G-point decimation-in-frequency network across the group's lanes with shfl_xor.  Lane g
+// ends with X[k1 + R*bitrev(g)] in register k1.  Shared memory is only used to turn the
+// strided/bit-reversed orders into coalesced global accesses; there is no block barrier
+// inside a transform.  Lengths whose R is not in {1,2,3,4,6,8} use fft_kernels.cu.
+#include "lsb_fftdev.cuh"
+#include "lsb_internal.cuh"
+
+namespace lsb {
+namespace {
+
+constexpr int WKC = 16;  // kx columns per spanwise work item
+
+__device__ __forceinline__ int brev(int g, int lgg) {
+    return lgg ? (int)(__brev((unsigned)g) >> (32 - lgg)) : 0;
+}
+
+template <int R, int SIGN>
+__device__ __forceinline__ void wfft(double2 (&v)[R], int G, int g, const double2* __restrict__ tw) {
+    dft_reg<R, SIGN>(v);
+    if (R > 1 && g != 0) {
+#pragma unroll
+        for (int k1 = 1; k1 < R; ++k1) {
+            double2 w = __ldg(&tw[g * k1]);
+            if (SIGN > 0) w.y = -w.y;
+            v[k1] = cmul(v[k1], w);
+        }
+    }
+    int st = R;  // N / (2h) for 2h = G
+    for (int h = G >> 1; h >= 1; h >>= 1) {
+        const int j = g & (h - 1);
+        const bool up = (g & h) != 0;
+        double2 w = __ldg(&tw[j * st]);
+        if (SIGN > 0) w.y = -w.y;
+#pragma unroll
+        for (int k1 = 0; k1 < R; ++k1) {
+            double2 o;
+            o.x = __shfl_xor_sync(0xffffffffu, v[k1].x, h);
+            o.y = __shfl_xor_sync(0xffffffffu, v[k1].y, h);
+            v[k1] = up ? cmul(csub(o, v[k1]), w) : cadd(v[k1], o);
+        }
+        st <<= 1;
+    }
+}
+
+// Inverse of the order produced by wfft: input "slot" layout (lane g' register k1 holds
+// z[k1 + R*bitrev(g')]), cross-lane decimation-in-time network, twiddles, R-point DFT in
+// registers; output in natural order (lane g register r holds X[g + G*r]).
+template <int R, int SIGN>
+__device__ __forceinline__ void wfft_dit(double2 (&v)[R], int G, int g, const double2* __restrict__ tw) {
+    int st = R * (G >> 1);  // N / (2h) for h = 1
+    for (int h = 1; h < G; h <<= 1) {
+        const int j = g & (h - 1);
+        const bool up = (g & h) != 0;
+        double2 w = __ldg(&tw[j * st]);
+        if (SIGN > 0) w.y = -w.y;
+#pragma unroll
+        for (int k1 = 0; k1 < R; ++k1) {
+            double2 o;
+            o.x = __shfl_xor_sync(0xffffffffu, v[k1].x, h);
+            o.y = __shfl_xor_sync(0xffffffffu, v[k1].y, h);
+            v[k1] = up ? csub(o, cmul(w, v[k1])) : cadd(v[k1], cmul(w, o));
+        }
+        st >>= 1;
+    }
+    if (R > 1 && g != 0) {
+#pragma unroll
+        for (int k1 = 1; k1 < R; ++k1) {
+            double2 w = __ldg(&tw[g * k1]);
+            if (SIGN > 0) w.y = -w.y;
+            v[k1] = cmul(v[k1], w);
+        }
+    }
+    dft_reg<R, SIGN>(v);
+}
+
+// lane g of a group receives the registers of lane bitrev(g): after wfft, lane g then
+// holds X[k1 + R*g] (R consecutive outputs)
+template <int R>
+__device__ __forceinline__ void lane_bitrev(double2 (&v)[R], int G, int lane, int g, int lgg) {
+    const int src = (lane & ~(G - 1)) | brev(g, lgg);
+#pragma unroll
+    for (int k1 = 0; k1 < R; ++k1) {
+        v[k1].x = __shfl_sync(0xffffffffu, v[k1].x, src);
+        v[k1].y = __shfl_sync(0xffffffffu, v[k1].y, src);
+    }
+}
+
+__device__ __forceinline__ void cpa16(void* sdst, const void* gsrc) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc));
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cpa_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
+
+__device__ __forceinline__ int pad_row_w(int j, int ny, int nyl, int layout) {
+    if (layout == 0 || nyl == ny) return j;
+    return (j < ny / 2) ? j : j + (nyl - ny);
+}
+// inverse of pad_row_w: padded row -> input row, or -1 for a zero-pad row
+__device__ __forceinline__ int unpad_row(int n, int ny, int nyl, int layout) {
+    if (layout == 0 || nyl == ny) return n < ny ? n : -1;
+    if (n < ny / 2) return n;
+    if (n >= nyl - (ny - ny / 2)) return n - (nyl - ny);
+    return -1;
+}
+
+// ----------------------------------------------------------------------------- spanwise
+// One kernel for both directions.  Work item = (job, z, chunk of WKC kx columns); the tile
+// [nyl][WKC+1] is staged with cp.async (double-buffered), each column is transformed by a
+// lane group, and the tile is written back in coalesced rows.
+template <int R, bool INV>
+__global__ void __launch_bounds__(256) k_ywarp(YInvJobList ij, YFwdJobList fj, YPassArgs a, int nch) {
+    extern __shared__ double2 smem[];
+    const int ny = a.ny, nyl = a.nyl, G = a.plan.g, lgg = a.plan.lgg;
+    constexpr int TS = WKC + 1;  // tile row stride (complex)
+    double2* Buf[2] = {smem, smem + nyl * TS};
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int njobs = INV ? ij.n : fj.n;
+    const int nitems = njobs * a.nzp * nch;
+    const int lpw = 32 / G;              // lines per warp per pass
+    const int q = lane / G, g = lane - q * G;
+    auto issue = [&](int item, double2* T) {
+        const int ch = item % nch, rest = item / nch, z = rest % a.nzp, jb = rest / a.nzp;
+        const int c0 = ch * WKC;
+        if (INV) {
+            const double* in = ij.j[jb].in;
+            for (int idx = tid; idx < ny * WKC; idx += 256) {
+                const int j = idx / WKC, cc = idx - j * WKC, c = c0 + cc;
+                double2* d = &T[pad_row_w(j, ny, nyl, a.layout) * TS + cc];
+                if (c < a.kxc) cpa16(d, in + ((long long)z * ny + j) * a.nx + 2 * c);
+                else *d = make_double2(0.0, 0.0);
+            }
+            const int npad = nyl - ny;
+            for (int idx = tid; idx < npad * WKC; idx += 256) {
+                const int r = idx / WKC, cc = idx - r * WKC;
+                const int jl = (a.layout == 0 || nyl == ny) ? ny + r : ny / 2 + r;
+                T[jl * TS + cc] = make_double2(0.0, 0.0);
+            }
+        } else {
+            const double* in = fj.j[jb].in;
+            for (int idx = tid; idx < nyl * WKC; idx += 256) {
+                const int jl = idx / WKC, cc = idx - jl * WKC, c = c0 + cc;
+                double2* d = &T[jl * TS + cc];
+                if (c < a.kxc) cpa16(d, in + ((long long)z * nyl + jl) * a.nx + 2 * c);
+                else *d = make_double2(0.0, 0.0);
+            }
+        }
+        cpa_commit();
+    };
+    int cur = 0;
+    int item = blockIdx.x;
+    if (item < nitems) issue(item, Buf[0]);
+    for (; item < nitems; item += gridDim.x) {
+        const int ch = item % nch, rest = item / nch, z = rest % a.nzp, jb = rest / a.nzp;
+        const int c0 = ch * WKC;
+        double2* T = Buf[cur];
+        cpa_wait_all();
+        __syncthreads();
+        const int next = item + gridDim.x;
+        if (next < nitems) issue(next, Buf[cur ^ 1]);
+        const int mode = INV ? ij.j[jb].mode : YM_COPY;
+        for (int L0 = warp * lpw; L0 < WKC; L0 += 8 * lpw) {
+            const int L = L0 + q;
+            const bool act = L < WKC;
+            const int Lc = act ? L : 0;
+            double2 v[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int n = g + G * r;
+                double2 x = T[n * TS + Lc];
+                if (INV && mode != YM_COPY) {
+                    double k = 0.0;
+                    if (mode == YM_IKY) {
+                        const int j = unpad_row(n, ny, nyl, a.layout);
+                        k = (j >= 0) ? a.wavy[j] : 0.0;
+                    } else {
+                        const int c = min(c0 + Lc, a.kxc - 1);
+                        k = a.wavx[2 * c];
+                    }
+                    x = make_double2(-k * x.y, k * x.x);
+                }
+                v[r] = x;
+            }
+            wfft<R, INV ? +1 : -1>(v, G, g, a.plan.tw);
+            lane_bitrev<R>(v, G, lane, g, lgg);
+            if (act) {
+#pragma unroll
+                for (int k1 = 0; k1 < R; ++k1) T[(R * g + k1) * TS + L] = v[k1];
+            }
+        }
+        __syncthreads();
+        if (INV) {
+            double* out = ij.j[jb].out;
+            for (int idx = tid; idx < nyl * WKC; idx += 256) {
+                const int jl = idx / WKC, cc = idx - jl * WKC, c = c0 + cc;
+                if (c >= a.kxc) continue;
+                *reinterpret_cast<double2*>(out + ((long long)z * nyl + jl) * a.nx + 2 * c) = T[jl * TS + cc];
+            }
+        } else {
+            const YFwdJob job = fj.j[jb];
+            for (int idx = tid; idx < ny * WKC; idx += 256) {
+                const int j = idx / WKC, cc = idx - j * WKC, c = c0 + cc;
+                if (c >= a.kxc) continue;
+                double2 v = T[pad_row_w(j, ny, nyl, a.layout) * TS + cc];
+                if (job.sym && c == 0) {
+                    const int jm = (ny - j) % ny;
+                    const double2 w = T[pad_row_w(jm, ny, nyl, a.layout) * TS + cc];
+                    v = make_double2(0.5 * (v.x + w.x), 0.5 * (v.y - w.y));
+                }
+                v.x *= a.scale;
+                v.y *= a.scale;
+                double2* o = reinterpret_cast<double2*>(job.out + ((long long)z * ny + j) * a.nx + 2 * c);
+                double2 rr;
+                if (job.beta != 0.0) {
+                    const double2 old = *o;
+                    rr = make_double2(fma(job.alpha, v.x, job.beta * old.x), fma(job.alpha, v.y, job.beta * old.y));
+                } else {
+                    rr = make_double2(job.alpha * v.x, job.alpha * v.y);
+                }
+                *o = rr;
+            }
+        }
+        __syncthreads();
+        cur ^= 1;
+    }
+}
+
+// ----------------------------------------------------------------------------- rows
+// c2r of the modes in X (N+1 entries; zero beyond kxc, DC imaginary part dropped) into
+// registers: lane g returns z[k1 + R*bitrev(g)] in v[k1] (z = x[2m] + i x[2m+1]).
+template <int R>
+__device__ __forceinline__ void row_c2r_regs(const double2* X, int N, int G, int g, const RealPlan& rp,
+                                             double2 (&v)[R]) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int n = g + G * r;
+        const double2 xa = X[n];
+        const double2 xb = cconj(X[N - n]);
+        const double2 e = cadd(xa, xb);
+        const double2 o = cmul(csub(xa, xb), cconj(__ldg(&rp.twr[n])));
+        v[r] = make_double2(e.x - o.y, e.y + o.x);
+    }
+    wfft<R, +1>(v, G, g, rp.half.tw);
+}
+
+__device__ __forceinline__ double2 r2c_mode_w(const double2* Z, int k, int N, const double2* __restrict__ twr) {
+    const double2 za = Z[k];
+    const double2 zb = cconj(Z[k == 0 ? 0 : N - k]);
+    const double2 e = make_double2(0.5 * (za.x + zb.x), 0.5 * (za.y + zb.y));
+    const double2 o = make_double2(0.5 * (za.x - zb.x), 0.5 * (za.y - zb.y));
+    const double2 t = cmul(__ldg(&twr[k]), o);
+    return make_double2(e.x + t.y, e.y - t.x);
+}
+
+// Generic row transforms: each lane group of each warp owns one row at a time.
+template <int R>
+__global__ void __launch_bounds__(256) k_row_c2r_w(RowJobList jobs, RowArgs a) {
+    extern __shared__ double2 smem[];
+    const int N = a.nxl / 2, G = a.rp.half.g, lgg = a.rp.half.lgg;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int lpw = 32 / G, q = lane / G, g = lane - q * G;
+    double2* X = smem + (warp * lpw + q) * (N + 1);
+    const int nrows = a.nyl * a.nzp;
+    const int nunits = jobs.n * nrows;
+    const int gw = blockIdx.x * 8 + warp, TW = gridDim.x * 8;
+    for (int u0 = gw * lpw; u0 < nunits; u0 += TW * lpw) {
+        const int u = u0 + q;
+        const bool act = u < nunits;
+        const int uc = act ? u : u0;
+        const int jb = uc / nrows, row = uc - jb * nrows;
+        const RowIO job = jobs.j[jb];
+        const double* yrow = job.yin + (long long)row * 2 * a.kxc;
+        double2 ld[R + 1];
+#pragma unroll
+        for (int it = 0; it <= R; ++it) {
+            const int k = g + G * it;
+            ld[it] = (k < a.kxc) ? *reinterpret_cast<const double2*>(yrow + 2 * k) : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int it = 0; it <= R; ++it) {
+            const int k = g + G * it;
+            if (k > N) break;
+            double2 v = ld[it];
+            if (job.mode == YM_IKX && k < a.kxc) {
+                const double kk = a.wavx[2 * k];
+                v = make_double2(-kk * v.y, kk * v.x);
+            }
+            if (k == 0) v.y = 0.0;
+            X[k] = v;
+        }
+        __syncwarp();
+        double2 v[R];
+        row_c2r_regs<R>(X, N, G, g, a.rp, v);
+        double m = 0.0;
+        if (job.mean != nullptr && job.add_mean != 0.0) m = job.mean[row / a.nyl] * job.add_mean;
+        lane_bitrev<R>(v, G, lane, g, lgg);
+        __syncwarp();
+#pragma unroll
+        for (int k1 = 0; k1 < R; ++k1) X[R * g + k1] = make_double2(v[k1].x + m, v[k1].y + m);
+        __syncwarp();
+        if (act) {
+            double2* o = reinterpret_cast<double2*>(job.out + (long long)row * a.row_pitch);
+            for (int k = g; k < N; k += G) o[k] = X[k];
+        }
+        __syncwarp();
+    }
+}
+
+template <int R>
+__global__ void __launch_bounds__(256) k_row_r2c_w(RowJobList jobs, RowArgs a) {
+    extern __shared__ double2 smem[];
+    const int N = a.nxl / 2, G = a.rp.half.g, lgg = a.rp.half.lgg;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int lpw = 32 / G, q = lane / G, g = lane - q * G;
+    double2* Z = smem + (warp * lpw + q) * (N + 1);
+    const int nrows = a.nyl * a.nzp;
+    const int nunits = jobs.n * nrows;
+    const int gw = blockIdx.x * 8 + warp, TW = gridDim.x * 8;
+    for (int u0 = gw * lpw; u0 < nunits; u0 += TW * lpw) {
+        const int u = u0 + q;
+        const bool act = u < nunits;
+        const int uc = act ? u : u0;
+        const int jb = uc / nrows, row = uc - jb * nrows;
+        const RowIO job = jobs.j[jb];
+        const double2* in = reinterpret_cast<const double2*>(job.yin + (long long)row * a.row_pitch);
+        double2 v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[r] = in[g + G * r];
+        wfft<R, -1>(v, G, g, a.rp.half.tw);
+        lane_bitrev<R>(v, G, lane, g, lgg);
+#pragma unroll
+        for (int k1 = 0; k1 < R; ++k1) Z[R * g + k1] = v[k1];
+        __syncwarp();
+        if (act) {
+            double* yrow = job.out + (long long)row * 2 * a.kxc;
+            for (int k = g; k < a.kxc; k += G)
+                *reinterpret_cast<double2*>(yrow + 2 * k) = r2c_mode_w(Z, k, N, a.rp.twr);
+        }
+        __syncwarp();
+    }
+}
+
+// The fused nonlinear-product row: 12 c2r (u_l, du_l/dx, du_l/dy, du_l/dz), the skew-
+// symmetric products and fringe of nlterm_skewsym (src/navierstokes.f90:725-769), 9 r2c.
+// A block owns one (z, y) row at a time; the 9 input rows of the next row are staged with
+// cp.async while the current one is transformed.
+template <int R>
+__global__ void __launch_bounds__(256, 2) k_row_nl_w(NlRowArgs a) {
+    extern __shared__ double2 smem[];
+    const RowArgs& r = a.r;
+    const int N = r.nxl / 2, G = r.rp.half.g, lgg = r.rp.half.lgg, K = r.kxc;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int lpw = 32 / G, q = lane / G, g = lane - q * G;
+    double2* Stg[2] = {smem, smem + 9 * K};   // staged rows: U0..2, DY0..2, DZ0..2
+    double2* P = smem + 18 * K;               // 12 physical rows of N complex (2N reals)
+    double2* W = P + 12 * N + (warp * lpw + q) * (N + 1);
+    const int nitems = r.nyl * r.nzp;
+    auto issue = [&](int row, double2* S) {
+        for (int idx = tid; idx < 9 * K; idx += 256) {
+            const int f = idx / K, k = idx - f * K;
+            const int l = f % 3, kind = f / 3;
+            const double* src = (kind == 0) ? a.U[l] : (kind == 1 ? a.DY[l] : a.DZ[l]);
+            cpa16(&S[idx], src + (long long)row * 2 * K + 2 * k);
+        }
+        cpa_commit();
+    };
+    int cur = 0;
+    int row = blockIdx.x;
+    if (row < nitems) issue(row, Stg[0]);
+    for (; row < nitems; row += gridDim.x) {
+        const int z = row / r.nyl;
+        const double2* S = Stg[cur];
+        cpa_wait_all();
+        __syncthreads();
+        const int next = row + gridDim.x;
+        if (next < nitems) issue(next, Stg[cur ^ 1]);
+        // 12 c2r: field f = 3*kind + l with kind 0 u, 1 du/dx (= i kx u), 2 du/dy, 3 du/dz
+        for (int f0 = warp * lpw; f0 < 12; f0 += 8 * lpw) {
+            const int f = f0 + q;
+            const bool act = f < 12;
+            const int fc = act ? f : f0;
+            const int l = fc % 3, kind = fc / 3;
+            const double2* Xs = S + (kind <= 1 ? l : 3 * (kind - 1) + l) * K;
+            double2 v[R];
+#pragma unroll
+            for (int rr = 0; rr < R; ++rr) {
+                const int n = g + G * rr;
+                double2 xa = (n < K) ? Xs[n] : make_double2(0.0, 0.0);
+                double2 xb = (N - n < K) ? Xs[N - n] : make_double2(0.0, 0.0);
+                if (kind == 1) {
+                    const double ka = (n < K) ? r.wavx[2 * n] : 0.0;
+                    const double kb = (N - n < K) ? r.wavx[2 * (N - n)] : 0.0;
+                    xa = make_double2(-ka * xa.y, ka * xa.x);
+                    xb = make_double2(-kb * xb.y, kb * xb.x);
+                }
+                if (n == 0) xa.y = 0.0;  // FFTW c2r ignores Im of the DC input
+                xb = cconj(xb);
+                const double2 e = cadd(xa, xb);
+                const double2 o = cmul(csub(xa, xb), cconj(__ldg(&r.rp.twr[n])));
+                v[rr] = make_double2(e.x - o.y, e.y + o.x);
+            }
+            wfft<R, +1>(v, G, g, r.rp.half.tw);
+            if (act) {
+                // slot layout: slot k1*G + g holds z[k1 + R*bitrev(g)] (conflict-free)
+#pragma unroll
+                for (int k1 = 0; k1 < R; ++k1) P[fc * N + k1 * G + g] = v[k1];
+            }
+        }
+        __syncthreads();
+        const double* p = reinterpret_cast<const double*>(P);
+        double* qo = reinterpret_cast<double*>(P);
+        const int n = r.nxl, L2 = 2 * N;
+        const double ub = a.ubar[z], ubp = a.ubarp[z];
+        for (int xs = tid; xs < n; xs += 256) {
+            // physical point of the slot value: complex slot s = xs/2 holds z[m], m = k1 + R*bitrev(g)
+            const int sl = xs >> 1, k1s = sl / G, gs = sl - k1s * G;
+            const int x = 2 * (k1s + R * brev(gs, lgg)) + (xs & 1);
+            double u[3], gr[3][3];
+#pragma unroll
+            for (int l = 0; l < 3; ++l) {
+                u[l] = p[(0 + l) * L2 + xs];
+                gr[l][0] = p[(3 + l) * L2 + xs];
+                gr[l][1] = p[(6 + l) * L2 + xs];
+                gr[l][2] = p[(9 + l) * L2 + xs];
+            }
+            u[0] += ub;
+            gr[0][2] += ubp;
+            double nl[3];
+#pragma unroll
+            for (int l = 0; l < 3; ++l) {
+                double acc = 0.0;
+                acc = acc - 0.5 * (u[0] * gr[l][0]);
+                acc = acc - 0.5 * (u[1] * gr[l][1]);
+                acc = acc - 0.5 * (u[2] * gr[l][2]);
+                nl[l] = acc;
+            }
+            if (a.lamx != nullptr) {
+                const double lx = a.lamx[x];
+                nl[0] = nl[0] + lx * (ub - u[0]);
+                nl[1] = nl[1] + lx * (0.0 - u[1]);
+                nl[2] = nl[2] + lx * (0.0 - u[2]);
+            }
+            qo[0 * L2 + xs] = nl[0];
+            qo[1 * L2 + xs] = nl[1];
+            qo[2 * L2 + xs] = nl[2];
+            qo[3 * L2 + xs] = 0.5 * (u[0] * u[0]);
+            qo[4 * L2 + xs] = 0.5 * (u[0] * u[1]);
+            qo[5 * L2 + xs] = 0.5 * (u[0] * u[2]);
+            qo[6 * L2 + xs] = 0.5 * (u[1] * u[1]);
+            qo[7 * L2 + xs] = 0.5 * (u[1] * u[2]);
+            qo[8 * L2 + xs] = 0.5 * (u[2] * u[2]);
+        }
+        __syncthreads();
+        for (int f0 = warp * lpw; f0 < 9; f0 += 8 * lpw) {
+            const int f = f0 + q;
+            const bool act = f < 9;
+            const int fc = act ? f : f0;
+            double2 v[R];
+#pragma unroll
+            for (int k1 = 0; k1 < R; ++k1) v[k1] = P[fc * N + k1 * G + g];
+            wfft_dit<R, -1>(v, G, g, r.rp.half.tw);
+            // natural order: lane g register rr holds Z[g + G*rr]
+#pragma unroll
+            for (int rr = 0; rr < R; ++rr) W[g + G * rr] = v[rr];
+            __syncwarp();
+            if (act) {
+                double* dst = (fc < 3) ? a.N[fc] : a.H[fc - 3];
+                double* yrow = dst + (long long)row * 2 * K;
+                for (int k = g; k < K; k += G)
+                    *reinterpret_cast<double2*>(yrow + 2 * k) = r2c_mode_w(W, k, N, r.rp.twr);
+            }
+            __syncwarp();
+        }
+        __syncthreads();
+        cur ^= 1;
+    }
+}
+
+template <class K>
+int persistent_grid_w(K kern, size_t smem, long long nitems) {
+    static int nsm = 0;
+    if (nsm == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        if (nsm <= 0) nsm = 148;
+    }
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 256, smem);
+    if (occ < 1) occ = 1;
+    const long long gsz = (long long)occ * nsm;
+    return (int)(gsz < nitems ? gsz : (nitems > 0 ? nitems : 1));
+}
+
+template <int R, bool INV>
+void ylaunch(const YInvJobList& ij, const YFwdJobList& fj, const YPassArgs& a, cudaStream_t s) {
+    const int nch = (a.kxc + WKC - 1) / WKC;
+    const int nitems = (INV ? ij.n : fj.n) * a.nzp * nch;
+    const size_t sm = (size_t)2 * a.nyl * (WKC + 1) * sizeof(double2);
+    k_ywarp<R, INV><<<persistent_grid_w(k_ywarp<R, INV>, sm, nitems), 256, sm, s>>>(ij, fj, a, nch);
+}
+
+template <bool INV>
+bool ydispatch(const YInvJobList& ij, const YFwdJobList& fj, const YPassArgs& a, cudaStream_t s) {
+    switch (a.plan.r) {
+        case 1: ylaunch<1, INV>(ij, fj, a, s); return true;
+        case 2: ylaunch<2, INV>(ij, fj, a, s); return true;
+        case 3: ylaunch<3, INV>(ij, fj, a, s); return true;
+        case 4: ylaunch<4, INV>(ij, fj, a, s); return true;
+        case 6: ylaunch<6, INV>(ij, fj, a, s); return true;
+        case 8: ylaunch<8, INV>(ij, fj, a, s); return true;
+        default: return false;
+    }
+}
+
+template <int R>
+void rowlaunch(const RowJobList& jobs, const RowArgs& a, cudaStream_t s, bool c2r) {
+    const int N = a.nxl / 2;
+    const size_t sm = (size_t)8 * 32 * (N + 1) * sizeof(double2) / a.rp.half.g;
+    const long long units = (long long)jobs.n * a.nyl * a.nzp;
+    const long long blocks = (units + 8 * 32 / a.rp.half.g - 1) / (8 * 32 / a.rp.half.g);
+    if (c2r) k_row_c2r_w<R><<<persistent_grid_w(k_row_c2r_w<R>, sm, blocks), 256, sm, s>>>(jobs, a);
+    else k_row_r2c_w<R><<<persistent_grid_w(k_row_r2c_w<R>, sm, blocks), 256, sm, s>>>(jobs, a);
+}
+
+bool rowdispatch(const RowJobList& jobs, const RowArgs& a, cudaStream_t s, bool c2r) {
+    switch (a.rp.half.r) {
+        case 1: rowlaunch<1>(jobs, a, s, c2r); return true;
+        case 2: rowlaunch<2>(jobs, a, s, c2r); return true;
+        case 3: rowlaunch<3>(jobs, a, s, c2r); return true;
+        case 4: rowlaunch<4>(jobs, a, s, c2r); return true;
+        case 6: rowlaunch<6>(jobs, a, s, c2r); return true;
+        case 8: rowlaunch<8>(jobs, a, s, c2r); return true;
+        default: return false;
+    }
+}
+
+template <int R>
+void nllaunch(const NlRowArgs& a, cudaStream_t s) {
+    const int N = a.r.nxl / 2;
+    const size_t sm =
+        ((size_t)18 * a.r.kxc + (size_t)12 * N + (size_t)8 * 32 / a.r.rp.half.g * (N + 1)) * sizeof(double2);
+    const int nitems = a.r.nyl * a.r.nzp;
+    k_row_nl_w<R><<<persistent_grid_w(k_row_nl_w<R>, sm, nitems), 256, sm, s>>>(a);
+}
+
+}  // namespace
+
+bool launch_yinv_warp(const YInvJobList& jobs, const YPassArgs& a, cudaStream_t s) {
+    if (a.plan.g == 0) return false;
+    YFwdJobList none{};
+    return ydispatch<true>(jobs, none, a, s);
+}
+
+bool launch_yfwd_warp(const YFwdJobList& jobs, const YPassArgs& a, cudaStream_t s) {
+    if (a.plan.g == 0) return false;
+    YInvJobList none{};
+    return ydispatch<false>(none, jobs, a, s);
+}
+
+bool launch_row_c2r_warp(const RowJobList& jobs, const RowArgs& a, cudaStream_t s) {
+    if (a.rp.half.g == 0) return false;
+    return rowdispatch(jobs, a, s, true);
+}
+
+bool launch_row_r2c_warp(const RowJobList& jobs, const RowArgs& a, cudaStream_t s) {
+    if (a.rp.half.g == 0) return false;
+    return rowdispatch(jobs, a, s, false);
+}
+
+bool launch_row_nl_warp(const NlRowArgs& a, cudaStream_t s) {
+    if (a.r.rp.half.g == 0) return false;
+    switch (a.r.rp.half.r) {
+        case 1: nllaunch<1>(a, s); return true;
+        case 2: nllaunch<2>(a, s); return true;
+        case 3: nllaunch<3>(a, s); return true;
+        case 4: nllaunch<4>(a, s); return true;
+        case 6: nllaunch<6>(a, s); return true;
+        case 8: nllaunch<8>(a, s); return true;
+        default: return false;
+    }
+}
+
+}  // namespace lsb

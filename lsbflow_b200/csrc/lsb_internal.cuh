@@ -35,6 +35,9 @@ struct FftPlan {
     FastDiv fdT[kMaxStages];
     FastDiv fdP[kMaxStages];
     const double2* tw = nullptr;   // device, n entries
+    int n1 = 0, n2 = 0;            // register two-pass split n = n1*n2 (n1 = 0: Stockham stages)
+    int g = 0, r = 0, lgg = 0;     // warp-group split n = g*r (g lanes, r registers; g = 0: none)
+    int ls = 0;                    // shared-memory line stride (complex) a kernel must use
 };
 
 // A real transform of length nr (even) done through a complex FFT of length nr/2.
@@ -115,6 +118,14 @@ struct NlRowArgs {
     const double* lamx;   // [nxl] fringe lambda(x) or nullptr (only on the unpadded grid)
 };
 void launch_row_nl(const NlRowArgs& a, cudaStream_t s);
+
+// warp-group register FFT variants (fft_warp.cu); they return false when the plan has no
+// warp split, in which case the block-batched kernels of fft_kernels.cu run instead
+bool launch_yinv_warp(const YInvJobList& jobs, const YPassArgs& a, cudaStream_t s);
+bool launch_yfwd_warp(const YFwdJobList& jobs, const YPassArgs& a, cudaStream_t s);
+bool launch_row_c2r_warp(const RowJobList& jobs, const RowArgs& a, cudaStream_t s);
+bool launch_row_r2c_warp(const RowJobList& jobs, const RowArgs& a, cudaStream_t s);
+bool launch_row_nl_warp(const NlRowArgs& a, cudaStream_t s);
 
 // ---------------------------------------------------------------- z contractions (gemm_kernels.cu)
 // out[f][r][c] = epi( sum_k A[r][k] * in[f][k + koff][c] ) for r < M (rows written at r + roff)

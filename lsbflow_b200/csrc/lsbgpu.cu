@@ -82,6 +82,39 @@ void make_plan(lsb_handle* h, int n, FftPlan& P) {
         tw[2 * m + 1] = (double)-sinl(a);
     }
     P.tw = (const double2*)h->upload(tw.data(), tw.size());
+    // register two-pass split: n = n1 * n2 with both factors in {1,2,3,4,6,8,12,16}
+    static const int pairs[][2] = {{2, 1},  {3, 1},  {4, 1},  {6, 1},  {8, 1},   {12, 1},  {16, 1},
+                                   {3, 3},  {6, 3},  {8, 3},  {8, 4},  {12, 3},  {8, 6},   {16, 3},
+                                   {8, 8},  {12, 6}, {12, 8}, {16, 6}, {12, 12}, {16, 8},  {16, 12},
+                                   {16, 16}};
+    P.n1 = P.n2 = 0;
+    for (auto& pr : pairs)
+        if (pr[0] * pr[1] == n) {
+            P.n1 = pr[0];
+            P.n2 = pr[1];
+            break;
+        }
+    int ls = n + 1;
+    if (P.n1 > 0 && P.n2 > 1) {
+        const int pb = (P.n2 % 2 == 0) ? P.n2 + 1 : P.n2;
+        ls = std::max(ls, P.n1 * pb);
+    }
+    if (ls % 2 == 0) ++ls;
+    P.ls = ls;
+    // warp-group split: g = largest power of two <= 32 dividing n, r = n / g in {1,2,3,4,6,8}
+    P.g = P.r = P.lgg = 0;
+    {
+        int gg = 1;
+        while (gg < 32 && n % (gg * 2) == 0) gg *= 2;
+        const int rr = n / gg;
+        if (rr == 1 || rr == 2 || rr == 3 || rr == 4 || rr == 6 || rr == 8) {
+            P.g = gg;
+            P.r = rr;
+            int lg = 0;
+            while ((1 << lg) < gg) ++lg;
+            P.lgg = lg;
+        }
+    }
 }
 
 void make_real_plan(lsb_handle* h, int nr, RealPlan& R) {

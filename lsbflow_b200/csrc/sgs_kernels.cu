@@ -61,28 +61,36 @@ __global__ void __launch_bounds__(256) k_filter3(FieldList fl, int nx, int ny, i
     const int i0 = blockIdx.x * FIB, j0 = blockIdx.y * FJB;
     const int k0 = zc * FZC, k1 = min(nzp, k0 + FZC);  // output planes [k0, k1)
     const int ks = max(0, k0 - 1), ke = min(nzp - 1, k1);
-    const double s = 2.0 * a + b;
+    const double rs = 1.0 / (2.0 * a + b);  // the reference divides by 2a+b; one rounding apart
     const int tid = threadIdx.x;
     const int jj = tid / FIB, ii = tid % FIB;  // this thread's output column (256 = FJB * FIB)
     const int jo = j0 + jj, io = i0 + ii;
     const bool mine = (jo < ny) && (io < nx);
+    // periodic source indices of the two tile elements this thread loads per plane
+    long long off[2];
+    bool ld[2];
+    for (int r = 0; r < 2; ++r) {
+        const int idx = tid + 256 * r;
+        ld[r] = idx < (FJB + 2) * (FIB + 2);
+        const int jr = idx / (FIB + 2), ir = idx % (FIB + 2);
+        int j = j0 + jr - 1, i = i0 + ir - 1;
+        j = ((j % ny) + ny) % ny;
+        i = ((i % nx) + nx) % nx;
+        off[r] = (long long)j * nx + i;
+    }
     double y0 = 0.0, y1 = 0.0, y2 = 0.0;  // y-filtered planes kk-2, kk-1, kk
+    double* tflat = &tile[0][0];
     for (int kk = ks; kk <= ke; ++kk) {
         const double* pl = q + (long long)kk * ny * nx;
-        for (int idx = tid; idx < (FJB + 2) * (FIB + 2); idx += 256) {
-            const int jr = idx / (FIB + 2), ir = idx % (FIB + 2);
-            int j = j0 + jr - 1, i = i0 + ir - 1;
-            j = (j % ny + ny) % ny;
-            i = (i % nx + nx) % nx;
-            tile[jr][ir] = pl[(long long)j * nx + i];
-        }
+        if (ld[0]) tflat[tid] = __ldg(pl + off[0]);
+        if (ld[1]) tflat[tid + 256] = __ldg(pl + off[1]);
         __syncthreads();
         for (int idx = tid; idx < (FJB + 2) * FIB; idx += 256) {
             const int jr = idx / FIB, ir = idx % FIB;
-            X[jr][ir] = (a * tile[jr][ir] + b * tile[jr][ir + 1] + a * tile[jr][ir + 2]) / s;
+            X[jr][ir] = (a * tile[jr][ir] + b * tile[jr][ir + 1] + a * tile[jr][ir + 2]) * rs;
         }
         __syncthreads();
-        const double yn = (a * X[jj][ii] + b * X[jj + 1][ii] + a * X[jj + 2][ii]) / s;
+        const double yn = (a * X[jj][ii] + b * X[jj + 1][ii] + a * X[jj + 2][ii]) * rs;
         y0 = y1;
         y1 = y2;
         y2 = yn;
@@ -91,7 +99,7 @@ __global__ void __launch_bounds__(256) k_filter3(FieldList fl, int nx, int ny, i
             if (ko >= k0 && ko < k1) {
                 double v;
                 if (ko == 0) v = y1;
-                else v = (az[ko] * y0 + bz[ko] * y1 + cz[ko] * y2) / s;
+                else v = (az[ko] * y0 + bz[ko] * y1 + cz[ko] * y2) * rs;
                 out[((long long)ko * ny + jo) * nx + io] = v;
             }
             if (kk == nzp - 1 && kk >= k0 && kk < k1) out[((long long)kk * ny + jo) * nx + io] = yn;

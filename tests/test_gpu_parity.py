@@ -115,6 +115,27 @@ def test_nlterm(over):
         assert rel(got[l], ref[l]) < TOL_OP, l
 
 
+@pytest.mark.parametrize("nx,ny,nz,layout", [(128, 32, 64, "correct"), (256, 64, 128, "correct"),
+                                              (256, 64, 128, "ref"), (128, 16, 32, "ref")])
+def test_nlterm_production_sizes(nx, ny, nz, layout):
+    # the full-warp transform paths: x half-lengths 96 / 192 (padded) and spanwise 48 / 96 / 24
+    st, s = solver(workload("les256", nx=nx, ny=ny, nz=nz, sgsflag=0, dealiasflag=1, dealias_layout=layout))
+    u, v, w = ic.seeded_noise(st, 12, 1e-2)
+    ref = O.nlterm_skewsym(st, [u, v, w])
+    got = s.nlterm(np.array([u, v, w]))
+    for l in range(3):
+        assert rel(got[l], ref[l]) < TOL_OP, (l, rel(got[l], ref[l]))
+
+
+@pytest.mark.parametrize("nx,ny,nz", [(128, 32, 64), (256, 64, 128), (64, 48, 16)])
+def test_horfft_production_sizes(nx, ny, nz):
+    st, s = solver(workload("les256", nx=nx, ny=ny, nz=nz, sgsflag=0, dealiasflag=0))
+    a = rand_phys(st, 21)
+    assert rel(s.horfft(a, None, -1), O.horfft_fwd(a, nx, ny)) < TOL_OP
+    g = np.random.default_rng(22).standard_normal((nz + 1, ny, nx))
+    assert rel(s.horfft(None, g, 1), O.horfft_inv(g, nx, ny)) < TOL_OP
+
+
 def run_both(cfg, nsteps, seed=3, amp=1e-3, zder="dct"):
     st, s = solver(cfg)
     u, v, w = ic.seeded_noise(st, seed, amp)
