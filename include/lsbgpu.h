@@ -52,6 +52,10 @@ typedef struct {
     double istartbound, samp;
     double bc3_amp, bc3_xc, bc3_s;
     double fsize;          /* fringe fraction (bounds the z-CFL region in the diagnostics) */
+    int dtadapt, iomod;    /* maxcalc every 5 steps and every iomod steps (src/navierstokes.f90:78-87) */
+    int ifilt, modfilt;    /* filtering hook at the start of timestep (src/navierstokes.f90:33-40):
+                              TNS automatic filtering when sgsmodel = 4, else filterall3pt */
+    int otfavg, istartavg; /* on-the-fly time averages of u, v, w, p (src/main.f90:70-76) */
 } lsb_config;
 
 /* Host set-up arrays (inputs, as the reference passes diag/smat/simat): see
@@ -114,6 +118,9 @@ int lsb_download_velocity(lsb_handle* h, double* uf, double* vf, double* wf);
 /* CUDA-event timers per kernel group: enable=1 clears and starts, 0 stops;
  * the report has one "group launches total_ms" line per group */
 int lsb_timers(lsb_handle* h, int enable);
+/* the on-the-fly time averages (src/main.f90:70-76, sum of q/iomod since the last reset);
+ * reset = 1 zeroes them afterwards as main.f90:104-106 does after writing qavg files */
+int lsb_tavg(lsb_handle* h, double* uf, double* vf, double* wf, double* pf, int reset);
 int lsb_timer_report(lsb_handle* h, char* buf, int buflen);
 
 /* ---------------- Tier 1: the reference's subroutine interfaces (host arrays) --------- */

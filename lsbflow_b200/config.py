@@ -53,6 +53,8 @@ class LsbConfig:
     ifilt: int = 0
     modfilt: int = 0
     dealiasflag: int = 2
+    otfavg: int = 0
+    istartavg: int = 0
     # &param
     xlen: float = 333.3333
     ylen: float = 20.0

@@ -36,7 +36,8 @@ struct SgsWork {
     double* H9 = nullptr;       // 9 spectral fields h(l,m) when tau is not symmetric
     double* w = nullptr;        // model work fields
     int nw = 0;
-    double* zf = nullptr;       // z filter coefficients: az, bz, cz for (a, b) and for (1, 1): 6*nzp
+    double* zf = nullptr;       // z filter coefficients az, bz, cz (3*nzp each set) for the weight
+                                // pairs (a, b), (1, 1), (1, 6), (1, 2)
     double* delta = nullptr;    // [nzp] (dx dy dz)^(1/3) of dynamic/sigma
     double* sdelta = nullptr;   // [nzp] static-Smagorinsky delta (its own quirks)
     double* scal = nullptr;     // device scalars (u_tau average)
@@ -72,6 +73,8 @@ struct lsb_handle {
     double *io = nullptr;    // host-transfer staging, 12 S
     double *red = nullptr;   // reduction scratch
     lsb::SgsWork sgs;
+    double* tavg = nullptr;  // on-the-fly averages of u, v, w, p (4 S)
+    double tns_ratio = 0.0;  // last TNS <I(h)>/<I(delta)>
     int* sgs_wall = nullptr;
     int sgs_nwall = 0;
     // per kernel-group CUDA-event timers (lsb_timers / lsb_timer_report)
@@ -126,7 +129,10 @@ struct TimerScope {
     }
 };
 // sgs_kernels.cu
+void filters_init(lsb_handle* h);
 void sgs_init(lsb_handle* h);
+// the ifilt hook of timestep (src/navierstokes.f90:33-40) on the current u, v, w, p
+void filter_hook(lsb_handle* h);
 void sgs_add_tau(lsb_handle* h, double* const* ph, bool dealias);
 void sgs_tau_phys(lsb_handle* h, const double* ui, const double* g, const double* uiuj, double* tau);
 void sgs_mul(double* y, const double* x, long long n, cudaStream_t s);

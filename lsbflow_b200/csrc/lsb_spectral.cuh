@@ -73,5 +73,6 @@ void launch_norm(double* f0, double* f1, double* f2, int nx, int ny, int nzp, in
 void launch_force_phys(const double* u0, const double* u1, const double* u2, double* f0, double* f1, double* f2,
                        const double* lamx, const double* ubar, int nx, int ny, long long P, cudaStream_t s);
 void launch_axpby(double* y, const double* x, double a, double b, long long n, cudaStream_t s);
+void launch_tavg_add(double* a, const double* q, double iomod, long long n, cudaStream_t s);
 
 }  // namespace lsb

@@ -520,6 +520,7 @@ void step_one(lsb_handle* h) {
     const long long S = d.S(), C = d.C();
     cudaStream_t st = h->stream;
     h->istep += 1;
+    if (c.ifilt >= 1 && c.modfilt > 0 && h->istep % c.modfilt == 0) filter_hook(h);
     coefficients(h);
     const double dt = h->dt;
     // 1-2. nonlinear term (from spectrally filtered velocities when dealiasflag >= 2)
@@ -761,7 +762,11 @@ int lsb_create(const lsb_config* cfg, const lsb_setup* su, lsb_handle** out) {
         h->bshape = h->alloc(3 * C);
         h->io = h->alloc(12 * S);
         h->red = h->alloc(512);
+        filters_init(h.get());
         if (cfg->sgsflag == 1) sgs_init(h.get());
+        if (cfg->otfavg == 1) h->tavg = h->alloc(4 * S);
+        if (cfg->ifilt >= 1 && cfg->modfilt <= 0) fail(LSB_ERR_ARG, "ifilt needs modfilt > 0");
+        if (cfg->dtadapt == 1 && cfg->iomod <= 0) fail(LSB_ERR_ARG, "dtadapt needs iomod > 0");
         build_bound_shapes(h.get());
         CK(cudaStreamSynchronize(h->stream));
         check_launch();
@@ -871,9 +876,29 @@ int lsb_step(lsb_handle* h, int nsteps) {
         if (!h) fail(LSB_ERR_ARG, "null handle");
         if (nsteps < 0) fail(LSB_ERR_ARG, "nsteps < 0");
         if (!(h->dt > 0.0) || !std::isfinite(h->dt)) fail(LSB_ERR_STATE, "dt must be finite and > 0");
+        const lsb_config& c = h->cfg;
+        const long long S = h->d.S();
         for (int i = 0; i < nsteps; ++i) {
             step_one(h);
             check_launch();
+            // adaptive dt: NaN check + maxcalc every 5 steps and every iomod steps
+            if (c.dtadapt == 1 && (h->istep % c.iomod == 0 || h->istep % 5 == 0)) {
+                lsb_diagnostics dg;
+                diag_compute(h, &dg);
+                if (dg.nonfinite) fail(LSB_ERR_NONFINITE, "NaN detected at step " + std::to_string(h->istep));
+                const bool exceed = dg.cflz > 0.45 || dg.cflx > 0.25 || dg.cfly > 0.25;
+                const bool below = dg.cflz < 0.25 && dg.cflx < 0.10 && dg.cfly < 0.12 && h->dt < 1.0;
+                if (exceed || below) {
+                    const double cdt = exceed ? 1.25 : 1.0 / 1.25;
+                    h->dt2 = h->dt;
+                    h->dt = h->dt / cdt;
+                }
+            }
+            // on-the-fly averages (src/main.f90:70-76): q_tavg += q / iomod
+            if (c.otfavg == 1 && h->istep > c.istartavg) {
+                const double* q[4] = {h->vel, h->vel + S, h->vel + 2 * S, h->p};
+                for (int k = 0; k < 4; ++k) launch_tavg_add(h->tavg + k * S, q[k], (double)c.iomod, S, h->stream);
+            }
         }
     });
 }
@@ -1082,6 +1107,19 @@ int lsb_tau_sgs(lsb_handle* h, const double* ui, const double* uiuj, const doubl
             for (int m = 0; m < 3; ++m) from_dev_phys(h, h->sgs.tau + (3 * l + m) * P, tauij + (l + 3 * m) * F, 1);
         CK(cudaStreamSynchronize(h->stream));
         check_launch();
+    });
+}
+
+int lsb_tavg(lsb_handle* h, double* uf, double* vf, double* wf, double* pf, int reset) {
+    return guard([&] {
+        if (!h) fail(LSB_ERR_ARG, "null handle");
+        if (!h->tavg) fail(LSB_ERR_STATE, "handle was created without otfavg = 1");
+        const long long S = h->d.S();
+        double* outs[4] = {uf, vf, wf, pf};
+        for (int k = 0; k < 4; ++k)
+            if (outs[k]) CK(cudaMemcpyAsync(outs[k], h->tavg + k * S, S * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        if (reset) CK(cudaMemsetAsync(h->tavg, 0, 4 * S * sizeof(double), h->stream));
+        CK(cudaStreamSynchronize(h->stream));
     });
 }
 

@@ -118,7 +118,7 @@ void filter3(lsb_handle* h, const double* const* in, double* const* out, int n, 
             fl.in[i] = in[f0 + i];
             fl.out[i] = out[f0 + i];
         }
-        const double* zf = h->sgs.zf + (long long)which * 3 * d.nzp;
+        const double* zf = h->sgs.zf + (long long)which * 3 * d.nzp;  // which: 0 (a,b) 1 (1,1) 2 (1,6) 3 (1,2)
         TimerScope ts(h, "sgs_filter3");
         dim3 grid((d.nx + FIB - 1) / FIB, (d.ny + FJB - 1) / FJB, nzc * fl.n);
         k_filter3<<<grid, 256, 0, h->stream>>>(fl, d.nx, d.ny, d.nzp, a, b, zf, zf + d.nzp, zf + 2 * d.nzp, nzc);
@@ -362,6 +362,17 @@ static void zfilter_coeffs(const std::vector<double>& zp, int mapping, double a,
     }
 }
 
+void filters_init(lsb_handle* h) {
+    const Dims& d = h->d;
+    const lsb_config& c = h->cfg;
+    const double ab[4][2] = {{c.a, c.b}, {1.0, 1.0}, {1.0, 6.0}, {1.0, 2.0}};
+    std::vector<double> zf(12 * (size_t)d.nzp);
+    for (int w = 0; w < 4; ++w)
+        zfilter_coeffs(h->h_zpts, c.mapping, ab[w][0], ab[w][1], &zf[(3 * w) * d.nzp], &zf[(3 * w + 1) * d.nzp],
+                       &zf[(3 * w + 2) * d.nzp]);
+    h->sgs.zf = h->upload(zf.data(), zf.size());
+}
+
 void sgs_init(lsb_handle* h) {
     const Dims& d = h->d;
     const lsb_config& c = h->cfg;
@@ -371,10 +382,6 @@ void sgs_init(lsb_handle* h) {
     if (s.nonsym) s.H9 = h->alloc(9 * d.S());
     s.nw = 40;
     s.w = h->alloc((size_t)s.nw * h->P);
-    std::vector<double> zf(6 * (size_t)d.nzp);
-    zfilter_coeffs(h->h_zpts, c.mapping, c.a, c.b, &zf[0], &zf[d.nzp], &zf[2 * d.nzp]);
-    zfilter_coeffs(h->h_zpts, c.mapping, 1.0, 1.0, &zf[3 * d.nzp], &zf[4 * d.nzp], &zf[5 * d.nzp]);
-    s.zf = h->upload(zf.data(), zf.size());
     // delta of the dynamic and sigma models (src/sgsterm.f90:159-164, 367-376)
     const std::vector<double>& zp = h->h_zpts;
     const int n = d.nzp;
@@ -558,6 +565,99 @@ void sgs_tau_phys(lsb_handle* h, const double* ui, const double* g, const double
     for (int l = 0; l < 3; ++l)
         for (int m = l; m < 3; ++m) uu6[sym6(l, m)] = uiuj + (3 * l + m) * P;
     model_tau(h, u3, g9, uu6, tau);
+}
+
+// ---------------------------------------------------------------- filtering hook
+namespace {
+// per plane: sum over the 3 velocity fields and the plane of (q - qf)^2
+__global__ void k_plane_sqdiff(P9 q, P9 qf, int nx, int ny, double* out) {
+    const int k = blockIdx.x;
+    const long long base = (long long)k * nx * ny;
+    __shared__ double red[256];
+    double acc = 0.0;
+    for (int f = 0; f < 3; ++f)
+        for (int e = threadIdx.x; e < nx * ny; e += blockDim.x) {
+            const double dd = q.p[f][base + e] - qf.p[f][base + e];
+            acc += dd * dd;
+        }
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+        if (threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[k] = red[0];
+}
+
+// modecutFC (src/filters.f90:617-654): qb = sum_l coef_l F^l(q), coef = (6,-15,20,-15,6,-1)
+void modecut(lsb_handle* h, double* const* q, double* const* qb, double* const* ping, double* const* pong, int nf,
+             double a, double b, int which) {
+    const double coef[6] = {6., -15., 20., -15., 6., -1.};
+    const long long P = h->P;
+    const double* cur[4];
+    for (int f = 0; f < nf; ++f) cur[f] = q[f];
+    for (int l = 0; l < 6; ++l) {
+        double* const* dst = (l % 2 == 0) ? ping : pong;
+        filter3(h, cur, dst, nf, a, b, which);
+        for (int f = 0; f < nf; ++f) {
+            launch_axpby(qb[f], dst[f], coef[l], l == 0 ? 0.0 : 1.0, P, h->stream);
+            cur[f] = dst[f];
+        }
+    }
+}
+}  // namespace
+
+void filter_hook(lsb_handle* h) {
+    const Dims& d = h->d;
+    const lsb_config& c = h->cfg;
+    const long long S = d.S(), P = h->P;
+    TimerScope ts(h, "filter_hook");
+    double* q[4];
+    double* A[4];
+    double* B[4];
+    double* pi[4];
+    double* po[4];
+    for (int f = 0; f < 4; ++f) {
+        q[f] = h->phys + f * P;
+        A[f] = h->phys + (4 + f) * P;
+        B[f] = h->phys + (8 + f) * P;
+        pi[f] = h->phys + (12 + f) * P;
+        po[f] = h->phys + (16 + f) * P;
+    }
+    const double* spec[4] = {h->vel, h->vel + S, h->vel + 2 * S, h->p};
+    spec_to_phys(h, spec, q, 4, d.nzp, nullptr, nullptr);
+    double* outs[4] = {h->vel, h->vel + S, h->vel + 2 * S, h->p};
+    if (c.sgsflag == 1 && c.sgsmodel == 4) {
+        // tns_automatic_filtering (src/filters.f90:62-161)
+        modecut(h, q, A, pi, po, 4, 1.0, 6.0, 2);  // q_filt_2kc
+        modecut(h, q, B, pi, po, 4, 1.0, 2.0, 3);  // q_filt
+        P9 qq{}, qa{}, qb{};
+        for (int f = 0; f < 3; ++f) {
+            qq.p[f] = q[f];
+            qa.p[f] = A[f];
+            qb.p[f] = B[f];
+        }
+        double* e = h->red;
+        k_plane_sqdiff<<<d.nzp, 256, 0, h->stream>>>(qq, qb, d.nx, d.ny, e);             // energy(:,3)
+        k_plane_sqdiff<<<d.nzp, 256, 0, h->stream>>>(qq, qa, d.nx, d.ny, e + d.nzp);     // energy(:,4)
+        std::vector<double> en(2 * (size_t)d.nzp);
+        CK(cudaMemcpyAsync(en.data(), e, en.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        const double nxy = (double)d.ny * d.nx;
+        const std::vector<double>& zp = h->h_zpts;
+        double ih = 0.0, idel = 0.0;
+        for (int k = d.nz - 1; k >= 0; --k) {
+            const double dz = zp[k] - zp[k + 1];
+            ih += 0.5 * (en[d.nzp + k] / nxy + en[d.nzp + k + 1] / nxy) * dz;
+            idel += 0.5 * (en[k] / nxy + en[k + 1] / nxy) * dz;
+        }
+        h->tns_ratio = ih / idel;
+        if (ih / idel > 0.007) phys_to_spec(h, (const double* const*)A, outs, 4, d.nzp, 1.0, 0.0, nullptr);
+    } else {
+        // filterall3pt (src/filters.f90:9-59)
+        modecut(h, q, A, pi, po, 4, c.a, c.b, 0);
+        phys_to_spec(h, (const double* const*)A, outs, 4, d.nzp, 1.0, 0.0, nullptr);
+    }
 }
 
 // ---------------------------------------------------------------- diagnostics

@@ -239,6 +239,11 @@ __global__ void k_force_phys(const double* __restrict__ u0, const double* __rest
     }
 }
 
+__global__ void k_tavg_add(double* __restrict__ a, const double* __restrict__ q, double iomod, long long n) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+        a[e] = a[e] + q[e] / iomod;
+}
+
 __global__ void k_axpby(double* __restrict__ y, const double* __restrict__ x, double a, double b, long long n) {
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
         y[e] = a * x[e] + (b != 0.0 ? b * y[e] : 0.0);
@@ -278,6 +283,9 @@ void launch_norm(double* f0, double* f1, double* f2, int nx, int ny, int nzp, in
 void launch_force_phys(const double* u0, const double* u1, const double* u2, double* f0, double* f1, double* f2,
                        const double* lamx, const double* ubar, int nx, int ny, long long P, cudaStream_t s) {
     k_force_phys<<<nblk(P), 256, 0, s>>>(u0, u1, u2, f0, f1, f2, lamx, ubar, nx, ny, P);
+}
+void launch_tavg_add(double* a, const double* q, double iomod, long long n, cudaStream_t s) {
+    k_tavg_add<<<nblk(n), 256, 0, s>>>(a, q, iomod, n);
 }
 void launch_axpby(double* y, const double* x, double a, double b, long long n, cudaStream_t s) {
     k_axpby<<<nblk(n), 256, 0, s>>>(y, x, a, b, n);

@@ -27,7 +27,7 @@ EXPORTS = [
     "lsb_synchronize", "lsb_horfft", "lsb_dealias_product", "lsb_dfdx", "lsb_dfdy", "lsb_dfdz", "lsb_d2fdz2",
     "lsb_lapl", "lsb_divuv", "lsb_solve_helmholtz", "lsb_solve_nhom_helmholtz", "lsb_nlterm", "lsb_tau_sgs",
     "lsb_upload_velocity", "lsb_download_velocity", "lsb_timers", "lsb_timer_report",
-    "lsb_solve_helmholtz_noalloc",
+    "lsb_solve_helmholtz_noalloc", "lsb_tavg",
 ]
 
 
@@ -44,6 +44,8 @@ class LsbConfigC(C.Structure):
         ("istartbound", C.c_double), ("samp", C.c_double),
         ("bc3_amp", C.c_double), ("bc3_xc", C.c_double), ("bc3_s", C.c_double),
         ("fsize", C.c_double),
+        ("dtadapt", C.c_int), ("iomod", C.c_int), ("ifilt", C.c_int), ("modfilt", C.c_int),
+        ("otfavg", C.c_int), ("istartavg", C.c_int),
     ]
 
 
@@ -106,6 +108,7 @@ def config_struct(cfg: LsbConfig) -> LsbConfigC:
         cfg.xnu, cfg.u0, cfg.x0, cfg.xlen, cfg.ylen, cfg.zlen, cfg.a, cfg.b, cfg.CS,
         cfg.kc, cfg.filt_order, cfg.filt_amp, cfg.istartbound, cfg.samp,
         cfg.bc3_amp, cfg.bc3_xc, cfg.bc3_s, cfg.fsize,
+        cfg.dtadapt, cfg.iomod, cfg.ifilt, cfg.modfilt, getattr(cfg, "otfavg", 0), getattr(cfg, "istartavg", 0),
     )
 
 
@@ -216,6 +219,12 @@ class Solver:
 
     def download_velocity_ptr(self, u_ptr: int, v_ptr: int, w_ptr: int):
         _ck(self._lib.lsb_download_velocity(self._h, C.c_void_p(u_ptr), C.c_void_p(v_ptr), C.c_void_p(w_ptr)))
+
+    def tavg(self, reset: bool = False):
+        sh = self.spec_shape()
+        out = [np.empty(sh) for _ in range(4)]
+        _ck(self._lib.lsb_tavg(self._h, *[_ptr(a) for a in out], C.c_int(1 if reset else 0)))
+        return out
 
     def timers(self, enable: bool):
         _ck(self._lib.lsb_timers(self._h, C.c_int(1 if enable else 0)))

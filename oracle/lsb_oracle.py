@@ -665,6 +665,7 @@ class State:
     abfac: tuple = (0.0, 0.0, 0.0)
     bdf: tuple = (0.0, 0.0, 0.0)
     bdfv: float = 0.0
+    tavg: list = None
 
     @staticmethod
     def zeros_like(st: Setup, uf, vf, wf, dt):
@@ -780,6 +781,18 @@ def timestep(st: Setup, s: State):
     s.dt2 = s.dt
     if c.dtadapt == 1 and (s.istep % c.iomod == 0 or s.istep % 5 == 0):
         maxcalc(st, s)
+
+
+def main_step(st: Setup, s: State):
+    """One pass of the main loop body (src/main.f90:64-76): timestep, then the
+    on-the-fly average q_tavg += q/iomod while its > istartavg."""
+    timestep(st, s)
+    c = st.cfg
+    if c.otfavg == 1 and s.istep > c.istartavg:
+        if s.tavg is None:
+            s.tavg = [np.zeros_like(s.uf) for _ in range(4)]
+        for a, q in zip(s.tavg, (s.uf, s.vf, s.wf, s.pf)):
+            a += q / c.iomod
 
 
 def filter_hook(st: Setup, s: State):

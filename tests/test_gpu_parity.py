@@ -253,3 +253,76 @@ def test_diag_divergence_and_energy():
     assert abs(d["energy_total"] - e1) <= 1e-11 * abs(e1)
     assert abs(d["energy_pert"] - e2) <= 1e-9 * abs(e2) + 1e-30
     assert d["nonfinite"] == 0
+
+
+# ------------------------------------------------------------------ main-loop features
+def run_main(cfg, nsteps, u=None, v=None, w=None, seed=3, amp=1e-3, dt=None):
+    st, s = solver(cfg)
+    if u is None:
+        u, v, w = ic.seeded_noise(st, seed, amp)
+    dt = st.dt if dt is None else dt
+    ost = O.State.zeros_like(st, u, v, w, dt)
+    s.upload(u, v, w, dt=dt)
+    old = O.ZDER
+    O.ZDER = "dense"
+    try:
+        for _ in range(nsteps):
+            O.main_step(st, ost)
+    finally:
+        O.ZDER = old
+    s.step(nsteps)
+    return st, s, ost, s.download()
+
+
+def test_shipped_input_run_on_device():
+    # the reference's own run/input.dat case (224x24x33, spectral filter, adaptive dt):
+    # device vs oracle, and the u profile of the reference's float32 snapshot at step 20
+    import os
+    gold = np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_run.npz"))
+    from lsbflow_b200.config import parse_namelist
+    cfg = parse_namelist(str(gold["input_dat"]))
+    st = hs.make_setup(cfg)
+    z = np.zeros((cfg.nzp, cfg.ny, cfg.nx))
+    st2, s, ost, got = run_main(cfg, 20, z, z, z)
+    assert got["istep"] == 20 and got["dt"] == ost.dt and np.float32(got["dt"]) == gold["q20_header"][2]
+    for key, ref in (("uf", ost.uf), ("vf", ost.vf), ("wf", ost.wf)):
+        assert np.abs(got[key] - ref).max() <= 1e-10 * max(1.0, np.abs(ref).max()), key
+    u = O.horfft_inv(got["uf"], cfg.nx, cfg.ny)[..., : cfg.nx] + st.ubar[:, None, None]
+    np.testing.assert_allclose(u[:, 0, 0], gold["q20_uprof"], rtol=0, atol=1.2e-7)
+
+
+@pytest.mark.parametrize("name,over", [
+    ("filterall3pt", dict(ifilt=1, modfilt=3, sgsflag=0)),
+    ("tns", dict(ifilt=1, modfilt=2, sgsflag=1, sgsmodel=4)),
+    ("tavg", dict(otfavg=1, istartavg=3, iomod=4)),
+    ("dtadapt", dict(dtadapt=1, iomod=7, dt_fixed=0.05)),
+])
+def test_main_loop_features(name, over):
+    cfg = workload("dns64", nx=32, ny=8, nz=32, dealiasflag=2, **over)
+    st, s, ost, got = run_main(cfg, 12, amp=2e-2)
+    for key, ref in (("uf", ost.uf), ("vf", ost.vf), ("wf", ost.wf), ("pf", ost.pf)):
+        assert rel(got[key], ref) < TOL_STEP, (key, rel(got[key], ref))
+    assert got["dt"] == ost.dt and got["dt2"] == ost.dt2
+    if name == "tavg":
+        avg = s.tavg()
+        for a, r in zip(avg, ost.tavg):
+            assert rel(a, r) < TOL_STEP
+    if name == "dtadapt":
+        assert ost.dt != 0.05  # the CFL limits changed dt
+
+
+def test_tns_filter_applied():
+    # a white-noise field puts enough energy near the cutoff for <I(h)>/<I(delta)> > 0.007,
+    # so the automatic filter replaces u, v, w, p (src/filters.f90:133-137)
+    cfg = workload("dns64", nx=32, ny=8, nz=32, dealiasflag=2, ifilt=1, modfilt=2, sgsflag=1, sgsmodel=4)
+    st = hs.make_setup(cfg)
+    rng = np.random.default_rng(5)
+    f = [rng.standard_normal((cfg.nzp, cfg.ny, cfg.nx)) * 1e-3 for _ in range(3)]
+    for x in f:
+        x[0] = 0.0
+        x[-1] = 0.0
+    O.norm(f, cfg.ny)
+    assert O.filter_hook(st, O.State.zeros_like(st, *f, st.dt)) > 0.007
+    st, s, ost, got = run_main(cfg, 4, *f)
+    for key, ref in (("uf", ost.uf), ("vf", ost.vf), ("wf", ost.wf), ("pf", ost.pf)):
+        assert rel(got[key], ref) < TOL_STEP, (key, rel(got[key], ref))
