@@ -74,7 +74,19 @@ class ClockSampler:
         for line in self._proc.stdout:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) >= 9:
-                self.samples.append(parts)
+                self.samples.append((time.perf_counter(), parts))
+
+    def wait_first(self, timeout_s: float = 5.0):
+        """Block until nvidia-smi delivered its first sample, so the timed region is covered."""
+        t0 = time.perf_counter()
+        while self._proc is not None and not self.samples and time.perf_counter() - t0 < timeout_s:
+            time.sleep(0.01)
+
+    def mark(self, start: bool):
+        if start:
+            self.t_start = time.perf_counter()
+        else:
+            self.t_end = time.perf_counter()
 
     def __exit__(self, *exc):
         if self._proc is not None:
@@ -85,14 +97,17 @@ class ClockSampler:
                 self._proc.kill()
 
     def summary(self):
-        if not self.samples:
+        t0, t1 = getattr(self, "t_start", 0.0), getattr(self, "t_end", float("inf"))
+        inside = [s for ts, s in self.samples if t0 <= ts <= t1 + 0.25]
+        if not inside:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        self_samples = inside
+        sm = [float(s[1]) for s in self_samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self_samples if s[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({n for s in self.samples for n, v in zip(names, s[5:9]) if v.lower() == "active"})
+        reasons = sorted({n for s in self_samples for n, v in zip(names, s[5:9]) if v.lower() == "active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+                "reasons": reasons, "samples": len(self_samples)}
 
 
 def cpu_reference_step_time(cfg, max_steps: int, budget_s: float, warmup: int, threads: int):
@@ -138,11 +153,26 @@ def run_reference(args, cfg):
     print(json.dumps(line), flush=True)
 
 
+ROW_NL_PROFILE = os.path.join(ROOT, "profiles", "row_nl_les256_fp64.txt")
+
+
+def profiled_traffic(path: str):
+    """DRAM bytes per launch of the dominant kernel from its committed ncu summary."""
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -154,11 +184,9 @@ def main():
 
     import torch
     import torch.distributed as dist
-    from lsbflow_b200 import lib
+    from lsbflow_b200 import lib, replicas
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank, world, local = replicas.rank_info()
     torch.cuda.set_device(local)
     if world > 1:
         import datetime
@@ -169,14 +197,10 @@ def main():
             dist.barrier()
 
     def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x, world, device="cuda")
 
     st = hs.make_setup(cfg)
-    u, v, w = ic.seeded_noise(st, 1000 + rank, 5e-3)
+    u, v, w = ic.seeded_noise(st, replicas.replica_seed(1000, rank), 5e-3)
     sol = lib.Solver(st)
     stream = torch.cuda.Stream()
     sol.set_stream(stream.cuda_stream)
@@ -184,71 +208,63 @@ def main():
     pts = cfg.nx * cfg.ny * cfg.nzp
 
     # ---- warm-up
-    with torch.cuda.stream(stream):
-        sol.step(args.warmup)
+    sol.step(args.warmup)
     torch.cuda.synchronize()
 
-    # ---- device-resident timed region
+    # ---- device-resident timed region (CUDA events on the library's stream)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    barrier()
-    torch.cuda.synchronize()
     with ClockSampler(local) as clk:
+        clk.wait_first()
+        barrier()
+        torch.cuda.synchronize()
+        clk.mark(True)
+        n0 = lib.kernel_launches()
         ev0.record(stream)
         sol.step(args.steps)
         ev1.record(stream)
+        launches = lib.kernel_launches() - n0
         torch.cuda.synchronize()
+        clk.mark(False)
     barrier()
-    ms = ev0.elapsed_time(ev1)
-    ms = max_over_ranks(ms)
-    value = pts * args.steps * world / (ms / 1e3)
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    value = replicas.job_throughput(pts, args.steps, world, ms / 1e3)
     clocks = clk.summary()
 
     # ---- per kernel-group timing (same workload, separate region with event timers on)
     sol.timers(True)
-    with torch.cuda.stream(stream):
-        sol.step(args.steps)
+    sol.step(min(args.steps, 40))
     torch.cuda.synchronize()
     rep = sol.timer_report()
     sol.timers(False)
-    tot = sum(v[1] for v in rep.values())
-    groups = {k: {"launches": v[0], "ms_total": round(v[1], 4), "share": round(v[1] / tot, 4)} for k, v in rep.items()}
-    top = max(rep.items(), key=lambda kv: kv[1][1])
+    # sgs_filter3 runs inside sgs_total: the step total counts it once
+    tot = sum(v[1] for k, v in rep.items() if k != "sgs_filter3")
+    groups = {k: {"launches": v[0], "ms_total": round(v[1], 4), "share": round(v[1] / tot, 4)}
+              for k, v in rep.items()}
 
-    # ---- roofline of the dominant kernel group (HBM-bound FFT / stencil work)
+    # ---- roofline of the dominant kernel, the fused nonlinear-product row pass (k_row_nl):
+    # per (z, y) row of the padded y-intermediate grid it reads 9 rows of kx modes
+    # (u_l, du_l/dy, du_l/dz) and writes 9 (3 convective terms, 6 fluxes), nx doubles each
     hbm, hbm_kind = peaks()
     nx, ny, nzp = cfg.nx, cfg.ny, cfg.nzp
     nxl, nyl = st.nx_lg, st.ny_lg
     S8 = nx * ny * nzp * 8
-    Yl8 = nx * nyl * nzp * 8
-    P8 = nx * ny * nzp * 8
-    alg_bytes = {
-        # row_nl: 9 y-intermediate rows in, 9 out per launch
-        "row_nl": 18 * Yl8,
-        # spanwise passes: 9 spectral -> 9 padded intermediates; 9 padded -> 9 spectral
-        "yinv_nl": 9 * (S8 // 1) // 1 * 0 + 6 * S8 + 9 * Yl8,
-        "yfwd_nl": 9 * Yl8 + 9 * S8,
-        # the 3-point filter: one field in, one out per component (counted per launch of 6 fields avg)
-        "sgs_filter3": None,
-        "gemm_dz": 6 * S8,
-        "helmholtz_uvw": 3 * (2 * S8 + 2 * S8),
-        "sgs_total": None,
-    }
-    per_launch_ms = top[1][1] / max(top[1][0], 1)
-    ab = alg_bytes.get(top[0])
-    if ab is None:
-        ab = 2 * P8 * 4  # a conservative 4-field in/out estimate for SGS groups
-    achieved = ab / (per_launch_ms / 1e3) / 1e9
-    roofline = {"kernel": top[0], "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
-                "frac": round(achieved / hbm, 4), "peak_kind": hbm_kind, "traffic": None,
-                "alg_bytes_per_launch": ab, "avg_launch_ms": round(per_launch_ms, 4)}
+    alg_bytes = 18 * nx * nyl * nzp * 8
+    n_nl, ms_nl = rep["row_nl"]
+    per_launch_ms = ms_nl / max(n_nl, 1)
+    achieved = alg_bytes / (per_launch_ms / 1e3) / 1e9
+    roofline = {"kernel": "k_row_nl_r (fused 12 c2r + skew-symmetric products + 9 r2c)", "bound": "hbm",
+                "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
+                "peak_kind": hbm_kind, "traffic": profiled_traffic(ROW_NL_PROFILE),
+                "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": round(per_launch_ms, 4),
+                "share_of_step": round(ms_nl / tot, 4)}
 
     # ---- end-to-end through the C ABI with host buffers (pinned): per step the velocity
     # (u, v, w) goes host->device, one time step runs, the new velocity comes back.
-    hb = [torch.empty(pts * 3 // 3 * 1, dtype=torch.float64, pin_memory=True) for _ in range(3)]
+    hb = [torch.empty(pts, dtype=torch.float64, pin_memory=True) for _ in range(3)]
     for i, f in enumerate((u, v, w)):
         hb[i].copy_(torch.from_numpy(np.ascontiguousarray(f).ravel()))
-    e2e_steps = max(3, args.steps // 2)
+    e2e_steps = max(3, min(args.steps, 100))
     barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -257,9 +273,8 @@ def main():
         sol.step(1)
         sol.download_velocity_ptr(hb[0].data_ptr(), hb[1].data_ptr(), hb[2].data_ptr())
     sol.synchronize()
-    e2e_s = time.perf_counter() - t0
-    e2e_s = max_over_ranks(e2e_s)
-    e2e_val = pts * e2e_steps * world / e2e_s
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_val = replicas.job_throughput(pts, e2e_steps, world, e2e_s)
 
     # ---- the CPU baseline (rank 0, N = 1 only), bounded sample
     cpu = None
@@ -267,7 +282,8 @@ def main():
         threads = os.cpu_count() or 1
         t_step, n = cpu_reference_step_time(cfg, 2, 40.0, 0, threads)
         cpu = {"value": pts / t_step, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"{n} time step(s) of the same workload with the FP64 NumPy oracle"}
+               "sample": f"{n} time step(s) of the same {nx}x{ny}x{nzp} workload with the FP64 NumPy oracle "
+                         f"(scipy.fft with {threads} workers)"}
 
     if rank == 0:
         line = {
@@ -277,15 +293,14 @@ def main():
             "config": {"workload": f"{args.workload}: {nx}x{ny}x{nzp} (ref nx,ny,nzp), padded {nxl}x{nyl}, "
                                    f"dyn-Smagorinsky LES, dealias 3/2, fringe, dipole BC, dt={st.dt}",
                        "global_batch": world, "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (resident state 24 fields x 17 MB)"},
+                       "l2": "inputs larger than L2 (resident state 24 fields x 17 MB = 405 MB)"},
             "roofline": roofline,
             "kernel_groups": groups,
             "clocks": clocks,
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": 3 * S8, "d2h_bytes_per_step": 3 * S8},
-            "gpu_launches": None,
+            "gpu_launches": launches,
             "cpu_baseline": cpu,
         }
-        line["gpu_launches"] = sum(v[0] for v in rep.values())
         print(json.dumps(line), flush=True)
     sol.close()
     if world > 1:

@@ -89,6 +89,9 @@ typedef struct {
 
 const char* lsb_last_error(void);
 int lsb_version(void);
+/* kernels this library has launched since it was loaded, over all handles (no reference
+   counterpart: a launch count for profiling and for checking that the GPU path ran) */
+unsigned long long lsb_kernel_launches(void);
 
 /* ---------------- Tier 2: resident state --------------------------------------------- */
 /* replaces initialize()'s device-side part (src/init.f90:7-127) */

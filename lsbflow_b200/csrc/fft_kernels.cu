@@ -370,8 +370,8 @@ void launch_yinv(const YInvJobList& jobs, const YPassArgs& a, cudaStream_t s) {
     const int nch = (a.kxc + KC - 1) / KC;
     const int nitems = jobs.n * a.nzp * nch;
     const size_t sm = (size_t)3 * KC * a.plan.ls * sizeof(double2);
-    if (wide(a.plan)) k_yinv<true><<<persistent_grid(k_yinv<true>, sm, nitems), 256, sm, s>>>(jobs, a, nch);
-    else k_yinv<false><<<persistent_grid(k_yinv<false>, sm, nitems), 256, sm, s>>>(jobs, a, nch);
+    if (wide(a.plan)) { lsb::note_launch(); k_yinv<true><<<persistent_grid(k_yinv<true>, sm, nitems), 256, sm, s>>>(jobs, a, nch); }
+    else { lsb::note_launch(); k_yinv<false><<<persistent_grid(k_yinv<false>, sm, nitems), 256, sm, s>>>(jobs, a, nch); }
 }
 
 void launch_yfwd(const YFwdJobList& jobs, const YPassArgs& a, cudaStream_t s) {
@@ -380,8 +380,8 @@ void launch_yfwd(const YFwdJobList& jobs, const YPassArgs& a, cudaStream_t s) {
     const int nch = (a.kxc + KC - 1) / KC;
     const int nitems = jobs.n * a.nzp * nch;
     const size_t sm = (size_t)3 * KC * a.plan.ls * sizeof(double2);
-    if (wide(a.plan)) k_yfwd<true><<<persistent_grid(k_yfwd<true>, sm, nitems), 256, sm, s>>>(jobs, a, nch);
-    else k_yfwd<false><<<persistent_grid(k_yfwd<false>, sm, nitems), 256, sm, s>>>(jobs, a, nch);
+    if (wide(a.plan)) { lsb::note_launch(); k_yfwd<true><<<persistent_grid(k_yfwd<true>, sm, nitems), 256, sm, s>>>(jobs, a, nch); }
+    else { lsb::note_launch(); k_yfwd<false><<<persistent_grid(k_yfwd<false>, sm, nitems), 256, sm, s>>>(jobs, a, nch); }
 }
 
 // ----------------------------------------------------------------------------- rows
@@ -535,8 +535,8 @@ void launch_row_c2r(const RowJobList& jobs, const RowArgs& a, cudaStream_t s) {
     if (launch_row_c2r_warp(jobs, a, s)) return;
     const int nitems = jobs.n * ((a.nyl * a.nzp + RB - 1) / RB);
     const size_t sm = (size_t)3 * RB * a.rp.half.ls * sizeof(double2);
-    if (wide(a.rp.half)) k_row_c2r<true><<<persistent_grid(k_row_c2r<true>, sm, nitems), 256, sm, s>>>(jobs, a);
-    else k_row_c2r<false><<<persistent_grid(k_row_c2r<false>, sm, nitems), 256, sm, s>>>(jobs, a);
+    if (wide(a.rp.half)) { lsb::note_launch(); k_row_c2r<true><<<persistent_grid(k_row_c2r<true>, sm, nitems), 256, sm, s>>>(jobs, a); }
+    else { lsb::note_launch(); k_row_c2r<false><<<persistent_grid(k_row_c2r<false>, sm, nitems), 256, sm, s>>>(jobs, a); }
 }
 
 void launch_row_r2c(const RowJobList& jobs, const RowArgs& a, cudaStream_t s) {
@@ -544,8 +544,8 @@ void launch_row_r2c(const RowJobList& jobs, const RowArgs& a, cudaStream_t s) {
     if (launch_row_r2c_warp(jobs, a, s)) return;
     const int nitems = jobs.n * ((a.nyl * a.nzp + RB - 1) / RB);
     const size_t sm = (size_t)3 * RB * a.rp.half.ls * sizeof(double2);
-    if (wide(a.rp.half)) k_row_r2c<true><<<persistent_grid(k_row_r2c<true>, sm, nitems), 256, sm, s>>>(jobs, a);
-    else k_row_r2c<false><<<persistent_grid(k_row_r2c<false>, sm, nitems), 256, sm, s>>>(jobs, a);
+    if (wide(a.rp.half)) { lsb::note_launch(); k_row_r2c<true><<<persistent_grid(k_row_r2c<true>, sm, nitems), 256, sm, s>>>(jobs, a); }
+    else { lsb::note_launch(); k_row_r2c<false><<<persistent_grid(k_row_r2c<false>, sm, nitems), 256, sm, s>>>(jobs, a); }
 }
 
 // ----------------------------------------------------------------------------- NL row
@@ -655,8 +655,8 @@ void launch_row_nl(const NlRowArgs& a, cudaStream_t s) {
     if (launch_row_nl_warp(a, s)) return;
     const size_t sm = (size_t)36 * a.r.rp.half.ls * sizeof(double2);
     const int nitems = a.r.nyl * a.r.nzp;
-    if (wide(a.r.rp.half)) k_row_nl<true><<<persistent_grid(k_row_nl<true>, sm, nitems), 256, sm, s>>>(a);
-    else k_row_nl<false><<<persistent_grid(k_row_nl<false>, sm, nitems), 256, sm, s>>>(a);
+    if (wide(a.r.rp.half)) { lsb::note_launch(); k_row_nl<true><<<persistent_grid(k_row_nl<true>, sm, nitems), 256, sm, s>>>(a); }
+    else { lsb::note_launch(); k_row_nl<false><<<persistent_grid(k_row_nl<false>, sm, nitems), 256, sm, s>>>(a); }
 }
 
 }  // namespace lsb

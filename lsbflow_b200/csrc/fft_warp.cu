@@ -482,6 +482,133 @@ __global__ void __launch_bounds__(256, 2) k_row_nl_w(NlRowArgs a) {
     }
 }
 
+// Register-resident variant for rows of N = 32*R complex (G = 32): each warp owns a whole
+// (z, y) row.  Its lanes read the 9 input rows straight from global memory (coalesced),
+// and the 12 c2r, the products and the 9 r2c all stay in registers: every c2r leaves the
+// same slot layout (lane g, register k1 -> physical pair m = k1 + R*bitrev(g)), so the
+// products are lane-local, and the r2c (decimation in time from that layout) ends in
+// natural order, where the pair Z[k], Z[N-k] of the real-to-complex split is one shuffle
+// apart.  No shared memory and no block barrier.
+template <int R>
+__device__ __forceinline__ void nl_c2r_r(const double* __restrict__ src, bool ikx, int K, int N, int g,
+                                         const double* __restrict__ wavx, const RealPlan& rp, double2 (&v)[R]) {
+#pragma unroll
+    for (int rr = 0; rr < R; ++rr) {
+        const int n = g + 32 * rr;
+        double2 xa = make_double2(0.0, 0.0), xb = make_double2(0.0, 0.0);
+        if (n < K) xa = __ldg(reinterpret_cast<const double2*>(src) + n);
+        if (N - n < K) xb = __ldg(reinterpret_cast<const double2*>(src) + (N - n));
+        if (ikx) {
+            const double ka = (n < K) ? __ldg(&wavx[2 * n]) : 0.0;
+            const double kb = (N - n < K) ? __ldg(&wavx[2 * (N - n)]) : 0.0;
+            xa = make_double2(-ka * xa.y, ka * xa.x);
+            xb = make_double2(-kb * xb.y, kb * xb.x);
+        }
+        if (n == 0) xa.y = 0.0;  // FFTW c2r ignores Im of the DC input
+        xb = cconj(xb);
+        const double2 e = cadd(xa, xb);
+        const double2 o = cmul(csub(xa, xb), cconj(__ldg(&rp.twr[n])));
+        v[rr] = make_double2(e.x - o.y, e.y + o.x);
+    }
+    wfft<R, +1>(v, 32, g, rp.half.tw);
+}
+
+// r2c of a slot-layout row; writes the K stored modes of the row at dst
+template <int R>
+__device__ __forceinline__ void nl_r2c_r(double2 (&v)[R], double* __restrict__ dst, int K, int g,
+                                         const RealPlan& rp) {
+    wfft_dit<R, -1>(v, 32, g, rp.half.tw);
+    // natural order: lane g register rr holds Z[g + 32 rr]; Z[N-k] for k = g + 32 rr is
+    // lane (32-g) register R-1-rr (g > 0), or lane 0 register R-rr (g = 0, rr > 0)
+    const int src = (32 - g) & 31;
+#pragma unroll
+    for (int rr = 0; rr < R; ++rr) {
+        double2 zb;
+        zb.x = __shfl_sync(0xffffffffu, v[R - 1 - rr].x, src);
+        zb.y = __shfl_sync(0xffffffffu, v[R - 1 - rr].y, src);
+        if (g == 0) zb = v[rr == 0 ? 0 : R - rr];
+        const int k = g + 32 * rr;
+        if (32 * rr < K && k < K) {
+            const double2 za = v[rr];
+            zb = cconj(zb);
+            const double2 e = make_double2(0.5 * (za.x + zb.x), 0.5 * (za.y + zb.y));
+            const double2 o = make_double2(0.5 * (za.x - zb.x), 0.5 * (za.y - zb.y));
+            const double2 t = cmul(__ldg(&rp.twr[k]), o);
+            reinterpret_cast<double2*>(dst)[k] = make_double2(e.x + t.y, e.y - t.x);
+        }
+    }
+}
+
+template <int R>
+__global__ void __launch_bounds__(128, 3) k_row_nl_r(NlRowArgs a) {
+    const RowArgs& r = a.r;
+    const int N = 32 * R, K = r.kxc, lgg = r.rp.half.lgg;
+    const int g = threadIdx.x & 31;
+    const int nitems = r.nyl * r.nzp;
+    const int W = gridDim.x * (blockDim.x >> 5);
+    // physical x of the pair held in register k1: 2m, 2m+1 with m = k1 + R*bitrev(g)
+    const int mb = R * brev(g, lgg);
+    for (int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); row < nitems; row += W) {
+        const int z = row / r.nyl;
+        const long long off = (long long)row * 2 * K;
+        const double ub = a.ubar[z], ubp = a.ubarp[z];
+        double2 u[3][R];
+#pragma unroll
+        for (int l = 0; l < 3; ++l) nl_c2r_r<R>(a.U[l] + off, false, K, N, g, r.wavx, r.rp, u[l]);
+#pragma unroll
+        for (int k1 = 0; k1 < R; ++k1) {
+            u[0][k1].x += ub;
+            u[0][k1].y += ub;
+        }
+        // fluxes 0.5 u_l u_m for (11, 12, 13, 22, 23, 33)
+#pragma unroll
+        for (int p = 0; p < 6; ++p) {
+            const int l = (p < 3) ? 0 : (p < 5 ? 1 : 2);
+            const int m = (p < 3) ? p : (p < 5 ? p - 2 : 2);
+            double2 f[R];
+#pragma unroll
+            for (int k1 = 0; k1 < R; ++k1)
+                f[k1] = make_double2(0.5 * (u[l][k1].x * u[m][k1].x), 0.5 * (u[l][k1].y * u[m][k1].y));
+            nl_r2c_r<R>(f, a.H[p] + off, K, g, r.rp);
+        }
+        // convective terms -0.5 u_m d_m u_l, plus the fringe
+#pragma unroll 1
+        for (int l = 0; l < 3; ++l) {
+            double2 acc[R], d[R];
+            nl_c2r_r<R>(a.U[l] + off, true, K, N, g, r.wavx, r.rp, d);
+#pragma unroll
+            for (int k1 = 0; k1 < R; ++k1)
+                acc[k1] = make_double2(0.0 - 0.5 * (u[0][k1].x * d[k1].x), 0.0 - 0.5 * (u[0][k1].y * d[k1].y));
+            nl_c2r_r<R>(a.DY[l] + off, false, K, N, g, r.wavx, r.rp, d);
+#pragma unroll
+            for (int k1 = 0; k1 < R; ++k1) {
+                acc[k1].x = acc[k1].x - 0.5 * (u[1][k1].x * d[k1].x);
+                acc[k1].y = acc[k1].y - 0.5 * (u[1][k1].y * d[k1].y);
+            }
+            nl_c2r_r<R>(a.DZ[l] + off, false, K, N, g, r.wavx, r.rp, d);
+            const double dzb = (l == 0) ? ubp : 0.0;
+#pragma unroll
+            for (int k1 = 0; k1 < R; ++k1) {
+                acc[k1].x = acc[k1].x - 0.5 * (u[2][k1].x * (d[k1].x + dzb));
+                acc[k1].y = acc[k1].y - 0.5 * (u[2][k1].y * (d[k1].y + dzb));
+            }
+            if (a.lamx != nullptr) {
+                const double ut = (l == 0) ? ub : 0.0;
+#pragma unroll
+                for (int k1 = 0; k1 < R; ++k1) {
+                    const int x = 2 * (k1 + mb);
+                    const double lx0 = __ldg(&a.lamx[x]), lx1 = __ldg(&a.lamx[x + 1]);
+                    const double ua = (l == 0) ? u[0][k1].x : (l == 1 ? u[1][k1].x : u[2][k1].x);
+                    const double ubb = (l == 0) ? u[0][k1].y : (l == 1 ? u[1][k1].y : u[2][k1].y);
+                    acc[k1].x = acc[k1].x + lx0 * (ut - ua);
+                    acc[k1].y = acc[k1].y + lx1 * (ut - ubb);
+                }
+            }
+            nl_r2c_r<R>(acc, a.N[l] + off, K, g, r.rp);
+        }
+    }
+}
+
 template <class K>
 int persistent_grid_w(K kern, size_t smem, long long nitems) {
     static int nsm = 0;
@@ -504,7 +631,7 @@ void ylaunch(const YInvJobList& ij, const YFwdJobList& fj, const YPassArgs& a, c
     const int nch = (a.kxc + WKC - 1) / WKC;
     const int nitems = (INV ? ij.n : fj.n) * a.nzp * nch;
     const size_t sm = (size_t)2 * a.nyl * (WKC + 1) * sizeof(double2);
-    k_ywarp<R, INV><<<persistent_grid_w(k_ywarp<R, INV>, sm, nitems), 256, sm, s>>>(ij, fj, a, nch);
+    { lsb::note_launch(); k_ywarp<R, INV><<<persistent_grid_w(k_ywarp<R, INV>, sm, nitems), 256, sm, s>>>(ij, fj, a, nch); }
 }
 
 template <bool INV>
@@ -526,8 +653,8 @@ void rowlaunch(const RowJobList& jobs, const RowArgs& a, cudaStream_t s, bool c2
     const size_t sm = (size_t)8 * 32 * (N + 1) * sizeof(double2) / a.rp.half.g;
     const long long units = (long long)jobs.n * a.nyl * a.nzp;
     const long long blocks = (units + 8 * 32 / a.rp.half.g - 1) / (8 * 32 / a.rp.half.g);
-    if (c2r) k_row_c2r_w<R><<<persistent_grid_w(k_row_c2r_w<R>, sm, blocks), 256, sm, s>>>(jobs, a);
-    else k_row_r2c_w<R><<<persistent_grid_w(k_row_r2c_w<R>, sm, blocks), 256, sm, s>>>(jobs, a);
+    if (c2r) { lsb::note_launch(); k_row_c2r_w<R><<<persistent_grid_w(k_row_c2r_w<R>, sm, blocks), 256, sm, s>>>(jobs, a); }
+    else { lsb::note_launch(); k_row_r2c_w<R><<<persistent_grid_w(k_row_r2c_w<R>, sm, blocks), 256, sm, s>>>(jobs, a); }
 }
 
 bool rowdispatch(const RowJobList& jobs, const RowArgs& a, cudaStream_t s, bool c2r) {
@@ -545,10 +672,26 @@ bool rowdispatch(const RowJobList& jobs, const RowArgs& a, cudaStream_t s, bool 
 template <int R>
 void nllaunch(const NlRowArgs& a, cudaStream_t s) {
     const int N = a.r.nxl / 2;
+    const int nitems = a.r.nyl * a.r.nzp;
+    if (a.r.rp.half.g == 32) {
+        static int nsm = 0;
+        if (nsm == 0) {
+            int dev = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+            if (nsm <= 0) nsm = 148;
+        }
+        int occ = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_row_nl_r<R>, 128, 0);
+        if (occ < 1) occ = 1;
+        long long blocks = (long long)occ * nsm, need = (nitems + 3) / 4;
+        if (blocks > need) blocks = need > 0 ? need : 1;
+        { lsb::note_launch(); k_row_nl_r<R><<<(int)blocks, 128, 0, s>>>(a); }
+        return;
+    }
     const size_t sm =
         ((size_t)18 * a.r.kxc + (size_t)12 * N + (size_t)8 * 32 / a.r.rp.half.g * (N + 1)) * sizeof(double2);
-    const int nitems = a.r.nyl * a.r.nzp;
-    k_row_nl_w<R><<<persistent_grid_w(k_row_nl_w<R>, sm, nitems), 256, sm, s>>>(a);
+    { lsb::note_launch(); k_row_nl_w<R><<<persistent_grid_w(k_row_nl_w<R>, sm, nitems), 256, sm, s>>>(a); }
 }
 
 }  // namespace

@@ -164,7 +164,7 @@ void launch_gemm(const GemmArgs& g, cudaStream_t s) {
             cudaFuncSetAttribute(k_gemm<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);      \
             attr = true;                                                                                \
         }                                                                                               \
-        k_gemm<n><<<grid, 256, sm, s>>>(g);                                                             \
+        { lsb::note_launch(); k_gemm<n><<<grid, 256, sm, s>>>(g); }                                                             \
         break;                                                                                          \
     }
         LSB_MT(1) LSB_MT(2) LSB_MT(3) LSB_MT(4) LSB_MT(5) LSB_MT(6) LSB_MT(7) LSB_MT(8) LSB_MT(9)

@@ -17,6 +17,9 @@
 
 namespace lsb {
 
+// counts every kernel launch of the library (lsb_kernel_launches)
+void note_launch();
+
 constexpr int kMaxStages = 16;
 
 // exact unsigned division by a constant: q = (umulhi(n, m) + n) >> s  (d > 1), valid for

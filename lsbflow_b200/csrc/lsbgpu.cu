@@ -3,6 +3,7 @@
 // lsb_step() is timestep() / navierstokes_update() (src/navierstokes.f90:10-90, 1157-1496)
 // as a fixed sequence of kernels on one stream, with the histories (u^{n-1}, u^{n-2},
 // N^{n-1}, N^{n-2}, p^{n-1}) kept resident as rotating buffers: no copies between steps.
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -659,6 +660,10 @@ void check_launch() {
 
 namespace lsb {
 void set_last_error(const std::string& m) { g_err = m; }
+
+// kernels launched by this library since it was loaded (all handles, all threads)
+static std::atomic<unsigned long long> g_kernel_launches{0};
+void note_launch() { g_kernel_launches.fetch_add(1, std::memory_order_relaxed); }
 }  // namespace lsb
 
 // ====================================================================================== C ABI
@@ -666,6 +671,7 @@ extern "C" {
 
 const char* lsb_last_error(void) { return g_err.c_str(); }
 int lsb_version(void) { return 1; }
+unsigned long long lsb_kernel_launches(void) { return lsb::g_kernel_launches.load(); }
 
 int lsb_create(const lsb_config* cfg, const lsb_setup* su, lsb_handle** out) {
     return guard([&] {

@@ -27,6 +27,7 @@
 
 namespace lsb {
 void set_last_error(const std::string& m);  // lsbgpu.cu
+void note_launch();                         // lsbgpu.cu
 }
 
 namespace {
@@ -130,8 +131,8 @@ void launch_chunk(int mt, dim3 grid, cudaStream_t s, const double* A, int M, int
     switch (mt) {
 #define LSB_NA(n)                                                                                          \
     case n:                                                                                                \
-        k_helm_chunk<n, SCALE><<<grid, 256, 0, s>>>(A, M, K, kp, in, in_ld, koff, out, out_ld, c0, ncols, \
-                                                    in_c0, out_c0, lam, wavx, wavy, nx, sigma);            \
+        { lsb::note_launch(); k_helm_chunk<n, SCALE><<<grid, 256, 0, s>>>(A, M, K, kp, in, in_ld, koff, out, out_ld, c0, ncols, \
+                                                    in_c0, out_c0, lam, wavx, wavy, nx, sigma); }            \
         break;
         LSB_NA(1) LSB_NA(2) LSB_NA(3) LSB_NA(4) LSB_NA(5) LSB_NA(6) LSB_NA(7) LSB_NA(8) LSB_NA(9)
         LSB_NA(10) LSB_NA(11) LSB_NA(12) LSB_NA(13) LSB_NA(14) LSB_NA(15) LSB_NA(16) LSB_NA(17)
@@ -186,7 +187,7 @@ extern "C" int lsb_solve_helmholtz_noalloc(int nx, int ny, int nz, const double*
     double* a1 = base;                        // padded E^-1
     double* a2 = base + (long long)kMaxMp * kMaxKp;  // padded E with zero ceiling / wall rows
     double* tmp = base + kMatDoubles;         // nzm x chunk intermediate
-    k_pad_mats<<<64, 256, 0, s>>>(e, ei, nzm, mp1, mp2, kp, a1, a2);
+    { lsb::note_launch(); k_pad_mats<<<64, 256, 0, s>>>(e, ei, nzm, mp1, mp2, kp, a1, a2); }
     for (long long c0 = 0; c0 < C; c0 += chunk) {
         const long long nc = (C - c0 < chunk) ? C - c0 : chunk;
         dim3 grid((unsigned)((nc + kBN - 1) / kBN));

@@ -121,7 +121,7 @@ void filter3(lsb_handle* h, const double* const* in, double* const* out, int n, 
         const double* zf = h->sgs.zf + (long long)which * 3 * d.nzp;  // which: 0 (a,b) 1 (1,1) 2 (1,6) 3 (1,2)
         TimerScope ts(h, "sgs_filter3");
         dim3 grid((d.nx + FIB - 1) / FIB, (d.ny + FJB - 1) / FJB, nzc * fl.n);
-        k_filter3<<<grid, 256, 0, h->stream>>>(fl, d.nx, d.ny, d.nzp, a, b, zf, zf + d.nzp, zf + 2 * d.nzp, nzc);
+        { lsb::note_launch(); k_filter3<<<grid, 256, 0, h->stream>>>(fl, d.nx, d.ny, d.nzp, a, b, zf, zf + d.nzp, zf + 2 * d.nzp, nzc); }
     }
 }
 
@@ -330,7 +330,7 @@ __global__ void k_mul(double* y, const double* x, long long n) {
 
 }  // namespace
 
-void sgs_mul(double* y, const double* x, long long n, cudaStream_t s) { k_mul<<<nblk(n), 256, 0, s>>>(y, x, n); }
+void sgs_mul(double* y, const double* x, long long n, cudaStream_t s) { lsb::note_launch(); k_mul<<<nblk(n), 256, 0, s>>>(y, x, n); }
 
 static void zfilter_coeffs(const std::vector<double>& zp, int mapping, double a, double b, double* az, double* bz,
                            double* cz) {
@@ -446,18 +446,18 @@ static void model_tau(lsb_handle* h, const double* const* u, const double* const
         a.delta = s.delta;
         a.P = P;
         a.nxy = nxy;
-        k_dyn1<<<nblk(P), 256, 0, st>>>(a);
+        { lsb::note_launch(); k_dyn1<<<nblk(P), 256, 0, st>>>(a); }
         filter3(h, (const double* const*)a.sij, a.sijhat, 6, c.a, c.b, 0);
-        k_dyn2<<<nblk(P), 256, 0, st>>>(a);
+        { lsb::note_launch(); k_dyn2<<<nblk(P), 256, 0, st>>>(a); }
         filter3(h, (const double* const*)a.lij, a.mij, 6, c.a, c.b, 0);
         double* uh[3] = {W(30), W(31), W(32)};
         filter3(h, u, uh, 3, c.a, c.b, 0);
         filter3(h, uu6, a.lf, 6, c.a, c.b, 0);
-        k_dyn3<<<nblk(P), 256, 0, st>>>(a);
+        { lsb::note_launch(); k_dyn3<<<nblk(P), 256, 0, st>>>(a); }
         const double* nd[2] = {a.numc, a.denomc};
         double* cc[2] = {W(36), W(37)};
         filter3(h, nd, cc, 2, 1.0, 1.0, 1);
-        k_dyn4<<<nblk(P), 256, 0, st>>>(a);
+        { lsb::note_launch(); k_dyn4<<<nblk(P), 256, 0, st>>>(a); }
     } else if (c.sgsmodel == 0) {
         P9 gt{};
         W9 tt{};
@@ -465,8 +465,8 @@ static void model_tau(lsb_handle* h, const double* const* u, const double* const
             gt.p[q] = g[q];
             tt.p[q] = T[q];
         }
-        k_utau<<<1, 256, 0, st>>>(g[2], h->sgs_wall, h->sgs_nwall, d.C(), c.xnu, nxy, s.scal);
-        k_static<<<nblk(P), 256, 0, st>>>(gt, tt, s.sdelta, h->zpts, s.scal, c.cs, c.xnu, P, nxy);
+        { lsb::note_launch(); k_utau<<<1, 256, 0, st>>>(g[2], h->sgs_wall, h->sgs_nwall, d.C(), c.xnu, nxy, s.scal); }
+        { lsb::note_launch(); k_static<<<nblk(P), 256, 0, st>>>(gt, tt, s.sdelta, h->zpts, s.scal, c.cs, c.xnu, P, nxy); }
     } else if (c.sgsmodel == 2) {
         P9 gt{};
         W9 tt{};
@@ -474,7 +474,7 @@ static void model_tau(lsb_handle* h, const double* const* u, const double* const
             gt.p[q] = g[q];
             tt.p[q] = T[q];
         }
-        k_sigma<<<nblk(P), 256, 0, st>>>(gt, tt, s.delta, P, nxy);
+        { lsb::note_launch(); k_sigma<<<nblk(P), 256, 0, st>>>(gt, tt, s.delta, P, nxy); }
     } else if (c.sgsmodel == 3) {
         double* ub[3] = {W(0), W(1), W(2)};
         double* ub2[3] = {W(3), W(4), W(5)};
@@ -498,9 +498,9 @@ static void model_tau(lsb_handle* h, const double* const* u, const double* const
             pbt.p[q] = pb[q];
             tt.p[q] = T[q];
         }
-        k_prod9<<<nblk(P), 256, 0, st>>>(ubt, ut, prt, P);
+        { lsb::note_launch(); k_prod9<<<nblk(P), 256, 0, st>>>(ubt, ut, prt, P); }
         filter3(h, (const double* const*)pr, pb, 9, c.a, c.b, 0);
-        k_interscale<<<nblk(P), 256, 0, st>>>(ut, ubt, ub2t, pbt, tt, P);
+        { lsb::note_launch(); k_interscale<<<nblk(P), 256, 0, st>>>(ut, ubt, ub2t, pbt, tt, P); }
     } else {
         CK(cudaMemsetAsync(tau, 0, 9 * P * sizeof(double), st));
     }
@@ -527,7 +527,7 @@ void sgs_add_tau(lsb_handle* h, double* const* ph, bool dealias) {
         W9 ot{};
         for (int l = 0; l < 3; ++l) ut.p[l] = ph[l];
         for (int q = 0; q < 6; ++q) ot.p[q] = uu6[q];
-        k_uiuj<<<nblk(P), 256, 0, st>>>(ut, ot, P);
+        { lsb::note_launch(); k_uiuj<<<nblk(P), 256, 0, st>>>(ut, ot, P); }
     }
     const double* g[9];
     for (int q = 0; q < 9; ++q) g[q] = ph[3 + q];
@@ -638,8 +638,8 @@ void filter_hook(lsb_handle* h) {
             qb.p[f] = B[f];
         }
         double* e = h->red;
-        k_plane_sqdiff<<<d.nzp, 256, 0, h->stream>>>(qq, qb, d.nx, d.ny, e);             // energy(:,3)
-        k_plane_sqdiff<<<d.nzp, 256, 0, h->stream>>>(qq, qa, d.nx, d.ny, e + d.nzp);     // energy(:,4)
+        { lsb::note_launch(); k_plane_sqdiff<<<d.nzp, 256, 0, h->stream>>>(qq, qb, d.nx, d.ny, e); }             // energy(:,3)
+        { lsb::note_launch(); k_plane_sqdiff<<<d.nzp, 256, 0, h->stream>>>(qq, qa, d.nx, d.ny, e + d.nzp); }     // energy(:,4)
         std::vector<double> en(2 * (size_t)d.nzp);
         CK(cudaMemcpyAsync(en.data(), e, en.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
@@ -726,7 +726,7 @@ void diag_compute(lsb_handle* h, lsb_diagnostics* out) {
     // physical u (+ubar), v, w; perturbation copies (mean mode removed); divergence
     double* io = h->io;
     CK(cudaMemcpyAsync(io, h->vel, 3 * S * sizeof(double), cudaMemcpyDeviceToDevice, st));
-    for (int l = 0; l < 3; ++l) k_zero_mean<<<(d.nzp + 127) / 128, 128, 0, st>>>(io + l * S, S, C, d.nzp);
+    for (int l = 0; l < 3; ++l) { lsb::note_launch(); k_zero_mean<<<(d.nzp + 127) / 128, 128, 0, st>>>(io + l * S, S, C, d.nzp); }
     // divergence = dfdx(u) + dfdy(v) + dfdz(w)
     double* dv = io + 3 * S;
     zgemm(h, h->m_dz1, h->vel + 2 * S, dv, 1, EPI_STORE, 1.0, 0.0, nullptr);
@@ -752,8 +752,8 @@ void diag_compute(lsb_handle* h, lsb_diagnostics* out) {
     int findex = d.nx;
     if (h->t > h->cfg.istartbound) findex = (int)((1. - 0.8 * fsz) * d.nx);
     double* stats = h->T;
-    k_plane_stats<<<d.nzp, 256, 0, st>>>(ph[0], ph[1], ph[2], ph[3], ph[4], ph[5], ph[6], wsd, findex, d.nx, d.ny,
-                                         stats);
+    { lsb::note_launch(); k_plane_stats<<<d.nzp, 256, 0, st>>>(ph[0], ph[1], ph[2], ph[3], ph[4], ph[5], ph[6], wsd, findex, d.nx, d.ny,
+                                         stats); }
     std::vector<double> hs((size_t)d.nzp * kStats);
     CK(cudaMemcpyAsync(hs.data(), stats, hs.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));

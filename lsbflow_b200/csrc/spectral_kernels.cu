@@ -257,38 +257,38 @@ static inline int nblk(long long n) {
     return (int)b;
 }
 
-void launch_specfilter(const SpecFilterArgs& a, cudaStream_t s) { k_specfilter<<<nblk(3 * a.S / 2), 256, 0, s>>>(a); }
-void launch_rhs(const RhsArgs& a, cudaStream_t s) { k_rhs<<<nblk(3 * a.S), 256, 0, s>>>(a); }
-void launch_bc_planes(const BcArgs& a, cudaStream_t s) { k_bc_planes<<<nblk(a.C / 2), 256, 0, s>>>(a); }
+void launch_specfilter(const SpecFilterArgs& a, cudaStream_t s) { lsb::note_launch(); k_specfilter<<<nblk(3 * a.S / 2), 256, 0, s>>>(a); }
+void launch_rhs(const RhsArgs& a, cudaStream_t s) { lsb::note_launch(); k_rhs<<<nblk(3 * a.S), 256, 0, s>>>(a); }
+void launch_bc_planes(const BcArgs& a, cudaStream_t s) { lsb::note_launch(); k_bc_planes<<<nblk(a.C / 2), 256, 0, s>>>(a); }
 void launch_divuv(const double* u, const double* v, double* out, const double* wavx, const double* wavy, int nx,
                   long long S, long long C, cudaStream_t s) {
-    k_divuv<<<nblk(S / 2), 256, 0, s>>>(u, v, out, wavx, wavy, nx, S, C);
+    { lsb::note_launch(); k_divuv<<<nblk(S / 2), 256, 0, s>>>(u, v, out, wavx, wavy, nx, S, C); }
 }
 void launch_dxy(const double* in, double* out, const double* wavx, const double* wavy, int nx, long long S,
                 long long C, int mode, cudaStream_t s) {
-    k_dxy<<<nblk(S / 2), 256, 0, s>>>(in, out, wavx, wavy, nx, S, C, mode);
+    { lsb::note_launch(); k_dxy<<<nblk(S / 2), 256, 0, s>>>(in, out, wavx, wavy, nx, S, C, mode); }
 }
 void launch_lapl_xy(const double* u, double* d2, const double* wavx, const double* wavy, int nx, long long S,
                     long long C, cudaStream_t s) {
-    k_lapl_xy<<<nblk(S), 256, 0, s>>>(u, d2, wavx, wavy, nx, S, C);
+    { lsb::note_launch(); k_lapl_xy<<<nblk(S), 256, 0, s>>>(u, d2, wavx, wavy, nx, S, C); }
 }
-void launch_nl_div_xy(const NlDivArgs& a, cudaStream_t s) { k_nl_div_xy<<<nblk(3 * a.S / 2), 256, 0, s>>>(a); }
+void launch_nl_div_xy(const NlDivArgs& a, cudaStream_t s) { lsb::note_launch(); k_nl_div_xy<<<nblk(3 * a.S / 2), 256, 0, s>>>(a); }
 void launch_pressure_update(double* u, double* v, const double* p, const double* wavx, const double* wavy, int nx,
                             long long S, long long C, double dtb, cudaStream_t s) {
-    k_pressure_update<<<nblk(S / 2), 256, 0, s>>>(u, v, p, wavx, wavy, nx, S, C, dtb);
+    { lsb::note_launch(); k_pressure_update<<<nblk(S / 2), 256, 0, s>>>(u, v, p, wavx, wavy, nx, S, C, dtb); }
 }
 void launch_norm(double* f0, double* f1, double* f2, int nx, int ny, int nzp, int ifrz, cudaStream_t s) {
-    k_norm<<<dim3(nzp, 3), 128, 0, s>>>(f0, f1, f2, nx, ny, nzp, ifrz);
+    { lsb::note_launch(); k_norm<<<dim3(nzp, 3), 128, 0, s>>>(f0, f1, f2, nx, ny, nzp, ifrz); }
 }
 void launch_force_phys(const double* u0, const double* u1, const double* u2, double* f0, double* f1, double* f2,
                        const double* lamx, const double* ubar, int nx, int ny, long long P, cudaStream_t s) {
-    k_force_phys<<<nblk(P), 256, 0, s>>>(u0, u1, u2, f0, f1, f2, lamx, ubar, nx, ny, P);
+    { lsb::note_launch(); k_force_phys<<<nblk(P), 256, 0, s>>>(u0, u1, u2, f0, f1, f2, lamx, ubar, nx, ny, P); }
 }
 void launch_tavg_add(double* a, const double* q, double iomod, long long n, cudaStream_t s) {
-    k_tavg_add<<<nblk(n), 256, 0, s>>>(a, q, iomod, n);
+    { lsb::note_launch(); k_tavg_add<<<nblk(n), 256, 0, s>>>(a, q, iomod, n); }
 }
 void launch_axpby(double* y, const double* x, double a, double b, long long n, cudaStream_t s) {
-    k_axpby<<<nblk(n), 256, 0, s>>>(y, x, a, b, n);
+    { lsb::note_launch(); k_axpby<<<nblk(n), 256, 0, s>>>(y, x, a, b, n); }
 }
 
 }  // namespace lsb

@@ -27,7 +27,7 @@ EXPORTS = [
     "lsb_synchronize", "lsb_horfft", "lsb_dealias_product", "lsb_dfdx", "lsb_dfdy", "lsb_dfdz", "lsb_d2fdz2",
     "lsb_lapl", "lsb_divuv", "lsb_solve_helmholtz", "lsb_solve_nhom_helmholtz", "lsb_nlterm", "lsb_tau_sgs",
     "lsb_upload_velocity", "lsb_download_velocity", "lsb_timers", "lsb_timer_report",
-    "lsb_solve_helmholtz_noalloc", "lsb_tavg",
+    "lsb_solve_helmholtz_noalloc", "lsb_tavg", "lsb_kernel_launches",
 ]
 
 
@@ -81,7 +81,9 @@ def load() -> C.CDLL:
         lib.lsb_last_error.restype = C.c_char_p
         for name in EXPORTS:
             f = getattr(lib, name)
-            if name != "lsb_last_error":
+            if name == "lsb_kernel_launches":
+                f.restype = C.c_ulonglong
+            elif name != "lsb_last_error":
                 f.restype = C.c_int
         _lib = lib
     return _lib
@@ -99,6 +101,11 @@ def _ck(rc: int):
 def _ptr(a: np.ndarray):
     assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
     return a.ctypes.data_as(_dp)
+
+
+def kernel_launches() -> int:
+    """Kernels the library has launched since it was loaded (all handles)."""
+    return int(load().lsb_kernel_launches())
 
 
 def config_struct(cfg: LsbConfig) -> LsbConfigC:

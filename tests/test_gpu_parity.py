@@ -127,6 +127,18 @@ def test_nlterm_production_sizes(nx, ny, nz, layout):
         assert rel(got[l], ref[l]) < TOL_OP, (l, rel(got[l], ref[l]))
 
 
+@pytest.mark.parametrize("nx,ny,nz", [(64, 8, 16), (128, 8, 16), (256, 16, 32), (384, 8, 16)])
+def test_nlterm_fringe_full_warp(nx, ny, nz):
+    # unpadded rows of 32 R complex (R = 1, 2, 4, 6) with the fringe term: the
+    # register-resident product kernel, one warp per row
+    st, s = solver(workload("dns64", nx=nx, ny=ny, nz=nz, dealiasflag=0, forcing=1))
+    u, v, w = ic.seeded_noise(st, 13, 1e-2)
+    ref = O.nlterm_skewsym(st, [u, v, w])
+    got = s.nlterm(np.array([u, v, w]))
+    for l in range(3):
+        assert rel(got[l], ref[l]) < TOL_OP, (l, rel(got[l], ref[l]))
+
+
 @pytest.mark.parametrize("nx,ny,nz", [(128, 32, 64), (256, 64, 128), (64, 48, 16)])
 def test_horfft_production_sizes(nx, ny, nz):
     st, s = solver(workload("les256", nx=nx, ny=ny, nz=nz, sgsflag=0, dealiasflag=0))
