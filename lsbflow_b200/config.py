@@ -31,6 +31,8 @@ class LsbConfig:
     nx: int = 64
     ny: int = 16
     nz: int = 64
+    # &flaglist
+    nstart: int = 0
     # &run
     cfl: float = 0.1
     dtadapt: int = 0
@@ -93,7 +95,7 @@ _NML_KEYS = {f.name.lower(): f.name for f in dataclasses.fields(LsbConfig)}
 def parse_namelist(text: str, base: LsbConfig | None = None) -> LsbConfig:
     """Parse the reference's input.dat namelist text (run/input.dat layout).
 
-    Unknown keys (``nstart``, ``iwrite``, ``prtl`` ...) are accepted and ignored,
+    Unknown keys (``iwrite``, ``prtl`` ...) are accepted and ignored,
     as they do not touch the time-step path.
     """
     cfg = dataclasses.replace(base) if base is not None else LsbConfig()
@@ -127,7 +129,8 @@ def workload(name: str, **over) -> LsbConfig:
     """Named workloads in the reference's axes (x stream, y span, z Chebyshev).
 
     dns64   : 64 x 16 x 64 (nzp 65) plain DNS, Re_d*=500, fringe 10%, dipole ceiling BC.
-    os128   : 128 x 4 x 96 (nzp 97) Orr-Sommerfeld linear test grid, Re_d*=1000.
+    os128   : 128 x 4 x 96 (nzp 97) Orr-Sommerfeld linear test, Re_d*=1000 (displacement
+              thickness), alpha d* = 0.25: the domain is one wavelength (linstab = 1).
     les256  : 256 x 64 x 128 (nzp 129) dynamic-Smagorinsky LES with the 3/2 rule.
     ens128  : 128 x 32 x 64 (nzp 65) sigma-model LES member.
     Lengths are 200/20/20 displacement thicknesses (xlen/ylen/zlen).
@@ -158,4 +161,9 @@ def workload(name: str, **over) -> LsbConfig:
         sgsflag=sgs, sgsmodel=model, dealiasflag=dal, dealias_layout="correct",
         a=1.0, b=6.0, ic=2,
     )
+    if name == "os128":
+        # one wavelength 2 pi / alpha; astar is the reference's alpha * 6.02 sqrt(nu x0 / U)
+        alpha = 0.25 / dstar
+        cfg = dataclasses.replace(cfg, linstab=1, astar=alpha * 6.02 * math.sqrt(xnu * cfg.x0 / u0),
+                                  cguess=0.36 + 0.0j, zlen=20.0 * dstar, nsteps=500)
     return dataclasses.replace(cfg, **over)

@@ -111,7 +111,7 @@ def kernel_launches() -> int:
 def config_struct(cfg: LsbConfig) -> LsbConfigC:
     return LsbConfigC(
         cfg.nx, cfg.ny, cfg.nz, cfg.dealiasflag, 0 if cfg.dealias_layout == "ref" else 1,
-        cfg.sgsflag, cfg.sgsmodel, cfg.forcing, cfg.bctype, cfg.ifrz, 0, cfg.mapping,
+        cfg.sgsflag, cfg.sgsmodel, cfg.forcing, cfg.bctype, cfg.ifrz, cfg.nstart, cfg.mapping,
         cfg.xnu, cfg.u0, cfg.x0, cfg.xlen, cfg.ylen, cfg.zlen, cfg.a, cfg.b, cfg.CS,
         cfg.kc, cfg.filt_order, cfg.filt_amp, cfg.istartbound, cfg.samp,
         cfg.bc3_amp, cfg.bc3_xc, cfg.bc3_s, cfg.fsize,

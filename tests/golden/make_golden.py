@@ -13,6 +13,9 @@ What is extracted (all from the reference's run/ folder):
   deviations of u from that profile and of |v|, |w|, |p| over the whole grid
 * input.dat  : copied as text (the namelist of that run)
 * energy.dat : the Orr-Sommerfeld sweep table (Re, alpha*, omega_i, <dE/dt>, err%)
+* output_lintest.txt : per case of that sweep the header (Re_d, x0, alpha*, Re(cguess)),
+               the last omega of the inverse iteration (10 digits), the final dt
+               and the number of time steps
 """
 import os
 import re
@@ -80,6 +83,17 @@ def main(ref):
     d["input_dat"] = np.array(open(os.path.join(run, "input.dat")).read())
     en = open(os.path.join(run, "energy.dat")).read().strip().splitlines()[1:]
     d["os_energy_table"] = np.array([[float(x) for x in l.strip().rstrip(",").split(",")] for l in en])
+    lt = open(os.path.join(run, "output_lintest.txt")).read()
+    cases = []
+    for blk in lt.split(" Re_d =")[1:]:
+        h = re.match(r"\s*([-\d.Ee+]+)\s*, x0 =\s*([-\d.Ee+]+)\s*, astar =\s*([-\d.Ee+]+)\s*, "
+                     r"cguess = \(\s*([-\d.Ee+]+)", blk)
+        sec = blk.split("solving for most unstable eigenvalue")[1].split("time reqd")[0]
+        it = re.findall(r"\n\s+\d+,\s*([-\d.Ee+]+)\s*,\s*([-\d.Ee+]+)\s*,", sec)[-1]
+        dt = float(re.search(r"final time step dt =\s*([-\d.Ee+]+)", blk).group(1))
+        nst = float(re.search(r"# of its performed =\s*(\d+)", blk).group(1))
+        cases.append([float(x) for x in h.groups()] + [float(it[0]), float(it[1]), dt, nst])
+    d["os_cases"] = np.array(cases)  # Re_d, x0, alpha*, cguess_r, omega_r, omega_i, dt, nsteps
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_run.npz")
     np.savez_compressed(out, **d)
     print("wrote", out, os.path.getsize(out), "bytes")
