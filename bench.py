@@ -176,6 +176,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serve-runs", type=int, default=12)
     args = ap.parse_args()
     cfg = workload(args.workload)
     if args.impl == "reference":
@@ -276,6 +278,23 @@ def main():
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e_val = replicas.job_throughput(pts, e2e_steps, world, e2e_s)
 
+    # ---- serving: a Poisson stream of ensemble runs (continuous batching on this GPU)
+    serving = None
+    if not args.no_serving:
+        from lsbflow_b200 import serving as S
+        shapes = [workload("ens128"), workload("ens128", sgsmodel=1), workload("dns64", dealiasflag=1)]
+        reqs = S.poisson_requests(args.serve_runs, 4.0, 11 + rank, shapes, steps_range=(100, 400))
+        srv = S.Server(chunk=20)
+        for r in reqs:
+            srv.submit(r)
+        res = srv.run()
+        summ = S.summary(res, srv.elapsed)
+        serving = {"runs": summ["runs"], "runs_per_hour": round(summ["runs_per_hour"], 1),
+                   "p50_s": round(summ["p50"], 4), "p99_s": round(summ["p99"], 4),
+                   "pt_steps_per_s": summ["pt_steps_per_s"], "elapsed_s": round(summ["elapsed_s"], 3),
+                   "arrivals": "Poisson 4/s, seeded", "mix": "ens128 sigma / ens128 dyn-Smagorinsky / dns64",
+                   "horizon_steps": [100, 400]}
+
     # ---- the CPU baseline (rank 0, N = 1 only), bounded sample
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -300,6 +319,7 @@ def main():
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": 3 * S8, "d2h_bytes_per_step": 3 * S8},
             "gpu_launches": launches,
             "cpu_baseline": cpu,
+            "serving": serving,
         }
         print(json.dumps(line), flush=True)
     sol.close()

@@ -92,6 +92,9 @@ int lsb_version(void);
 /* kernels this library has launched since it was loaded, over all handles (no reference
    counterpart: a launch count for profiling and for checking that the GPU path ran) */
 unsigned long long lsb_kernel_launches(void);
+/* device memory held by a handle, in bytes (no reference counterpart: the serving loop
+   admits runs by this footprint) */
+int lsb_device_bytes(lsb_handle* h, unsigned long long* bytes);
 
 /* ---------------- Tier 2: resident state --------------------------------------------- */
 /* replaces initialize()'s device-side part (src/init.f90:7-127) */

@@ -88,9 +88,11 @@ struct lsb_handle {
     double abfac[3] = {0, 0, 0}, bdf[3] = {0, 0, 0}, bdfv = 0;
     double bshape_norm = 0.0;  // bctype 1: S_top(0,0) / S_wall(0,0) helper
 
+    size_t device_bytes = 0;  // sum of this handle's device allocations
     double* alloc(size_t n) {
         void* q = nullptr;
         CK(cudaMalloc(&q, n * sizeof(double) > 0 ? n * sizeof(double) : 8));
+        device_bytes += n * sizeof(double) > 0 ? n * sizeof(double) : 8;
         CK(cudaMemsetAsync(q, 0, n * sizeof(double), stream));
         allocs.push_back(q);
         return (double*)q;

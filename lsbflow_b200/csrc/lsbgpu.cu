@@ -673,6 +673,13 @@ const char* lsb_last_error(void) { return g_err.c_str(); }
 int lsb_version(void) { return 1; }
 unsigned long long lsb_kernel_launches(void) { return lsb::g_kernel_launches.load(); }
 
+int lsb_device_bytes(lsb_handle* h, unsigned long long* bytes) {
+    return guard([&] {
+        if (!h || !bytes) fail(LSB_ERR_ARG, "null argument");
+        *bytes = h->device_bytes;
+    });
+}
+
 int lsb_create(const lsb_config* cfg, const lsb_setup* su, lsb_handle** out) {
     return guard([&] {
         if (!cfg || !su || !out) fail(LSB_ERR_ARG, "null argument");

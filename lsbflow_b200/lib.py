@@ -27,7 +27,7 @@ EXPORTS = [
     "lsb_synchronize", "lsb_horfft", "lsb_dealias_product", "lsb_dfdx", "lsb_dfdy", "lsb_dfdz", "lsb_d2fdz2",
     "lsb_lapl", "lsb_divuv", "lsb_solve_helmholtz", "lsb_solve_nhom_helmholtz", "lsb_nlterm", "lsb_tau_sgs",
     "lsb_upload_velocity", "lsb_download_velocity", "lsb_timers", "lsb_timer_report",
-    "lsb_solve_helmholtz_noalloc", "lsb_tavg", "lsb_kernel_launches",
+    "lsb_solve_helmholtz_noalloc", "lsb_tavg", "lsb_kernel_launches", "lsb_device_bytes",
 ]
 
 
@@ -209,6 +209,11 @@ class Solver:
 
     def synchronize(self):
         _ck(self._lib.lsb_synchronize(self._h))
+
+    def device_bytes(self) -> int:
+        b = C.c_ulonglong()
+        _ck(self._lib.lsb_device_bytes(self._h, C.byref(b)))
+        return int(b.value)
 
     def set_stream(self, stream_handle: int | None):
         _ck(self._lib.lsb_set_stream(self._h, C.c_void_p(stream_handle or 0)))

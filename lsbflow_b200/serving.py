@@ -1,0 +1,209 @@
+"""Request loop for ensemble runs on one GPU (continuous batching of independent runs).
+
+Each admitted run is one library handle on its own CUDA stream; its state stays resident in
+HBM from admission to result.  The loop works at step boundaries:
+
+* admission -- queued requests that have arrived are admitted, oldest first, while the
+  sum of device footprints stays inside the memory budget and a slot is free.  The
+  footprint of a (grid, model) shape is the measured ``lsb_device_bytes`` of the first
+  handle of that shape; before one exists it is estimated as 64 spectral fields.
+* stepping -- every active run has at most one chunk of ``chunk`` steps in flight on its
+  stream; when a chunk's event has completed the next chunk is queued, so runs of
+  different sizes advance concurrently and kernels of different streams overlap.
+* completion -- a run that has done its steps is downloaded, its handle freed, and its
+  slot and memory go to the next arrival.
+
+Results do not depend on what else runs: handles share no device memory and every kernel
+of a run is on that run's stream.  ``percentiles`` gives p50/p99 of time-to-result
+(completion minus arrival) and the loop reports runs per hour and grid-point-steps/s.
+"""
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .config import LsbConfig
+
+
+@dataclass
+class RunRequest:
+    rid: int
+    cfg: LsbConfig
+    nsteps: int
+    seed: int = 0
+    amp: float = 1e-3
+    arrival: float = 0.0          # seconds after the loop starts
+
+
+@dataclass
+class RunResult:
+    rid: int
+    state: dict
+    arrival: float
+    admitted: float
+    done: float
+    nsteps: int
+    points: int
+
+    @property
+    def time_to_result(self) -> float:
+        return self.done - self.arrival
+
+
+def shape_key(cfg: LsbConfig):
+    return (cfg.nx, cfg.ny, cfg.nz, cfg.dealiasflag, cfg.sgsflag, cfg.sgsmodel, cfg.otfavg)
+
+
+def estimate_bytes(cfg: LsbConfig) -> int:
+    return 64 * cfg.nx * cfg.ny * cfg.nzp * 8
+
+
+class DeviceBackend:
+    """Handles and streams on the current CUDA device (the library's C ABI)."""
+
+    def __init__(self):
+        import torch  # device plumbing: streams and events
+        from . import lib
+        self.torch = torch
+        self.lib = lib
+        self._free, _ = torch.cuda.mem_get_info()
+
+    def free_bytes(self) -> int:
+        return int(self._free)
+
+    def start(self, req: RunRequest):
+        from . import hostsetup as hs
+        from . import ic
+        st = hs.make_setup(req.cfg)
+        s = self.lib.Solver(st)
+        stream = self.torch.cuda.Stream()
+        s.set_stream(stream.cuda_stream)
+        u, v, w = ic.seeded_noise(st, req.seed, req.amp)
+        s.upload(u, v, w, dt=st.dt)
+        return {"solver": s, "stream": stream, "event": None, "bytes": s.device_bytes()}
+
+    def launch(self, run, nsteps: int):
+        run["solver"].step(nsteps)
+        ev = self.torch.cuda.Event()
+        ev.record(run["stream"])
+        run["event"] = ev
+
+    def ready(self, run) -> bool:
+        return run["event"] is None or run["event"].query()
+
+    def finish(self, run) -> dict:
+        run["stream"].synchronize()
+        state = run["solver"].download()
+        run["solver"].close()
+        return state
+
+
+@dataclass
+class _Active:
+    req: RunRequest
+    run: dict
+    admitted: float
+    remaining: int
+    nbytes: int
+
+
+@dataclass
+class Server:
+    backend: object = None
+    memory_budget: int | None = None     # bytes; default 90% of free device memory
+    max_active: int = 32
+    chunk: int = 10
+    footprints: dict = field(default_factory=dict)
+
+    def __post_init__(self):
+        if self.backend is None:
+            self.backend = DeviceBackend()
+        if self.memory_budget is None:
+            self.memory_budget = int(0.9 * self.backend.free_bytes())
+        self.queue: list = []
+
+    def submit(self, req: RunRequest):
+        if req.nsteps <= 0:
+            raise ValueError("a run needs at least one step")
+        need = self.footprints.get(shape_key(req.cfg), estimate_bytes(req.cfg))
+        if need > self.memory_budget:
+            raise ValueError(f"run {req.rid} needs {need} bytes, more than the budget {self.memory_budget}")
+        self.queue.append(req)
+
+    def run(self, clock=time.perf_counter, idle_sleep: float = 1e-4) -> list:
+        queue = sorted(self.queue, key=lambda r: (r.arrival, r.rid))
+        self.queue = []
+        active: list = []
+        results = []
+        used = 0
+        t0 = clock()
+        while queue or active:
+            now = clock() - t0
+            # admission at a step boundary, oldest arrival first, no overtaking
+            while queue and queue[0].arrival <= now and len(active) < self.max_active:
+                req = queue[0]
+                need = self.footprints.get(shape_key(req.cfg), estimate_bytes(req.cfg))
+                if used + need > self.memory_budget and active:
+                    break
+                queue.pop(0)
+                run = self.backend.start(req)
+                nb = int(run.get("bytes") or need)
+                self.footprints[shape_key(req.cfg)] = nb
+                used += nb
+                active.append(_Active(req, run, clock() - t0, req.nsteps, nb))
+            progressed = False
+            for a in list(active):
+                if not self.backend.ready(a.run):
+                    continue
+                if a.remaining > 0:
+                    k = min(self.chunk, a.remaining)
+                    self.backend.launch(a.run, k)
+                    a.remaining -= k
+                    progressed = True
+                else:
+                    state = self.backend.finish(a.run)
+                    c = a.req.cfg
+                    results.append(RunResult(a.req.rid, state, a.req.arrival, a.admitted, clock() - t0,
+                                             a.req.nsteps, c.nx * c.ny * c.nzp))
+                    active.remove(a)
+                    used -= a.nbytes
+                    progressed = True
+            if not progressed:
+                if not active and queue:
+                    wait = queue[0].arrival - (clock() - t0)
+                    if wait > 0:
+                        time.sleep(min(wait, 0.05))
+                else:
+                    time.sleep(idle_sleep)
+        self.elapsed = clock() - t0
+        return sorted(results, key=lambda r: r.rid)
+
+
+def percentiles(results, qs=(50, 99)) -> dict:
+    ttr = np.array([r.time_to_result for r in results])
+    return {f"p{q}": float(np.percentile(ttr, q)) for q in qs}
+
+
+def summary(results, elapsed: float) -> dict:
+    out = percentiles(results)
+    out["runs"] = len(results)
+    out["runs_per_hour"] = len(results) / elapsed * 3600.0
+    out["pt_steps_per_s"] = sum(r.points * r.nsteps for r in results) / elapsed
+    out["elapsed_s"] = elapsed
+    return out
+
+
+def poisson_requests(n: int, rate: float, seed: int, shapes, steps_range=(300, 3000)) -> list:
+    """Poisson arrivals at ``rate`` per second, each drawing a grid/model from ``shapes``
+    and a horizon uniformly from ``steps_range``."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for i in range(n):
+        t += rng.exponential(1.0 / rate)
+        cfg = shapes[int(rng.integers(len(shapes)))]
+        out.append(RunRequest(i, cfg, int(rng.integers(steps_range[0], steps_range[1] + 1)), seed=1000 + i,
+                              amp=1e-3, arrival=t))
+    return out

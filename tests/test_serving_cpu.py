@@ -1,0 +1,92 @@
+"""The serving loop's admission and scheduling, with a fake device backend."""
+import pytest
+
+from lsbflow_b200 import serving as S
+from lsbflow_b200.config import workload
+
+
+class FakeBackend:
+    """Each launch completes after ``lag`` polls; records the device bytes in use."""
+
+    def __init__(self, free=10_000_000, lag=2, nbytes=None):
+        self.free = free
+        self.lag = lag
+        self.nbytes = nbytes or {}
+        self.in_use = 0
+        self.peak = 0
+        self.log = []
+
+    def free_bytes(self):
+        return self.free
+
+    def start(self, req):
+        b = self.nbytes.get(req.rid, S.estimate_bytes(req.cfg))
+        self.in_use += b
+        self.peak = max(self.peak, self.in_use)
+        self.log.append(("start", req.rid))
+        return {"rid": req.rid, "steps": 0, "polls": 0, "bytes": b}
+
+    def launch(self, run, n):
+        run["steps"] += n
+        run["polls"] = self.lag
+
+    def ready(self, run):
+        if run["polls"] > 0:
+            run["polls"] -= 1
+            return False
+        return True
+
+    def finish(self, run):
+        self.in_use -= run["bytes"]
+        self.log.append(("finish", run["rid"]))
+        return {"steps": run["steps"]}
+
+
+def cfg(nx):
+    return workload("dns64", nx=nx, ny=8, nz=16)
+
+
+def test_all_runs_complete_with_their_steps():
+    be = FakeBackend()
+    srv = S.Server(backend=be, memory_budget=10_000_000, chunk=7)
+    for i in range(5):
+        srv.submit(S.RunRequest(i, cfg(32), nsteps=10 + 3 * i, arrival=0.001 * i))
+    res = srv.run()
+    assert [r.rid for r in res] == list(range(5))
+    assert [r.state["steps"] for r in res] == [10 + 3 * i for i in range(5)]
+    s = S.summary(res, srv.elapsed)
+    assert s["runs"] == 5 and s["p50"] <= s["p99"]
+
+
+def test_admission_respects_memory_budget_and_order():
+    one = S.estimate_bytes(cfg(32))
+    be = FakeBackend()
+    srv = S.Server(backend=be, memory_budget=int(2.5 * one), chunk=5)
+    for i in range(6):
+        srv.submit(S.RunRequest(i, cfg(32), nsteps=20, arrival=0.0))
+    srv.run()
+    assert be.peak <= 2 * one                      # never three resident at once
+    starts = [rid for ev, rid in be.log if ev == "start"]
+    assert starts == sorted(starts)                 # first come, first admitted
+
+
+def test_measured_footprint_replaces_estimate():
+    be = FakeBackend(nbytes={0: 1000})
+    srv = S.Server(backend=be, memory_budget=10_000_000)
+    srv.submit(S.RunRequest(0, cfg(32), nsteps=3))
+    srv.run()
+    assert srv.footprints[S.shape_key(cfg(32))] == 1000
+
+
+def test_oversize_request_rejected():
+    srv = S.Server(backend=FakeBackend(), memory_budget=1000)
+    with pytest.raises(ValueError, match="budget"):
+        srv.submit(S.RunRequest(0, cfg(64), nsteps=3))
+
+
+def test_poisson_requests_are_seeded():
+    shapes = [cfg(32), cfg(64)]
+    a = S.poisson_requests(8, 4.0, 7, shapes)
+    b = S.poisson_requests(8, 4.0, 7, shapes)
+    assert [(r.arrival, r.nsteps, r.cfg.nx) for r in a] == [(r.arrival, r.nsteps, r.cfg.nx) for r in b]
+    assert all(x.arrival < y.arrival for x, y in zip(a, a[1:]))
