@@ -13,6 +13,8 @@ run/input.dat, plus the explicit extensions this implementation adds:
                        src/dealiasing.f90:329-330,435 bit for bit (negative ky modes
                        land at positive frequencies); "correct" is the textbook 3/2 rule.
 * ``ic = 2``        -- start from caller-supplied (seeded) perturbation fields.
+* ``precision``     -- 0: FP64 throughout (the reference's arithmetic); 1: the mixed form,
+                       with the nonlinear-term transforms and products in FP32.
 
 Sizes follow the reference's axes: x streamwise Fourier (nx), y spanwise Fourier
 (ny), z vertical Chebyshev with nzp = nz+1 points, k=1 the ceiling, k=nzp the wall.
@@ -79,6 +81,7 @@ class LsbConfig:
     bc3_xc: float = 40.0
     bc3_s: float = 7.5
     dealias_layout: str = "ref"
+    precision: int = 0      # 0: FP64 throughout; 1: mixed form (FP32 nonlinear-term transforms)
     debug: int = 0
 
     @property

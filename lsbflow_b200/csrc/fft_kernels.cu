@@ -14,6 +14,8 @@
 // The complex FFTs are mixed-radix (2,3,4,5,7) Stockham autosort transforms in shared
 // memory; every stage runs over all lines a block holds, with all its threads.  FFTW's c2r semantics are kept: the imaginary parts of
 // the DC and Nyquist inputs are ignored and the kx Nyquist mode is dropped / zero.
+#include <stdexcept>
+
 #include "lsb_internal.cuh"
 #include "lsb_fftdev.cuh"
 
@@ -367,6 +369,7 @@ static int persistent_grid(K kern, size_t smem, int nitems) {
 void launch_yinv(const YInvJobList& jobs, const YPassArgs& a, cudaStream_t s) {
     if (jobs.n <= 0) return;
     if (launch_yinv_warp(jobs, a, s)) return;
+    if (a.f32) throw std::runtime_error("mixed precision: y transform length has no warp plan");
     const int nch = (a.kxc + KC - 1) / KC;
     const int nitems = jobs.n * a.nzp * nch;
     const size_t sm = (size_t)3 * KC * a.plan.ls * sizeof(double2);
@@ -377,6 +380,7 @@ void launch_yinv(const YInvJobList& jobs, const YPassArgs& a, cudaStream_t s) {
 void launch_yfwd(const YFwdJobList& jobs, const YPassArgs& a, cudaStream_t s) {
     if (jobs.n <= 0) return;
     if (launch_yfwd_warp(jobs, a, s)) return;
+    if (a.f32) throw std::runtime_error("mixed precision: y transform length has no warp plan");
     const int nch = (a.kxc + KC - 1) / KC;
     const int nitems = jobs.n * a.nzp * nch;
     const size_t sm = (size_t)3 * KC * a.plan.ls * sizeof(double2);
@@ -533,6 +537,7 @@ __global__ void __launch_bounds__(256, 2) k_row_r2c(RowJobList jobs, RowArgs a) 
 void launch_row_c2r(const RowJobList& jobs, const RowArgs& a, cudaStream_t s) {
     if (jobs.n <= 0) return;
     if (launch_row_c2r_warp(jobs, a, s)) return;
+    if (a.f32) throw std::runtime_error("mixed precision: x transform length has no warp plan");
     const int nitems = jobs.n * ((a.nyl * a.nzp + RB - 1) / RB);
     const size_t sm = (size_t)3 * RB * a.rp.half.ls * sizeof(double2);
     if (wide(a.rp.half)) { lsb::note_launch(); k_row_c2r<true><<<persistent_grid(k_row_c2r<true>, sm, nitems), 256, sm, s>>>(jobs, a); }
@@ -542,6 +547,7 @@ void launch_row_c2r(const RowJobList& jobs, const RowArgs& a, cudaStream_t s) {
 void launch_row_r2c(const RowJobList& jobs, const RowArgs& a, cudaStream_t s) {
     if (jobs.n <= 0) return;
     if (launch_row_r2c_warp(jobs, a, s)) return;
+    if (a.f32) throw std::runtime_error("mixed precision: x transform length has no warp plan");
     const int nitems = jobs.n * ((a.nyl * a.nzp + RB - 1) / RB);
     const size_t sm = (size_t)3 * RB * a.rp.half.ls * sizeof(double2);
     if (wide(a.rp.half)) { lsb::note_launch(); k_row_r2c<true><<<persistent_grid(k_row_r2c<true>, sm, nitems), 256, sm, s>>>(jobs, a); }
@@ -653,6 +659,7 @@ __global__ void __launch_bounds__(256, 2) k_row_nl(NlRowArgs a) {
 
 void launch_row_nl(const NlRowArgs& a, cudaStream_t s) {
     if (launch_row_nl_warp(a, s)) return;
+    if (a.r.f32) throw std::runtime_error("mixed precision: x transform length has no warp plan");
     const size_t sm = (size_t)36 * a.r.rp.half.ls * sizeof(double2);
     const int nitems = a.r.nyl * a.r.nzp;
     if (wide(a.r.rp.half)) { lsb::note_launch(); k_row_nl<true><<<persistent_grid(k_row_nl<true>, sm, nitems), 256, sm, s>>>(a); }

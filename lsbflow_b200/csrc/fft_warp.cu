@@ -8,6 +8,8 @@
 // ends with X[k1 + R*bitrev(g)] in register k1.  Shared memory is only used to turn the
 // strided/bit-reversed orders into coalesced global accesses; there is no block barrier
 // inside a transform.  Lengths whose R is not in {1,2,3,4,6,8} use fft_kernels.cu.
+#include <stdexcept>
+
 #include "lsb_fftdev.cuh"
 #include "lsb_internal.cuh"
 
@@ -20,13 +22,13 @@ __device__ __forceinline__ int brev(int g, int lgg) {
     return lgg ? (int)(__brev((unsigned)g) >> (32 - lgg)) : 0;
 }
 
-template <int R, int SIGN>
-__device__ __forceinline__ void wfft(double2 (&v)[R], int G, int g, const double2* __restrict__ tw) {
+template <int R, int SIGN, class V>
+__device__ __forceinline__ void wfft(V (&v)[R], int G, int g, const V* __restrict__ tw) {
     dft_reg<R, SIGN>(v);
     if (R > 1 && g != 0) {
 #pragma unroll
         for (int k1 = 1; k1 < R; ++k1) {
-            double2 w = __ldg(&tw[g * k1]);
+            V w = __ldg(&tw[g * k1]);
             if (SIGN > 0) w.y = -w.y;
             v[k1] = cmul(v[k1], w);
         }
@@ -35,11 +37,11 @@ __device__ __forceinline__ void wfft(double2 (&v)[R], int G, int g, const double
     for (int h = G >> 1; h >= 1; h >>= 1) {
         const int j = g & (h - 1);
         const bool up = (g & h) != 0;
-        double2 w = __ldg(&tw[j * st]);
+        V w = __ldg(&tw[j * st]);
         if (SIGN > 0) w.y = -w.y;
 #pragma unroll
         for (int k1 = 0; k1 < R; ++k1) {
-            double2 o;
+            V o;
             o.x = __shfl_xor_sync(0xffffffffu, v[k1].x, h);
             o.y = __shfl_xor_sync(0xffffffffu, v[k1].y, h);
             v[k1] = up ? cmul(csub(o, v[k1]), w) : cadd(v[k1], o);
@@ -51,17 +53,17 @@ __device__ __forceinline__ void wfft(double2 (&v)[R], int G, int g, const double
 // Inverse of the order produced by wfft: input "slot" layout (lane g' register k1 holds
 // z[k1 + R*bitrev(g')]), cross-lane decimation-in-time network, twiddles, R-point DFT in
 // registers; output in natural order (lane g register r holds X[g + G*r]).
-template <int R, int SIGN>
-__device__ __forceinline__ void wfft_dit(double2 (&v)[R], int G, int g, const double2* __restrict__ tw) {
+template <int R, int SIGN, class V>
+__device__ __forceinline__ void wfft_dit(V (&v)[R], int G, int g, const V* __restrict__ tw) {
     int st = R * (G >> 1);  // N / (2h) for h = 1
     for (int h = 1; h < G; h <<= 1) {
         const int j = g & (h - 1);
         const bool up = (g & h) != 0;
-        double2 w = __ldg(&tw[j * st]);
+        V w = __ldg(&tw[j * st]);
         if (SIGN > 0) w.y = -w.y;
 #pragma unroll
         for (int k1 = 0; k1 < R; ++k1) {
-            double2 o;
+            V o;
             o.x = __shfl_xor_sync(0xffffffffu, v[k1].x, h);
             o.y = __shfl_xor_sync(0xffffffffu, v[k1].y, h);
             v[k1] = up ? csub(o, cmul(w, v[k1])) : cadd(v[k1], cmul(w, o));
@@ -71,7 +73,7 @@ __device__ __forceinline__ void wfft_dit(double2 (&v)[R], int G, int g, const do
     if (R > 1 && g != 0) {
 #pragma unroll
         for (int k1 = 1; k1 < R; ++k1) {
-            double2 w = __ldg(&tw[g * k1]);
+            V w = __ldg(&tw[g * k1]);
             if (SIGN > 0) w.y = -w.y;
             v[k1] = cmul(v[k1], w);
         }
@@ -81,8 +83,8 @@ __device__ __forceinline__ void wfft_dit(double2 (&v)[R], int G, int g, const do
 
 // lane g of a group receives the registers of lane bitrev(g): after wfft, lane g then
 // holds X[k1 + R*g] (R consecutive outputs)
-template <int R>
-__device__ __forceinline__ void lane_bitrev(double2 (&v)[R], int G, int lane, int g, int lgg) {
+template <int R, class V>
+__device__ __forceinline__ void lane_bitrev(V (&v)[R], int G, int lane, int g, int lgg) {
     const int src = (lane & ~(G - 1)) | brev(g, lgg);
 #pragma unroll
     for (int k1 = 0; k1 < R; ++k1) {
@@ -489,52 +491,55 @@ __global__ void __launch_bounds__(256, 2) k_row_nl_w(NlRowArgs a) {
 // products are lane-local, and the r2c (decimation in time from that layout) ends in
 // natural order, where the pair Z[k], Z[N-k] of the real-to-complex split is one shuffle
 // apart.  No shared memory and no block barrier.
-template <int R>
-__device__ __forceinline__ void nl_c2r_r(const double* __restrict__ src, bool ikx, int K, int N, int g,
-                                         const double* __restrict__ wavx, const RealPlan& rp, double2 (&v)[R]) {
+template <int R, class S, class V>
+__device__ __forceinline__ void nl_c2r_r(const S* __restrict__ src, bool ikx, int K, int N, int g,
+                                         const double* __restrict__ wavx, const V* __restrict__ twr,
+                                         const V* __restrict__ tw, V (&v)[R]) {
+    const V zero = CT<V>::make((S)0, (S)0);
 #pragma unroll
     for (int rr = 0; rr < R; ++rr) {
         const int n = g + 32 * rr;
-        double2 xa = make_double2(0.0, 0.0), xb = make_double2(0.0, 0.0);
-        if (n < K) xa = __ldg(reinterpret_cast<const double2*>(src) + n);
-        if (N - n < K) xb = __ldg(reinterpret_cast<const double2*>(src) + (N - n));
+        V xa = zero, xb = zero;
+        if (n < K) xa = __ldg(reinterpret_cast<const V*>(src) + n);
+        if (N - n < K) xb = __ldg(reinterpret_cast<const V*>(src) + (N - n));
         if (ikx) {
-            const double ka = (n < K) ? __ldg(&wavx[2 * n]) : 0.0;
-            const double kb = (N - n < K) ? __ldg(&wavx[2 * (N - n)]) : 0.0;
-            xa = make_double2(-ka * xa.y, ka * xa.x);
-            xb = make_double2(-kb * xb.y, kb * xb.x);
+            const S ka = (n < K) ? (S)__ldg(&wavx[2 * n]) : (S)0;
+            const S kb = (N - n < K) ? (S)__ldg(&wavx[2 * (N - n)]) : (S)0;
+            xa = CT<V>::make(-ka * xa.y, ka * xa.x);
+            xb = CT<V>::make(-kb * xb.y, kb * xb.x);
         }
-        if (n == 0) xa.y = 0.0;  // FFTW c2r ignores Im of the DC input
+        if (n == 0) xa.y = (S)0;  // FFTW c2r ignores Im of the DC input
         xb = cconj(xb);
-        const double2 e = cadd(xa, xb);
-        const double2 o = cmul(csub(xa, xb), cconj(__ldg(&rp.twr[n])));
-        v[rr] = make_double2(e.x - o.y, e.y + o.x);
+        const V e = cadd(xa, xb);
+        const V o = cmul(csub(xa, xb), cconj(__ldg(&twr[n])));
+        v[rr] = CT<V>::make(e.x - o.y, e.y + o.x);
     }
-    wfft<R, +1>(v, 32, g, rp.half.tw);
+    wfft<R, +1>(v, 32, g, tw);
 }
 
 // r2c of a slot-layout row; writes the K stored modes of the row at dst
-template <int R>
-__device__ __forceinline__ void nl_r2c_r(double2 (&v)[R], double* __restrict__ dst, int K, int g,
-                                         const RealPlan& rp) {
-    wfft_dit<R, -1>(v, 32, g, rp.half.tw);
+template <int R, class S, class V>
+__device__ __forceinline__ void nl_r2c_r(V (&v)[R], S* __restrict__ dst, int K, int g, const V* __restrict__ twr,
+                                         const V* __restrict__ tw) {
+    wfft_dit<R, -1>(v, 32, g, tw);
     // natural order: lane g register rr holds Z[g + 32 rr]; Z[N-k] for k = g + 32 rr is
     // lane (32-g) register R-1-rr (g > 0), or lane 0 register R-rr (g = 0, rr > 0)
     const int src = (32 - g) & 31;
+    const S h = (S)0.5;
 #pragma unroll
     for (int rr = 0; rr < R; ++rr) {
-        double2 zb;
+        V zb;
         zb.x = __shfl_sync(0xffffffffu, v[R - 1 - rr].x, src);
         zb.y = __shfl_sync(0xffffffffu, v[R - 1 - rr].y, src);
         if (g == 0) zb = v[rr == 0 ? 0 : R - rr];
         const int k = g + 32 * rr;
         if (32 * rr < K && k < K) {
-            const double2 za = v[rr];
+            const V za = v[rr];
             zb = cconj(zb);
-            const double2 e = make_double2(0.5 * (za.x + zb.x), 0.5 * (za.y + zb.y));
-            const double2 o = make_double2(0.5 * (za.x - zb.x), 0.5 * (za.y - zb.y));
-            const double2 t = cmul(__ldg(&rp.twr[k]), o);
-            reinterpret_cast<double2*>(dst)[k] = make_double2(e.x + t.y, e.y - t.x);
+            const V e = CT<V>::make(h * (za.x + zb.x), h * (za.y + zb.y));
+            const V o = CT<V>::make(h * (za.x - zb.x), h * (za.y - zb.y));
+            const V tt = cmul(__ldg(&twr[k]), o);
+            reinterpret_cast<V*>(dst)[k] = CT<V>::make(e.x + tt.y, e.y - tt.x);
         }
     }
 }
@@ -554,7 +559,7 @@ __global__ void __launch_bounds__(128, 3) k_row_nl_r(NlRowArgs a) {
         const double ub = a.ubar[z], ubp = a.ubarp[z];
         double2 u[3][R];
 #pragma unroll
-        for (int l = 0; l < 3; ++l) nl_c2r_r<R>(a.U[l] + off, false, K, N, g, r.wavx, r.rp, u[l]);
+        for (int l = 0; l < 3; ++l) nl_c2r_r<R>(a.U[l] + off, false, K, N, g, r.wavx, r.rp.twr, r.rp.half.tw, u[l]);
 #pragma unroll
         for (int k1 = 0; k1 < R; ++k1) {
             u[0][k1].x += ub;
@@ -569,23 +574,23 @@ __global__ void __launch_bounds__(128, 3) k_row_nl_r(NlRowArgs a) {
 #pragma unroll
             for (int k1 = 0; k1 < R; ++k1)
                 f[k1] = make_double2(0.5 * (u[l][k1].x * u[m][k1].x), 0.5 * (u[l][k1].y * u[m][k1].y));
-            nl_r2c_r<R>(f, a.H[p] + off, K, g, r.rp);
+            nl_r2c_r<R>(f, a.H[p] + off, K, g, r.rp.twr, r.rp.half.tw);
         }
         // convective terms -0.5 u_m d_m u_l, plus the fringe
 #pragma unroll 1
         for (int l = 0; l < 3; ++l) {
             double2 acc[R], d[R];
-            nl_c2r_r<R>(a.U[l] + off, true, K, N, g, r.wavx, r.rp, d);
+            nl_c2r_r<R>(a.U[l] + off, true, K, N, g, r.wavx, r.rp.twr, r.rp.half.tw, d);
 #pragma unroll
             for (int k1 = 0; k1 < R; ++k1)
                 acc[k1] = make_double2(0.0 - 0.5 * (u[0][k1].x * d[k1].x), 0.0 - 0.5 * (u[0][k1].y * d[k1].y));
-            nl_c2r_r<R>(a.DY[l] + off, false, K, N, g, r.wavx, r.rp, d);
+            nl_c2r_r<R>(a.DY[l] + off, false, K, N, g, r.wavx, r.rp.twr, r.rp.half.tw, d);
 #pragma unroll
             for (int k1 = 0; k1 < R; ++k1) {
                 acc[k1].x = acc[k1].x - 0.5 * (u[1][k1].x * d[k1].x);
                 acc[k1].y = acc[k1].y - 0.5 * (u[1][k1].y * d[k1].y);
             }
-            nl_c2r_r<R>(a.DZ[l] + off, false, K, N, g, r.wavx, r.rp, d);
+            nl_c2r_r<R>(a.DZ[l] + off, false, K, N, g, r.wavx, r.rp.twr, r.rp.half.tw, d);
             const double dzb = (l == 0) ? ubp : 0.0;
 #pragma unroll
             for (int k1 = 0; k1 < R; ++k1) {
@@ -604,7 +609,192 @@ __global__ void __launch_bounds__(128, 3) k_row_nl_r(NlRowArgs a) {
                     acc[k1].y = acc[k1].y + lx1 * (ut - ubb);
                 }
             }
-            nl_r2c_r<R>(acc, a.N[l] + off, K, g, r.rp);
+            nl_r2c_r<R>(acc, a.N[l] + off, K, g, r.rp.twr, r.rp.half.tw);
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------- mixed form
+// FP32 variants for the mixed-precision step: y-intermediates are FP32, the transforms run
+// in FP32 with FP32 twiddles; the spectral fields on either side stay FP64 (converted on
+// load and store).  Same work items and layouts as k_ywarp.
+template <int R, bool INV>
+__global__ void __launch_bounds__(256) k_ywarp_f(YInvJobList ij, YFwdJobList fj, YPassArgs a, int nch) {
+    extern __shared__ float2 fsm[];
+    const int ny = a.ny, nyl = a.nyl, G = a.plan.g, lgg = a.plan.lgg;
+    constexpr int TS = WKC + 1;
+    float2* T = fsm;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int njobs = INV ? ij.n : fj.n;
+    const int nitems = njobs * a.nzp * nch;
+    const int lpw = 32 / G;
+    const int q = lane / G, g = lane - q * G;
+    for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+        const int ch = item % nch, rest = item / nch, z = rest % a.nzp, jb = rest / a.nzp;
+        const int c0 = ch * WKC;
+        if (INV) {
+            const double* in = ij.j[jb].in;
+            for (int idx = tid; idx < nyl * WKC; idx += 256) {
+                const int jl = idx / WKC, cc = idx - jl * WKC, c = c0 + cc;
+                const int j = unpad_row(jl, ny, nyl, a.layout);
+                float2 v = make_float2(0.f, 0.f);
+                if (j >= 0 && c < a.kxc) {
+                    const double2 d = __ldg(reinterpret_cast<const double2*>(in + ((long long)z * ny + j) * a.nx) + c);
+                    v = make_float2((float)d.x, (float)d.y);
+                }
+                T[jl * TS + cc] = v;
+            }
+        } else {
+            const float* in = reinterpret_cast<const float*>(fj.j[jb].in);
+            for (int idx = tid; idx < nyl * WKC; idx += 256) {
+                const int jl = idx / WKC, cc = idx - jl * WKC, c = c0 + cc;
+                T[jl * TS + cc] = (c < a.kxc)
+                    ? __ldg(reinterpret_cast<const float2*>(in + ((long long)z * nyl + jl) * a.nx) + c)
+                    : make_float2(0.f, 0.f);
+            }
+        }
+        __syncthreads();
+        const int mode = INV ? ij.j[jb].mode : YM_COPY;
+        for (int L0 = warp * lpw; L0 < WKC; L0 += 8 * lpw) {
+            const int L = L0 + q;
+            const bool act = L < WKC;
+            const int Lc = act ? L : 0;
+            float2 v[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int n = g + G * r;
+                float2 x = T[n * TS + Lc];
+                if (INV && mode != YM_COPY) {
+                    float k = 0.f;
+                    if (mode == YM_IKY) {
+                        const int j = unpad_row(n, ny, nyl, a.layout);
+                        k = (j >= 0) ? (float)a.wavy[j] : 0.f;
+                    } else {
+                        const int c = min(c0 + Lc, a.kxc - 1);
+                        k = (float)a.wavx[2 * c];
+                    }
+                    x = make_float2(-k * x.y, k * x.x);
+                }
+                v[r] = x;
+            }
+            wfft<R, INV ? +1 : -1>(v, G, g, a.plan.twf);
+            lane_bitrev<R>(v, G, lane, g, lgg);
+            __syncwarp();
+            if (act) {
+#pragma unroll
+                for (int k1 = 0; k1 < R; ++k1) T[(R * g + k1) * TS + L] = v[k1];
+            }
+        }
+        __syncthreads();
+        if (INV) {
+            float* out = reinterpret_cast<float*>(ij.j[jb].out);
+            for (int idx = tid; idx < nyl * WKC; idx += 256) {
+                const int jl = idx / WKC, cc = idx - jl * WKC, c = c0 + cc;
+                if (c >= a.kxc) continue;
+                *reinterpret_cast<float2*>(out + ((long long)z * nyl + jl) * a.nx + 2 * c) = T[jl * TS + cc];
+            }
+        } else {
+            const YFwdJob job = fj.j[jb];
+            for (int idx = tid; idx < ny * WKC; idx += 256) {
+                const int j = idx / WKC, cc = idx - j * WKC, c = c0 + cc;
+                if (c >= a.kxc) continue;
+                const float2 vf = T[pad_row_w(j, ny, nyl, a.layout) * TS + cc];
+                double2 v = make_double2((double)vf.x, (double)vf.y);
+                if (job.sym && c == 0) {
+                    const int jm = (ny - j) % ny;
+                    const float2 wf = T[pad_row_w(jm, ny, nyl, a.layout) * TS + cc];
+                    v = make_double2(0.5 * (v.x + (double)wf.x), 0.5 * (v.y - (double)wf.y));
+                }
+                v.x *= a.scale;
+                v.y *= a.scale;
+                double2* o = reinterpret_cast<double2*>(job.out + ((long long)z * ny + j) * a.nx + 2 * c);
+                double2 rr;
+                if (job.beta != 0.0) {
+                    const double2 old = *o;
+                    rr = make_double2(fma(job.alpha, v.x, job.beta * old.x), fma(job.alpha, v.y, job.beta * old.y));
+                } else {
+                    rr = make_double2(job.alpha * v.x, job.alpha * v.y);
+                }
+                *o = rr;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// k_row_nl_r in FP32: FP32 rows in and out, same slot layout.  The streamwise velocity is
+// kept as the perturbation u' and the mean ubar(z) is added inside each product, so that
+// FP32 rounding of ubar + u' (|ubar| ~ 1 >> |u'|) never enters the perturbation terms:
+//   h_11 = u'(ubar + u'/2)   (0.5 ubar^2 dropped: a kx = 0 function of z that only ever
+//                              enters the step through d/dx, where it vanishes)
+//   h_1m = (ubar + u') u_m / 2,  fringe lambda (ubar - u) = -lambda u'.
+template <int R>
+__global__ void __launch_bounds__(128, 4) k_row_nl_f(NlRowArgs a) {
+    const RowArgs& r = a.r;
+    const int N = 32 * R, K = r.kxc, lgg = r.rp.half.lgg;
+    const int g = threadIdx.x & 31;
+    const int nitems = r.nyl * r.nzp;
+    const int W = gridDim.x * (blockDim.x >> 5);
+    const int mb = R * brev(g, lgg);
+    auto F = [](const double* p) { return reinterpret_cast<const float*>(p); };
+    for (int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); row < nitems; row += W) {
+        const int z = row / r.nyl;
+        const long long off = (long long)row * 2 * K;
+        const float ub = (float)a.ubar[z], ubp = (float)a.ubarp[z];
+        float2 u[3][R];  // u', v, w
+#pragma unroll
+        for (int l = 0; l < 3; ++l) nl_c2r_r<R>(F(a.U[l]) + off, false, K, N, g, r.wavx, r.rp.twrf, r.rp.half.twf, u[l]);
+#pragma unroll
+        for (int p = 0; p < 6; ++p) {
+            float2 f[R];
+#pragma unroll
+            for (int k1 = 0; k1 < R; ++k1) {
+                const float2 up = u[0][k1];
+                if (p == 0) {
+                    f[k1] = make_float2(up.x * (ub + 0.5f * up.x), up.y * (ub + 0.5f * up.y));
+                } else if (p < 3) {
+                    const float2 um = u[p][k1];
+                    f[k1] = make_float2(0.5f * ((ub + up.x) * um.x), 0.5f * ((ub + up.y) * um.y));
+                } else {
+                    const int l = (p < 5) ? 1 : 2;
+                    const int m = (p < 5) ? p - 2 : 2;
+                    f[k1] = make_float2(0.5f * (u[l][k1].x * u[m][k1].x), 0.5f * (u[l][k1].y * u[m][k1].y));
+                }
+            }
+            nl_r2c_r<R>(f, reinterpret_cast<float*>(a.H[p]) + off, K, g, r.rp.twrf, r.rp.half.twf);
+        }
+#pragma unroll 1
+        for (int l = 0; l < 3; ++l) {
+            float2 acc[R], d[R];
+            nl_c2r_r<R>(F(a.U[l]) + off, true, K, N, g, r.wavx, r.rp.twrf, r.rp.half.twf, d);
+#pragma unroll
+            for (int k1 = 0; k1 < R; ++k1)
+                acc[k1] = make_float2(0.f - 0.5f * ((ub + u[0][k1].x) * d[k1].x),
+                                      0.f - 0.5f * ((ub + u[0][k1].y) * d[k1].y));
+            nl_c2r_r<R>(F(a.DY[l]) + off, false, K, N, g, r.wavx, r.rp.twrf, r.rp.half.twf, d);
+#pragma unroll
+            for (int k1 = 0; k1 < R; ++k1) {
+                acc[k1].x = acc[k1].x - 0.5f * (u[1][k1].x * d[k1].x);
+                acc[k1].y = acc[k1].y - 0.5f * (u[1][k1].y * d[k1].y);
+            }
+            nl_c2r_r<R>(F(a.DZ[l]) + off, false, K, N, g, r.wavx, r.rp.twrf, r.rp.half.twf, d);
+            const float dzb = (l == 0) ? ubp : 0.f;
+#pragma unroll
+            for (int k1 = 0; k1 < R; ++k1) {
+                acc[k1].x = acc[k1].x - 0.5f * (u[2][k1].x * (d[k1].x + dzb));
+                acc[k1].y = acc[k1].y - 0.5f * (u[2][k1].y * (d[k1].y + dzb));
+            }
+            if (a.lamx != nullptr) {
+#pragma unroll
+                for (int k1 = 0; k1 < R; ++k1) {
+                    const int x = 2 * (k1 + mb);
+                    const float lx0 = (float)__ldg(&a.lamx[x]), lx1 = (float)__ldg(&a.lamx[x + 1]);
+                    const float2 ul = (l == 0) ? u[0][k1] : (l == 1 ? u[1][k1] : u[2][k1]);
+                    acc[k1].x = acc[k1].x - lx0 * ul.x;
+                    acc[k1].y = acc[k1].y - lx1 * ul.y;
+                }
+            }
+            nl_r2c_r<R>(acc, reinterpret_cast<float*>(a.N[l]) + off, K, g, r.rp.twrf, r.rp.half.twf);
         }
     }
 }
@@ -630,6 +820,11 @@ template <int R, bool INV>
 void ylaunch(const YInvJobList& ij, const YFwdJobList& fj, const YPassArgs& a, cudaStream_t s) {
     const int nch = (a.kxc + WKC - 1) / WKC;
     const int nitems = (INV ? ij.n : fj.n) * a.nzp * nch;
+    if (a.f32) {
+        const size_t smf = (size_t)a.nyl * (WKC + 1) * sizeof(float2);
+        { lsb::note_launch(); k_ywarp_f<R, INV><<<persistent_grid_w(k_ywarp_f<R, INV>, smf, nitems), 256, smf, s>>>(ij, fj, a, nch); }
+        return;
+    }
     const size_t sm = (size_t)2 * a.nyl * (WKC + 1) * sizeof(double2);
     { lsb::note_launch(); k_ywarp<R, INV><<<persistent_grid_w(k_ywarp<R, INV>, sm, nitems), 256, sm, s>>>(ij, fj, a, nch); }
 }
@@ -673,6 +868,23 @@ template <int R>
 void nllaunch(const NlRowArgs& a, cudaStream_t s) {
     const int N = a.r.nxl / 2;
     const int nitems = a.r.nyl * a.r.nzp;
+    if (a.r.f32) {
+        if (a.r.rp.half.g != 32) throw std::runtime_error("mixed precision: x transform length has no full-warp plan");
+        static int nsmf = 0;
+        if (nsmf == 0) {
+            int dev = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&nsmf, cudaDevAttrMultiProcessorCount, dev);
+            if (nsmf <= 0) nsmf = 148;
+        }
+        int occ = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_row_nl_f<R>, 128, 0);
+        if (occ < 1) occ = 1;
+        long long blocks = (long long)occ * nsmf, need = (nitems + 3) / 4;
+        if (blocks > need) blocks = need > 0 ? need : 1;
+        { lsb::note_launch(); k_row_nl_f<R><<<(int)blocks, 128, 0, s>>>(a); }
+        return;
+    }
     if (a.r.rp.half.g == 32) {
         static int nsm = 0;
         if (nsm == 0) {

@@ -38,6 +38,7 @@ struct FftPlan {
     FastDiv fdT[kMaxStages];
     FastDiv fdP[kMaxStages];
     const double2* tw = nullptr;   // device, n entries
+    const float2* twf = nullptr;   // the same in FP32
     int n1 = 0, n2 = 0;            // register two-pass split n = n1*n2 (n1 = 0: Stockham stages)
     int g = 0, r = 0, lgg = 0;     // warp-group split n = g*r (g lanes, r registers; g = 0: none)
     int ls = 0;                    // shared-memory line stride (complex) a kernel must use
@@ -48,6 +49,7 @@ struct RealPlan {
     int nr = 0;                    // real length
     FftPlan half;                  // complex plan of length nr/2
     const double2* twr = nullptr;  // device, nr entries: exp(-2 pi i m / nr)
+    const float2* twrf = nullptr;  // the same in FP32
 };
 
 struct Dims {
@@ -82,6 +84,7 @@ struct YPassArgs {
     const double* wavy;         // [ny] device
     const double* wavx;         // [nx] device
     FftPlan plan;               // length nyl
+    int f32 = 0;                // 1: y-intermediates in FP32, transforms in FP32 (mixed form)
 };
 
 constexpr int kMaxJobs = 12;
@@ -99,6 +102,7 @@ struct RowIO {
     const double* mean; // [nzp] or nullptr
 };
 struct RowArgs {
+    int f32 = 0;                // 1: y-intermediate and physical rows in FP32 (mixed form)
     int kxc, nxl, nyl, nzp;
     long long row_pitch;        // physical row pitch in doubles (nxl)
     const double* wavx;

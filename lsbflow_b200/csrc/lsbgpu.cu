@@ -50,6 +50,13 @@ bool factor(int n, std::vector<int>& rad) {
 
 namespace {
 
+// single-precision copy of a table (the mixed-precision kernels read their twiddles in FP32)
+const float2* upload_f32(lsb_handle* h, const std::vector<double>& v) {
+    std::vector<float> f(v.size() + 1);  // +1 keeps the byte count a whole number of doubles
+    for (size_t i = 0; i < v.size(); ++i) f[i] = (float)v[i];
+    return (const float2*)h->upload((const double*)f.data(), (f.size() * sizeof(float) + 7) / 8);
+}
+
 void make_plan(lsb_handle* h, int n, FftPlan& P) {
     std::vector<int> rad;
     if (!factor(n, rad) || (int)rad.size() > kMaxStages)
@@ -83,6 +90,7 @@ void make_plan(lsb_handle* h, int n, FftPlan& P) {
         tw[2 * m + 1] = (double)-sinl(a);
     }
     P.tw = (const double2*)h->upload(tw.data(), tw.size());
+    P.twf = upload_f32(h, tw);
     // register two-pass split: n = n1 * n2 with both factors in {1,2,3,4,6,8,12,16}
     static const int pairs[][2] = {{2, 1},  {3, 1},  {4, 1},  {6, 1},  {8, 1},   {12, 1},  {16, 1},
                                    {3, 3},  {6, 3},  {8, 3},  {8, 4},  {12, 3},  {8, 6},   {16, 3},
@@ -130,6 +138,7 @@ void make_real_plan(lsb_handle* h, int nr, RealPlan& R) {
         tw[2 * m + 1] = (double)-sinl(a);
     }
     R.twr = (const double2*)h->upload(tw.data(), tw.size());
+    R.twrf = upload_f32(h, tw);
 }
 
 Mat make_mat(lsb_handle* h, const double* A, int M, int K, int row0 = 0, int nrows = -1, int zero_pad_rows_top = 0,
@@ -318,9 +327,13 @@ void nlterm(lsb_handle* h, const double* uin, double* Nout) {
         yj.j[3 + l] = YInvJob{uin + l * S, h->Y + (long long)(3 + l) * h->Yl, YM_IKY};
         yj.j[6 + l] = YInvJob{h->dz + l * S, h->Y + (long long)(6 + l) * h->Yl, YM_COPY};
     }
-    { TimerScope ts(h, "yinv_nl"); launch_yinv(yj, ypass(h, dealias, d.nzp), h->stream); }
+    const int f32 = h->cfg.precision == 1 ? 1 : 0;
+    YPassArgs ya = ypass(h, dealias, d.nzp);
+    ya.f32 = f32;
+    { TimerScope ts(h, "yinv_nl"); launch_yinv(yj, ya, h->stream); }
     NlRowArgs na{};
     na.r = rowargs(h, dealias, d.nzp);
+    na.r.f32 = f32;
     for (int l = 0; l < 3; ++l) {
         na.U[l] = h->Y + (long long)l * h->Yl;
         na.DY[l] = h->Y + (long long)(3 + l) * h->Yl;
@@ -336,7 +349,8 @@ void nlterm(lsb_handle* h, const double* uin, double* Nout) {
     yf.n = 9;
     for (int l = 0; l < 3; ++l) yf.j[l] = YFwdJob{na.N[l], Nout + l * S, 1.0, 0.0, dealias ? 1 : 0};
     for (int m = 0; m < 6; ++m) yf.j[3 + m] = YFwdJob{na.H[m], h->H + m * S, 1.0, 0.0, dealias ? 1 : 0};
-    { TimerScope ts(h, "yfwd_nl"); launch_yfwd(yf, ypass(h, dealias, d.nzp), h->stream); }
+    { TimerScope ts(h, "yfwd_nl"); launch_yfwd(yf, ya, h->stream); }
+    if (f32) launch_add_half_sq(h->H, h->ubar, d.C(), d.nzp, h->stream);
 
     const bool need_phys = (dealias && h->cfg.forcing == 1) || h->cfg.sgsflag == 1;
     if (need_phys) {
@@ -748,6 +762,13 @@ int lsb_create(const lsb_config* cfg, const lsb_setup* su, lsb_handle** out) {
         make_plan(h.get(), d.nyl, h->pyl);
         make_real_plan(h.get(), nx, h->rx);
         make_real_plan(h.get(), d.nxl, h->rxl);
+        if (cfg->precision != 0 && cfg->precision != 1) fail(LSB_ERR_ARG, "precision must be 0 (FP64) or 1 (mixed)");
+        if (cfg->precision == 1) {
+            const bool dl = cfg->dealiasflag == 1;
+            if ((dl ? h->pyl : h->py).g == 0 || (dl ? h->rxl : h->rx).half.g != 32)
+                fail(LSB_ERR_ARG, "mixed precision needs transform lengths with register plans: x/2 a multiple of "
+                                  "32 (32 R, R in 1,2,3,4,6,8) and y a power of two times 1,2,3,4,6,8");
+        }
         const long long S = d.S(), C = d.C();
         h->Yl = (long long)nzp * d.nyl * nx;
         h->Yu1 = (long long)nzp * ny * nx;

@@ -284,6 +284,16 @@ void launch_force_phys(const double* u0, const double* u1, const double* u2, dou
                        const double* lamx, const double* ubar, int nx, int ny, long long P, cudaStream_t s) {
     { lsb::note_launch(); k_force_phys<<<nblk(P), 256, 0, s>>>(u0, u1, u2, f0, f1, f2, lamx, ubar, nx, ny, P); }
 }
+// mixed form: the FP32 product kernel leaves 0.5 ubar(z)^2 out of h_11; its (kx, ky) = (0, 0)
+// coefficient is restored here in FP64 (the dynamic model filters u_1 u_1 in physical space)
+__global__ void k_add_half_sq(double* h11, const double* ubar, long long C, int nzp) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < nzp) h11[(long long)k * C] += 0.5 * (ubar[k] * ubar[k]);
+}
+void launch_add_half_sq(double* h11, const double* ubar, long long C, int nzp, cudaStream_t s) {
+    { lsb::note_launch(); k_add_half_sq<<<(nzp + 127) / 128, 128, 0, s>>>(h11, ubar, C, nzp); }
+}
+
 void launch_tavg_add(double* a, const double* q, double iomod, long long n, cudaStream_t s) {
     { lsb::note_launch(); k_tavg_add<<<nblk(n), 256, 0, s>>>(a, q, iomod, n); }
 }
