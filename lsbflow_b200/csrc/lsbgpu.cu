@@ -710,6 +710,7 @@ int lsb_create(const lsb_config* cfg, const lsb_setup* su, lsb_handle** out) {
         d.nzm = cfg->nz - 1;
         d.kx = cfg->nx / 2;
         if (d.nx < 4 || d.nx % 2 || d.ny < 1 || d.nz < 3) fail(LSB_ERR_ARG, "bad grid size");
+        if ((long long)d.nx * d.ny * (d.nz + 1) >= (1LL << 31)) fail(LSB_ERR_ARG, "grid too large (2^31 points or more)");
         if (cfg->dealiasflag == 1) {
             // setup_dealiasing, nproch = 1 (src/dealiasing.f90:133-154)
             if (d.nx % 2 == 0 && d.nx % 4 == 0) d.nxl = 3 * d.nx / 2;

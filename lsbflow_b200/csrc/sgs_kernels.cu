@@ -108,21 +108,138 @@ __global__ void __launch_bounds__(256) k_filter3(FieldList fl, int nx, int ny, i
     }
 }
 
-void filter3(lsb_handle* h, const double* const* in, double* const* out, int n, double a, double b, int which) {
+// Row-tile version of the same filter (nx a power of two, 4..512): a block owns FJ
+// full x rows (FJ * nx <= 2048) and marches a chunk of zch planes.  Each plane with its
+// periodic y halo rows is copied into shared memory by cp.async, three planes deep, so
+// two planes are in flight while one is filtered; the x halo is the row itself (periodic).
+// The only re-reads are the two y halo rows and the two z halo planes of the chunk.
+constexpr int RT_MAX = 2048, RT_NX = 512, RT_ST = 3;
+
+__device__ __forceinline__ void cpa16s(void* sdst, const void* gsrc) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc));
+}
+__device__ __forceinline__ void cpa_commit_s() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cpa_wait_s() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+template <class T>
+__global__ void __launch_bounds__(256, 2) k_filter3p(FieldList fl, int lgx, int ny, int nzp, int FJ, int zch, T a, T b,
+                                                     const double* __restrict__ az, const double* __restrict__ bz,
+                                                     const double* __restrict__ cz) {
+    const int nx = 1 << lgx;
+    extern __shared__ __align__(16) unsigned char fsm_raw[];
+    const int tsz = (FJ + 2) * nx;
+    T* tiles = reinterpret_cast<T*>(fsm_raw);  // RT_ST tiles of (FJ + 2) rows
+    T* X = tiles + RT_ST * tsz;                // x-filtered rows
+    const int f = blockIdx.z, zc = blockIdx.y;
+    const T* q = reinterpret_cast<const T*>(fl.in[f]);
+    T* out = reinterpret_cast<T*>(fl.out[f]);
+    const int j0 = blockIdx.x * FJ;
+    const int rows = min(FJ, ny - j0);
+    const int k0 = zc * zch, k1 = min(nzp, k0 + zch);
+    const int ks = max(0, k0 - 1), ke = min(nzp - 1, k1);
+    const T rs = (T)(1.0 / (2.0 * (double)a + (double)b));
+    const int tid = threadIdx.x;
+    constexpr int V = 16 / sizeof(T);          // elements per 16-byte copy
+    constexpr int LGV = (V == 2) ? 1 : 2;
+    const int lgrv = lgx - LGV;                // log2 of the copies per row
+    const int nld_v = (rows + 2) << lgrv;
+    const long long plane = (long long)ny * nx;
+    auto issue = [&](int kk) {
+        if (kk <= ke) {
+            T* dst = tiles + (kk % RT_ST) * tsz;
+            const T* src = q + (long long)kk * plane;
+            for (int c = tid; c < nld_v; c += 256) {
+                const int r = c >> lgrv, cv = c & ((1 << lgrv) - 1);
+                int j = j0 + r - 1;
+                j = (j < 0) ? j + ny : (j >= ny ? j - ny : j);
+                cpa16s(dst + (r << lgx) + cv * V, src + ((long long)j << lgx) + cv * V);
+            }
+        }
+        cpa_commit_s();  // one group per plane slot, empty past the end
+    };
+    issue(ks);
+    issue(ks + 1);
+    constexpr int OPT = RT_MAX / 256;
+    T y0[OPT], y1[OPT], y2[OPT];
+#pragma unroll
+    for (int o = 0; o < OPT; ++o) y0[o] = y1[o] = y2[o] = (T)0;
+    for (int kk = ks; kk <= ke; ++kk) {
+        issue(kk + 2);
+        cpa_wait_s<2>();
+        __syncthreads();
+        const T* tile = tiles + (kk % RT_ST) * tsz;
+        for (int e = tid; e < ((rows + 2) << lgx); e += 256) {
+            const int i = e & (nx - 1);
+            const T l = tile[i == 0 ? e + nx - 1 : e - 1];
+            const T rr = tile[i == nx - 1 ? e - nx + 1 : e + 1];
+            X[e] = (a * l + b * tile[e] + a * rr) * rs;
+        }
+        __syncthreads();
+        const int ko = kk - 1;
+        const T za = (ko >= 1) ? (T)az[ko] : (T)0, zb = (ko >= 1) ? (T)bz[ko] : (T)0,
+                zcf = (ko >= 1) ? (T)cz[ko] : (T)0;
+#pragma unroll
+        for (int o = 0; o < OPT; ++o) {
+            const int e = tid + 256 * o;
+            if (e >= rows * nx) continue;
+            const T yn = (a * X[e] + b * X[e + nx] + a * X[e + 2 * nx]) * rs;
+            y0[o] = y1[o];
+            y1[o] = y2[o];
+            y2[o] = yn;
+            const long long ob = (long long)j0 * nx + e;
+            if (ko >= k0 && ko < k1) out[(long long)ko * plane + ob] = (ko == 0) ? y1[o] : (za * y0[o] + zb * y1[o] + zcf * y2[o]) * rs;
+            if (kk == nzp - 1 && kk >= k0 && kk < k1) out[(long long)kk * plane + ob] = yn;
+        }
+    }
+    cpa_wait_s<0>();
+}
+
+void filter3_any(lsb_handle* h, const void* const* in, void* const* out, int n, double a, double b, int which,
+                 bool f32) {
     const Dims& d = h->d;
-    const int nzc = (d.nzp + FZC - 1) / FZC;
+    const double* zf = h->sgs.zf + (long long)which * 3 * d.nzp;  // which: 0 (a,b) 1 (1,1) 2 (1,6) 3 (1,2)
+    int lgx = 0;
+    while ((1 << lgx) < d.nx) ++lgx;
+    const bool rowtile = d.nx <= RT_NX && d.nx >= 4 && (1 << lgx) == d.nx;
+    if (!rowtile && f32) sfail(LSB_ERR_UNSUPPORTED, "mixed precision: the SGS filter needs nx a power of two, 4..512");
     for (int f0 = 0; f0 < n; f0 += 9) {
         FieldList fl{};
         fl.n = std::min(9, n - f0);
         for (int i = 0; i < fl.n; ++i) {
-            fl.in[i] = in[f0 + i];
-            fl.out[i] = out[f0 + i];
+            fl.in[i] = reinterpret_cast<const double*>(in[f0 + i]);
+            fl.out[i] = reinterpret_cast<double*>(out[f0 + i]);
         }
-        const double* zf = h->sgs.zf + (long long)which * 3 * d.nzp;  // which: 0 (a,b) 1 (1,1) 2 (1,6) 3 (1,2)
         TimerScope ts(h, "sgs_filter3");
-        dim3 grid((d.nx + FIB - 1) / FIB, (d.ny + FJB - 1) / FJB, nzc * fl.n);
-        { lsb::note_launch(); k_filter3<<<grid, 256, 0, h->stream>>>(fl, d.nx, d.ny, d.nzp, a, b, zf, zf + d.nzp, zf + 2 * d.nzp, nzc); }
+        if (rowtile) {
+            const int FJ = std::max(1, std::min(d.ny, RT_MAX / d.nx));
+            const int nyb = (d.ny + FJ - 1) / FJ;
+            // z chunks: about four blocks per SM over the launch, at least 4 planes each
+            int nzc = (4 * 148 + nyb * fl.n - 1) / (nyb * fl.n);
+            nzc = std::max(1, std::min(nzc, (d.nzp + 3) / 4));
+            const int zch = (d.nzp + nzc - 1) / nzc;
+            nzc = (d.nzp + zch - 1) / zch;
+            dim3 grid(nyb, nzc, fl.n);
+            const size_t es = f32 ? sizeof(float) : sizeof(double);
+            const size_t sm = (size_t)(RT_ST + 1) * (FJ + 2) * d.nx * es;
+            if (f32) {
+                if (sm > 48 * 1024) cudaFuncSetAttribute(k_filter3p<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+                { lsb::note_launch(); k_filter3p<float><<<grid, 256, sm, h->stream>>>(fl, lgx, d.ny, d.nzp, FJ, zch, (float)a, (float)b, zf, zf + d.nzp, zf + 2 * d.nzp); }
+            } else {
+                if (sm > 48 * 1024) cudaFuncSetAttribute(k_filter3p<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+                { lsb::note_launch(); k_filter3p<double><<<grid, 256, sm, h->stream>>>(fl, lgx, d.ny, d.nzp, FJ, zch, a, b, zf, zf + d.nzp, zf + 2 * d.nzp); }
+            }
+        } else {
+            const int nzc = (d.nzp + FZC - 1) / FZC;
+            dim3 grid((d.nx + FIB - 1) / FIB, (d.ny + FJB - 1) / FJB, nzc * fl.n);
+            { lsb::note_launch(); k_filter3<<<grid, 256, 0, h->stream>>>(fl, d.nx, d.ny, d.nzp, a, b, zf, zf + d.nzp, zf + 2 * d.nzp, nzc); }
+        }
     }
+}
+
+void filter3(lsb_handle* h, const double* const* in, double* const* out, int n, double a, double b, int which) {
+    filter3_any(h, reinterpret_cast<const void* const*>(in), reinterpret_cast<void* const*>(out), n, a, b, which, false);
 }
 
 // ---------------------------------------------------------------- dynamic Smagorinsky
@@ -163,7 +280,7 @@ __global__ void k_dyn1(DynArgs a) {  // S_ij, |S|
 
 __global__ void k_dyn2(DynArgs a) {  // |[S]|, L' = delta^2 |S| S_ij, [delta]^2 |[S]| [S_ij]
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < a.P; e += (long long)gridDim.x * blockDim.x) {
-        const int k = (int)(e / a.nxy);
+        const int k = (int)((unsigned)e / (unsigned)a.nxy);  // P < 2^31 (checked at create)
         const double dl = a.delta[k], cd = 2.0 * dl;
         double sh = 0.0;
         for (int m = 0; m < 3; ++m)
@@ -201,7 +318,7 @@ __global__ void k_dyn3(DynArgs a) {  // M_ij, L_ij, <M L>, <M M> integrands
 __global__ void k_dyn4(DynArgs a) {  // C clip, nu_sgs, tau = -2 nu S_ij
     const double cmax = 0.2 * 0.2;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < a.P; e += (long long)gridDim.x * blockDim.x) {
-        const int k = (int)(e / a.nxy);
+        const int k = (int)((unsigned)e / (unsigned)a.nxy);  // P < 2^31 (checked at create)
         const double dl = a.delta[k];
         double c = a.ctot[e] / a.cdd[e];
         if (c < 0.0 || isnan(c)) c = 0.0;
@@ -235,7 +352,7 @@ __global__ void k_static(P9 g, W9 tau, const double* __restrict__ sdelta,
                          const double* __restrict__ zpts, const double* __restrict__ utau, double cs, double xnu,
                          long long P, int nxy) {
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < P; e += (long long)gridDim.x * blockDim.x) {
-        const int k = (int)(e / nxy);
+        const int k = (int)((unsigned)e / (unsigned)nxy);  // P < 2^31 (checked at create)
         double sn = 0.0;
         for (int j = 0; j < 3; ++j)
             for (int i = 0; i < 3; ++i) {
@@ -256,7 +373,7 @@ __global__ void k_sigma(P9 g, W9 tau, const double* __restrict__ delta, long lon
                         int nxy) {
     const double pi = 4. * atan(1.);
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < P; e += (long long)gridDim.x * blockDim.x) {
-        const int k = (int)(e / nxy);
+        const int k = (int)((unsigned)e / (unsigned)nxy);  // P < 2^31 (checked at create)
         double gij[3][3], G[3][3], G2[3][3];
         for (int l = 0; l < 3; ++l)
             for (int m = 0; m < 3; ++m) gij[l][m] = g.p[3 * l + m][e];
