@@ -236,91 +236,102 @@ __global__ void __launch_bounds__(256) k_ywarp(YInvJobList ij, YFwdJobList fj, Y
 // ----------------------------------------------------------------------------- rows
 // c2r of the modes in X (N+1 entries; zero beyond kxc, DC imaginary part dropped) into
 // registers: lane g returns z[k1 + R*bitrev(g)] in v[k1] (z = x[2m] + i x[2m+1]).
-template <int R>
-__device__ __forceinline__ void row_c2r_regs(const double2* X, int N, int G, int g, const RealPlan& rp,
-                                             double2 (&v)[R]) {
+template <int R, class V>
+__device__ __forceinline__ void row_c2r_regs(const V* X, int N, int G, int g, const V* __restrict__ twr,
+                                             const V* __restrict__ tw, V (&v)[R]) {
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int n = g + G * r;
-        const double2 xa = X[n];
-        const double2 xb = cconj(X[N - n]);
-        const double2 e = cadd(xa, xb);
-        const double2 o = cmul(csub(xa, xb), cconj(__ldg(&rp.twr[n])));
-        v[r] = make_double2(e.x - o.y, e.y + o.x);
+        const V xa = X[n];
+        const V xb = cconj(X[N - n]);
+        const V e = cadd(xa, xb);
+        const V o = cmul(csub(xa, xb), cconj(__ldg(&twr[n])));
+        v[r] = CT<V>::make(e.x - o.y, e.y + o.x);
     }
-    wfft<R, +1>(v, G, g, rp.half.tw);
+    wfft<R, +1>(v, G, g, tw);
 }
 
-__device__ __forceinline__ double2 r2c_mode_w(const double2* Z, int k, int N, const double2* __restrict__ twr) {
-    const double2 za = Z[k];
-    const double2 zb = cconj(Z[k == 0 ? 0 : N - k]);
-    const double2 e = make_double2(0.5 * (za.x + zb.x), 0.5 * (za.y + zb.y));
-    const double2 o = make_double2(0.5 * (za.x - zb.x), 0.5 * (za.y - zb.y));
-    const double2 t = cmul(__ldg(&twr[k]), o);
-    return make_double2(e.x + t.y, e.y - t.x);
+template <class V>
+__device__ __forceinline__ V r2c_mode_w(const V* Z, int k, int N, const V* __restrict__ twr) {
+    using S = typename CT<V>::S;
+    const V za = Z[k];
+    const V zb = cconj(Z[k == 0 ? 0 : N - k]);
+    const V e = CT<V>::make((S)0.5 * (za.x + zb.x), (S)0.5 * (za.y + zb.y));
+    const V o = CT<V>::make((S)0.5 * (za.x - zb.x), (S)0.5 * (za.y - zb.y));
+    const V t = cmul(__ldg(&twr[k]), o);
+    return CT<V>::make(e.x + t.y, e.y - t.x);
 }
 
 // Generic row transforms: each lane group of each warp owns one row at a time.
-template <int R>
+template <int R, class V>
 __global__ void __launch_bounds__(256) k_row_c2r_w(RowJobList jobs, RowArgs a) {
-    extern __shared__ double2 smem[];
+    using S = typename CT<V>::S;
+    extern __shared__ unsigned char rsm_raw[];
+    V* smem = reinterpret_cast<V*>(rsm_raw);
+    const V* twr = sizeof(S) == 4 ? reinterpret_cast<const V*>(a.rp.twrf) : reinterpret_cast<const V*>(a.rp.twr);
+    const V* tw = sizeof(S) == 4 ? reinterpret_cast<const V*>(a.rp.half.twf) : reinterpret_cast<const V*>(a.rp.half.tw);
     const int N = a.nxl / 2, G = a.rp.half.g, lgg = a.rp.half.lgg;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int lpw = 32 / G, q = lane / G, g = lane - q * G;
-    double2* X = smem + (warp * lpw + q) * (N + 1);
+    V* X = smem + (warp * lpw + q) * (N + 1);
     const int nrows = a.nyl * a.nzp;
     const int nunits = jobs.n * nrows;
     const int gw = blockIdx.x * 8 + warp, TW = gridDim.x * 8;
+    const V zero = CT<V>::make((S)0, (S)0);
     for (int u0 = gw * lpw; u0 < nunits; u0 += TW * lpw) {
         const int u = u0 + q;
         const bool act = u < nunits;
         const int uc = act ? u : u0;
         const int jb = uc / nrows, row = uc - jb * nrows;
         const RowIO job = jobs.j[jb];
-        const double* yrow = job.yin + (long long)row * 2 * a.kxc;
-        double2 ld[R + 1];
+        const S* yrow = reinterpret_cast<const S*>(job.yin) + (long long)row * 2 * a.kxc;
+        V ld[R + 1];
 #pragma unroll
         for (int it = 0; it <= R; ++it) {
             const int k = g + G * it;
-            ld[it] = (k < a.kxc) ? *reinterpret_cast<const double2*>(yrow + 2 * k) : make_double2(0.0, 0.0);
+            ld[it] = (k < a.kxc) ? *reinterpret_cast<const V*>(yrow + 2 * k) : zero;
         }
 #pragma unroll
         for (int it = 0; it <= R; ++it) {
             const int k = g + G * it;
             if (k > N) break;
-            double2 v = ld[it];
+            V v = ld[it];
             if (job.mode == YM_IKX && k < a.kxc) {
-                const double kk = a.wavx[2 * k];
-                v = make_double2(-kk * v.y, kk * v.x);
+                const S kk = (S)a.wavx[2 * k];
+                v = CT<V>::make(-kk * v.y, kk * v.x);
             }
-            if (k == 0) v.y = 0.0;
+            if (k == 0) v.y = (S)0;
             X[k] = v;
         }
         __syncwarp();
-        double2 v[R];
-        row_c2r_regs<R>(X, N, G, g, a.rp, v);
-        double m = 0.0;
-        if (job.mean != nullptr && job.add_mean != 0.0) m = job.mean[row / a.nyl] * job.add_mean;
+        V v[R];
+        row_c2r_regs<R>(X, N, G, g, twr, tw, v);
+        S m = (S)0;
+        if (job.mean != nullptr && job.add_mean != 0.0) m = (S)(job.mean[row / a.nyl] * job.add_mean);
         lane_bitrev<R>(v, G, lane, g, lgg);
         __syncwarp();
 #pragma unroll
-        for (int k1 = 0; k1 < R; ++k1) X[R * g + k1] = make_double2(v[k1].x + m, v[k1].y + m);
+        for (int k1 = 0; k1 < R; ++k1) X[R * g + k1] = CT<V>::make(v[k1].x + m, v[k1].y + m);
         __syncwarp();
         if (act) {
-            double2* o = reinterpret_cast<double2*>(job.out + (long long)row * a.row_pitch);
+            V* o = reinterpret_cast<V*>(reinterpret_cast<S*>(job.out) + (long long)row * a.row_pitch);
             for (int k = g; k < N; k += G) o[k] = X[k];
         }
         __syncwarp();
     }
 }
 
-template <int R>
+template <int R, class V>
 __global__ void __launch_bounds__(256) k_row_r2c_w(RowJobList jobs, RowArgs a) {
-    extern __shared__ double2 smem[];
+    using S = typename CT<V>::S;
+    extern __shared__ unsigned char rsm_raw[];
+    V* smem = reinterpret_cast<V*>(rsm_raw);
+    const V* twr = sizeof(S) == 4 ? reinterpret_cast<const V*>(a.rp.twrf) : reinterpret_cast<const V*>(a.rp.twr);
+    const V* tw = sizeof(S) == 4 ? reinterpret_cast<const V*>(a.rp.half.twf) : reinterpret_cast<const V*>(a.rp.half.tw);
     const int N = a.nxl / 2, G = a.rp.half.g, lgg = a.rp.half.lgg;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int lpw = 32 / G, q = lane / G, g = lane - q * G;
-    double2* Z = smem + (warp * lpw + q) * (N + 1);
+    V* Z = smem + (warp * lpw + q) * (N + 1);
     const int nrows = a.nyl * a.nzp;
     const int nunits = jobs.n * nrows;
     const int gw = blockIdx.x * 8 + warp, TW = gridDim.x * 8;
@@ -330,19 +341,19 @@ __global__ void __launch_bounds__(256) k_row_r2c_w(RowJobList jobs, RowArgs a) {
         const int uc = act ? u : u0;
         const int jb = uc / nrows, row = uc - jb * nrows;
         const RowIO job = jobs.j[jb];
-        const double2* in = reinterpret_cast<const double2*>(job.yin + (long long)row * a.row_pitch);
-        double2 v[R];
+        const V* in = reinterpret_cast<const V*>(reinterpret_cast<const S*>(job.yin) + (long long)row * a.row_pitch);
+        V v[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) v[r] = in[g + G * r];
-        wfft<R, -1>(v, G, g, a.rp.half.tw);
+        wfft<R, -1>(v, G, g, tw);
         lane_bitrev<R>(v, G, lane, g, lgg);
 #pragma unroll
         for (int k1 = 0; k1 < R; ++k1) Z[R * g + k1] = v[k1];
         __syncwarp();
         if (act) {
-            double* yrow = job.out + (long long)row * 2 * a.kxc;
+            S* yrow = reinterpret_cast<S*>(job.out) + (long long)row * 2 * a.kxc;
             for (int k = g; k < a.kxc; k += G)
-                *reinterpret_cast<double2*>(yrow + 2 * k) = r2c_mode_w(Z, k, N, a.rp.twr);
+                *reinterpret_cast<V*>(yrow + 2 * k) = r2c_mode_w(Z, k, N, twr);
         }
         __syncwarp();
     }
@@ -842,14 +853,20 @@ bool ydispatch(const YInvJobList& ij, const YFwdJobList& fj, const YPassArgs& a,
     }
 }
 
-template <int R>
-void rowlaunch(const RowJobList& jobs, const RowArgs& a, cudaStream_t s, bool c2r) {
+template <int R, class V>
+void rowlaunch_t(const RowJobList& jobs, const RowArgs& a, cudaStream_t s, bool c2r) {
     const int N = a.nxl / 2;
-    const size_t sm = (size_t)8 * 32 * (N + 1) * sizeof(double2) / a.rp.half.g;
+    const size_t sm = (size_t)8 * 32 * (N + 1) * sizeof(V) / a.rp.half.g;
     const long long units = (long long)jobs.n * a.nyl * a.nzp;
     const long long blocks = (units + 8 * 32 / a.rp.half.g - 1) / (8 * 32 / a.rp.half.g);
-    if (c2r) { lsb::note_launch(); k_row_c2r_w<R><<<persistent_grid_w(k_row_c2r_w<R>, sm, blocks), 256, sm, s>>>(jobs, a); }
-    else { lsb::note_launch(); k_row_r2c_w<R><<<persistent_grid_w(k_row_r2c_w<R>, sm, blocks), 256, sm, s>>>(jobs, a); }
+    if (c2r) { lsb::note_launch(); k_row_c2r_w<R, V><<<persistent_grid_w(k_row_c2r_w<R, V>, sm, blocks), 256, sm, s>>>(jobs, a); }
+    else { lsb::note_launch(); k_row_r2c_w<R, V><<<persistent_grid_w(k_row_r2c_w<R, V>, sm, blocks), 256, sm, s>>>(jobs, a); }
+}
+
+template <int R>
+void rowlaunch(const RowJobList& jobs, const RowArgs& a, cudaStream_t s, bool c2r) {
+    if (a.f32) rowlaunch_t<R, float2>(jobs, a, s, c2r);
+    else rowlaunch_t<R, double2>(jobs, a, s, c2r);
 }
 
 bool rowdispatch(const RowJobList& jobs, const RowArgs& a, cudaStream_t s, bool c2r) {

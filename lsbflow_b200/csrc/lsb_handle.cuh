@@ -140,10 +140,11 @@ void sgs_tau_phys(lsb_handle* h, const double* ui, const double* g, const double
 void sgs_mul(double* y, const double* x, long long n, cudaStream_t s);
 void diag_compute(lsb_handle* h, lsb_diagnostics* out);
 // lsbgpu.cu helpers used by sgs_kernels.cu
+// f32: physical fields and y-intermediates in FP32 (mixed form); spectral fields are FP64
 void phys_to_spec(lsb_handle* h, const double* const* phys, double* const* spec, int nf, int nzp, double alpha,
-                  double beta, double* const* ybuf);
+                  double beta, double* const* ybuf, bool f32 = false);
 void spec_to_phys(lsb_handle* h, const double* const* spec, double* const* phys, int nf, int nzp,
-                  const double* const* means, const int* modes);
+                  const double* const* means, const int* modes, bool f32 = false);
 void zgemm(lsb_handle* h, const Mat& m, const double* in, double* out, int nf, int epi, double alpha, double beta,
            const double* aux);
 }  // namespace lsb

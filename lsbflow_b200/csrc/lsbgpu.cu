@@ -268,7 +268,7 @@ RowArgs rowargs(lsb_handle* h, bool padded, int nzp) {
 namespace lsb {
 // horfft(-1): physical (unpadded, [nzp][ny][nx]) -> spectral, nf fields
 void phys_to_spec(lsb_handle* h, const double* const* phys, double* const* spec, int nf, int nzp, double alpha,
-                  double beta, double* const* ybuf) {
+                  double beta, double* const* ybuf, bool f32) {
     for (int f0 = 0; f0 < nf; f0 += kMaxJobs) {
         const int n = std::min(kMaxJobs, nf - f0);
         RowJobList rj{};
@@ -279,14 +279,17 @@ void phys_to_spec(lsb_handle* h, const double* const* phys, double* const* spec,
             rj.j[i] = RowIO{phys[f0 + i], y, YM_COPY, 0.0, nullptr};
             yj.j[i] = YFwdJob{y, spec[f0 + i], alpha, beta, 0};
         }
-        launch_row_r2c(rj, rowargs(h, false, nzp), h->stream);
-        launch_yfwd(yj, ypass(h, false, nzp), h->stream);
+        RowArgs ra = rowargs(h, false, nzp);
+        YPassArgs ya = ypass(h, false, nzp);
+        ra.f32 = ya.f32 = f32 ? 1 : 0;
+        launch_row_r2c(rj, ra, h->stream);
+        launch_yfwd(yj, ya, h->stream);
     }
 }
 
 // horfft(+1): spectral -> physical (unpadded), optional mean added to field 0
 void spec_to_phys(lsb_handle* h, const double* const* spec, double* const* phys, int nf, int nzp,
-                  const double* const* means, const int* modes) {
+                  const double* const* means, const int* modes, bool f32) {
     for (int f0 = 0; f0 < nf; f0 += kMaxJobs) {
         const int n = std::min(kMaxJobs, nf - f0);
         YInvJobList yj{};
@@ -299,8 +302,11 @@ void spec_to_phys(lsb_handle* h, const double* const* spec, double* const* phys,
             const double* mean = means ? means[f0 + i] : nullptr;
             rj.j[i] = RowIO{y, phys[f0 + i], mode == YM_IKX ? YM_IKX : YM_COPY, mean ? 1.0 : 0.0, mean};
         }
-        launch_yinv(yj, ypass(h, false, nzp), h->stream);
-        launch_row_c2r(rj, rowargs(h, false, nzp), h->stream);
+        RowArgs ra = rowargs(h, false, nzp);
+        YPassArgs ya = ypass(h, false, nzp);
+        ra.f32 = ya.f32 = f32 ? 1 : 0;
+        launch_yinv(yj, ya, h->stream);
+        launch_row_c2r(rj, ra, h->stream);
     }
 }
 
@@ -354,10 +360,14 @@ void nlterm(lsb_handle* h, const double* uin, double* Nout) {
 
     const bool need_phys = (dealias && h->cfg.forcing == 1) || h->cfg.sgsflag == 1;
     if (need_phys) {
-        // unpadded physical u_l (+ubar), du_l/dx_m (+ubarp on du/dz)
+        // unpadded physical u_l (+ubar), du_l/dx_m (+ubarp on du/dz); FP32 fields in the
+        // mixed form (field i at float offset i * P)
         const long long P = h->P;
+        auto PH = [&](long long i) {
+            return f32 ? reinterpret_cast<double*>(reinterpret_cast<float*>(h->phys) + i * P) : h->phys + i * P;
+        };
         double* ph[12];
-        for (int i = 0; i < 12; ++i) ph[i] = h->phys + i * P;
+        for (int i = 0; i < 12; ++i) ph[i] = PH(i);
         const double* spec[12];
         int modes[12];
         const double* means[12] = {nullptr};
@@ -374,13 +384,22 @@ void nlterm(lsb_handle* h, const double* uin, double* Nout) {
         means[0] = h->ubar;
         means[3 + 2] = h->ubarp;
         const int nphys = (h->cfg.sgsflag == 1) ? 12 : 3;
-        { TimerScope ts(h, "phys_fields"); spec_to_phys(h, spec, ph, nphys, d.nzp, means, modes); }
+        { TimerScope ts(h, "phys_fields"); spec_to_phys(h, spec, ph, nphys, d.nzp, means, modes, f32); }
         if (dealias && h->cfg.forcing == 1) {
             TimerScope ts(h, "forcing");
-            double* fo[3] = {h->phys + 12 * P, h->phys + 13 * P, h->phys + 14 * P};
-            launch_force_phys(ph[0], ph[1], ph[2], fo[0], fo[1], fo[2], h->lamx, h->ubar, d.nx, d.ny, P, h->stream);
+            double* fo[3] = {PH(12), PH(13), PH(14)};
+            if (f32) {
+                // lambda (ubar - u) = -lambda u' from an FP32 u' without the mean (no cancellation)
+                double* up = PH(15);
+                const double* sp1[1] = {uin};
+                double* pp1[1] = {up};
+                spec_to_phys(h, sp1, pp1, 1, d.nzp, nullptr, nullptr, true);
+                launch_force_phys_f32(up, ph[1], ph[2], fo[0], fo[1], fo[2], h->lamx, d.nx, P, h->stream);
+            } else {
+                launch_force_phys(ph[0], ph[1], ph[2], fo[0], fo[1], fo[2], h->lamx, h->ubar, d.nx, d.ny, P, h->stream);
+            }
             double* no[3] = {Nout, Nout + S, Nout + 2 * S};
-            phys_to_spec(h, fo, no, 3, d.nzp, 1.0, 1.0, nullptr);
+            phys_to_spec(h, fo, no, 3, d.nzp, 1.0, 1.0, nullptr, f32);
         }
         if (h->cfg.sgsflag == 1) { TimerScope ts(h, "sgs_total"); sgs_add_tau(h, ph, dealias); }
     }
@@ -766,7 +785,9 @@ int lsb_create(const lsb_config* cfg, const lsb_setup* su, lsb_handle** out) {
         if (cfg->precision != 0 && cfg->precision != 1) fail(LSB_ERR_ARG, "precision must be 0 (FP64) or 1 (mixed)");
         if (cfg->precision == 1) {
             const bool dl = cfg->dealiasflag == 1;
-            if ((dl ? h->pyl : h->py).g == 0 || (dl ? h->rxl : h->rx).half.g != 32)
+            const bool phys = cfg->sgsflag == 1 || (dl && cfg->forcing == 1);
+            if ((dl ? h->pyl : h->py).g == 0 || (dl ? h->rxl : h->rx).half.g != 32 ||
+                (phys && (h->py.g == 0 || h->rx.half.g == 0)))
                 fail(LSB_ERR_ARG, "mixed precision needs transform lengths with register plans: x/2 a multiple of "
                                   "32 (32 R, R in 1,2,3,4,6,8) and y a power of two times 1,2,3,4,6,8");
         }

@@ -262,81 +262,93 @@ struct DynArgs {
     int nxy;
 };
 
+// The pointwise SGS kernels are templated on the working type T (double for the FP64 form,
+// float for the mixed form); pointer fields of the argument blocks are reinterpreted as T.
+template <class T> __device__ __forceinline__ const T* cp_(const double* p) { return reinterpret_cast<const T*>(p); }
+template <class T> __device__ __forceinline__ T* wp_(double* p) { return reinterpret_cast<T*>(p); }
+
+template <class T>
 __global__ void k_dyn1(DynArgs a) {  // S_ij, |S|
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < a.P; e += (long long)gridDim.x * blockDim.x) {
-        double s6[6];
+        T s6[6];
         for (int l = 0; l < 3; ++l)
-            for (int m = l; m < 3; ++m) s6[sym6(l, m)] = 0.5 * (a.g[3 * l + m][e] + a.g[3 * m + l][e]);
-        double sn = 0.0;
+            for (int m = l; m < 3; ++m) s6[sym6(l, m)] = (T)0.5 * (cp_<T>(a.g[3 * l + m])[e] + cp_<T>(a.g[3 * m + l])[e]);
+        T sn = (T)0;
         for (int m = 0; m < 3; ++m)
             for (int l = 0; l < 3; ++l) {
-                const double v = s6[sym6(l, m)];
-                sn = sn + 2. * v * v;
+                const T v = s6[sym6(l, m)];
+                sn = sn + (T)2 * v * v;
             }
-        for (int q = 0; q < 6; ++q) a.sij[q][e] = s6[q];
-        a.snorm[e] = sqrt(sn);
+        for (int q = 0; q < 6; ++q) wp_<T>(a.sij[q])[e] = s6[q];
+        wp_<T>(a.snorm)[e] = sqrt(sn);
     }
 }
 
+template <class T>
 __global__ void k_dyn2(DynArgs a) {  // |[S]|, L' = delta^2 |S| S_ij, [delta]^2 |[S]| [S_ij]
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < a.P; e += (long long)gridDim.x * blockDim.x) {
         const int k = (int)((unsigned)e / (unsigned)a.nxy);  // P < 2^31 (checked at create)
-        const double dl = a.delta[k], cd = 2.0 * dl;
-        double sh = 0.0;
+        const T dl = (T)a.delta[k], cd = (T)2 * dl;
+        T sh = (T)0;
         for (int m = 0; m < 3; ++m)
             for (int l = 0; l < 3; ++l) {
-                const double v = a.sijhat[sym6(l, m)][e];
-                sh = sh + 2. * v * v;
+                const T v = cp_<T>(a.sijhat[sym6(l, m)])[e];
+                sh = sh + (T)2 * v * v;
             }
         sh = sqrt(sh);
-        const double sn = a.snorm[e];
+        const T sn = cp_<T>(a.snorm)[e];
         for (int q = 0; q < 6; ++q) {
-            a.lij[q][e] = dl * dl * sn * a.sij[q][e];
-            a.sijhat[q][e] = cd * cd * sh * a.sijhat[q][e];
+            wp_<T>(a.lij[q])[e] = dl * dl * sn * cp_<T>(a.sij[q])[e];
+            wp_<T>(a.sijhat[q])[e] = cd * cd * sh * cp_<T>(a.sijhat[q])[e];
         }
     }
 }
 
+template <class T>
 __global__ void k_dyn3(DynArgs a) {  // M_ij, L_ij, <M L>, <M M> integrands
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < a.P; e += (long long)gridDim.x * blockDim.x) {
-        double m6[6], l6[6];
-        for (int q = 0; q < 6; ++q) m6[q] = 2.0 * (a.mij[q][e] - a.sijhat[q][e]);
+        T m6[6], l6[6];
+        for (int q = 0; q < 6; ++q) m6[q] = (T)2 * (cp_<T>(a.mij[q])[e] - cp_<T>(a.sijhat[q])[e]);
         for (int l = 0; l < 3; ++l)
-            for (int m = l; m < 3; ++m) l6[sym6(l, m)] = a.lf[sym6(l, m)][e] - a.uihat[l][e] * a.uihat[m][e];
-        double num = 0.0, den = 0.0;
+            for (int m = l; m < 3; ++m)
+                l6[sym6(l, m)] = cp_<T>(a.lf[sym6(l, m)])[e] - cp_<T>(a.uihat[l])[e] * cp_<T>(a.uihat[m])[e];
+        T num = (T)0, den = (T)0;
         for (int m = 0; m < 3; ++m)
             for (int l = 0; l < 3; ++l) {
                 const int q = sym6(l, m);
                 num = num + m6[q] * l6[q];
                 den = den + m6[q] * m6[q];
             }
-        a.numc[e] = num;
-        a.denomc[e] = den;
+        wp_<T>(a.numc)[e] = num;
+        wp_<T>(a.denomc)[e] = den;
     }
 }
 
+template <class T>
 __global__ void k_dyn4(DynArgs a) {  // C clip, nu_sgs, tau = -2 nu S_ij
-    const double cmax = 0.2 * 0.2;
+    const T cmax = (T)(0.2 * 0.2);
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < a.P; e += (long long)gridDim.x * blockDim.x) {
         const int k = (int)((unsigned)e / (unsigned)a.nxy);  // P < 2^31 (checked at create)
-        const double dl = a.delta[k];
-        double c = a.ctot[e] / a.cdd[e];
-        if (c < 0.0 || isnan(c)) c = 0.0;
+        const T dl = (T)a.delta[k];
+        T c = cp_<T>(a.ctot)[e] / cp_<T>(a.cdd)[e];
+        if (c < (T)0 || isnan(c)) c = (T)0;
         if (c > cmax) c = cmax;
-        const double nu = c * dl * dl * a.snorm[e];
+        const T nu = c * dl * dl * cp_<T>(a.snorm)[e];
         for (int l = 0; l < 3; ++l)
-            for (int m = 0; m < 3; ++m) a.tau[3 * l + m][e] = -2.0 * nu * a.sij[sym6(l, m)][e];
+            for (int m = 0; m < 3; ++m) wp_<T>(a.tau[3 * l + m])[e] = (T)-2 * nu * cp_<T>(a.sij[sym6(l, m)])[e];
     }
 }
 
 // ---------------------------------------------------------------- static Smagorinsky
-__global__ void k_utau(const double* __restrict__ dudz, const int* __restrict__ wall, int nwall, long long C,
+template <class T>
+__global__ void k_utau(const double* __restrict__ dudz_, const int* __restrict__ wall, int nwall, long long C,
                        double xnu, int nxy, double* out) {
+    const T* dudz = cp_<T>(dudz_);
     __shared__ double red[256];
     double acc = 0.0;
     for (long long c = threadIdx.x; c < C; c += blockDim.x) {
         double u = 0.0;
-        for (int w = 0; w < nwall; ++w) u = u + xnu * dudz[(long long)wall[w] * C + c];
+        for (int w = 0; w < nwall; ++w) u = u + xnu * (double)dudz[(long long)wall[w] * C + c];
         acc += u / nwall;
     }
     red[threadIdx.x] = acc;
@@ -348,102 +360,113 @@ __global__ void k_utau(const double* __restrict__ dudz, const int* __restrict__ 
     if (threadIdx.x == 0) out[0] = sqrt(fabs(red[0] / (double)nxy));
 }
 
+template <class T>
 __global__ void k_static(P9 g, W9 tau, const double* __restrict__ sdelta,
                          const double* __restrict__ zpts, const double* __restrict__ utau, double cs, double xnu,
                          long long P, int nxy) {
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < P; e += (long long)gridDim.x * blockDim.x) {
         const int k = (int)((unsigned)e / (unsigned)nxy);  // P < 2^31 (checked at create)
-        double sn = 0.0;
+        T sn = (T)0;
         for (int j = 0; j < 3; ++j)
             for (int i = 0; i < 3; ++i) {
-                const double v = 0.5 * (g.p[3 * i + j][e] + g.p[3 * j + i][e]);
+                const T v = (T)0.5 * (cp_<T>(g.p[3 * i + j])[e] + cp_<T>(g.p[3 * j + i])[e]);
                 sn = sn + v * v;
             }
-        sn = sqrt(2. * sn);
+        sn = sqrt((T)2 * sn);
         const double zplus = zpts[k] * utau[0] / xnu;
-        const double f = cs * sdelta[k] * (1. - exp(-zplus / 25.));
-        const double nu = -(f * f) * sn;
+        const T f = (T)(cs * sdelta[k] * (1. - exp(-zplus / 25.)));
+        const T nu = -(f * f) * sn;
         for (int j = 0; j < 3; ++j)
-            for (int i = 0; i < 3; ++i) tau.p[3 * i + j][e] = nu * 0.5 * (g.p[3 * i + j][e] + g.p[3 * j + i][e]);
+            for (int i = 0; i < 3; ++i)
+                wp_<T>(tau.p[3 * i + j])[e] = nu * (T)0.5 * (cp_<T>(g.p[3 * i + j])[e] + cp_<T>(g.p[3 * j + i])[e]);
     }
 }
 
 // ---------------------------------------------------------------- sigma model
-__global__ void k_sigma(P9 g, W9 tau, const double* __restrict__ delta, long long P,
-                        int nxy) {
-    const double pi = 4. * atan(1.);
+template <class T>
+__global__ void k_sigma(P9 g, W9 tau, const double* __restrict__ delta, long long P, int nxy) {
+    const T pi = (T)(4. * atan(1.));
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < P; e += (long long)gridDim.x * blockDim.x) {
         const int k = (int)((unsigned)e / (unsigned)nxy);  // P < 2^31 (checked at create)
-        double gij[3][3], G[3][3], G2[3][3];
+        T gij[3][3], G[3][3], G2[3][3];
         for (int l = 0; l < 3; ++l)
-            for (int m = 0; m < 3; ++m) gij[l][m] = g.p[3 * l + m][e];
+            for (int m = 0; m < 3; ++m) gij[l][m] = cp_<T>(g.p[3 * l + m])[e];
         for (int l = 0; l < 3; ++l)
             for (int m = 0; m < 3; ++m) {
-                double s = 0.0;
+                T s = (T)0;
                 for (int q = 0; q < 3; ++q) s += gij[q][l] * gij[q][m];  // (g^T g)(l,m)
                 G[l][m] = s;
             }
         for (int l = 0; l < 3; ++l)
             for (int m = 0; m < 3; ++m) {
-                double s = 0.0;
+                T s = (T)0;
                 for (int q = 0; q < 3; ++q) s += G[l][q] * G[q][m];
                 G2[l][m] = s;
             }
-        const double i1 = G[0][0] + G[1][1] + G[2][2];
-        const double i2 = 0.5 * (i1 * i1 - (G2[0][0] + G2[1][1] + G2[2][2]));
-        const double i3 = G[0][0] * (G[1][1] * G[2][2] - G[1][2] * G[2][1]) -
-                          G[0][1] * (G[1][0] * G[2][2] - G[1][2] * G[2][0]) +
-                          G[0][2] * (G[1][0] * G[2][1] - G[1][1] * G[2][0]);
-        double a1 = i1 * i1 / 9. - i2 / 3.;
-        const double a2 = i1 * i1 * i1 / 27. - i1 * i2 / 6. + 0.5 * i3;
-        if (a1 < 0.0) a1 = fabs(a1);
-        const double sq = sqrt(a1);
-        const double pre = a2 / pow(sq, 3.0);
-        double a3;
-        if (pre >= 1. || isnan(pre)) a3 = 0.0;
-        else if (pre <= -1.) a3 = pi / 3.;
-        else a3 = acos(pre) / 3.;
-        const double s1 = sqrt(fabs(i1 / 3. + 2. * sq * cos(a3)));
-        const double s2 = sqrt(fabs(i1 / 3. - 2. * sq * cos(pi / 3. + a3)));
-        const double s3 = sqrt(fabs(i1 / 3. - 2. * sq * cos(pi / 3. - a3)));
-        double ds = s3 * (s1 - s2) * (s2 - s3);
-        if (s1 != 0.) ds = ds / (s1 * s1);
-        if (ds < 0.0 || isnan(ds)) ds = 0.0;
-        const double cd = 1.35 * delta[k];
-        const double nu = -(cd * cd) * ds;
+        const T i1 = G[0][0] + G[1][1] + G[2][2];
+        const T i2 = (T)0.5 * (i1 * i1 - (G2[0][0] + G2[1][1] + G2[2][2]));
+        const T i3 = G[0][0] * (G[1][1] * G[2][2] - G[1][2] * G[2][1]) -
+                     G[0][1] * (G[1][0] * G[2][2] - G[1][2] * G[2][0]) +
+                     G[0][2] * (G[1][0] * G[2][1] - G[1][1] * G[2][0]);
+        T a1 = i1 * i1 / (T)9 - i2 / (T)3;
+        const T a2 = i1 * i1 * i1 / (T)27 - i1 * i2 / (T)6 + (T)0.5 * i3;
+        if (a1 < (T)0) a1 = fabs(a1);
+        const T sq = sqrt(a1);
+        const T pre = a2 / pow(sq, (T)3);
+        T a3;
+        if (pre >= (T)1 || isnan(pre)) a3 = (T)0;
+        else if (pre <= (T)-1) a3 = pi / (T)3;
+        else a3 = acos(pre) / (T)3;
+        const T s1 = sqrt(fabs(i1 / (T)3 + (T)2 * sq * cos(a3)));
+        const T s2 = sqrt(fabs(i1 / (T)3 - (T)2 * sq * cos(pi / (T)3 + a3)));
+        const T s3 = sqrt(fabs(i1 / (T)3 - (T)2 * sq * cos(pi / (T)3 - a3)));
+        T ds = s3 * (s1 - s2) * (s2 - s3);
+        if (s1 != (T)0) ds = ds / (s1 * s1);
+        if (ds < (T)0 || isnan(ds)) ds = (T)0;
+        const T cd = (T)(1.35 * delta[k]);
+        const T nu = -(cd * cd) * ds;
         for (int l = 0; l < 3; ++l)
-            for (int m = 0; m < 3; ++m) tau.p[3 * l + m][e] = 2.0 * nu * 0.5 * (gij[l][m] + gij[m][l]);
+            for (int m = 0; m < 3; ++m) wp_<T>(tau.p[3 * l + m])[e] = (T)2 * nu * (T)0.5 * (gij[l][m] + gij[m][l]);
     }
 }
 
 // ---------------------------------------------------------------- interscale
+template <class T>
 __global__ void k_prod9(P9 a, P9 b, W9 out, long long P) {
     // out[3l+m] = a[l] * b[m]
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < P; e += (long long)gridDim.x * blockDim.x)
         for (int l = 0; l < 3; ++l)
-            for (int m = 0; m < 3; ++m) out.p[3 * l + m][e] = a.p[l][e] * b.p[m][e];
+            for (int m = 0; m < 3; ++m) wp_<T>(out.p[3 * l + m])[e] = cp_<T>(a.p[l])[e] * cp_<T>(b.p[m])[e];
 }
 
+template <class T>
 __global__ void k_interscale(P9 u, P9 ub, P9 ub2, P9 uibujbar, W9 tau, long long P) {
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < P; e += (long long)gridDim.x * blockDim.x)
         for (int l = 0; l < 3; ++l)
             for (int m = 0; m < 3; ++m)
-                tau.p[3 * l + m][e] = uibujbar.p[3 * l + m][e] - ub2.p[l][e] * ub2.p[m][e] -
-                                      ub.p[l][e] * (u.p[m][e] - ub.p[m][e]);
+                wp_<T>(tau.p[3 * l + m])[e] = cp_<T>(uibujbar.p[3 * l + m])[e] - cp_<T>(ub2.p[l])[e] * cp_<T>(ub2.p[m])[e] -
+                                              cp_<T>(ub.p[l])[e] * (cp_<T>(u.p[m])[e] - cp_<T>(ub.p[m])[e]);
 }
 
+template <class T>
 __global__ void k_uiuj(P9 u, W9 out, long long P) {
     // out[sym(l,m)] = u_l u_m   (src/navierstokes.f90:744)
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < P; e += (long long)gridDim.x * blockDim.x)
         for (int l = 0; l < 3; ++l)
-            for (int m = l; m < 3; ++m) out.p[sym6(l, m)][e] = u.p[m][e] * u.p[l][e];
+            for (int m = l; m < 3; ++m) wp_<T>(out.p[sym6(l, m)])[e] = cp_<T>(u.p[m])[e] * cp_<T>(u.p[l])[e];
+}
+
+template <class T>
+__global__ void k_scale(double* y_, T s, long long n) {
+    T* y = wp_<T>(y_);
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+        y[e] = s * y[e];
 }
 
 __global__ void k_mul(double* y, const double* x, long long n) {
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
         y[e] = y[e] * x[e];
 }
-
 
 }  // namespace
 
@@ -530,19 +553,31 @@ void sgs_init(lsb_handle* h) {
     h->sgs_nwall = (int)wall.size();
 }
 
+// field i of an array of P-point fields of type T (T = float in the mixed form)
+template <class T>
+double* fld(double* base, long long i, long long P) {
+    return reinterpret_cast<double*>(reinterpret_cast<T*>(base) + i * P);
+}
+
 // tau (9 components, index 3l+m) from physical u_l, g = du_l/dx_m (9), uiuj (9, index 3l+m or sym)
+template <class T>
 static void model_tau(lsb_handle* h, const double* const* u, const double* const* g, const double* const* uu6,
                       double* tau) {
     const Dims& d = h->d;
     const lsb_config& c = h->cfg;
     const long long P = h->P;
     const int nxy = d.nx * d.ny;
+    const bool f32 = sizeof(T) == 4;
     SgsWork& s = h->sgs;
     cudaStream_t st = h->stream;
     double* w = s.w;
-    auto W = [&](int i) { return w + (long long)i * P; };
-    double* T[9];
-    for (int q = 0; q < 9; ++q) T[q] = tau + (long long)q * P;
+    auto W = [&](int i) { return fld<T>(w, i, P); };
+    auto F3 = [&](const double* const* in, double* const* out, int n, double fa, double fb, int which) {
+        filter3_any(h, reinterpret_cast<const void* const*>(in), reinterpret_cast<void* const*>(out), n, fa, fb,
+                    which, f32);
+    };
+    double* Tq[9];
+    for (int q = 0; q < 9; ++q) Tq[q] = fld<T>(tau, q, P);
     if (c.sgsmodel == 1) {
         DynArgs a{};
         for (int q = 0; q < 9; ++q) a.g[q] = g[q];
@@ -559,39 +594,39 @@ static void model_tau(lsb_handle* h, const double* const* u, const double* const
         a.denomc = W(35);
         a.ctot = W(36);
         a.cdd = W(37);
-        for (int q = 0; q < 9; ++q) a.tau[q] = T[q];
+        for (int q = 0; q < 9; ++q) a.tau[q] = Tq[q];
         a.delta = s.delta;
         a.P = P;
         a.nxy = nxy;
-        { lsb::note_launch(); k_dyn1<<<nblk(P), 256, 0, st>>>(a); }
-        filter3(h, (const double* const*)a.sij, a.sijhat, 6, c.a, c.b, 0);
-        { lsb::note_launch(); k_dyn2<<<nblk(P), 256, 0, st>>>(a); }
-        filter3(h, (const double* const*)a.lij, a.mij, 6, c.a, c.b, 0);
+        { lsb::note_launch(); k_dyn1<T><<<nblk(P), 256, 0, st>>>(a); }
+        F3((const double* const*)a.sij, a.sijhat, 6, c.a, c.b, 0);
+        { lsb::note_launch(); k_dyn2<T><<<nblk(P), 256, 0, st>>>(a); }
+        F3((const double* const*)a.lij, a.mij, 6, c.a, c.b, 0);
         double* uh[3] = {W(30), W(31), W(32)};
-        filter3(h, u, uh, 3, c.a, c.b, 0);
-        filter3(h, uu6, a.lf, 6, c.a, c.b, 0);
-        { lsb::note_launch(); k_dyn3<<<nblk(P), 256, 0, st>>>(a); }
+        F3(u, uh, 3, c.a, c.b, 0);
+        F3(uu6, a.lf, 6, c.a, c.b, 0);
+        { lsb::note_launch(); k_dyn3<T><<<nblk(P), 256, 0, st>>>(a); }
         const double* nd[2] = {a.numc, a.denomc};
         double* cc[2] = {W(36), W(37)};
-        filter3(h, nd, cc, 2, 1.0, 1.0, 1);
-        { lsb::note_launch(); k_dyn4<<<nblk(P), 256, 0, st>>>(a); }
+        F3(nd, cc, 2, 1.0, 1.0, 1);
+        { lsb::note_launch(); k_dyn4<T><<<nblk(P), 256, 0, st>>>(a); }
     } else if (c.sgsmodel == 0) {
         P9 gt{};
         W9 tt{};
         for (int q = 0; q < 9; ++q) {
             gt.p[q] = g[q];
-            tt.p[q] = T[q];
+            tt.p[q] = Tq[q];
         }
-        { lsb::note_launch(); k_utau<<<1, 256, 0, st>>>(g[2], h->sgs_wall, h->sgs_nwall, d.C(), c.xnu, nxy, s.scal); }
-        { lsb::note_launch(); k_static<<<nblk(P), 256, 0, st>>>(gt, tt, s.sdelta, h->zpts, s.scal, c.cs, c.xnu, P, nxy); }
+        { lsb::note_launch(); k_utau<T><<<1, 256, 0, st>>>(g[2], h->sgs_wall, h->sgs_nwall, d.C(), c.xnu, nxy, s.scal); }
+        { lsb::note_launch(); k_static<T><<<nblk(P), 256, 0, st>>>(gt, tt, s.sdelta, h->zpts, s.scal, c.cs, c.xnu, P, nxy); }
     } else if (c.sgsmodel == 2) {
         P9 gt{};
         W9 tt{};
         for (int q = 0; q < 9; ++q) {
             gt.p[q] = g[q];
-            tt.p[q] = T[q];
+            tt.p[q] = Tq[q];
         }
-        { lsb::note_launch(); k_sigma<<<nblk(P), 256, 0, st>>>(gt, tt, s.delta, P, nxy); }
+        { lsb::note_launch(); k_sigma<T><<<nblk(P), 256, 0, st>>>(gt, tt, s.delta, P, nxy); }
     } else if (c.sgsmodel == 3) {
         double* ub[3] = {W(0), W(1), W(2)};
         double* ub2[3] = {W(3), W(4), W(5)};
@@ -601,8 +636,8 @@ static void model_tau(lsb_handle* h, const double* const* u, const double* const
             pr[q] = W(6 + q);
             pb[q] = W(15 + q);
         }
-        filter3(h, u, ub, 3, c.a, c.b, 0);
-        filter3(h, (const double* const*)ub, ub2, 3, c.a, c.b, 0);
+        F3(u, ub, 3, c.a, c.b, 0);
+        F3((const double* const*)ub, ub2, 3, c.a, c.b, 0);
         P9 ubt{}, ut{}, ub2t{}, pbt{};
         W9 prt{}, tt{};
         for (int l = 0; l < 3; ++l) {
@@ -613,52 +648,63 @@ static void model_tau(lsb_handle* h, const double* const* u, const double* const
         for (int q = 0; q < 9; ++q) {
             prt.p[q] = pr[q];
             pbt.p[q] = pb[q];
-            tt.p[q] = T[q];
+            tt.p[q] = Tq[q];
         }
-        { lsb::note_launch(); k_prod9<<<nblk(P), 256, 0, st>>>(ubt, ut, prt, P); }
-        filter3(h, (const double* const*)pr, pb, 9, c.a, c.b, 0);
-        { lsb::note_launch(); k_interscale<<<nblk(P), 256, 0, st>>>(ut, ubt, ub2t, pbt, tt, P); }
+        { lsb::note_launch(); k_prod9<T><<<nblk(P), 256, 0, st>>>(ubt, ut, prt, P); }
+        F3((const double* const*)pr, pb, 9, c.a, c.b, 0);
+        { lsb::note_launch(); k_interscale<T><<<nblk(P), 256, 0, st>>>(ut, ubt, ub2t, pbt, tt, P); }
     } else {
-        CK(cudaMemsetAsync(tau, 0, 9 * P * sizeof(double), st));
+        CK(cudaMemsetAsync(tau, 0, 9 * P * sizeof(T), st));
     }
 }
 
-// nlterm hook: ph[0..2] = u_l (+ubar), ph[3+3l+m] = du_l/dx_m; adds the forward transform of
-// tau into the spectral h fields.
+// nlterm hook: ph[0..2] = u_l (+ubar), ph[3+3l+m] = du_l/dx_m (physical fields of the
+// working type: FP32 in the mixed form); adds the forward transform of tau into the
+// spectral h fields.
 void sgs_add_tau(lsb_handle* h, double* const* ph, bool dealias) {
     const Dims& d = h->d;
     const long long P = h->P, S = d.S();
     SgsWork& s = h->sgs;
     cudaStream_t st = h->stream;
+    const bool f32 = h->cfg.precision == 1;
+    auto PH = [&](long long i) { return f32 ? fld<float>(h->phys, i, P) : fld<double>(h->phys, i, P); };
+    auto TAU = [&](long long i) { return f32 ? fld<float>(s.tau, i, P) : fld<double>(s.tau, i, P); };
     // u_i u_j on the unpadded grid: the dealiased products (2 * horfft(+1) of h) or plain products
     double* uu6[6];
-    for (int q = 0; q < 6; ++q) uu6[q] = h->phys + (12 + q) * P;
+    for (int q = 0; q < 6; ++q) uu6[q] = PH(12 + q);
     const double* u3[3] = {ph[0], ph[1], ph[2]};
     if (dealias) {
         const double* hs[6];
         for (int q = 0; q < 6; ++q) hs[q] = h->H + q * S;
-        spec_to_phys(h, hs, uu6, 6, d.nzp, nullptr, nullptr);
-        for (int q = 0; q < 6; ++q) launch_axpby(uu6[q], uu6[q], 2.0, 0.0, P, st);
+        spec_to_phys(h, hs, uu6, 6, d.nzp, nullptr, nullptr, f32);
+        for (int q = 0; q < 6; ++q) {
+            lsb::note_launch();
+            if (f32) k_scale<float><<<nblk(P), 256, 0, st>>>(uu6[q], 2.0f, P);
+            else k_scale<double><<<nblk(P), 256, 0, st>>>(uu6[q], 2.0, P);
+        }
     } else {
         P9 ut{};
         W9 ot{};
         for (int l = 0; l < 3; ++l) ut.p[l] = ph[l];
         for (int q = 0; q < 6; ++q) ot.p[q] = uu6[q];
-        { lsb::note_launch(); k_uiuj<<<nblk(P), 256, 0, st>>>(ut, ot, P); }
+        lsb::note_launch();
+        if (f32) k_uiuj<float><<<nblk(P), 256, 0, st>>>(ut, ot, P);
+        else k_uiuj<double><<<nblk(P), 256, 0, st>>>(ut, ot, P);
     }
     const double* g[9];
     for (int q = 0; q < 9; ++q) g[q] = ph[3 + q];
-    model_tau(h, u3, g, (const double* const*)uu6, s.tau);
+    if (f32) model_tau<float>(h, u3, g, (const double* const*)uu6, s.tau);
+    else model_tau<double>(h, u3, g, (const double* const*)uu6, s.tau);
     if (!s.nonsym) {
         // symmetric: add T(tau_lm) to h_lm for the 6 independent components
         const double* tp[6];
         double* hp[6];
         for (int l = 0; l < 3; ++l)
             for (int m = l; m < 3; ++m) {
-                tp[sym6(l, m)] = s.tau + (3 * l + m) * P;
+                tp[sym6(l, m)] = TAU(3 * l + m);
                 hp[sym6(l, m)] = h->H + sym6(l, m) * S;
             }
-        phys_to_spec(h, tp, hp, 6, d.nzp, 1.0, 1.0, nullptr);
+        phys_to_spec(h, tp, hp, 6, d.nzp, 1.0, 1.0, nullptr, f32);
     } else {
         const double* tp[9];
         double* hp[9];
@@ -666,10 +712,10 @@ void sgs_add_tau(lsb_handle* h, double* const* ph, bool dealias) {
             for (int m = 0; m < 3; ++m) {
                 CK(cudaMemcpyAsync(s.H9 + (3 * l + m) * S, h->H + sym6(l, m) * S, S * sizeof(double),
                                    cudaMemcpyDeviceToDevice, st));
-                tp[3 * l + m] = s.tau + (3 * l + m) * P;
+                tp[3 * l + m] = TAU(3 * l + m);
                 hp[3 * l + m] = s.H9 + (3 * l + m) * S;
             }
-        phys_to_spec(h, tp, hp, 9, d.nzp, 1.0, 1.0, nullptr);
+        phys_to_spec(h, tp, hp, 9, d.nzp, 1.0, 1.0, nullptr, f32);
     }
 }
 
@@ -681,7 +727,7 @@ void sgs_tau_phys(lsb_handle* h, const double* ui, const double* g, const double
     const double* uu6[6];
     for (int l = 0; l < 3; ++l)
         for (int m = l; m < 3; ++m) uu6[sym6(l, m)] = uiuj + (3 * l + m) * P;
-    model_tau(h, u3, g9, uu6, tau);
+    model_tau<double>(h, u3, g9, uu6, tau);
 }
 
 // ---------------------------------------------------------------- filtering hook

@@ -284,6 +284,24 @@ void launch_force_phys(const double* u0, const double* u1, const double* u2, dou
                        const double* lamx, const double* ubar, int nx, int ny, long long P, cudaStream_t s) {
     { lsb::note_launch(); k_force_phys<<<nblk(P), 256, 0, s>>>(u0, u1, u2, f0, f1, f2, lamx, ubar, nx, ny, P); }
 }
+// mixed form: fringe forcing in FP32 from the perturbation u' (field without the mean)
+__global__ void k_force_phys_f32(const float* __restrict__ up, const float* __restrict__ u1,
+                                 const float* __restrict__ u2, float* __restrict__ f0, float* __restrict__ f1,
+                                 float* __restrict__ f2, const double* __restrict__ lamx, int nx, long long P) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < P; e += (long long)gridDim.x * blockDim.x) {
+        const float l = (float)lamx[(int)((unsigned)e % (unsigned)nx)];
+        f0[e] = -l * up[e];
+        f1[e] = -l * u1[e];
+        f2[e] = -l * u2[e];
+    }
+}
+void launch_force_phys_f32(const double* up, const double* u1, const double* u2, double* f0, double* f1, double* f2,
+                           const double* lamx, int nx, long long P, cudaStream_t s) {
+    auto c = [](const double* p) { return reinterpret_cast<const float*>(p); };
+    auto w = [](double* p) { return reinterpret_cast<float*>(p); };
+    { lsb::note_launch(); k_force_phys_f32<<<nblk(P), 256, 0, s>>>(c(up), c(u1), c(u2), w(f0), w(f1), w(f2), lamx, nx, P); }
+}
+
 // mixed form: the FP32 product kernel leaves 0.5 ubar(z)^2 out of h_11; its (kx, ky) = (0, 0)
 // coefficient is restored here in FP64 (the dynamic model filters u_1 u_1 in physical space)
 __global__ void k_add_half_sq(double* h11, const double* ubar, long long C, int nzp) {
