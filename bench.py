@@ -34,7 +34,7 @@ from lsbflow_b200 import ic  # noqa: E402
 from lsbflow_b200.config import workload  # noqa: E402
 
 WORKLOAD = "les256"
-METRIC = "grid-point-steps/s (FP64 dynamic-Smagorinsky LES time step)"
+METRIC = "grid-point-steps/s (FP64 dynamic-Smagorinsky LES time step; mixed form beside it)"
 UNIT = "pt-steps/s"
 
 
@@ -177,6 +177,7 @@ def main():
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--serve-runs", type=int, default=12)
     args = ap.parse_args()
     cfg = workload(args.workload)
@@ -278,6 +279,48 @@ def main():
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e_val = replicas.job_throughput(pts, e2e_steps, world, e2e_s)
 
+    # ---- the mixed-precision form on the same workload: throughput and its error against
+    # the FP64 form after 100 steps from the same initial field
+    mixed = None
+    if not args.no_mixed:
+        cfg_m = cfg.replace(precision=1)
+        sm = lib.Solver(hs.make_setup(cfg_m))
+        sm.set_stream(stream.cuda_stream)
+        sm.upload(u, v, w, dt=st.dt)
+        sm.step(args.warmup)
+        torch.cuda.synchronize()
+        barrier()
+        em0 = torch.cuda.Event(enable_timing=True)
+        em1 = torch.cuda.Event(enable_timing=True)
+        em0.record(stream)
+        sm.step(args.steps)
+        em1.record(stream)
+        torch.cuda.synchronize()
+        ms_m = max_over_ranks(em0.elapsed_time(em1))
+        nerr = 100
+        sm.upload(u, v, w, dt=st.dt)
+        sm.step(nerr)
+        got = sm.download()
+        sm.close()
+        sref = lib.Solver(st)
+        sref.set_stream(stream.cuda_stream)
+        sref.upload(u, v, w, dt=st.dt)
+        sref.step(nerr)
+        ref = sref.download()
+        sref.close()
+
+        def rel(a, b):
+            return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+        vg = np.concatenate([got[k].ravel() for k in ("uf", "vf", "wf")])
+        vr = np.concatenate([ref[k].ravel() for k in ("uf", "vf", "wf")])
+        mixed = {"value": replicas.job_throughput(pts, args.steps, world, ms_m / 1e3), "unit": UNIT,
+                 "ms_per_step": ms_m / args.steps, "speedup_vs_fp64": (ms / args.steps) / (ms_m / args.steps),
+                 "rel_err_velocity_after_100_steps": rel(vg, vr),
+                 "rel_err_components": {k: rel(got[k], ref[k]) for k in ("uf", "vf", "wf", "pf")},
+                 "form": "FP32 transforms, products, physical fields and SGS; FP64 state, time integration, "
+                         "boundary conditions, Chebyshev derivatives and eigenbasis solves"}
+
     # ---- serving: a Poisson stream of ensemble runs (continuous batching on this GPU)
     serving = None
     if not args.no_serving:
@@ -319,6 +362,7 @@ def main():
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": 3 * S8, "d2h_bytes_per_step": 3 * S8},
             "gpu_launches": launches,
             "cpu_baseline": cpu,
+            "mixed": mixed,
             "serving": serving,
         }
         print(json.dumps(line), flush=True)

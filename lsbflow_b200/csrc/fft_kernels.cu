@@ -351,18 +351,7 @@ static bool wide(const FftPlan& P) {
 // persistent grid: resident blocks per SM x SMs, capped by the number of work items
 template <class K>
 static int persistent_grid(K kern, size_t smem, int nitems) {
-    static int nsm = 0;
-    if (nsm == 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        if (nsm <= 0) nsm = 148;
-    }
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 256, smem);
-    if (occ < 1) occ = 1;
-    const int g = occ * nsm;
+    const int g = resident_blocks((const void*)kern, 256, smem) * sm_count();
     return g < nitems ? g : nitems;
 }
 

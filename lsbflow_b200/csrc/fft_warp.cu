@@ -812,18 +812,7 @@ __global__ void __launch_bounds__(128, 4) k_row_nl_f(NlRowArgs a) {
 
 template <class K>
 int persistent_grid_w(K kern, size_t smem, long long nitems) {
-    static int nsm = 0;
-    if (nsm == 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        if (nsm <= 0) nsm = 148;
-    }
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 256, smem);
-    if (occ < 1) occ = 1;
-    const long long gsz = (long long)occ * nsm;
+    const long long gsz = (long long)resident_blocks((const void*)kern, 256, smem) * sm_count();
     return (int)(gsz < nitems ? gsz : (nitems > 0 ? nitems : 1));
 }
 
@@ -887,33 +876,15 @@ void nllaunch(const NlRowArgs& a, cudaStream_t s) {
     const int nitems = a.r.nyl * a.r.nzp;
     if (a.r.f32) {
         if (a.r.rp.half.g != 32) throw std::runtime_error("mixed precision: x transform length has no full-warp plan");
-        static int nsmf = 0;
-        if (nsmf == 0) {
-            int dev = 0;
-            cudaGetDevice(&dev);
-            cudaDeviceGetAttribute(&nsmf, cudaDevAttrMultiProcessorCount, dev);
-            if (nsmf <= 0) nsmf = 148;
-        }
-        int occ = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_row_nl_f<R>, 128, 0);
-        if (occ < 1) occ = 1;
-        long long blocks = (long long)occ * nsmf, need = (nitems + 3) / 4;
+        const int occ = resident_blocks((const void*)k_row_nl_f<R>, 128, 0);
+        long long blocks = (long long)occ * sm_count(), need = (nitems + 3) / 4;
         if (blocks > need) blocks = need > 0 ? need : 1;
         { lsb::note_launch(); k_row_nl_f<R><<<(int)blocks, 128, 0, s>>>(a); }
         return;
     }
     if (a.r.rp.half.g == 32) {
-        static int nsm = 0;
-        if (nsm == 0) {
-            int dev = 0;
-            cudaGetDevice(&dev);
-            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-            if (nsm <= 0) nsm = 148;
-        }
-        int occ = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_row_nl_r<R>, 128, 0);
-        if (occ < 1) occ = 1;
-        long long blocks = (long long)occ * nsm, need = (nitems + 3) / 4;
+        const int occ = resident_blocks((const void*)k_row_nl_r<R>, 128, 0);
+        long long blocks = (long long)occ * sm_count(), need = (nitems + 3) / 4;
         if (blocks > need) blocks = need > 0 ? need : 1;
         { lsb::note_launch(); k_row_nl_r<R><<<(int)blocks, 128, 0, s>>>(a); }
         return;

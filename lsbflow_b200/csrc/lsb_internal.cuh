@@ -20,6 +20,13 @@ namespace lsb {
 // counts every kernel launch of the library (lsb_kernel_launches)
 void note_launch();
 
+// resident blocks of a kernel on one SM for a block size and dynamic shared memory,
+// queried once per (device, kernel, threads, shared memory) and cached; the first query
+// also raises the kernel's dynamic shared memory limit to 200 KB
+int resident_blocks(const void* kern, int threads, size_t smem);
+// SMs of the current device (cached per device)
+int sm_count();
+
 constexpr int kMaxStages = 16;
 
 // exact unsigned division by a constant: q = (umulhi(n, m) + n) >> s  (d > 1), valid for

@@ -4,6 +4,9 @@
 // as a fixed sequence of kernels on one stream, with the histories (u^{n-1}, u^{n-2},
 // N^{n-1}, N^{n-2}, p^{n-1}) kept resident as rotating buffers: no copies between steps.
 #include <atomic>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -697,6 +700,41 @@ void set_last_error(const std::string& m) { g_err = m; }
 // kernels launched by this library since it was loaded (all handles, all threads)
 static std::atomic<unsigned long long> g_kernel_launches{0};
 void note_launch() { g_kernel_launches.fetch_add(1, std::memory_order_relaxed); }
+
+static std::mutex g_occ_mu;
+static std::map<std::tuple<int, const void*, int, size_t>, int> g_occ;
+static std::map<int, int> g_nsm;
+
+int sm_count() {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(g_occ_mu);
+    auto it = g_nsm.find(dev);
+    if (it != g_nsm.end()) return it->second;
+    int n = 0;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+    g_nsm[dev] = n;
+    return n;
+}
+
+int resident_blocks(const void* kern, int threads, size_t smem) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const auto key = std::make_tuple(dev, kern, threads, smem);
+    {
+        std::lock_guard<std::mutex> lk(g_occ_mu);
+        auto it = g_occ.find(key);
+        if (it != g_occ.end()) return it->second;
+    }
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, smem);
+    if (occ < 1) occ = 1;
+    std::lock_guard<std::mutex> lk(g_occ_mu);
+    g_occ[key] = occ;
+    return occ;
+}
 }  // namespace lsb
 
 // ====================================================================================== C ABI
