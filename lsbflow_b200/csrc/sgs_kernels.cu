@@ -224,10 +224,10 @@ void filter3_any(lsb_handle* h, const void* const* in, void* const* out, int n, 
             const size_t es = f32 ? sizeof(float) : sizeof(double);
             const size_t sm = (size_t)(RT_ST + 1) * (FJ + 2) * d.nx * es;
             if (f32) {
-                if (sm > 48 * 1024) cudaFuncSetAttribute(k_filter3p<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+                if (sm > 48 * 1024) resident_blocks((const void*)k_filter3p<float>, 256, sm);  // raises the limit once
                 { lsb::note_launch(); k_filter3p<float><<<grid, 256, sm, h->stream>>>(fl, lgx, d.ny, d.nzp, FJ, zch, (float)a, (float)b, zf, zf + d.nzp, zf + 2 * d.nzp); }
             } else {
-                if (sm > 48 * 1024) cudaFuncSetAttribute(k_filter3p<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+                if (sm > 48 * 1024) resident_blocks((const void*)k_filter3p<double>, 256, sm);  // raises the limit once
                 { lsb::note_launch(); k_filter3p<double><<<grid, 256, sm, h->stream>>>(fl, lgx, d.ny, d.nzp, FJ, zch, a, b, zf, zf + d.nzp, zf + 2 * d.nzp); }
             }
         } else {
