@@ -468,6 +468,8 @@ __global__ void __launch_bounds__(256, 2) k_row_c2r(RowJobList jobs, RowArgs a) 
         for (int idx = tid; idx < L * N; idx += 256) {
             const int l = idx / N, k = idx - l * N;
             double2 v = R[l * LS + k];
+            v.x *= job.scale;
+            v.y *= job.scale;
             if (job.mean != nullptr && job.add_mean != 0.0) {
                 const double m = job.mean[(row0 + l) / a.nyl] * job.add_mean;
                 v.x += m;

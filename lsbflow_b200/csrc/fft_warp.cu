@@ -308,10 +308,11 @@ __global__ void __launch_bounds__(256) k_row_c2r_w(RowJobList jobs, RowArgs a) {
         row_c2r_regs<R>(X, N, G, g, twr, tw, v);
         S m = (S)0;
         if (job.mean != nullptr && job.add_mean != 0.0) m = (S)(job.mean[row / a.nyl] * job.add_mean);
+        const S sc = (S)job.scale;
         lane_bitrev<R>(v, G, lane, g, lgg);
         __syncwarp();
 #pragma unroll
-        for (int k1 = 0; k1 < R; ++k1) X[R * g + k1] = CT<V>::make(v[k1].x + m, v[k1].y + m);
+        for (int k1 = 0; k1 < R; ++k1) X[R * g + k1] = CT<V>::make(sc * v[k1].x + m, sc * v[k1].y + m);
         __syncwarp();
         if (act) {
             V* o = reinterpret_cast<V*>(reinterpret_cast<S*>(job.out) + (long long)row * a.row_pitch);

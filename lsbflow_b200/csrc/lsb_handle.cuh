@@ -144,7 +144,7 @@ void diag_compute(lsb_handle* h, lsb_diagnostics* out);
 void phys_to_spec(lsb_handle* h, const double* const* phys, double* const* spec, int nf, int nzp, double alpha,
                   double beta, double* const* ybuf, bool f32 = false);
 void spec_to_phys(lsb_handle* h, const double* const* spec, double* const* phys, int nf, int nzp,
-                  const double* const* means, const int* modes, bool f32 = false);
+                  const double* const* means, const int* modes, bool f32 = false, double scale = 1.0);
 void zgemm(lsb_handle* h, const Mat& m, const double* in, double* out, int nf, int epi, double alpha, double beta,
            const double* aux);
 }  // namespace lsb

@@ -26,6 +26,11 @@ void note_launch();
 int resident_blocks(const void* kern, int threads, size_t smem);
 // SMs of the current device (cached per device)
 int sm_count();
+// opt-in maximum of dynamic shared memory per block on the current device (cached)
+size_t smem_optin();
+// raises a kernel's dynamic shared memory limit to smem (once per device, kernel and size);
+// false, with the CUDA error cleared, when the device refuses it
+bool allow_smem(const void* kern, size_t smem);
 
 constexpr int kMaxStages = 16;
 
@@ -107,6 +112,7 @@ struct RowIO {
     int mode;           // YM_COPY or YM_IKX (c2r only)
     double add_mean;    // c2r only: 0 or 1 -> add mean[k] to the physical row (u + ubar)
     const double* mean; // [nzp] or nullptr
+    double scale;       // c2r only: the physical row is scale * c2r (+ mean)
 };
 struct RowArgs {
     int f32 = 0;                // 1: y-intermediate and physical rows in FP32 (mixed form)
@@ -177,5 +183,6 @@ struct GemmArgs {
     double lift_sigma;
 };
 void launch_gemm(const GemmArgs& g, cudaStream_t s);
+
 
 }  // namespace lsb

@@ -9,6 +9,7 @@
 #include <tuple>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <stdexcept>
@@ -279,7 +280,7 @@ void phys_to_spec(lsb_handle* h, const double* const* phys, double* const* spec,
         rj.n = yj.n = n;
         for (int i = 0; i < n; ++i) {
             double* y = ybuf ? ybuf[f0 + i] : h->Yu + (long long)i * h->Yu1;
-            rj.j[i] = RowIO{phys[f0 + i], y, YM_COPY, 0.0, nullptr};
+            rj.j[i] = RowIO{phys[f0 + i], y, YM_COPY, 0.0, nullptr, 1.0};
             yj.j[i] = YFwdJob{y, spec[f0 + i], alpha, beta, 0};
         }
         RowArgs ra = rowargs(h, false, nzp);
@@ -292,7 +293,7 @@ void phys_to_spec(lsb_handle* h, const double* const* phys, double* const* spec,
 
 // horfft(+1): spectral -> physical (unpadded), optional mean added to field 0
 void spec_to_phys(lsb_handle* h, const double* const* spec, double* const* phys, int nf, int nzp,
-                  const double* const* means, const int* modes, bool f32) {
+                  const double* const* means, const int* modes, bool f32, double scale) {
     for (int f0 = 0; f0 < nf; f0 += kMaxJobs) {
         const int n = std::min(kMaxJobs, nf - f0);
         YInvJobList yj{};
@@ -303,7 +304,7 @@ void spec_to_phys(lsb_handle* h, const double* const* spec, double* const* phys,
             const int mode = modes ? modes[f0 + i] : YM_COPY;
             yj.j[i] = YInvJob{spec[f0 + i], y, mode == YM_IKY ? YM_IKY : YM_COPY};
             const double* mean = means ? means[f0 + i] : nullptr;
-            rj.j[i] = RowIO{y, phys[f0 + i], mode == YM_IKX ? YM_IKX : YM_COPY, mean ? 1.0 : 0.0, mean};
+            rj.j[i] = RowIO{y, phys[f0 + i], mode == YM_IKX ? YM_IKX : YM_COPY, mean ? 1.0 : 0.0, mean, scale};
         }
         RowArgs ra = rowargs(h, false, nzp);
         YPassArgs ya = ypass(h, false, nzp);
@@ -718,6 +719,42 @@ int sm_count() {
     return n;
 }
 
+size_t smem_optin() {
+    static std::map<int, size_t> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(g_occ_mu);
+    auto it = cache.find(dev);
+    if (it != cache.end()) return it->second;
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cache[dev] = (size_t)(v > 0 ? v : 48 * 1024);
+    return cache[dev];
+}
+
+bool allow_smem(const void* kern, size_t smem) {
+    // the limit is a property of the kernel, not of a launch: keep the largest value set so
+    // far per (device, kernel) and only ever raise it
+    static std::map<std::pair<int, const void*>, size_t> cur;
+    if (smem <= 48 * 1024) return true;
+    if (smem > smem_optin()) return false;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const auto key = std::make_pair(dev, kern);
+    std::lock_guard<std::mutex> lk(g_occ_mu);
+    auto it = cur.find(key);
+    if (it != cur.end() && it->second >= smem) return true;
+    const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) {
+        cudaGetLastError();  // clear it: the caller falls back to another kernel
+        if (std::getenv("LSB_DEBUG"))
+            std::fprintf(stderr, "lsbgpu: dynamic shared memory %zu refused: %s\n", smem, cudaGetErrorString(e));
+        return false;
+    }
+    cur[key] = smem;
+    return true;
+}
+
 int resident_blocks(const void* kern, int threads, size_t smem) {
     int dev = 0;
     cudaGetDevice(&dev);
@@ -727,7 +764,9 @@ int resident_blocks(const void* kern, int threads, size_t smem) {
         auto it = g_occ.find(key);
         if (it != g_occ.end()) return it->second;
     }
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    size_t lim = smem > 200 * 1024 ? smem : 200 * 1024;
+    if (lim > smem_optin()) lim = smem_optin();
+    allow_smem(kern, lim);
     int occ = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, smem);
     if (occ < 1) occ = 1;
@@ -1152,14 +1191,14 @@ int lsb_dealias_product(lsb_handle* h, const double* a, const double* b, double*
         const long long PL = (long long)d.nxl * d.nyl * d.nzp;
         double* pl = h->Y + 2 * h->Yl;  // padded physical rows live after the two y-intermediates
         if (2 * h->Yl + 3 * PL > 18 * h->Yl) fail(LSB_ERR_STATE, "scratch too small");
-        rj.j[0] = RowIO{h->Y, pl, YM_COPY, 0.0, nullptr};
-        rj.j[1] = RowIO{h->Y + h->Yl, pl + PL, YM_COPY, 0.0, nullptr};
+        rj.j[0] = RowIO{h->Y, pl, YM_COPY, 0.0, nullptr, 1.0};
+        rj.j[1] = RowIO{h->Y + h->Yl, pl + PL, YM_COPY, 0.0, nullptr, 1.0};
         launch_row_c2r(rj, rowargs(h, true, d.nzp), h->stream);
         launch_axpby(pl + 2 * PL, pl, 1.0, 0.0, PL, h->stream);
         sgs_mul(pl + 2 * PL, pl + PL, PL, h->stream);
         RowJobList rf{};
         rf.n = 1;
-        rf.j[0] = RowIO{pl + 2 * PL, h->Y, YM_COPY, 0.0, nullptr};
+        rf.j[0] = RowIO{pl + 2 * PL, h->Y, YM_COPY, 0.0, nullptr, 1.0};
         launch_row_r2c(rf, rowargs(h, true, d.nzp), h->stream);
         YFwdJobList yf{};
         yf.n = 1;

@@ -456,13 +456,6 @@ __global__ void k_uiuj(P9 u, W9 out, long long P) {
             for (int m = l; m < 3; ++m) wp_<T>(out.p[sym6(l, m)])[e] = cp_<T>(u.p[m])[e] * cp_<T>(u.p[l])[e];
 }
 
-template <class T>
-__global__ void k_scale(double* y_, T s, long long n) {
-    T* y = wp_<T>(y_);
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
-        y[e] = s * y[e];
-}
-
 __global__ void k_mul(double* y, const double* x, long long n) {
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
         y[e] = y[e] * x[e];
@@ -676,12 +669,7 @@ void sgs_add_tau(lsb_handle* h, double* const* ph, bool dealias) {
     if (dealias) {
         const double* hs[6];
         for (int q = 0; q < 6; ++q) hs[q] = h->H + q * S;
-        spec_to_phys(h, hs, uu6, 6, d.nzp, nullptr, nullptr, f32);
-        for (int q = 0; q < 6; ++q) {
-            lsb::note_launch();
-            if (f32) k_scale<float><<<nblk(P), 256, 0, st>>>(uu6[q], 2.0f, P);
-            else k_scale<double><<<nblk(P), 256, 0, st>>>(uu6[q], 2.0, P);
-        }
+        spec_to_phys(h, hs, uu6, 6, d.nzp, nullptr, nullptr, f32, 2.0);  // u_i u_j = 2 h_ij
     } else {
         P9 ut{};
         W9 ot{};
