@@ -22,7 +22,9 @@ __device__ __forceinline__ int brev(int g, int lgg) {
     return lgg ? (int)(__brev((unsigned)g) >> (32 - lgg)) : 0;
 }
 
-template <int R, int SIGN, class V>
+// SEL = true: the butterflies as a per-lane select of both branches (fewer live registers,
+// more arithmetic; the FP64 product rows use it to stay within their register budget)
+template <int R, int SIGN, bool SEL = false, class V>
 __device__ __forceinline__ void wfft(V (&v)[R], int G, int g, const V* __restrict__ tw) {
     dft_reg<R, SIGN>(v);
     if (R > 1 && g != 0) {
@@ -33,18 +35,37 @@ __device__ __forceinline__ void wfft(V (&v)[R], int G, int g, const V* __restric
             v[k1] = cmul(v[k1], w);
         }
     }
+    // butterfly of the pair (g, g ^ h): the lower lane keeps v + o, the upper (o - v) w.
+    // Both are t = sg v + o times w', with sg = -1, w' = w on the upper lane and sg = 1,
+    // w' = 1 on the lower one, so no lane evaluates the other's branch (exactly the same
+    // roundings: fma(-1, v, o) = o - v and t * (1, 0) = t).
+    using S = typename CT<V>::S;
     int st = R;  // N / (2h) for 2h = G
     for (int h = G >> 1; h >= 1; h >>= 1) {
         const int j = g & (h - 1);
         const bool up = (g & h) != 0;
         V w = __ldg(&tw[j * st]);
         if (SIGN > 0) w.y = -w.y;
+        if (SEL) {
+#pragma unroll
+            for (int k1 = 0; k1 < R; ++k1) {
+                V o;
+                o.x = __shfl_xor_sync(0xffffffffu, v[k1].x, h);
+                o.y = __shfl_xor_sync(0xffffffffu, v[k1].y, h);
+                v[k1] = up ? cmul(csub(o, v[k1]), w) : cadd(v[k1], o);
+            }
+            st <<= 1;
+            continue;
+        }
+        if (!up) w = CT<V>::make((S)1, (S)0);
+        const S sg = up ? (S)-1 : (S)1;
 #pragma unroll
         for (int k1 = 0; k1 < R; ++k1) {
             V o;
             o.x = __shfl_xor_sync(0xffffffffu, v[k1].x, h);
             o.y = __shfl_xor_sync(0xffffffffu, v[k1].y, h);
-            v[k1] = up ? cmul(csub(o, v[k1]), w) : cadd(v[k1], o);
+            const V tt = CT<V>::make(fma(sg, v[k1].x, o.x), fma(sg, v[k1].y, o.y));
+            v[k1] = cmul(tt, w);
         }
         st <<= 1;
     }
@@ -53,20 +74,39 @@ __device__ __forceinline__ void wfft(V (&v)[R], int G, int g, const V* __restric
 // Inverse of the order produced by wfft: input "slot" layout (lane g' register k1 holds
 // z[k1 + R*bitrev(g')]), cross-lane decimation-in-time network, twiddles, R-point DFT in
 // registers; output in natural order (lane g register r holds X[g + G*r]).
-template <int R, int SIGN, class V>
+template <int R, int SIGN, bool SEL = false, class V>
 __device__ __forceinline__ void wfft_dit(V (&v)[R], int G, int g, const V* __restrict__ tw) {
+    // butterfly of the pair (g, g ^ h): the lower lane keeps v + w o, the upper o - w v.  The
+    // upper lane multiplies its own value by w before the exchange (the lower lane's factor is
+    // 1, exactly), so each lane then takes sg x + o_x with sg = 1 below and -1 above: the same
+    // roundings as forming w o on the lower lane, and no lane evaluates the other's branch
+    using S = typename CT<V>::S;
     int st = R * (G >> 1);  // N / (2h) for h = 1
     for (int h = 1; h < G; h <<= 1) {
         const int j = g & (h - 1);
         const bool up = (g & h) != 0;
         V w = __ldg(&tw[j * st]);
         if (SIGN > 0) w.y = -w.y;
+        if (SEL) {
+#pragma unroll
+            for (int k1 = 0; k1 < R; ++k1) {
+                V o;
+                o.x = __shfl_xor_sync(0xffffffffu, v[k1].x, h);
+                o.y = __shfl_xor_sync(0xffffffffu, v[k1].y, h);
+                v[k1] = up ? csub(o, cmul(w, v[k1])) : cadd(v[k1], cmul(w, o));
+            }
+            st >>= 1;
+            continue;
+        }
+        if (!up) w = CT<V>::make((S)1, (S)0);
+        const S sg = up ? (S)-1 : (S)1;
 #pragma unroll
         for (int k1 = 0; k1 < R; ++k1) {
+            const V x = cmul(w, v[k1]);
             V o;
-            o.x = __shfl_xor_sync(0xffffffffu, v[k1].x, h);
-            o.y = __shfl_xor_sync(0xffffffffu, v[k1].y, h);
-            v[k1] = up ? csub(o, cmul(w, v[k1])) : cadd(v[k1], cmul(w, o));
+            o.x = __shfl_xor_sync(0xffffffffu, x.x, h);
+            o.y = __shfl_xor_sync(0xffffffffu, x.y, h);
+            v[k1] = CT<V>::make(fma(sg, x.x, o.x), fma(sg, x.y, o.y));
         }
         st >>= 1;
     }
@@ -503,7 +543,7 @@ __global__ void __launch_bounds__(256, 2) k_row_nl_w(NlRowArgs a) {
 // products are lane-local, and the r2c (decimation in time from that layout) ends in
 // natural order, where the pair Z[k], Z[N-k] of the real-to-complex split is one shuffle
 // apart.  No shared memory and no block barrier.
-template <int R, class S, class V>
+template <int R, class S, class V, bool SEL = (sizeof(S) == 8)>
 __device__ __forceinline__ void nl_c2r_r(const S* __restrict__ src, bool ikx, int K, int N, int g,
                                          const double* __restrict__ wavx, const V* __restrict__ twr,
                                          const V* __restrict__ tw, V (&v)[R]) {
@@ -526,14 +566,14 @@ __device__ __forceinline__ void nl_c2r_r(const S* __restrict__ src, bool ikx, in
         const V o = cmul(csub(xa, xb), cconj(__ldg(&twr[n])));
         v[rr] = CT<V>::make(e.x - o.y, e.y + o.x);
     }
-    wfft<R, +1>(v, 32, g, tw);
+    wfft<R, +1, SEL>(v, 32, g, tw);
 }
 
 // r2c of a slot-layout row; writes the K stored modes of the row at dst
-template <int R, class S, class V>
+template <int R, class S, class V, bool SEL = (sizeof(S) == 8)>
 __device__ __forceinline__ void nl_r2c_r(V (&v)[R], S* __restrict__ dst, int K, int g, const V* __restrict__ twr,
                                          const V* __restrict__ tw) {
-    wfft_dit<R, -1>(v, 32, g, tw);
+    wfft_dit<R, -1, SEL>(v, 32, g, tw);
     // natural order: lane g register rr holds Z[g + 32 rr]; Z[N-k] for k = g + 32 rr is
     // lane (32-g) register R-1-rr (g > 0), or lane 0 register R-rr (g = 0, rr > 0)
     const int src = (32 - g) & 31;

@@ -61,7 +61,10 @@ const float2* upload_f32(lsb_handle* h, const std::vector<double>& v) {
     return (const float2*)h->upload((const double*)f.data(), (f.size() * sizeof(float) + 7) / 8);
 }
 
-void make_plan(lsb_handle* h, int n, FftPlan& P) {
+// max_g: the widest lane group the warp-group split may use (fewer lanes and more registers
+// per lane mean fewer shuffle stages per element; the register product rows need 32; the
+// spanwise passes use 16, which fills their 16-column tiles in one round of 8 warps)
+void make_plan(lsb_handle* h, int n, FftPlan& P, int max_g = 32) {
     std::vector<int> rad;
     if (!factor(n, rad) || (int)rad.size() > kMaxStages)
         fail(LSB_ERR_UNSUPPORTED, "FFT length " + std::to_string(n) + " is not a product of 2,3,5,7");
@@ -114,13 +117,16 @@ void make_plan(lsb_handle* h, int n, FftPlan& P) {
     }
     if (ls % 2 == 0) ++ls;
     P.ls = ls;
-    // warp-group split: g = largest power of two <= 32 dividing n, r = n / g in {1,2,3,4,6,8}
+    // warp-group split: g = the largest power of two <= max_g dividing n, widened (up to 32)
+    // until r = n / g is in {1,2,3,4,6,8}
     P.g = P.r = P.lgg = 0;
     {
         int gg = 1;
-        while (gg < 32 && n % (gg * 2) == 0) gg *= 2;
+        while (gg < max_g && n % (gg * 2) == 0) gg *= 2;
+        auto ok = [](int r) { return r == 1 || r == 2 || r == 3 || r == 4 || r == 6 || r == 8; };
+        while (!ok(n / gg) && gg < 32 && n % (gg * 2) == 0) gg *= 2;
         const int rr = n / gg;
-        if (rr == 1 || rr == 2 || rr == 3 || rr == 4 || rr == 6 || rr == 8) {
+        if (n % gg == 0 && ok(rr)) {
             P.g = gg;
             P.r = rr;
             int lg = 0;
@@ -130,10 +136,10 @@ void make_plan(lsb_handle* h, int n, FftPlan& P) {
     }
 }
 
-void make_real_plan(lsb_handle* h, int nr, RealPlan& R) {
+void make_real_plan(lsb_handle* h, int nr, RealPlan& R, int max_g = 32) {
     if (nr % 2) fail(LSB_ERR_UNSUPPORTED, "real transform length must be even");
     R.nr = nr;
-    make_plan(h, nr / 2, R.half);
+    make_plan(h, nr / 2, R.half, max_g);
     std::vector<double> tw(2 * (size_t)nr);
     const long double pi = 3.141592653589793238462643383279502884L;
     for (int m = 0; m < nr; ++m) {
@@ -855,8 +861,8 @@ int lsb_create(const lsb_config* cfg, const lsb_setup* su, lsb_handle** out) {
         }
         h->m_ei = make_mat(h.get(), su->ei, nzm, nzm);
         h->m_eext = make_mat(h.get(), su->e, nzm, nzm, 0, nzm, 1, nzp);  // zero ceiling / wall rows
-        make_plan(h.get(), ny, h->py);
-        make_plan(h.get(), d.nyl, h->pyl);
+        make_plan(h.get(), ny, h->py, 16);
+        make_plan(h.get(), d.nyl, h->pyl, 16);
         make_real_plan(h.get(), nx, h->rx);
         make_real_plan(h.get(), d.nxl, h->rxl);
         if (cfg->precision != 0 && cfg->precision != 1) fail(LSB_ERR_ARG, "precision must be 0 (FP64) or 1 (mixed)");
