@@ -8,9 +8,9 @@
 // (src/navierstokes.f90:1411-1476) fused in.
 //
 // tcgen05 has no FP64 kind, so the FP64 form uses the FP64 tensor-core MMA
-// (mma.sync m8n8k4 f64).  One CTA owns all Mp rows of a 64-column block: 8 warps x
-// 8 columns, Mp/8 row tiles per warp, A and B staged through shared memory in
-// k-chunks of 16 with conflict-free strides.
+// (mma.sync m16n8k8 f64: 1024 FMAs per instruction).  One CTA owns all Mp rows of a
+// 64-column block: 8 warps x 8 columns, Mp/16 row tiles per warp, A and B staged through
+// shared memory in k-chunks of 16 with conflict-free strides.
 #include "lsb_internal.cuh"
 
 namespace lsb {
@@ -20,10 +20,14 @@ constexpr int GBK = 16;
 constexpr int LDA_S = 20;  // doubles; 8r mod 32 distinct for r = 0..3 -> no bank conflicts
 constexpr int LDB_S = 68;
 
-__device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-                 : "+d"(c[0]), "+d"(c[1])
-                 : "d"(a), "d"(b));
+// D (16x8) += A (16x8) B (8x8).  Fragments (g = lane / 4, t = lane % 4): a = A[g][t],
+// A[g+8][t], A[g][t+4], A[g+8][t+4]; b = B[t][g], B[t+4][g]; c = D[g][2t], D[g][2t+1],
+// D[g+8][2t], D[g+8][2t+1]
+__device__ __forceinline__ void dmma16(double (&c)[4], double a0, double a1, double a2, double a3, double b0,
+                                       double b1) {
+    asm volatile("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+                 : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+                 : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1));
 }
 
 __device__ __forceinline__ double w2_of(const GemmArgs& g, long long c) {
@@ -44,8 +48,8 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 template <int MT>
 __global__ void __launch_bounds__(256) k_gemm(GemmArgs g) {
     extern __shared__ double gsm[];
-    double (*As)[MT * 8][LDA_S] = reinterpret_cast<double (*)[MT * 8][LDA_S]>(gsm);
-    double (*Bs)[GBK][LDB_S] = reinterpret_cast<double (*)[GBK][LDB_S]>(gsm + 2 * MT * 8 * LDA_S);
+    double (*As)[MT * 16][LDA_S] = reinterpret_cast<double (*)[MT * 16][LDA_S]>(gsm);
+    double (*Bs)[GBK][LDB_S] = reinterpret_cast<double (*)[GBK][LDB_S]>(gsm + 2 * MT * 16 * LDA_S);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int f = blockIdx.y;
     const long long c0 = (long long)blockIdx.x * GBN;
@@ -53,12 +57,12 @@ __global__ void __launch_bounds__(256) k_gemm(GemmArgs g) {
     const double* bcb = g.bcb ? g.bcb + f * g.bc_fstride : nullptr;
     const double* bct = g.bct ? g.bct + f * g.bc_fstride : nullptr;
     const bool lift = (g.epi != 5) && (bcb != nullptr);
-    double acc[MT][2];
+    double acc[MT][4];
 #pragma unroll
-    for (int t = 0; t < MT; ++t) acc[t][0] = acc[t][1] = 0.0;
+    for (int t = 0; t < MT; ++t) acc[t][0] = acc[t][1] = acc[t][2] = acc[t][3] = 0.0;
 
     auto load_chunk = [&](int buf, int kc) {
-        for (int idx = tid; idx < MT * 8 * GBK; idx += 256) {
+        for (int idx = tid; idx < MT * 16 * GBK; idx += 256) {
             const int r = idx / GBK, cc = idx % GBK;
             cp_async8(&As[buf][r][cc], &g.A[(long long)r * g.Kp + kc + cc], 8);
         }
@@ -98,13 +102,18 @@ __global__ void __launch_bounds__(256) k_gemm(GemmArgs g) {
             cp_async_wait<0>();
         }
         __syncthreads();
+        const int gq = lane >> 2, tq = lane & 3;
 #pragma unroll
-        for (int k4 = 0; k4 < GBK / 4; ++k4) {
-            const double b = Bs[buf][k4 * 4 + (lane & 3)][warp * 8 + (lane >> 2)];
+        for (int k8 = 0; k8 < GBK / 8; ++k8) {
+            const double b0 = Bs[buf][k8 * 8 + tq][warp * 8 + gq];
+            const double b1 = Bs[buf][k8 * 8 + tq + 4][warp * 8 + gq];
 #pragma unroll
             for (int t = 0; t < MT; ++t) {
-                const double a = As[buf][t * 8 + (lane >> 2)][k4 * 4 + (lane & 3)];
-                dmma(acc[t], a, b);
+                const double a0 = As[buf][t * 16 + gq][k8 * 8 + tq];
+                const double a1 = As[buf][t * 16 + gq + 8][k8 * 8 + tq];
+                const double a2 = As[buf][t * 16 + gq][k8 * 8 + tq + 4];
+                const double a3 = As[buf][t * 16 + gq + 8][k8 * 8 + tq + 4];
+                dmma16(acc[t], a0, a1, a2, a3, b0, b1);
             }
         }
         __syncthreads();
@@ -113,8 +122,10 @@ __global__ void __launch_bounds__(256) k_gemm(GemmArgs g) {
     double* out = g.out + f * g.out_fstride;
     const double* aux = g.aux ? g.aux + f * g.out_fstride : nullptr;
 #pragma unroll
-    for (int t = 0; t < MT; ++t) {
-        const int r = t * 8 + (lane >> 2);
+    for (int t = 0; t < MT; ++t)
+#pragma unroll
+    for (int hh = 0; hh < 2; ++hh) {
+        const int r = t * 16 + hh * 8 + (lane >> 2);
         if (r >= g.M) continue;
         const long long cb = c0 + warp * 8 + (lane & 3) * 2;
 #pragma unroll
@@ -122,7 +133,7 @@ __global__ void __launch_bounds__(256) k_gemm(GemmArgs g) {
             const long long c = cb + e;
             if (c >= g.C) continue;
             const long long o = (long long)(r + g.roff) * g.C + c;
-            double v = acc[t][e];
+            double v = acc[t][2 * hh + e];
             switch (g.epi) {
                 case EPI_STORE: break;
                 case EPI_AXPBY: v = g.alpha * v + (g.beta != 0.0 ? g.beta * out[o] : 0.0); break;
@@ -154,11 +165,11 @@ __global__ void __launch_bounds__(256) k_gemm(GemmArgs g) {
 
 void launch_gemm(const GemmArgs& g, cudaStream_t s) {
     dim3 grid((unsigned)((g.C + GBN - 1) / GBN), g.nfields);
-    const int mt = g.Mp / 8;
+    const int mt = g.Mp / 16;
     switch (mt) {
 #define LSB_MT(n)                                                                                       \
     case n: {                                                                                           \
-        const size_t sm = (size_t)(2 * n * 8 * LDA_S + 2 * GBK * LDB_S) * sizeof(double);               \
+        const size_t sm = (size_t)(2 * n * 16 * LDA_S + 2 * GBK * LDB_S) * sizeof(double);              \
         static bool attr = false;                                                                       \
         if (!attr) {                                                                                    \
             cudaFuncSetAttribute(k_gemm<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);      \
@@ -168,7 +179,6 @@ void launch_gemm(const GemmArgs& g, cudaStream_t s) {
         break;                                                                                          \
     }
         LSB_MT(1) LSB_MT(2) LSB_MT(3) LSB_MT(4) LSB_MT(5) LSB_MT(6) LSB_MT(7) LSB_MT(8) LSB_MT(9)
-        LSB_MT(10) LSB_MT(11) LSB_MT(12) LSB_MT(13) LSB_MT(14) LSB_MT(15) LSB_MT(16) LSB_MT(17)
 #undef LSB_MT
         default: break;
     }

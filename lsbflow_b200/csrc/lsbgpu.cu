@@ -160,9 +160,9 @@ Mat make_mat(lsb_handle* h, const double* A, int M, int K, int row0 = 0, int nro
     Mat m;
     m.M = total_rows;
     m.K = K;
-    m.Mp = ((total_rows + 7) / 8) * 8;
+    m.Mp = ((total_rows + 15) / 16) * 16;  // m16 row tiles of the FP64 MMA
     m.Kp = ((K + 15) / 16) * 16;
-    if (m.Mp > 136) fail(LSB_ERR_UNSUPPORTED, "nz too large (nzp <= 136 supported)");
+    if (m.Mp > 144) fail(LSB_ERR_UNSUPPORTED, "nz too large (nzp <= 144 supported)");
     std::vector<double> buf((size_t)m.Mp * m.Kp, 0.0);
     for (int r = 0; r < nrows; ++r)
         for (int k = 0; k < K; ++k) buf[(size_t)(r + zero_pad_rows_top) * m.Kp + k] = A[(size_t)(row0 + r) * K + k];
