@@ -15,10 +15,9 @@
 
 namespace lsb {
 
-constexpr int GBN = 64;
 constexpr int GBK = 16;
 constexpr int LDA_S = 20;  // doubles; 8r mod 32 distinct for r = 0..3 -> no bank conflicts
-constexpr int LDB_S = 68;
+// B rows: GBN + 4 doubles (GBN = 8 columns per warp)
 
 // D (16x8) += A (16x8) B (8x8).  Fragments (g = lane / 4, t = lane % 4): a = A[g][t],
 // A[g+8][t], A[g][t+4], A[g+8][t+4]; b = B[t][g], B[t+4][g]; c = D[g][2t], D[g][2t+1],
@@ -31,29 +30,31 @@ __device__ __forceinline__ void dmma16(double (&c)[4], double a0, double a1, dou
 }
 
 __device__ __forceinline__ double w2_of(const GemmArgs& g, long long c) {
-    const int i = (int)(c % g.nx);
-    const int j = (int)(c / g.nx);
+    // c < C = nx * ny < 2^31 (checked at create): 32-bit division
+    const int i = (int)((unsigned)c % (unsigned)g.nx);
+    const int j = (int)((unsigned)c / (unsigned)g.nx);
     const double wx = g.wavx[i], wy = g.wavy[j];
     return wx * wx + wy * wy;
 }
 
-__device__ __forceinline__ void cp_async8(void* smem_ptr, const void* gptr, int src_bytes) {
+__device__ __forceinline__ void cp_async16(void* smem_ptr, const void* gptr, int src_bytes) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(smem_ptr);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gptr), "r"(src_bytes));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gptr), "r"(src_bytes));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
-template <int MT>
-__global__ void __launch_bounds__(256) k_gemm(GemmArgs g) {
+template <int MT, int NW>
+__global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
+    constexpr int NT = NW * 32, GBN = NW * 8, LDB_S = GBN + 4;
     extern __shared__ double gsm[];
     double (*As)[MT * 16][LDA_S] = reinterpret_cast<double (*)[MT * 16][LDA_S]>(gsm);
     double (*Bs)[GBK][LDB_S] = reinterpret_cast<double (*)[GBK][LDB_S]>(gsm + 2 * MT * 16 * LDA_S);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int f = blockIdx.y;
     const long long c0 = (long long)blockIdx.x * GBN;
-    const double* in = g.in + f * g.in_fstride;
+    const double* in = (f < 4 && g.inf[f]) ? g.inf[f] : g.in + f * g.in_fstride;
     const double* bcb = g.bcb ? g.bcb + f * g.bc_fstride : nullptr;
     const double* bct = g.bct ? g.bct + f * g.bc_fstride : nullptr;
     const bool lift = (g.epi != 5) && (bcb != nullptr);
@@ -61,31 +62,45 @@ __global__ void __launch_bounds__(256) k_gemm(GemmArgs g) {
 #pragma unroll
     for (int t = 0; t < MT; ++t) acc[t][0] = acc[t][1] = acc[t][2] = acc[t][3] = 0.0;
 
+    // this thread's column in the lifting prologue is fixed: its per-column factors once
+    const int ln = tid & (GBN - 1);
+    const long long lc = c0 + ln;
+    double lw2 = 0.0, lbcb = 0.0, lbct = 0.0;
+    if (lift && lc < g.C) {
+        lw2 = w2_of(g, lc);
+        lbcb = bcb[lc];
+        lbct = bct[lc];
+    }
+    const double lfac = (-lw2) - g.lift_sigma;
     auto load_chunk = [&](int buf, int kc) {
-        for (int idx = tid; idx < MT * 16 * GBK; idx += 256) {
-            const int r = idx / GBK, cc = idx % GBK;
-            cp_async8(&As[buf][r][cc], &g.A[(long long)r * g.Kp + kc + cc], 8);
+        // A: 16-byte copies (Kp and the chunk start are multiples of 16 doubles)
+        for (int idx = tid; idx < MT * 16 * (GBK / 2); idx += NT) {
+            const int r = idx / (GBK / 2), cp = idx % (GBK / 2);
+            cp_async16(&As[buf][r][2 * cp], &g.A[(long long)r * g.Kp + kc + 2 * cp], 16);
         }
-        for (int idx = tid; idx < GBK * GBN; idx += 256) {
-            const int kk = idx / GBN, n = idx % GBN;
-            const int k = kc + kk;
-            const long long c = c0 + n;
-            const bool ok = (k < g.K && c < g.C);
-            const int kin = k + g.koff;
-            if (!lift) {
-                cp_async8(&Bs[buf][kk][n], ok ? (const void*)&in[(long long)kin * g.C + c] : (const void*)in, ok ? 8 : 0);
-            } else {
+        if (!lift) {
+            // B: 16-byte copies of column pairs (C and the field stride are even)
+            for (int idx = tid; idx < GBK * (GBN / 2); idx += NT) {
+                const int kk = idx / (GBN / 2), n2 = idx % (GBN / 2);
+                const int k = kc + kk;
+                const long long c = c0 + 2 * n2;
+                const bool ok = (k < g.K && c < g.C);
+                cp_async16(&Bs[buf][kk][2 * n2], ok ? (const void*)&in[(long long)(k + g.koff) * g.C + c] : (const void*)in,
+                           ok ? 16 : 0);
+            }
+        } else {
+            for (int kk = tid / GBN; kk < GBK; kk += NT / GBN) {
+                const int k = kc + kk;
                 double v = 0.0;
-                if (ok) {
-                    v = in[(long long)kin * g.C + c];
-                    const double w2 = w2_of(g, c);
-                    const double fac = (-w2) - g.lift_sigma;
-                    const double abot = g.d2hb[kin] + fac * g.hb[kin];
-                    v = v - abot * bcb[c];
-                    const double atop = g.d2ht[kin] + fac * g.ht[kin];
-                    v = v - atop * bct[c];
+                if (k < g.K && lc < g.C) {
+                    const int kin = k + g.koff;
+                    v = in[(long long)kin * g.C + lc];
+                    const double abot = g.d2hb[kin] + lfac * g.hb[kin];
+                    v = v - abot * lbcb;
+                    const double atop = g.d2ht[kin] + lfac * g.ht[kin];
+                    v = v - atop * lbct;
                 }
-                Bs[buf][kk][n] = v;
+                Bs[buf][kk][ln] = v;
             }
         }
         cp_async_commit();
@@ -119,8 +134,15 @@ __global__ void __launch_bounds__(256) k_gemm(GemmArgs g) {
         __syncthreads();
     }
 
-    double* out = g.out + f * g.out_fstride;
+    double* out = (f < 4 && g.outf[f]) ? g.outf[f] : g.out + f * g.out_fstride;
     const double* aux = g.aux ? g.aux + f * g.out_fstride : nullptr;
+    // the two columns this thread writes, and their k^2 for the epilogues that need it
+    double ew2[2] = {0.0, 0.0};
+    if (g.epi == EPI_HELM_SCALE || g.epi == EPI_PRESSURE || g.epi == EPI_POISSON_RHS) {
+        const long long cb = c0 + warp * 8 + (lane & 3) * 2;
+        for (int e = 0; e < 2; ++e)
+            if (cb + e < g.C) ew2[e] = w2_of(g, cb + e);
+    }
 #pragma unroll
     for (int t = 0; t < MT; ++t)
 #pragma unroll
@@ -138,18 +160,18 @@ __global__ void __launch_bounds__(256) k_gemm(GemmArgs g) {
                 case EPI_STORE: break;
                 case EPI_AXPBY: v = g.alpha * v + (g.beta != 0.0 ? g.beta * out[o] : 0.0); break;
                 case EPI_HELM_SCALE: {
-                    const double w2 = w2_of(g, c);
+                    const double w2 = ew2[e];
                     const double dfac = (-w2) - g.sigma;
                     v = v / (g.lam[r] + dfac);
                     break;
                 }
                 case EPI_PRESSURE: {
-                    const double w2 = w2_of(g, c);
+                    const double w2 = ew2[e];
                     v = (w2 == 0.0) ? 0.0 : -(v + aux[o]) / (w2 * g.alpha * g.beta);
                     break;
                 }
                 case EPI_POISSON_RHS: {
-                    const double w2 = w2_of(g, c);
+                    const double w2 = ew2[e];
                     v = -v - w2 * aux[o];
                     break;
                 }
@@ -163,21 +185,26 @@ __global__ void __launch_bounds__(256) k_gemm(GemmArgs g) {
     }
 }
 
-void launch_gemm(const GemmArgs& g, cudaStream_t s) {
+template <int MT, int NW>
+void gemm_launch_t(const GemmArgs& g, cudaStream_t s) {
+    constexpr int GBN = NW * 8;
+    const size_t sm = (size_t)(2 * MT * 16 * LDA_S + 2 * GBK * (GBN + 4)) * sizeof(double);
+    allow_smem((const void*)k_gemm<MT, NW>, sm);
     dim3 grid((unsigned)((g.C + GBN - 1) / GBN), g.nfields);
+    lsb::note_launch();
+    k_gemm<MT, NW><<<grid, NW * 32, sm, s>>>(g);
+}
+
+// single-field launches use 4-warp CTAs over 32 columns, so that they fill the SMs
+void launch_gemm(const GemmArgs& g, cudaStream_t s) {
     const int mt = g.Mp / 16;
+    const bool narrow = g.nfields == 1;
     switch (mt) {
-#define LSB_MT(n)                                                                                       \
-    case n: {                                                                                           \
-        const size_t sm = (size_t)(2 * n * 16 * LDA_S + 2 * GBK * LDB_S) * sizeof(double);              \
-        static bool attr = false;                                                                       \
-        if (!attr) {                                                                                    \
-            cudaFuncSetAttribute(k_gemm<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);      \
-            attr = true;                                                                                \
-        }                                                                                               \
-        { lsb::note_launch(); k_gemm<n><<<grid, 256, sm, s>>>(g); }                                                             \
-        break;                                                                                          \
-    }
+#define LSB_MT(n)                                                  \
+    case n:                                                        \
+        if (narrow) gemm_launch_t<n, 4>(g, s);                     \
+        else gemm_launch_t<n, 8>(g, s);                            \
+        break;
         LSB_MT(1) LSB_MT(2) LSB_MT(3) LSB_MT(4) LSB_MT(5) LSB_MT(6) LSB_MT(7) LSB_MT(8) LSB_MT(9)
 #undef LSB_MT
         default: break;

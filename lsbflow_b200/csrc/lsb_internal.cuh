@@ -181,6 +181,9 @@ struct GemmArgs {
     long long bc_fstride;
     const double* hb; const double* ht; const double* d2hb; const double* d2ht;
     double lift_sigma;
+    // optional per-field pointers (fields that are not a fixed stride apart); used when set
+    const double* inf[4];
+    double* outf[4];
 };
 void launch_gemm(const GemmArgs& g, cudaStream_t s);
 

@@ -428,10 +428,19 @@ void nlterm(lsb_handle* h, const double* uin, double* Nout) {
     nd.C = d.C();
     TimerScope ts(h, "nl_divergence");
     launch_nl_div_xy(nd, h->stream);
+    // N_l -= d h_l3 / dz for the three components in one launch
+    GemmArgs gz = gemm_base(h, h->m_dz1);
     for (int l = 0; l < 3; ++l) {
-        const double* hz = full9 ? h->sgs.H9 + (l * 3 + 2) * S : Hsym(h, l, 2);
-        zgemm(h, h->m_dz1, hz, Nout + l * S, 1, EPI_AXPBY, -1.0, 1.0, nullptr);
+        gz.inf[l] = full9 ? h->sgs.H9 + (l * 3 + 2) * S : Hsym(h, l, 2);
+        gz.outf[l] = Nout + l * S;
     }
+    gz.in = gz.inf[0];
+    gz.out = gz.outf[0];
+    gz.nfields = 3;
+    gz.epi = EPI_AXPBY;
+    gz.alpha = -1.0;
+    gz.beta = 1.0;
+    launch_gemm(gz, h->stream);
 }
 
 void coefficients(lsb_handle* h) {
