@@ -260,6 +260,7 @@ struct DynArgs {
     const double* delta;    // [nzp]
     long long P;
     int nxy;
+    int full9;              // 0: only the 6 components l <= m are written (tau is symmetric)
 };
 
 // The pointwise SGS kernels are templated on the working type T (double for the FP64 form,
@@ -335,7 +336,8 @@ __global__ void k_dyn4(DynArgs a) {  // C clip, nu_sgs, tau = -2 nu S_ij
         if (c > cmax) c = cmax;
         const T nu = c * dl * dl * cp_<T>(a.snorm)[e];
         for (int l = 0; l < 3; ++l)
-            for (int m = 0; m < 3; ++m) wp_<T>(a.tau[3 * l + m])[e] = (T)-2 * nu * cp_<T>(a.sij[sym6(l, m)])[e];
+            for (int m = 0; m < 3; ++m)
+                if (a.full9 || m >= l) wp_<T>(a.tau[3 * l + m])[e] = (T)-2 * nu * cp_<T>(a.sij[sym6(l, m)])[e];
     }
 }
 
@@ -553,9 +555,10 @@ double* fld(double* base, long long i, long long P) {
 }
 
 // tau (9 components, index 3l+m) from physical u_l, g = du_l/dx_m (9), uiuj (9, index 3l+m or sym)
+// full9: write all 9 stress components (the tier-1 tau_sgs); the step only reads l <= m
 template <class T>
 static void model_tau(lsb_handle* h, const double* const* u, const double* const* g, const double* const* uu6,
-                      double* tau) {
+                      double* tau, bool full9 = true) {
     const Dims& d = h->d;
     const lsb_config& c = h->cfg;
     const long long P = h->P;
@@ -591,6 +594,7 @@ static void model_tau(lsb_handle* h, const double* const* u, const double* const
         a.delta = s.delta;
         a.P = P;
         a.nxy = nxy;
+        a.full9 = full9 ? 1 : 0;
         { lsb::note_launch(); k_dyn1<T><<<nblk(P), 256, 0, st>>>(a); }
         F3((const double* const*)a.sij, a.sijhat, 6, c.a, c.b, 0);
         { lsb::note_launch(); k_dyn2<T><<<nblk(P), 256, 0, st>>>(a); }
@@ -681,8 +685,8 @@ void sgs_add_tau(lsb_handle* h, double* const* ph, bool dealias) {
     }
     const double* g[9];
     for (int q = 0; q < 9; ++q) g[q] = ph[3 + q];
-    if (f32) model_tau<float>(h, u3, g, (const double* const*)uu6, s.tau);
-    else model_tau<double>(h, u3, g, (const double* const*)uu6, s.tau);
+    if (f32) model_tau<float>(h, u3, g, (const double* const*)uu6, s.tau, s.nonsym);
+    else model_tau<double>(h, u3, g, (const double* const*)uu6, s.tau, s.nonsym);
     if (!s.nonsym) {
         // symmetric: add T(tau_lm) to h_lm for the 6 independent components
         const double* tp[6];
