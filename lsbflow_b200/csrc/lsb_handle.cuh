@@ -66,6 +66,8 @@ struct lsb_handle {
     double *p = nullptr, *pn = nullptr;                       // S each
     // scratch
     double *filt = nullptr, *dz = nullptr, *H = nullptr, *rhs = nullptr, *T = nullptr, *divf = nullptr;
+    lsb::UmmaMat u_dz1;          // mixed form: split dz1 for the tcgen05 z derivatives
+    int* uerr = nullptr;         // device word raised by a tensor-core kernel whose wait timed out
     double *Y = nullptr;     // 18 y-intermediates on the (padded) transform grid
     double *Yu = nullptr;    // 12 y-intermediates on the unpadded grid
     double *phys = nullptr;  // physical scratch (unpadded grid), kPhys fields

@@ -187,5 +187,15 @@ struct GemmArgs {
 };
 void launch_gemm(const GemmArgs& g, cudaStream_t s);
 
+// mixed form: the z derivative as BF16-split tcgen05 MMAs (umma_kernels.cu)
+struct UmmaMat {
+    const uint16_t* img = nullptr;  // device: the three BF16 splits in the shared-memory image
+    unsigned img_bytes = 0;
+    int M = 0, K = 0, npad = 0, nsteps = 0;
+};
+UmmaMat make_umma_mat(const double* A, int M, int K, std::vector<uint16_t>& img);
+// false when it does not apply (epilogue other than store / axpby, N > 256, limits)
+bool launch_umma_dz(const GemmArgs& g, const UmmaMat& um, int* err, cudaStream_t s);
+
 
 }  // namespace lsb

@@ -334,7 +334,19 @@ void nlterm(lsb_handle* h, const double* uin, double* Nout) {
     const long long S = d.S();
     const bool dealias = h->cfg.dealiasflag == 1;
     // du_l/dz
-    { TimerScope ts(h, "gemm_dz"); zgemm1(h, h->m_dz1, uin, h->dz, 3); }
+    {
+        TimerScope ts(h, "gemm_dz");
+        bool done = false;
+        if (h->cfg.precision == 1) {
+            GemmArgs g = gemm_base(h, h->m_dz1);
+            g.in = uin;
+            g.out = h->dz;
+            g.nfields = 3;
+            g.epi = EPI_STORE;
+            done = launch_umma_dz(g, h->u_dz1, h->uerr, h->stream);
+        }
+        if (!done) zgemm1(h, h->m_dz1, uin, h->dz, 3);
+    }
     // spanwise inverse: u_l, du_l/dy, du_l/dz  -> Y[0..8]
     YInvJobList yj{};
     yj.n = 9;
@@ -440,7 +452,7 @@ void nlterm(lsb_handle* h, const double* uin, double* Nout) {
     gz.epi = EPI_AXPBY;
     gz.alpha = -1.0;
     gz.beta = 1.0;
-    launch_gemm(gz, h->stream);
+    if (!(h->cfg.precision == 1 && launch_umma_dz(gz, h->u_dz1, h->uerr, h->stream))) launch_gemm(gz, h->stream);
 }
 
 void coefficients(lsb_handle* h) {
@@ -703,6 +715,17 @@ void step_one(lsb_handle* h) {
     h->dt2 = dt;
 }
 
+// a tensor-core kernel raises h->uerr when one of its bounded waits ran out
+void check_uerr(lsb_handle* h) {
+    if (!h->uerr) return;
+    int e = 0;
+    CK(cudaMemcpy(&e, h->uerr, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e != 0) {
+        CK(cudaMemset(h->uerr, 0, sizeof(int)));
+        fail(LSB_ERR_CUDA, "tensor-core contraction: a completion wait timed out");
+    }
+}
+
 void check_launch() {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) fail(LSB_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
@@ -859,6 +882,13 @@ int lsb_create(const lsb_config* cfg, const lsb_setup* su, lsb_handle** out) {
         h->lam = h->upload(su->lam, nzm);
         h->lamx = h->upload(su->lamx, nx);
         h->m_dz1 = make_mat(h.get(), su->dz1, nzp, nzp);
+        h->uerr = reinterpret_cast<int*>(h->alloc(1));
+        if (cfg->precision == 1 && nzp <= 256) {
+            std::vector<uint16_t> img;
+            h->u_dz1 = make_umma_mat(su->dz1, nzp, nzp, img);
+            h->u_dz1.img = reinterpret_cast<const uint16_t*>(
+                h->upload(reinterpret_cast<const double*>(img.data()), (img.size() * sizeof(uint16_t) + 7) / 8));
+        }
         h->m_dz2 = make_mat(h.get(), su->dz2, nzp, nzp);
         {
             std::vector<double> rows(2 * (size_t)nzp);
@@ -939,6 +969,7 @@ int lsb_synchronize(lsb_handle* h) {
         if (!h) fail(LSB_ERR_ARG, "null handle");
         CK(cudaStreamSynchronize(h->stream));
         check_launch();
+        check_uerr(h);
     });
 }
 
@@ -991,6 +1022,7 @@ int lsb_download_state(lsb_handle* h, double* uf, double* vf, double* wf, double
         dn(nlnif, h->nln, 3 * B);
         dn(nlnmif, h->nlnm, 3 * B);
         CK(cudaStreamSynchronize(h->stream));
+        check_uerr(h);
         if (t) *t = h->t;
         if (dt) *dt = h->dt;
         if (dt2) *dt2 = h->dt2;
