@@ -8,16 +8,15 @@
 // (src/navierstokes.f90:1411-1476) fused in.
 //
 // tcgen05 has no FP64 kind, so the FP64 form uses the FP64 tensor-core MMA
-// (mma.sync m16n8k8 f64: 1024 FMAs per instruction).  One CTA owns all Mp rows of a
-// 64-column block: 8 warps x 8 columns, Mp/16 row tiles per warp, A and B staged through
-// shared memory in k-chunks of 16 with conflict-free strides.
+// (mma.sync m16n8k8 f64: 1024 FMAs per instruction).  One CTA owns all Mp rows of a block
+// of 32..64 columns (8 per warp), A and B staged through shared memory in k-chunks of 16 with
+// conflict-free strides.
 #include "lsb_internal.cuh"
 
 namespace lsb {
 
 constexpr int GBK = 16;
 constexpr int LDA_S = 20;  // doubles; 8r mod 32 distinct for r = 0..3 -> no bank conflicts
-// B rows: GBN + 4 doubles (GBN = 8 columns per warp)
 
 // D (16x8) += A (16x8) B (8x8).  Fragments (g = lane / 4, t = lane % 4): a = A[g][t],
 // A[g+8][t], A[g][t+4], A[g+8][t+4]; b = B[t][g], B[t+4][g]; c = D[g][2t], D[g][2t+1],
@@ -45,13 +44,22 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
+// CTA tile: all Mp rows x 8 * NW columns; warp w owns columns 8w..8w+7 over all MT row
+// tiles.  A and B chunks arrive by cp.async through a GSTAGES-deep ring with one barrier per
+// chunk; the lifted right-hand side of the non-homogeneous solve is formed from the raw
+// input as the B fragments are read (the lane's column is fixed, the row factors sit in
+// shared memory), so the lifted contractions stream like the plain ones.
+constexpr int GSTAGES = 3;
+
 template <int MT, int NW>
 __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
-    constexpr int NT = NW * 32, GBN = NW * 8, LDB_S = GBN + 4;
+    constexpr int NT = NW * 32, GBN = NW * 8, LDB_S = GBN + 4;  // GBN + 4 = 4 or 12 mod 16: conflict-free
     extern __shared__ double gsm[];
     double (*As)[MT * 16][LDA_S] = reinterpret_cast<double (*)[MT * 16][LDA_S]>(gsm);
-    double (*Bs)[GBK][LDB_S] = reinterpret_cast<double (*)[GBK][LDB_S]>(gsm + 2 * MT * 16 * LDA_S);
+    double (*Bs)[GBK][LDB_S] = reinterpret_cast<double (*)[GBK][LDB_S]>(gsm + GSTAGES * MT * 16 * LDA_S);
+    double* lrow = gsm + GSTAGES * (MT * 16 * LDA_S + GBK * LDB_S);  // [4][Kp]: d2hb, hb, d2ht, ht
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int gq = lane >> 2, tq = lane & 3;
     const int f = blockIdx.y;
     const long long c0 = (long long)blockIdx.x * GBN;
     const double* in = (f < 4 && g.inf[f]) ? g.inf[f] : g.in + f * g.in_fstride;
@@ -62,66 +70,71 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
 #pragma unroll
     for (int t = 0; t < MT; ++t) acc[t][0] = acc[t][1] = acc[t][2] = acc[t][3] = 0.0;
 
-    // this thread's column in the lifting prologue is fixed: its per-column factors once
-    const int ln = tid & (GBN - 1);
-    const long long lc = c0 + ln;
-    double lw2 = 0.0, lbcb = 0.0, lbct = 0.0;
-    if (lift && lc < g.C) {
-        lw2 = w2_of(g, lc);
-        lbcb = bcb[lc];
-        lbct = bct[lc];
+    // lifting: per-column factors of this lane's B column, per-row factors in shared memory
+    // (zero past K, so the padded rows stay zero)
+    const long long lc = c0 + warp * 8 + gq;
+    double lbcb = 0.0, lbct = 0.0, lfac = 0.0;
+    if (lift) {
+        for (int k = tid; k < g.Kp; k += NT) {
+            const bool ok = k < g.K;
+            const int kin = k + g.koff;
+            lrow[k] = ok ? g.d2hb[kin] : 0.0;
+            lrow[g.Kp + k] = ok ? g.hb[kin] : 0.0;
+            lrow[2 * g.Kp + k] = ok ? g.d2ht[kin] : 0.0;
+            lrow[3 * g.Kp + k] = ok ? g.ht[kin] : 0.0;
+        }
+        if (lc < g.C) {
+            lbcb = bcb[lc];
+            lbct = bct[lc];
+            lfac = (-w2_of(g, lc)) - g.lift_sigma;
+        }
     }
-    const double lfac = (-lw2) - g.lift_sigma;
     auto load_chunk = [&](int buf, int kc) {
         // A: 16-byte copies (Kp and the chunk start are multiples of 16 doubles)
         for (int idx = tid; idx < MT * 16 * (GBK / 2); idx += NT) {
             const int r = idx / (GBK / 2), cp = idx % (GBK / 2);
             cp_async16(&As[buf][r][2 * cp], &g.A[(long long)r * g.Kp + kc + 2 * cp], 16);
         }
-        if (!lift) {
-            // B: 16-byte copies of column pairs (C and the field stride are even)
-            for (int idx = tid; idx < GBK * (GBN / 2); idx += NT) {
-                const int kk = idx / (GBN / 2), n2 = idx % (GBN / 2);
-                const int k = kc + kk;
-                const long long c = c0 + 2 * n2;
-                const bool ok = (k < g.K && c < g.C);
-                cp_async16(&Bs[buf][kk][2 * n2], ok ? (const void*)&in[(long long)(k + g.koff) * g.C + c] : (const void*)in,
-                           ok ? 16 : 0);
-            }
-        } else {
-            for (int kk = tid / GBN; kk < GBK; kk += NT / GBN) {
-                const int k = kc + kk;
-                double v = 0.0;
-                if (k < g.K && lc < g.C) {
-                    const int kin = k + g.koff;
-                    v = in[(long long)kin * g.C + lc];
-                    const double abot = g.d2hb[kin] + lfac * g.hb[kin];
-                    v = v - abot * lbcb;
-                    const double atop = g.d2ht[kin] + lfac * g.ht[kin];
-                    v = v - atop * lbct;
-                }
-                Bs[buf][kk][ln] = v;
-            }
+        // B: 16-byte copies of column pairs (C and the field stride are even)
+        for (int idx = tid; idx < GBK * (GBN / 2); idx += NT) {
+            const int kk = idx / (GBN / 2), n2 = idx % (GBN / 2);
+            const int k = kc + kk;
+            const long long c = c0 + 2 * n2;
+            const bool ok = (k < g.K && c < g.C);
+            cp_async16(&Bs[buf][kk][2 * n2], ok ? (const void*)&in[(long long)(k + g.koff) * g.C + c] : (const void*)in,
+                       ok ? 16 : 0);
         }
-        cp_async_commit();
+    };
+    // B value of row k (chunk-relative kk) for this lane's column: raw, or lifted
+    auto bval = [&](int buf, int kk, int k) {
+        double v = Bs[buf][kk][warp * 8 + gq];
+        if (lift) {
+            const double abot = lrow[k] + lfac * lrow[g.Kp + k];
+            v = v - abot * lbcb;
+            const double atop = lrow[2 * g.Kp + k] + lfac * lrow[3 * g.Kp + k];
+            v = v - atop * lbct;
+        }
+        return v;
     };
 
     const int nchunks = g.Kp / GBK;
-    load_chunk(0, 0);
+#pragma unroll
+    for (int st = 0; st < GSTAGES - 1; ++st) {
+        if (st < nchunks) load_chunk(st, st * GBK);
+        cp_async_commit();
+    }
     for (int ch = 0; ch < nchunks; ++ch) {
-        const int buf = ch & 1;
-        if (ch + 1 < nchunks) {
-            load_chunk(buf ^ 1, (ch + 1) * GBK);
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
-        }
+        const int buf = ch % GSTAGES;
+        cp_async_wait<GSTAGES - 2>();
         __syncthreads();
-        const int gq = lane >> 2, tq = lane & 3;
+        // the ring slot refilled here was read in iteration ch - 1, before the barrier
+        if (ch + GSTAGES - 1 < nchunks) load_chunk((ch + GSTAGES - 1) % GSTAGES, (ch + GSTAGES - 1) * GBK);
+        cp_async_commit();
 #pragma unroll
         for (int k8 = 0; k8 < GBK / 8; ++k8) {
-            const double b0 = Bs[buf][k8 * 8 + tq][warp * 8 + gq];
-            const double b1 = Bs[buf][k8 * 8 + tq + 4][warp * 8 + gq];
+            const int kk = k8 * 8 + tq;
+            const double b0 = bval(buf, kk, ch * GBK + kk);
+            const double b1 = bval(buf, kk + 4, ch * GBK + kk + 4);
 #pragma unroll
             for (int t = 0; t < MT; ++t) {
                 const double a0 = As[buf][t * 16 + gq][k8 * 8 + tq];
@@ -131,15 +144,15 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
                 dmma16(acc[t], a0, a1, a2, a3, b0, b1);
             }
         }
-        __syncthreads();
     }
+    cp_async_wait<0>();
 
     double* out = (f < 4 && g.outf[f]) ? g.outf[f] : g.out + f * g.out_fstride;
     const double* aux = g.aux ? g.aux + f * g.out_fstride : nullptr;
+    const long long cb = c0 + warp * 8 + tq * 2;
     // the two columns this thread writes, and their k^2 for the epilogues that need it
     double ew2[2] = {0.0, 0.0};
     if (g.epi == EPI_HELM_SCALE || g.epi == EPI_PRESSURE || g.epi == EPI_POISSON_RHS) {
-        const long long cb = c0 + warp * 8 + (lane & 3) * 2;
         for (int e = 0; e < 2; ++e)
             if (cb + e < g.C) ew2[e] = w2_of(g, cb + e);
     }
@@ -147,9 +160,8 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
     for (int t = 0; t < MT; ++t)
 #pragma unroll
     for (int hh = 0; hh < 2; ++hh) {
-        const int r = t * 16 + hh * 8 + (lane >> 2);
+        const int r = t * 16 + hh * 8 + gq;
         if (r >= g.M) continue;
-        const long long cb = c0 + warp * 8 + (lane & 3) * 2;
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
             const long long c = cb + e;
@@ -160,8 +172,7 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
                 case EPI_STORE: break;
                 case EPI_AXPBY: v = g.alpha * v + (g.beta != 0.0 ? g.beta * out[o] : 0.0); break;
                 case EPI_HELM_SCALE: {
-                    const double w2 = ew2[e];
-                    const double dfac = (-w2) - g.sigma;
+                    const double dfac = (-ew2[e]) - g.sigma;
                     v = v / (g.lam[r] + dfac);
                     break;
                 }
@@ -171,8 +182,7 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
                     break;
                 }
                 case EPI_POISSON_RHS: {
-                    const double w2 = ew2[e];
-                    v = -v - w2 * aux[o];
+                    v = -v - ew2[e] * aux[o];
                     break;
                 }
                 default: {  // EPI_LIFT_ADD (5): acc + hb*bcb + ht*bct
@@ -186,25 +196,54 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
 }
 
 template <int MT, int NW>
+size_t gemm_smem(int Kp) {
+    return (size_t)(GSTAGES * (MT * 16 * LDA_S + GBK * (NW * 8 + 4)) + 4 * Kp) * sizeof(double);
+}
+
+template <int MT, int NW>
 void gemm_launch_t(const GemmArgs& g, cudaStream_t s) {
-    constexpr int GBN = NW * 8;
-    const size_t sm = (size_t)(2 * MT * 16 * LDA_S + 2 * GBK * (GBN + 4)) * sizeof(double);
+    const size_t sm = gemm_smem<MT, NW>(g.Kp);
     allow_smem((const void*)k_gemm<MT, NW>, sm);
-    dim3 grid((unsigned)((g.C + GBN - 1) / GBN), g.nfields);
+    dim3 grid((unsigned)((g.C + NW * 8 - 1) / (NW * 8)), g.nfields);
     lsb::note_launch();
     k_gemm<MT, NW><<<grid, NW * 32, sm, s>>>(g);
 }
 
-// single-field launches use 4-warp CTAs over 32 columns, so that they fill the SMs
+// fraction of the last wave's slots that are busy, averaged over the waves
+template <int MT, int NW>
+double gemm_wave_eff(const GemmArgs& g) {
+    const long long tiles = (g.C + NW * 8 - 1) / (NW * 8) * g.nfields;
+    const long long slots = (long long)resident_blocks((const void*)k_gemm<MT, NW>, NW * 32, gemm_smem<MT, NW>(g.Kp)) * sm_count();
+    if (slots <= 0) return 0.0;
+    const long long waves = (tiles + slots - 1) / slots;
+    return (double)tiles / (double)(waves * slots);
+}
+
+// 4..8 warps (32..64 columns) per CTA, whichever leaves the least idle in the last wave
+// (ties to the wider CTA, which re-reads the matrix less)
+template <int MT>
+void gemm_pick(const GemmArgs& g, cudaStream_t s) {
+    const double e8 = gemm_wave_eff<MT, 8>(g), e7 = gemm_wave_eff<MT, 7>(g), e6 = gemm_wave_eff<MT, 6>(g),
+                 e5 = gemm_wave_eff<MT, 5>(g), e4 = gemm_wave_eff<MT, 4>(g);
+    double best = e8;
+    int nw = 8;
+    if (e7 > best + 0.02) best = e7, nw = 7;
+    if (e6 > best + 0.02) best = e6, nw = 6;
+    if (e5 > best + 0.02) best = e5, nw = 5;
+    if (e4 > best + 0.02) best = e4, nw = 4;
+    switch (nw) {
+        case 8: gemm_launch_t<MT, 8>(g, s); break;
+        case 7: gemm_launch_t<MT, 7>(g, s); break;
+        case 6: gemm_launch_t<MT, 6>(g, s); break;
+        case 5: gemm_launch_t<MT, 5>(g, s); break;
+        default: gemm_launch_t<MT, 4>(g, s); break;
+    }
+}
+
 void launch_gemm(const GemmArgs& g, cudaStream_t s) {
-    const int mt = g.Mp / 16;
-    const bool narrow = g.nfields == 1;
-    switch (mt) {
-#define LSB_MT(n)                                                  \
-    case n:                                                        \
-        if (narrow) gemm_launch_t<n, 4>(g, s);                     \
-        else gemm_launch_t<n, 8>(g, s);                            \
-        break;
+    switch (g.Mp / 16) {
+#define LSB_MT(n) \
+    case n: gemm_pick<n>(g, s); break;
         LSB_MT(1) LSB_MT(2) LSB_MT(3) LSB_MT(4) LSB_MT(5) LSB_MT(6) LSB_MT(7) LSB_MT(8) LSB_MT(9)
 #undef LSB_MT
         default: break;
