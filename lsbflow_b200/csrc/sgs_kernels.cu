@@ -31,9 +31,10 @@ inline int nblk(long long n) {
     return (int)b;
 }
 
+constexpr int kFilterFields = 24;  // fields per filter launch
 struct FieldList {
-    const double* in[9];
-    double* out[9];
+    const double* in[kFilterFields];
+    double* out[kFilterFields];
     int n;
 };
 struct P9 {
@@ -204,9 +205,9 @@ void filter3_any(lsb_handle* h, const void* const* in, void* const* out, int n, 
     while ((1 << lgx) < d.nx) ++lgx;
     const bool rowtile = d.nx <= RT_NX && d.nx >= 4 && (1 << lgx) == d.nx;
     if (!rowtile && f32) sfail(LSB_ERR_UNSUPPORTED, "mixed precision: the SGS filter needs nx a power of two, 4..512");
-    for (int f0 = 0; f0 < n; f0 += 9) {
+    for (int f0 = 0; f0 < n; f0 += kFilterFields) {
         FieldList fl{};
-        fl.n = std::min(9, n - f0);
+        fl.n = std::min(kFilterFields, n - f0);
         for (int i = 0; i < fl.n; ++i) {
             fl.in[i] = reinterpret_cast<const double*>(in[f0 + i]);
             fl.out[i] = reinterpret_cast<double*>(out[f0 + i]);
@@ -251,7 +252,6 @@ struct DynArgs {
     double* mij[6];
     const double* uihat[3];
     double* lf[6];          // filtered u_i u_j
-    double* snorm;
     double* numc;
     double* denomc;
     const double* ctot;
@@ -268,39 +268,34 @@ struct DynArgs {
 template <class T> __device__ __forceinline__ const T* cp_(const double* p) { return reinterpret_cast<const T*>(p); }
 template <class T> __device__ __forceinline__ T* wp_(double* p) { return reinterpret_cast<T*>(p); }
 
+// products rounded one at a time, so that no multiply-add contraction changes them
+__device__ __forceinline__ double mul_rn(double x, double y) { return __dmul_rn(x, y); }
+__device__ __forceinline__ float mul_rn(float x, float y) { return __fmul_rn(x, y); }
+
+// |S| = sqrt(2 S_ij S_ij) from the six independent components
 template <class T>
-__global__ void k_dyn1(DynArgs a) {  // S_ij, |S|
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < a.P; e += (long long)gridDim.x * blockDim.x) {
-        T s6[6];
-        for (int l = 0; l < 3; ++l)
-            for (int m = l; m < 3; ++m) s6[sym6(l, m)] = (T)0.5 * (cp_<T>(a.g[3 * l + m])[e] + cp_<T>(a.g[3 * m + l])[e]);
-        T sn = (T)0;
-        for (int m = 0; m < 3; ++m)
-            for (int l = 0; l < 3; ++l) {
-                const T v = s6[sym6(l, m)];
-                sn = sn + (T)2 * v * v;
-            }
-        for (int q = 0; q < 6; ++q) wp_<T>(a.sij[q])[e] = s6[q];
-        wp_<T>(a.snorm)[e] = sqrt(sn);
-    }
+__device__ __forceinline__ T snorm6(const T (&s6)[6]) {
+    T sn = (T)0;
+    for (int m = 0; m < 3; ++m)
+        for (int l = 0; l < 3; ++l) {
+            const T v = s6[sym6(l, m)];
+            sn = sn + (T)2 * v * v;
+        }
+    return sqrt(sn);
 }
 
 template <class T>
-__global__ void k_dyn2(DynArgs a) {  // |[S]|, L' = delta^2 |S| S_ij, [delta]^2 |[S]| [S_ij]
+__global__ void k_dyn1(DynArgs a) {  // S_ij and L'_ij = delta^2 |S| S_ij
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < a.P; e += (long long)gridDim.x * blockDim.x) {
         const int k = (int)((unsigned)e / (unsigned)a.nxy);  // P < 2^31 (checked at create)
-        const T dl = (T)a.delta[k], cd = (T)2 * dl;
-        T sh = (T)0;
-        for (int m = 0; m < 3; ++m)
-            for (int l = 0; l < 3; ++l) {
-                const T v = cp_<T>(a.sijhat[sym6(l, m)])[e];
-                sh = sh + (T)2 * v * v;
-            }
-        sh = sqrt(sh);
-        const T sn = cp_<T>(a.snorm)[e];
+        const T dl = (T)a.delta[k];
+        T s6[6];
+        for (int l = 0; l < 3; ++l)
+            for (int m = l; m < 3; ++m) s6[sym6(l, m)] = (T)0.5 * (cp_<T>(a.g[3 * l + m])[e] + cp_<T>(a.g[3 * m + l])[e]);
+        const T sn = snorm6<T>(s6);
         for (int q = 0; q < 6; ++q) {
-            wp_<T>(a.lij[q])[e] = dl * dl * sn * cp_<T>(a.sij[q])[e];
-            wp_<T>(a.sijhat[q])[e] = cd * cd * sh * cp_<T>(a.sijhat[q])[e];
+            wp_<T>(a.sij[q])[e] = s6[q];
+            wp_<T>(a.lij[q])[e] = mul_rn(mul_rn(mul_rn(dl, dl), sn), s6[q]);
         }
     }
 }
@@ -308,8 +303,15 @@ __global__ void k_dyn2(DynArgs a) {  // |[S]|, L' = delta^2 |S| S_ij, [delta]^2 
 template <class T>
 __global__ void k_dyn3(DynArgs a) {  // M_ij, L_ij, <M L>, <M M> integrands
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < a.P; e += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)((unsigned)e / (unsigned)a.nxy);
+        const T cd = (T)2 * (T)a.delta[k];
+        T sh6[6];
+        for (int q = 0; q < 6; ++q) sh6[q] = cp_<T>(a.sijhat[q])[e];
+        const T sh = snorm6<T>(sh6);  // |[S]|
+        const T f = mul_rn(mul_rn(cd, cd), sh);
         T m6[6], l6[6];
-        for (int q = 0; q < 6; ++q) m6[q] = (T)2 * (cp_<T>(a.mij[q])[e] - cp_<T>(a.sijhat[q])[e]);
+        // M_ij = 2 ([delta^2 |S| S_ij] - [delta]^2 |[S]| [S_ij])
+        for (int q = 0; q < 6; ++q) m6[q] = (T)2 * (cp_<T>(a.mij[q])[e] - mul_rn(f, sh6[q]));
         for (int l = 0; l < 3; ++l)
             for (int m = l; m < 3; ++m)
                 l6[sym6(l, m)] = cp_<T>(a.lf[sym6(l, m)])[e] - cp_<T>(a.uihat[l])[e] * cp_<T>(a.uihat[m])[e];
@@ -331,13 +333,15 @@ __global__ void k_dyn4(DynArgs a) {  // C clip, nu_sgs, tau = -2 nu S_ij
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < a.P; e += (long long)gridDim.x * blockDim.x) {
         const int k = (int)((unsigned)e / (unsigned)a.nxy);  // P < 2^31 (checked at create)
         const T dl = (T)a.delta[k];
+        T s6[6];
+        for (int q = 0; q < 6; ++q) s6[q] = cp_<T>(a.sij[q])[e];
         T c = cp_<T>(a.ctot)[e] / cp_<T>(a.cdd)[e];
         if (c < (T)0 || isnan(c)) c = (T)0;
         if (c > cmax) c = cmax;
-        const T nu = c * dl * dl * cp_<T>(a.snorm)[e];
+        const T nu = c * dl * dl * snorm6<T>(s6);
         for (int l = 0; l < 3; ++l)
             for (int m = 0; m < 3; ++m)
-                if (a.full9 || m >= l) wp_<T>(a.tau[3 * l + m])[e] = (T)-2 * nu * cp_<T>(a.sij[sym6(l, m)])[e];
+                if (a.full9 || m >= l) wp_<T>(a.tau[3 * l + m])[e] = (T)-2 * nu * s6[sym6(l, m)];
     }
 }
 
@@ -585,7 +589,6 @@ static void model_tau(lsb_handle* h, const double* const* u, const double* const
             a.lf[q] = W(24 + q);
         }
         for (int l = 0; l < 3; ++l) a.uihat[l] = W(30 + l);
-        a.snorm = W(33);
         a.numc = W(34);
         a.denomc = W(35);
         a.ctot = W(36);
@@ -596,12 +599,23 @@ static void model_tau(lsb_handle* h, const double* const* u, const double* const
         a.nxy = nxy;
         a.full9 = full9 ? 1 : 0;
         { lsb::note_launch(); k_dyn1<T><<<nblk(P), 256, 0, st>>>(a); }
-        F3((const double* const*)a.sij, a.sijhat, 6, c.a, c.b, 0);
-        { lsb::note_launch(); k_dyn2<T><<<nblk(P), 256, 0, st>>>(a); }
-        F3((const double* const*)a.lij, a.mij, 6, c.a, c.b, 0);
-        double* uh[3] = {W(30), W(31), W(32)};
-        F3(u, uh, 3, c.a, c.b, 0);
-        F3(uu6, a.lf, 6, c.a, c.b, 0);
+        {  // one launch: [S_ij], [delta^2 |S| S_ij], [u_i], [u_i u_j]
+            const double* fin[21];
+            double* fout[21];
+            for (int q = 0; q < 6; ++q) {
+                fin[q] = a.sij[q];
+                fout[q] = a.sijhat[q];
+                fin[6 + q] = a.lij[q];
+                fout[6 + q] = a.mij[q];
+                fin[15 + q] = uu6[q];
+                fout[15 + q] = a.lf[q];
+            }
+            for (int l = 0; l < 3; ++l) {
+                fin[12 + l] = u[l];
+                fout[12 + l] = W(30 + l);
+            }
+            F3(fin, fout, 21, c.a, c.b, 0);
+        }
         { lsb::note_launch(); k_dyn3<T><<<nblk(P), 256, 0, st>>>(a); }
         const double* nd[2] = {a.numc, a.denomc};
         double* cc[2] = {W(36), W(37)};
