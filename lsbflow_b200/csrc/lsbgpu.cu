@@ -304,13 +304,21 @@ void spec_to_phys(lsb_handle* h, const double* const* spec, double* const* phys,
         const int n = std::min(kMaxJobs, nf - f0);
         YInvJobList yj{};
         RowJobList rj{};
-        yj.n = rj.n = n;
+        yj.n = 0;
+        rj.n = n;
         for (int i = 0; i < n; ++i) {
-            double* y = h->Yu + (long long)i * h->Yu1;
             const int mode = modes ? modes[f0 + i] : YM_COPY;
-            yj.j[i] = YInvJob{spec[f0 + i], y, mode == YM_IKY ? YM_IKY : YM_COPY};
+            const int ymode = mode == YM_IKY ? YM_IKY : YM_COPY;
+            // u and du/dx share one spanwise transform (ikx is applied in the row pass)
+            int yi = -1;
+            for (int j = 0; j < yj.n; ++j)
+                if (yj.j[j].in == spec[f0 + i] && yj.j[j].mode == ymode) yi = j;
+            if (yi < 0) {
+                yi = yj.n++;
+                yj.j[yi] = YInvJob{spec[f0 + i], h->Yu + (long long)yi * h->Yu1, ymode};
+            }
             const double* mean = means ? means[f0 + i] : nullptr;
-            rj.j[i] = RowIO{y, phys[f0 + i], mode == YM_IKX ? YM_IKX : YM_COPY, mean ? 1.0 : 0.0, mean, scale};
+            rj.j[i] = RowIO{yj.j[yi].out, phys[f0 + i], mode == YM_IKX ? YM_IKX : YM_COPY, mean ? 1.0 : 0.0, mean, scale};
         }
         RowArgs ra = rowargs(h, false, nzp);
         YPassArgs ya = ypass(h, false, nzp);
