@@ -132,6 +132,11 @@ int lsb_timers(lsb_handle* h, int enable);
  * reset = 1 zeroes them afterwards as main.f90:104-106 does after writing qavg files */
 int lsb_tavg(lsb_handle* h, double* uf, double* vf, double* wf, double* pf, int reset);
 int lsb_timer_report(lsb_handle* h, char* buf, int buflen);
+/* spanwise mean of u + ubar, v, w, p over y (run/spanwiseavg.m:1-7, the reference's
+ * post-processing of q snapshots, here on the device from the current state) and the rms
+ * about it, sqrt(mean_y (f - mean_y f)^2); mean and rms are host arrays [4][nzp][nx]
+ * (field u, v, w, p; z; x) */
+int lsb_spanwise_stats(lsb_handle* h, double* mean, double* rms);
 
 /* ---------------- Tier 1: the reference's subroutine interfaces (host arrays) --------- */
 /* horfft(ain, ainf, is)             src/horfft.f90:61      is = -1 phys->spec, +1 spec->phys */

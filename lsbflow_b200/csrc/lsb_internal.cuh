@@ -186,6 +186,8 @@ struct GemmArgs {
     double* outf[4];
 };
 void launch_gemm(const GemmArgs& g, cudaStream_t s);
+void launch_spanwise_stats(const double* ph, double* mean, double* rms, int nf, int nx, int ny, int nzp, long long P,
+                           cudaStream_t s);
 
 // mixed form: the z derivative as BF16-split tcgen05 MMAs (umma_kernels.cu)
 struct UmmaMat {

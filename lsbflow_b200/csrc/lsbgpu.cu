@@ -1311,6 +1311,28 @@ int lsb_tavg(lsb_handle* h, double* uf, double* vf, double* wf, double* pf, int 
     });
 }
 
+int lsb_spanwise_stats(lsb_handle* h, double* mean, double* rms) {
+    return guard([&] {
+        if (!h) fail(LSB_ERR_ARG, "null handle");
+        if (!mean || !rms) fail(LSB_ERR_ARG, "null output");
+        const Dims& d = h->d;
+        const long long S = d.S(), P = h->P, n = 4LL * d.nzp * d.nx;
+        // u + ubar, v, w, p on the physical grid in the first four scratch fields (FP64 in
+        // both precisions), the profiles after them
+        double* ph[4] = {h->phys, h->phys + P, h->phys + 2 * P, h->phys + 3 * P};
+        const double* spec[4] = {h->vel, h->vel + S, h->vel + 2 * S, h->p};
+        const double* means[4] = {h->ubar, nullptr, nullptr, nullptr};
+        spec_to_phys(h, spec, ph, 4, d.nzp, means, nullptr, false);
+        double* dm = h->phys + 4 * P;
+        double* dr = dm + n;
+        launch_spanwise_stats(h->phys, dm, dr, 4, d.nx, d.ny, d.nzp, P, h->stream);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(mean, dm, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(rms, dr, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    });
+}
+
 int lsb_timers(lsb_handle* h, int enable) {
     return guard([&] {
         if (!h) fail(LSB_ERR_ARG, "null handle");

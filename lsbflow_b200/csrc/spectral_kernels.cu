@@ -249,6 +249,29 @@ __global__ void k_axpby(double* __restrict__ y, const double* __restrict__ x, do
         y[e] = a * x[e] + (b != 0.0 ? b * y[e] : 0.0);
 }
 
+// spanwise mean and rms over y of nf physical fields [nzp][ny][nx] -> [nf][nzp][nx] each;
+// one thread per (field, z, x), consecutive x coalesced; rms about the mean (two passes)
+__global__ void k_spanwise_stats(const double* __restrict__ ph, double* __restrict__ mean, double* __restrict__ rms,
+                                 int nf, int nx, int ny, int nzp, long long P) {
+    const long long n = (long long)nf * nzp * nx;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(e % nx);
+        const long long fz = e / nx;
+        const int z = (int)(fz % nzp), f = (int)(fz / nzp);
+        const double* col = ph + f * P + (long long)z * ny * nx + x;
+        double s = 0.0;
+        for (int y = 0; y < ny; ++y) s += col[(long long)y * nx];
+        const double m = s / ny;
+        double s2 = 0.0;
+        for (int y = 0; y < ny; ++y) {
+            const double d = col[(long long)y * nx] - m;
+            s2 += d * d;
+        }
+        mean[e] = m;
+        rms[e] = sqrt(s2 / ny);
+    }
+}
+
 // ---------------------------------------------------------------- launchers
 static inline int nblk(long long n) {
     long long b = (n + 255) / 256;
@@ -317,6 +340,12 @@ void launch_tavg_add(double* a, const double* q, double iomod, long long n, cuda
 }
 void launch_axpby(double* y, const double* x, double a, double b, long long n, cudaStream_t s) {
     { lsb::note_launch(); k_axpby<<<nblk(n), 256, 0, s>>>(y, x, a, b, n); }
+}
+
+void launch_spanwise_stats(const double* ph, double* mean, double* rms, int nf, int nx, int ny, int nzp, long long P,
+                           cudaStream_t s) {
+    lsb::note_launch();
+    k_spanwise_stats<<<nblk((long long)nf * nzp * nx), 256, 0, s>>>(ph, mean, rms, nf, nx, ny, nzp, P);
 }
 
 }  // namespace lsb

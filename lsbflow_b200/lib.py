@@ -27,7 +27,7 @@ EXPORTS = [
     "lsb_synchronize", "lsb_horfft", "lsb_dealias_product", "lsb_dfdx", "lsb_dfdy", "lsb_dfdz", "lsb_d2fdz2",
     "lsb_lapl", "lsb_divuv", "lsb_solve_helmholtz", "lsb_solve_nhom_helmholtz", "lsb_nlterm", "lsb_tau_sgs",
     "lsb_upload_velocity", "lsb_download_velocity", "lsb_timers", "lsb_timer_report",
-    "lsb_solve_helmholtz_noalloc", "lsb_tavg", "lsb_kernel_launches", "lsb_device_bytes",
+    "lsb_solve_helmholtz_noalloc", "lsb_tavg", "lsb_spanwise_stats", "lsb_kernel_launches", "lsb_device_bytes",
 ]
 
 
@@ -238,6 +238,14 @@ class Solver:
         out = [np.empty(sh) for _ in range(4)]
         _ck(self._lib.lsb_tavg(self._h, *[_ptr(a) for a in out], C.c_int(1 if reset else 0)))
         return out
+
+    def spanwise_stats(self):
+        """Spanwise (y) mean and rms of u + ubar, v, w, p: two arrays (4, nzp, nx)."""
+        c = self.st.cfg
+        mean = np.empty((4, c.nzp, c.nx))
+        rms = np.empty((4, c.nzp, c.nx))
+        _ck(self._lib.lsb_spanwise_stats(self._h, _ptr(mean), _ptr(rms)))
+        return mean, rms
 
     def timers(self, enable: bool):
         _ck(self._lib.lsb_timers(self._h, C.c_int(1 if enable else 0)))

@@ -866,6 +866,17 @@ def divcheck(st: Setup, uf, vf, wf):
     return np.sum(np.abs(p[..., : c.nx])) / (c.nx * c.ny * c.nzp)
 
 
+def spanwise_stats(st: Setup, uf, vf, wf, pf):
+    """Spanwise mean (run/spanwiseavg.m:1-7: sum over y / ny, per (x, z)) of u + ubar, v, w,
+    p on the physical grid, and the rms about it; two arrays (4, nzp, nx)."""
+    c = st.cfg
+    ph = [horfft_inv(f, c.nx, c.ny)[..., : c.nx] for f in (uf, vf, wf, pf)]
+    ph[0] = ph[0] + st.ubar[:, None, None]
+    mean = np.stack([np.sum(f, axis=1) / float(c.ny) for f in ph])
+    rms = np.stack([np.sqrt(np.sum((f - m[:, None, :]) ** 2, axis=1) / float(c.ny)) for f, m in zip(ph, mean)])
+    return mean, rms
+
+
 def ener(st: Setup, uf, vf, wf, itot: int):
     """ener (src/orrsomm.f90:625-666)."""
     c = st.cfg

@@ -267,6 +267,26 @@ def test_diag_divergence_and_energy():
     assert d["nonfinite"] == 0
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_spanwise_stats(precision):
+    # the profiles are FP64 on the device in both forms: only the state differs
+    cfg = workload("dns64", nx=128, ny=16, nz=32, dealiasflag=1, precision=precision)
+    st, s = solver(cfg)
+    u, v, w = ic.seeded_noise(st, 7, 1e-2)
+    p = rand_spec(st, 8)
+    s.upload(u, v, w, pf=p, dt=st.dt)
+    s.step(3)
+    got = s.download()
+    mean, rms = s.spanwise_stats()
+    rm, rr = O.spanwise_stats(st, got["uf"], got["vf"], got["wf"], got["pf"])
+    assert mean.shape == rm.shape == (4, cfg.nzp, cfg.nx)
+    for k in range(4):
+        assert rel(mean[k], rm[k]) < TOL_OP, k
+        assert rel(rms[k], rr[k]) < 1e-11, k
+    # u carries the mean flow, the others average to small values
+    assert np.abs(mean[0]).max() > 0.5
+
+
 # ------------------------------------------------------------------ main-loop features
 def run_main(cfg, nsteps, u=None, v=None, w=None, seed=3, amp=1e-3, dt=None):
     st, s = solver(cfg)
