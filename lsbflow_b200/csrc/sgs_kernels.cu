@@ -110,11 +110,11 @@ __global__ void __launch_bounds__(256) k_filter3(FieldList fl, int nx, int ny, i
 }
 
 // Row-tile version of the same filter (nx a power of two, 4..512): a block owns FJ
-// full x rows (FJ * nx <= 2048) and marches a chunk of zch planes.  Each plane with its
+// full x rows (FJ * nx = 2048) and marches a chunk of zch planes.  Each plane with its
 // periodic y halo rows is copied into shared memory by cp.async, three planes deep, so
 // two planes are in flight while one is filtered; the x halo is the row itself (periodic).
 // The only re-reads are the two y halo rows and the two z halo planes of the chunk.
-constexpr int RT_MAX = 2048, RT_NX = 512, RT_ST = 3;
+constexpr int RT_NX = 512, RT_ST = 3;
 
 __device__ __forceinline__ void cpa16s(void* sdst, const void* gsrc) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
@@ -124,15 +124,24 @@ __device__ __forceinline__ void cpa_commit_s() { asm volatile("cp.async.commit_g
 template <int N>
 __device__ __forceinline__ void cpa_wait_s() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
+template <class T> struct Vec2;
+template <> struct Vec2<double> { using type = double2; };
+template <> struct Vec2<float> { using type = float2; };
+
+// Thread -> an x pair (2p, 2p+1) and FR consecutive output rows of the block's FJ rows
+// (FJ = FR * 512 / nx), so the x filter reads one vector and two neighbours per row straight
+// from the plane tile and the y and z filters run in registers: one barrier per plane.
+constexpr int FR = 4;
+
 template <class T>
 __global__ void __launch_bounds__(256, 2) k_filter3p(FieldList fl, int lgx, int ny, int nzp, int FJ, int zch, T a, T b,
                                                      const double* __restrict__ az, const double* __restrict__ bz,
                                                      const double* __restrict__ cz) {
-    const int nx = 1 << lgx;
+    using V2 = typename Vec2<T>::type;
+    const int nx = 1 << lgx, NP = nx >> 1;
     extern __shared__ __align__(16) unsigned char fsm_raw[];
     const int tsz = (FJ + 2) * nx;
     T* tiles = reinterpret_cast<T*>(fsm_raw);  // RT_ST tiles of (FJ + 2) rows
-    T* X = tiles + RT_ST * tsz;                // x-filtered rows
     const int f = blockIdx.z, zc = blockIdx.y;
     const T* q = reinterpret_cast<const T*>(fl.in[f]);
     T* out = reinterpret_cast<T*>(fl.out[f]);
@@ -142,6 +151,8 @@ __global__ void __launch_bounds__(256, 2) k_filter3p(FieldList fl, int lgx, int 
     const int ks = max(0, k0 - 1), ke = min(nzp - 1, k1);
     const T rs = (T)(1.0 / (2.0 * (double)a + (double)b));
     const int tid = threadIdx.x;
+    const int p = tid & (NP - 1), r0 = (tid >> (lgx - 1)) * FR;
+    const int xl = (2 * p - 1) & (nx - 1), xr = (2 * p + 2) & (nx - 1);
     constexpr int V = 16 / sizeof(T);          // elements per 16-byte copy
     constexpr int LGV = (V == 2) ? 1 : 2;
     const int lgrv = lgx - LGV;                // log2 of the copies per row
@@ -162,36 +173,56 @@ __global__ void __launch_bounds__(256, 2) k_filter3p(FieldList fl, int lgx, int 
     };
     issue(ks);
     issue(ks + 1);
-    constexpr int OPT = RT_MAX / 256;
-    T y0[OPT], y1[OPT], y2[OPT];
+    T y0[FR][2], y1[FR][2], y2[FR][2];
 #pragma unroll
-    for (int o = 0; o < OPT; ++o) y0[o] = y1[o] = y2[o] = (T)0;
+    for (int i = 0; i < FR; ++i) y0[i][0] = y0[i][1] = y1[i][0] = y1[i][1] = y2[i][0] = y2[i][1] = (T)0;
     for (int kk = ks; kk <= ke; ++kk) {
+        cpa_wait_s<1>();
+        __syncthreads();  // plane kk has landed; every thread is done with plane kk - 1's slot
         issue(kk + 2);
-        cpa_wait_s<2>();
-        __syncthreads();
         const T* tile = tiles + (kk % RT_ST) * tsz;
-        for (int e = tid; e < ((rows + 2) << lgx); e += 256) {
-            const int i = e & (nx - 1);
-            const T l = tile[i == 0 ? e + nx - 1 : e - 1];
-            const T rr = tile[i == nx - 1 ? e - nx + 1 : e + 1];
-            X[e] = (a * l + b * tile[e] + a * rr) * rs;
+        // x filter of tile rows r0 .. r0 + FR + 1 (grid rows j0 + r0 - 1 ..), then y filter
+        T xf[FR + 2][2];
+#pragma unroll
+        for (int i = 0; i < FR + 2; ++i) {
+            const T* row = tile + (r0 + i) * nx;
+            const V2 c = *reinterpret_cast<const V2*>(row + 2 * p);
+            const T l = row[xl], rr = row[xr];
+            xf[i][0] = (a * l + b * c.x + a * c.y) * rs;
+            xf[i][1] = (a * c.x + b * c.y + a * rr) * rs;
         }
-        __syncthreads();
         const int ko = kk - 1;
         const T za = (ko >= 1) ? (T)az[ko] : (T)0, zb = (ko >= 1) ? (T)bz[ko] : (T)0,
                 zcf = (ko >= 1) ? (T)cz[ko] : (T)0;
 #pragma unroll
-        for (int o = 0; o < OPT; ++o) {
-            const int e = tid + 256 * o;
-            if (e >= rows * nx) continue;
-            const T yn = (a * X[e] + b * X[e + nx] + a * X[e + 2 * nx]) * rs;
-            y0[o] = y1[o];
-            y1[o] = y2[o];
-            y2[o] = yn;
-            const long long ob = (long long)j0 * nx + e;
-            if (ko >= k0 && ko < k1) out[(long long)ko * plane + ob] = (ko == 0) ? y1[o] : (za * y0[o] + zb * y1[o] + zcf * y2[o]) * rs;
-            if (kk == nzp - 1 && kk >= k0 && kk < k1) out[(long long)kk * plane + ob] = yn;
+        for (int i = 0; i < FR; ++i) {
+            T yn[2];
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                yn[e] = (a * xf[i][e] + b * xf[i + 1][e] + a * xf[i + 2][e]) * rs;
+                y0[i][e] = y1[i][e];
+                y1[i][e] = y2[i][e];
+                y2[i][e] = yn[e];
+            }
+            if (r0 + i >= rows) continue;
+            const long long ob = (long long)(j0 + r0 + i) * nx + 2 * p;
+            if (ko >= k0 && ko < k1) {
+                V2 v;
+                if (ko == 0) {
+                    v.x = y1[i][0];
+                    v.y = y1[i][1];
+                } else {
+                    v.x = (za * y0[i][0] + zb * y1[i][0] + zcf * y2[i][0]) * rs;
+                    v.y = (za * y0[i][1] + zb * y1[i][1] + zcf * y2[i][1]) * rs;
+                }
+                *reinterpret_cast<V2*>(out + (long long)ko * plane + ob) = v;
+            }
+            if (kk == nzp - 1 && kk >= k0 && kk < k1) {
+                V2 v;
+                v.x = yn[0];
+                v.y = yn[1];
+                *reinterpret_cast<V2*>(out + (long long)kk * plane + ob) = v;
+            }
         }
     }
     cpa_wait_s<0>();
@@ -214,7 +245,7 @@ void filter3_any(lsb_handle* h, const void* const* in, void* const* out, int n, 
         }
         TimerScope ts(h, "sgs_filter3");
         if (rowtile) {
-            const int FJ = std::max(1, std::min(d.ny, RT_MAX / d.nx));
+            const int FJ = FR * 512 / d.nx;  // the thread map's rows (rows past ny are masked)
             const int nyb = (d.ny + FJ - 1) / FJ;
             // z chunks: about four blocks per SM over the launch, at least 4 planes each
             int nzc = (4 * 148 + nyb * fl.n - 1) / (nyb * fl.n);
@@ -223,7 +254,7 @@ void filter3_any(lsb_handle* h, const void* const* in, void* const* out, int n, 
             nzc = (d.nzp + zch - 1) / zch;
             dim3 grid(nyb, nzc, fl.n);
             const size_t es = f32 ? sizeof(float) : sizeof(double);
-            const size_t sm = (size_t)(RT_ST + 1) * (FJ + 2) * d.nx * es;
+            const size_t sm = (size_t)RT_ST * (FJ + 2) * d.nx * es;
             if (f32) {
                 if (sm > 48 * 1024) resident_blocks((const void*)k_filter3p<float>, 256, sm);  // raises the limit once
                 { lsb::note_launch(); k_filter3p<float><<<grid, 256, sm, h->stream>>>(fl, lgx, d.ny, d.nzp, FJ, zch, (float)a, (float)b, zf, zf + d.nzp, zf + 2 * d.nzp); }
