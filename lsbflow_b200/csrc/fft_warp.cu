@@ -18,6 +18,8 @@ namespace {
 
 constexpr int WKC = 16;  // kx columns per spanwise work item
 
+__host__ __device__ constexpr int ilog2c(int v) { return v <= 1 ? 0 : 1 + ilog2c(v >> 1); }
+
 __device__ __forceinline__ int brev(int g, int lgg) {
     return lgg ? (int)(__brev((unsigned)g) >> (32 - lgg)) : 0;
 }
@@ -156,10 +158,13 @@ __device__ __forceinline__ int unpad_row(int n, int ny, int nyl, int layout) {
 // One kernel for both directions.  Work item = (job, z, chunk of WKC kx columns); the tile
 // [nyl][WKC+1] is staged with cp.async (double-buffered), each column is transformed by a
 // lane group, and the tile is written back in coalesced rows.
-template <int R, bool INV>
-__global__ void __launch_bounds__(256) k_ywarp(YInvJobList ij, YFwdJobList fj, YPassArgs a, int nch) {
+// GC: the lane-group width as a compile-time constant (0: the plan's, at run time), so that
+// the transform's cross-lane stages unroll and their twiddle loads are issued up front;
+// 64 registers (4 blocks per SM) fit the unrolled FP64 form without spills
+template <int R, bool INV, int GC = 0>
+__global__ void __launch_bounds__(256, 4) k_ywarp(YInvJobList ij, YFwdJobList fj, YPassArgs a, int nch) {
     extern __shared__ double2 smem[];
-    const int ny = a.ny, nyl = a.nyl, G = a.plan.g, lgg = a.plan.lgg;
+    const int ny = a.ny, nyl = a.nyl, G = GC ? GC : a.plan.g, lgg = GC ? ilog2c(GC) : a.plan.lgg;
     constexpr int TS = WKC + 1;  // tile row stride (complex)
     double2* Buf[2] = {smem, smem + nyl * TS};
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -303,14 +308,14 @@ __device__ __forceinline__ V r2c_mode_w(const V* Z, int k, int N, const V* __res
 }
 
 // Generic row transforms: each lane group of each warp owns one row at a time.
-template <int R, class V>
+template <int R, class V, int GC = 0>
 __global__ void __launch_bounds__(256) k_row_c2r_w(RowJobList jobs, RowArgs a) {
     using S = typename CT<V>::S;
     extern __shared__ unsigned char rsm_raw[];
     V* smem = reinterpret_cast<V*>(rsm_raw);
     const V* twr = sizeof(S) == 4 ? reinterpret_cast<const V*>(a.rp.twrf) : reinterpret_cast<const V*>(a.rp.twr);
     const V* tw = sizeof(S) == 4 ? reinterpret_cast<const V*>(a.rp.half.twf) : reinterpret_cast<const V*>(a.rp.half.tw);
-    const int N = a.nxl / 2, G = a.rp.half.g, lgg = a.rp.half.lgg;
+    const int N = a.nxl / 2, G = GC ? GC : a.rp.half.g, lgg = GC ? ilog2c(GC) : a.rp.half.lgg;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int lpw = 32 / G, q = lane / G, g = lane - q * G;
     V* X = smem + (warp * lpw + q) * (N + 1);
@@ -362,14 +367,14 @@ __global__ void __launch_bounds__(256) k_row_c2r_w(RowJobList jobs, RowArgs a) {
     }
 }
 
-template <int R, class V>
+template <int R, class V, int GC = 0>
 __global__ void __launch_bounds__(256) k_row_r2c_w(RowJobList jobs, RowArgs a) {
     using S = typename CT<V>::S;
     extern __shared__ unsigned char rsm_raw[];
     V* smem = reinterpret_cast<V*>(rsm_raw);
     const V* twr = sizeof(S) == 4 ? reinterpret_cast<const V*>(a.rp.twrf) : reinterpret_cast<const V*>(a.rp.twr);
     const V* tw = sizeof(S) == 4 ? reinterpret_cast<const V*>(a.rp.half.twf) : reinterpret_cast<const V*>(a.rp.half.tw);
-    const int N = a.nxl / 2, G = a.rp.half.g, lgg = a.rp.half.lgg;
+    const int N = a.nxl / 2, G = GC ? GC : a.rp.half.g, lgg = GC ? ilog2c(GC) : a.rp.half.lgg;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int lpw = 32 / G, q = lane / G, g = lane - q * G;
     V* Z = smem + (warp * lpw + q) * (N + 1);
@@ -670,10 +675,10 @@ __global__ void __launch_bounds__(128, 3) k_row_nl_r(NlRowArgs a) {
 // FP32 variants for the mixed-precision step: y-intermediates are FP32, the transforms run
 // in FP32 with FP32 twiddles; the spectral fields on either side stay FP64 (converted on
 // load and store).  Same work items and layouts as k_ywarp.
-template <int R, bool INV>
+template <int R, bool INV, int GC = 0>
 __global__ void __launch_bounds__(256) k_ywarp_f(YInvJobList ij, YFwdJobList fj, YPassArgs a, int nch) {
     extern __shared__ float2 fsm[];
-    const int ny = a.ny, nyl = a.nyl, G = a.plan.g, lgg = a.plan.lgg;
+    const int ny = a.ny, nyl = a.nyl, G = GC ? GC : a.plan.g, lgg = GC ? ilog2c(GC) : a.plan.lgg;
     constexpr int TS = WKC + 1;
     float2* T = fsm;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -863,11 +868,15 @@ void ylaunch(const YInvJobList& ij, const YFwdJobList& fj, const YPassArgs& a, c
     const int nitems = (INV ? ij.n : fj.n) * a.nzp * nch;
     if (a.f32) {
         const size_t smf = (size_t)a.nyl * (WKC + 1) * sizeof(float2);
-        { lsb::note_launch(); k_ywarp_f<R, INV><<<persistent_grid_w(k_ywarp_f<R, INV>, smf, nitems), 256, smf, s>>>(ij, fj, a, nch); }
+        lsb::note_launch();
+        if (a.plan.g == 16) k_ywarp_f<R, INV, 16><<<persistent_grid_w(k_ywarp_f<R, INV, 16>, smf, nitems), 256, smf, s>>>(ij, fj, a, nch);
+        else k_ywarp_f<R, INV><<<persistent_grid_w(k_ywarp_f<R, INV>, smf, nitems), 256, smf, s>>>(ij, fj, a, nch);
         return;
     }
     const size_t sm = (size_t)2 * a.nyl * (WKC + 1) * sizeof(double2);
-    { lsb::note_launch(); k_ywarp<R, INV><<<persistent_grid_w(k_ywarp<R, INV>, sm, nitems), 256, sm, s>>>(ij, fj, a, nch); }
+    lsb::note_launch();
+    if (a.plan.g == 16) k_ywarp<R, INV, 16><<<persistent_grid_w(k_ywarp<R, INV, 16>, sm, nitems), 256, sm, s>>>(ij, fj, a, nch);
+    else k_ywarp<R, INV><<<persistent_grid_w(k_ywarp<R, INV>, sm, nitems), 256, sm, s>>>(ij, fj, a, nch);
 }
 
 template <bool INV>
@@ -889,8 +898,15 @@ void rowlaunch_t(const RowJobList& jobs, const RowArgs& a, cudaStream_t s, bool 
     const size_t sm = (size_t)8 * 32 * (N + 1) * sizeof(V) / a.rp.half.g;
     const long long units = (long long)jobs.n * a.nyl * a.nzp;
     const long long blocks = (units + 8 * 32 / a.rp.half.g - 1) / (8 * 32 / a.rp.half.g);
-    if (c2r) { lsb::note_launch(); k_row_c2r_w<R, V><<<persistent_grid_w(k_row_c2r_w<R, V>, sm, blocks), 256, sm, s>>>(jobs, a); }
-    else { lsb::note_launch(); k_row_r2c_w<R, V><<<persistent_grid_w(k_row_r2c_w<R, V>, sm, blocks), 256, sm, s>>>(jobs, a); }
+    lsb::note_launch();
+    const bool g32 = a.rp.half.g == 32;
+    if (c2r) {
+        if (g32) k_row_c2r_w<R, V, 32><<<persistent_grid_w(k_row_c2r_w<R, V, 32>, sm, blocks), 256, sm, s>>>(jobs, a);
+        else k_row_c2r_w<R, V><<<persistent_grid_w(k_row_c2r_w<R, V>, sm, blocks), 256, sm, s>>>(jobs, a);
+    } else {
+        if (g32) k_row_r2c_w<R, V, 32><<<persistent_grid_w(k_row_r2c_w<R, V, 32>, sm, blocks), 256, sm, s>>>(jobs, a);
+        else k_row_r2c_w<R, V><<<persistent_grid_w(k_row_r2c_w<R, V>, sm, blocks), 256, sm, s>>>(jobs, a);
+    }
 }
 
 template <int R>
