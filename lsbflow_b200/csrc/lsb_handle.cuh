@@ -137,7 +137,10 @@ void filters_init(lsb_handle* h);
 void sgs_init(lsb_handle* h);
 // the ifilt hook of timestep (src/navierstokes.f90:33-40) on the current u, v, w, p
 void filter_hook(lsb_handle* h);
-void sgs_add_tau(lsb_handle* h, double* const* ph, bool dealias);
+// xin/xout: nx further physical fields accumulated into spectral ones by the same forward
+// transform launch (the fringe forcing into N)
+void sgs_add_tau(lsb_handle* h, double* const* ph, bool dealias, const double* const* xin = nullptr,
+                 double* const* xout = nullptr, int nx = 0);
 void sgs_tau_phys(lsb_handle* h, const double* ui, const double* g, const double* uiuj, double* tau);
 void sgs_mul(double* y, const double* x, long long n, cudaStream_t s);
 void diag_compute(lsb_handle* h, lsb_diagnostics* out);

@@ -415,12 +415,16 @@ void nlterm(lsb_handle* h, const double* uin, double* Nout) {
         means[3 + 2] = h->ubarp;
         const int nphys = (h->cfg.sgsflag == 1) ? 12 : 3;
         { TimerScope ts(h, "phys_fields"); spec_to_phys(h, spec, ph, nphys, d.nzp, means, modes, f32); }
-        if (dealias && h->cfg.forcing == 1) {
+        // the forcing's physical fields in scratch fields 18..21 (the SGS model uses 12..17);
+        // with SGS they go to spectral space in the same launches as the stresses
+        double* fo[3] = {PH(18), PH(19), PH(20)};
+        double* no[3] = {Nout, Nout + S, Nout + 2 * S};
+        const bool forcing = dealias && h->cfg.forcing == 1;
+        if (forcing) {
             TimerScope ts(h, "forcing");
-            double* fo[3] = {PH(12), PH(13), PH(14)};
             if (f32) {
                 // lambda (ubar - u) = -lambda u' from an FP32 u' without the mean (no cancellation)
-                double* up = PH(15);
+                double* up = PH(21);
                 const double* sp1[1] = {uin};
                 double* pp1[1] = {up};
                 spec_to_phys(h, sp1, pp1, 1, d.nzp, nullptr, nullptr, true);
@@ -428,10 +432,12 @@ void nlterm(lsb_handle* h, const double* uin, double* Nout) {
             } else {
                 launch_force_phys(ph[0], ph[1], ph[2], fo[0], fo[1], fo[2], h->lamx, h->ubar, d.nx, d.ny, P, h->stream);
             }
-            double* no[3] = {Nout, Nout + S, Nout + 2 * S};
-            phys_to_spec(h, fo, no, 3, d.nzp, 1.0, 1.0, nullptr, f32);
+            if (h->cfg.sgsflag != 1) phys_to_spec(h, fo, no, 3, d.nzp, 1.0, 1.0, nullptr, f32);
         }
-        if (h->cfg.sgsflag == 1) { TimerScope ts(h, "sgs_total"); sgs_add_tau(h, ph, dealias); }
+        if (h->cfg.sgsflag == 1) {
+            TimerScope ts(h, "sgs_total");
+            sgs_add_tau(h, ph, dealias, forcing ? (const double* const*)fo : nullptr, forcing ? no : nullptr, forcing ? 3 : 0);
+        }
     }
     // N_l -= d h_l1/dx + d h_l2/dy + d h_l3/dz
     NlDivArgs nd{};

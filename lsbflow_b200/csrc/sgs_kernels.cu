@@ -703,7 +703,7 @@ static void model_tau(lsb_handle* h, const double* const* u, const double* const
 // nlterm hook: ph[0..2] = u_l (+ubar), ph[3+3l+m] = du_l/dx_m (physical fields of the
 // working type: FP32 in the mixed form); adds the forward transform of tau into the
 // spectral h fields.
-void sgs_add_tau(lsb_handle* h, double* const* ph, bool dealias) {
+void sgs_add_tau(lsb_handle* h, double* const* ph, bool dealias, const double* const* xin, double* const* xout, int nx) {
     const Dims& d = h->d;
     const long long P = h->P, S = d.S();
     SgsWork& s = h->sgs;
@@ -732,28 +732,31 @@ void sgs_add_tau(lsb_handle* h, double* const* ph, bool dealias) {
     for (int q = 0; q < 9; ++q) g[q] = ph[3 + q];
     if (f32) model_tau<float>(h, u3, g, (const double* const*)uu6, s.tau, s.nonsym);
     else model_tau<double>(h, u3, g, (const double* const*)uu6, s.tau, s.nonsym);
+    // add T(tau_lm) to h_lm (6 independent components, or all 9 when tau is not symmetric),
+    // after the caller's extra fields, in one batch of forward transforms
+    const double* tp[kMaxJobs];
+    double* hp[kMaxJobs];
+    int n = 0;
+    for (int i = 0; i < nx; ++i) {
+        tp[n] = xin[i];
+        hp[n++] = xout[i];
+    }
     if (!s.nonsym) {
-        // symmetric: add T(tau_lm) to h_lm for the 6 independent components
-        const double* tp[6];
-        double* hp[6];
         for (int l = 0; l < 3; ++l)
             for (int m = l; m < 3; ++m) {
-                tp[sym6(l, m)] = TAU(3 * l + m);
-                hp[sym6(l, m)] = h->H + sym6(l, m) * S;
+                tp[n] = TAU(3 * l + m);
+                hp[n++] = h->H + sym6(l, m) * S;
             }
-        phys_to_spec(h, tp, hp, 6, d.nzp, 1.0, 1.0, nullptr, f32);
     } else {
-        const double* tp[9];
-        double* hp[9];
         for (int l = 0; l < 3; ++l)
             for (int m = 0; m < 3; ++m) {
                 CK(cudaMemcpyAsync(s.H9 + (3 * l + m) * S, h->H + sym6(l, m) * S, S * sizeof(double),
                                    cudaMemcpyDeviceToDevice, st));
-                tp[3 * l + m] = TAU(3 * l + m);
-                hp[3 * l + m] = s.H9 + (3 * l + m) * S;
+                tp[n] = TAU(3 * l + m);
+                hp[n++] = s.H9 + (3 * l + m) * S;
             }
-        phys_to_spec(h, tp, hp, 9, d.nzp, 1.0, 1.0, nullptr, f32);
     }
+    phys_to_spec(h, tp, hp, n, d.nzp, 1.0, 1.0, nullptr, f32);
 }
 
 void sgs_tau_phys(lsb_handle* h, const double* ui, const double* g, const double* uiuj, double* tau) {
