@@ -133,8 +133,9 @@ template <> struct Vec2<float> { using type = float2; };
 // from the plane tile and the y and z filters run in registers: one barrier per plane.
 constexpr int FR = 4;
 
+// three blocks per SM fit the FP32 form in 80 registers; the FP64 form would spill there
 template <class T>
-__global__ void __launch_bounds__(256, 2) k_filter3p(FieldList fl, int lgx, int ny, int nzp, int FJ, int zch, T a, T b,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_filter3p(FieldList fl, int lgx, int ny, int nzp, int FJ, int zch, T a, T b,
                                                      const double* __restrict__ az, const double* __restrict__ bz,
                                                      const double* __restrict__ cz) {
     using V2 = typename Vec2<T>::type;
