@@ -58,8 +58,10 @@ typedef struct {
     int otfavg, istartavg; /* on-the-fly time averages of u, v, w, p (src/main.f90:70-76) */
     int precision;         /* 0: FP64 throughout (the reference's arithmetic); 1: mixed form --
                               the nonlinear-term transforms and products in FP32 with FP32
-                              y-intermediates, the time integration, boundary conditions and
-                              Chebyshev/eigenbasis solves in FP64 (no reference counterpart) */
+                              y-intermediates, the nonlinear term's first z derivatives on the
+                              tensor cores as BF16 three-way splits with FP32 accumulation, the
+                              time integration, boundary conditions, second derivatives and
+                              eigenbasis solves in FP64 (no reference counterpart) */
 } lsb_config;
 
 /* Host set-up arrays (inputs, as the reference passes diag/smat/simat): see

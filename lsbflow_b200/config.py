@@ -14,7 +14,9 @@ run/input.dat, plus the explicit extensions this implementation adds:
                        land at positive frequencies); "correct" is the textbook 3/2 rule.
 * ``ic = 2``        -- start from caller-supplied (seeded) perturbation fields.
 * ``precision``     -- 0: FP64 throughout (the reference's arithmetic); 1: the mixed form,
-                       with the nonlinear-term transforms and products in FP32.
+                       with the nonlinear-term transforms and products in FP32 and its
+                       first z derivatives on the tensor cores (BF16 three-way splits,
+                       FP32 accumulation).
 
 Sizes follow the reference's axes: x streamwise Fourier (nx), y spanwise Fourier
 (ny), z vertical Chebyshev with nzp = nz+1 points, k=1 the ceiling, k=nzp the wall.
