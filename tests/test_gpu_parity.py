@@ -252,6 +252,26 @@ def test_tau_sgs(model):
             assert rel(t, r) < 1e-11 or np.abs(t - r).max() < 1e-14, (l, m, rel(t, r))
 
 
+@pytest.mark.parametrize("nx,ny", [(8, 6), (64, 12), (256, 12), (512, 4)])
+def test_tau_sgs_dynamic_filter_shapes(nx, ny):
+    # the test filter's thread map (x pairs x 4 rows, 2048 / nx rows per block) at its
+    # extremes, with y blocks that are partly past ny
+    cfg = workload("dns64", nx=nx, ny=ny, nz=16, sgsflag=1, sgsmodel=1, dealiasflag=0)
+    st, s = solver(cfg)
+    u, v, w = ic.seeded_noise(st, 9, 5e-2)
+    _, parts = O.nlterm_skewsym(st, [u, v, w], return_parts=True)
+    ui, g, uu = parts["ui"], parts["duidxj"], parts["uiuj"]
+    ref = O.tau_sgs(st, ui, uu, g)
+    gF = np.array([[g[l][m] for l in range(3)] for m in range(3)])
+    uuF = np.array([[uu[l][m] for l in range(3)] for m in range(3)])
+    tau = s.tau_sgs(np.array(ui), uuF, gF)
+    for l in range(3):
+        for m in range(3):
+            r = ref[l][m][..., :nx]
+            t_ = tau[m][l][..., :nx]
+            assert rel(t_, r) < 1e-11 or np.abs(t_ - r).max() < 1e-14, (l, m, rel(t_, r))
+
+
 def test_diag_divergence_and_energy():
     cfg = workload("dns64", nx=32, ny=8, nz=32, dealiasflag=1)
     st, ost, got = run_both(cfg, 5)
