@@ -323,19 +323,30 @@ __global__ void __launch_bounds__(256) k_row_c2r_w(RowJobList jobs, RowArgs a) {
     const int nunits = jobs.n * nrows;
     const int gw = blockIdx.x * 8 + warp, TW = gridDim.x * 8;
     const V zero = CT<V>::make((S)0, (S)0);
+    // the next row's modes are loaded while the current row is transformed
+    auto load_unit = [&](int u0_, V (&ld_)[R + 1]) {
+        const int uu = u0_ + q;
+        const int ucc = uu < nunits ? uu : u0_;
+        const int jbb = ucc / nrows, roww = ucc - jbb * nrows;
+        const S* yr = reinterpret_cast<const S*>(jobs.j[jbb].yin) + (long long)roww * 2 * a.kxc;
+#pragma unroll
+        for (int it = 0; it <= R; ++it) {
+            const int k = g + G * it;
+            ld_[it] = (k < a.kxc) ? *reinterpret_cast<const V*>(yr + 2 * k) : zero;
+        }
+    };
+    V nx_ld[R + 1];
+    if (gw * lpw < nunits) load_unit(gw * lpw, nx_ld);
     for (int u0 = gw * lpw; u0 < nunits; u0 += TW * lpw) {
         const int u = u0 + q;
         const bool act = u < nunits;
         const int uc = act ? u : u0;
         const int jb = uc / nrows, row = uc - jb * nrows;
         const RowIO job = jobs.j[jb];
-        const S* yrow = reinterpret_cast<const S*>(job.yin) + (long long)row * 2 * a.kxc;
         V ld[R + 1];
 #pragma unroll
-        for (int it = 0; it <= R; ++it) {
-            const int k = g + G * it;
-            ld[it] = (k < a.kxc) ? *reinterpret_cast<const V*>(yrow + 2 * k) : zero;
-        }
+        for (int it = 0; it <= R; ++it) ld[it] = nx_ld[it];
+        if (u0 + TW * lpw < nunits) load_unit(u0 + TW * lpw, nx_ld);
 #pragma unroll
         for (int it = 0; it <= R; ++it) {
             const int k = g + G * it;
@@ -381,16 +392,27 @@ __global__ void __launch_bounds__(256) k_row_r2c_w(RowJobList jobs, RowArgs a) {
     const int nrows = a.nyl * a.nzp;
     const int nunits = jobs.n * nrows;
     const int gw = blockIdx.x * 8 + warp, TW = gridDim.x * 8;
+    // the next row is loaded while the current one is transformed
+    auto load_unit = [&](int u0_, V (&v_)[R]) {
+        const int uu = u0_ + q;
+        const int ucc = uu < nunits ? uu : u0_;
+        const int jbb = ucc / nrows, roww = ucc - jbb * nrows;
+        const V* in = reinterpret_cast<const V*>(reinterpret_cast<const S*>(jobs.j[jbb].yin) + (long long)roww * a.row_pitch);
+#pragma unroll
+        for (int r = 0; r < R; ++r) v_[r] = in[g + G * r];
+    };
+    V nx_v[R];
+    if (gw * lpw < nunits) load_unit(gw * lpw, nx_v);
     for (int u0 = gw * lpw; u0 < nunits; u0 += TW * lpw) {
         const int u = u0 + q;
         const bool act = u < nunits;
         const int uc = act ? u : u0;
         const int jb = uc / nrows, row = uc - jb * nrows;
         const RowIO job = jobs.j[jb];
-        const V* in = reinterpret_cast<const V*>(reinterpret_cast<const S*>(job.yin) + (long long)row * a.row_pitch);
         V v[R];
 #pragma unroll
-        for (int r = 0; r < R; ++r) v[r] = in[g + G * r];
+        for (int r = 0; r < R; ++r) v[r] = nx_v[r];
+        if (u0 + TW * lpw < nunits) load_unit(u0 + TW * lpw, nx_v);
         wfft<R, -1>(v, G, g, tw);
         lane_bitrev<R>(v, G, lane, g, lgg);
 #pragma unroll
