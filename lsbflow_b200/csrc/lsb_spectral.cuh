@@ -51,6 +51,7 @@ struct NlDivArgs {
     double* N[3];
     const double* hx[3];
     const double* hy[3];
+    const double* hz[3];  // d h_l3 / dz, already formed (subtracted after the x and y terms)
     const double* wavx;
     const double* wavy;
     int nx;

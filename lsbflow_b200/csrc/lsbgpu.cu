@@ -453,20 +453,20 @@ void nlterm(lsb_handle* h, const double* uin, double* Nout) {
     nd.S = S;
     nd.C = d.C();
     TimerScope ts(h, "nl_divergence");
-    launch_nl_div_xy(nd, h->stream);
-    // N_l -= d h_l3 / dz for the three components in one launch
+    // d h_l3 / dz for the three components in one launch, into the du/dz buffer (free by
+    // now); the elementwise pass then subtracts all three derivatives from N_l
     GemmArgs gz = gemm_base(h, h->m_dz1);
     for (int l = 0; l < 3; ++l) {
         gz.inf[l] = full9 ? h->sgs.H9 + (l * 3 + 2) * S : Hsym(h, l, 2);
-        gz.outf[l] = Nout + l * S;
+        gz.outf[l] = h->dz + l * S;
+        nd.hz[l] = h->dz + l * S;
     }
     gz.in = gz.inf[0];
     gz.out = gz.outf[0];
     gz.nfields = 3;
-    gz.epi = EPI_AXPBY;
-    gz.alpha = -1.0;
-    gz.beta = 1.0;
+    gz.epi = EPI_STORE;
     if (!(h->cfg.precision == 1 && launch_umma_dz(gz, h->u_dz1, h->uerr, h->stream))) launch_gemm(gz, h->stream);
+    launch_nl_div_xy(nd, h->stream);
 }
 
 void coefficients(lsb_handle* h) {

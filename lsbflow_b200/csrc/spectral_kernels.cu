@@ -170,6 +170,8 @@ __global__ void k_nl_div_xy(NlDivArgs a) {
         ni = ni - (wx * hx[2 * ce]);
         nr = nr - (-wy * hy[2 * ce + 1]);
         ni = ni - (wy * hy[2 * ce]);
+        nr = nr - a.hz[l][2 * ce];
+        ni = ni - a.hz[l][2 * ce + 1];
         a.N[l][2 * ce] = nr;
         a.N[l][2 * ce + 1] = ni;
     }
