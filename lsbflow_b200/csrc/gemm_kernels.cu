@@ -4,8 +4,10 @@
 // DCT-I path of src/chebyshev.f90:204-270 written as its dense matrix) and the two
 // eigenbasis products of solve_helmholtz (src/helmholtz.f90:130-208), with the
 // lifting-function prologue / epilogue of solve_nhom_helmholtz (src/helmholtz.f90:
-// 324-353) and the pressure / Poisson right-hand sides of navierstokes_update
-// (src/navierstokes.f90:1411-1476) fused in.
+// 324-353) and the Poisson right-hand side of navierstokes_update (src/navierstokes.f90:
+// 1411-1464) fused in.  Accumulating into a field that the epilogue must read back costs
+// the read's full latency at the end of every block, so the step stores plain products
+// (dz of h_l3, Dw for the pressure) and adds them in its elementwise passes.
 //
 // tcgen05 has no FP64 kind, so the FP64 form uses the FP64 tensor-core MMA
 // (mma.sync m16n8k8 f64: 1024 FMAs per instruction).  One CTA owns all Mp rows of a block
@@ -152,7 +154,7 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
     const long long cb = c0 + warp * 8 + tq * 2;
     // the two columns this thread writes, and their k^2 for the epilogues that need it
     double ew2[2] = {0.0, 0.0};
-    if (g.epi == EPI_HELM_SCALE || g.epi == EPI_PRESSURE || g.epi == EPI_POISSON_RHS) {
+    if (g.epi == EPI_HELM_SCALE || g.epi == EPI_POISSON_RHS) {
         for (int e = 0; e < 2; ++e)
             if (cb + e < g.C) ew2[e] = w2_of(g, cb + e);
     }
@@ -174,11 +176,6 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
                 case EPI_HELM_SCALE: {
                     const double dfac = (-ew2[e]) - g.sigma;
                     v = v / (g.lam[r] + dfac);
-                    break;
-                }
-                case EPI_PRESSURE: {
-                    const double w2 = ew2[e];
-                    v = (w2 == 0.0) ? 0.0 : -(v + aux[o]) / (w2 * g.alpha * g.beta);
                     break;
                 }
                 case EPI_POISSON_RHS: {

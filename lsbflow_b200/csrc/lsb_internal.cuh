@@ -153,7 +153,6 @@ enum GemmEpi {
     EPI_STORE = 0,          // out = acc
     EPI_AXPBY = 1,          // out = alpha*acc + beta*out
     EPI_HELM_SCALE = 2,     // out = acc / (lam[r] - w2(c) - sigma)
-    EPI_PRESSURE = 3,       // out = -(acc + aux)/(w2(c)*coef), 0 where w2 == 0
     EPI_POISSON_RHS = 4,    // out = -acc - w2(c)*aux
     EPI_LIFT_ADD = 5,       // out = acc + hb[row]*bcb(c) + ht[row]*bct(c)   (bcb may be null)
 };
@@ -171,7 +170,7 @@ struct GemmArgs {
     int epi;
     double alpha, beta, sigma, coef;
     const double* lam;      // EPI_HELM_SCALE
-    const double* aux;      // EPI_PRESSURE / EPI_POISSON_RHS: aux field (same layout as out)
+    const double* aux;      // EPI_POISSON_RHS: aux field (same layout as out)
     const double* wavx;     // [nx]
     const double* wavy;     // [ny]
     int nx;

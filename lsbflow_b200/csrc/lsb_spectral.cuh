@@ -68,8 +68,9 @@ void launch_dxy(const double* in, double* out, const double* wavx, const double*
 void launch_lapl_xy(const double* u, double* d2, const double* wavx, const double* wavy, int nx, long long S,
                     long long C, cudaStream_t s);
 void launch_nl_div_xy(const NlDivArgs& a, cudaStream_t s);
-void launch_pressure_update(double* u, double* v, const double* p, const double* wavx, const double* wavy, int nx,
-                            long long S, long long C, double dtb, cudaStream_t s);
+void launch_pressure_project(double* u, double* v, double* p, const double* dw, const double* div, const double* wavx,
+                             const double* wavy, int nx, long long S, long long C, double dt, double bdfv,
+                             cudaStream_t s);
 void launch_norm(double* f0, double* f1, double* f2, int nx, int ny, int nzp, int ifrz, cudaStream_t s);
 void launch_force_phys(const double* u0, const double* u1, const double* u2, double* f0, double* f1, double* f2,
                        const double* lamx, const double* ubar, int nx, int ny, long long P, cudaStream_t s);

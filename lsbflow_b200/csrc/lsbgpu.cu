@@ -706,22 +706,16 @@ void step_one(lsb_handle* h) {
         // 8-9. Poisson solve for w^{n+1}
         helmholtz(h, h->rhs, h->vel + 2 * S, 1, 0.0, h->bcp);
     }
-    // 10. pressure phi = -(Dw + div)/(k^2 dt bdfv) into pn, then swap
+    // 10. Dw^{n+1} (the eigenbasis temporary is free again)
     {
         TimerScope ts(h, "pressure");
-        GemmArgs g = gemm_base(h, h->m_dz1);
-        g.in = h->vel + 2 * S;
-        g.out = h->pn;
-        g.epi = EPI_PRESSURE;
-        g.aux = h->divf;
-        g.alpha = dt;
-        g.beta = h->bdfv;
-        launch_gemm(g, st);
-        std::swap(h->p, h->pn);
+        zgemm1(h, h->m_dz1, h->vel + 2 * S, h->T, 1);
     }
-    // 11. projection of u, v; norm; ifrz
+    // 11. pressure phi = -(Dw + div)/(k^2 dt bdfv) into pn (then swapped into p) and the
+    // projection of u, v in one pass; norm; ifrz
     TimerScope ts(h, "projection_norm");
-    launch_pressure_update(h->vel, h->vel + S, h->p, h->wavx, h->wavy, d.nx, S, C, dt * h->bdfv, st);
+    launch_pressure_project(h->vel, h->vel + S, h->pn, h->T, h->divf, h->wavx, h->wavy, d.nx, S, C, dt, h->bdfv, st);
+    std::swap(h->p, h->pn);
     launch_norm(h->vel, h->vel + S, h->vel + 2 * S, d.nx, d.ny, d.nzp, c.ifrz, st);
     // 12. time
     h->t = h->t + dt;
