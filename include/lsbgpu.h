@@ -119,8 +119,15 @@ int lsb_download_state(lsb_handle* h, double* uf, double* vf, double* wf, double
 /* device-resident variants: pointers are device addresses of the same layouts */
 int lsb_upload_state_device(lsb_handle* h, const double* uf, const double* vf, const double* wf);
 int lsb_download_velocity_device(lsb_handle* h, double* uf, double* vf, double* wf);
-/* nsteps calls of timestep() (src/navierstokes.f90:10-90) on the device */
+/* nsteps calls of timestep() (src/navierstokes.f90:10-90) on the device.  Steady steps
+ * (after the start-up steps, constant dt, no timers, dt adaptation or filter hook, a
+ * boundary forcing amplitude that no longer depends on t) are replayed from CUDA graphs
+ * captured on the handle's stream, one per rotation of the history buffers (at most 6);
+ * the results are those of ordinary launches, bit for bit. */
 int lsb_step(lsb_handle* h, int nsteps);
+/* enable = 0: drop the step graphs and launch every kernel of every step (no reference
+ * counterpart) */
+int lsb_graphs(lsb_handle* h, int enable);
 int lsb_diag(lsb_handle* h, lsb_diagnostics* out);
 int lsb_synchronize(lsb_handle* h);
 /* asynchronous host<->device copies of u, v, w only (the histories stay resident);

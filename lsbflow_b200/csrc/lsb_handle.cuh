@@ -90,6 +90,22 @@ struct lsb_handle {
     double abfac[3] = {0, 0, 0}, bdf[3] = {0, 0, 0}, bdfv = 0;
     double bshape_norm = 0.0;  // bctype 1: S_top(0,0) / S_wall(0,0) helper
 
+    // CUDA graphs of single steady steps (lsb_step), keyed by the history pointers (they
+    // rotate with period 6) and the scalars that the launches carry
+    struct StepGraph {
+        cudaGraphExec_t exec = nullptr;
+        const void* key[8] = {};
+        double dt = 0, ctop = 0, cwa = 0, cwb = 0;
+        unsigned long long kernels = 0;  // kernels in one replay
+    };
+    std::vector<StepGraph> graphs;
+    bool graphs_on = true;
+    void drop_graphs() {
+        for (auto& g : graphs)
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+        graphs.clear();
+    }
+
     size_t device_bytes = 0;  // sum of this handle's device allocations
     double* alloc(size_t n) {
         void* q = nullptr;
@@ -106,6 +122,7 @@ struct lsb_handle {
     }
     ~lsb_handle() {
         if (stream) cudaStreamSynchronize(stream);
+        drop_graphs();
         for (void* q : allocs) cudaFree(q);
         if (own) cudaStreamDestroy(own);
     }

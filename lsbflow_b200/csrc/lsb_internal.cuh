@@ -19,6 +19,8 @@ namespace lsb {
 
 // counts every kernel launch of the library (lsb_kernel_launches)
 void note_launch();
+void note_launches(long long n);       // n kernels run by a replayed graph (n < 0: a capture undone)
+unsigned long long launches_so_far();
 
 // resident blocks of a kernel on one SM for a block size and dynamic shared memory,
 // queried once per (device, kernel, threads, shared memory) and cached; the first query

@@ -739,6 +739,117 @@ void check_launch() {
     if (e != cudaSuccess) fail(LSB_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
 }
 
+// ---------------------------------------------------------------- step graphs
+// A step whose launches carry the same arguments as an earlier one can be replayed from a
+// CUDA graph: after the start-up steps, with a constant dt, no timers, no dt adaptation or
+// filter hook, a boundary forcing whose amplitude no longer depends on t, and the time-
+// average switch settled.  The graph key adds the history pointers (their rotation has
+// period 6, so at most 6 graphs) and the scalars passed by value.
+bool graph_eligible(lsb_handle* h) {
+    const lsb_config& c = h->cfg;
+    if (!h->graphs_on || h->timing || c.dtadapt == 1) return false;
+    if (c.ifilt >= 1 && c.modfilt > 0) return false;
+    if (h->istep < 3) return false;  // start-up coefficients and boundary-row factors
+    if (h->dt != h->dt2 || h->dt2 != h->dt3) return false;
+    if (c.otfavg == 1 && h->istep < c.istartavg) return false;
+    if (c.bctype == 2) return false;
+    if (c.bctype > 0 && h->t < c.istartbound) return false;
+    if (c.bctype == 1 && !(h->t - c.istartbound > c.xlen / c.u0)) return false;  // amplitude ramp
+    return true;
+}
+
+struct HostStep {
+    double t, dt, dt2, dt3, abfac[3], bdf[3], bdfv;
+    int istep;
+    double *vel, *veln, *velnm, *nlc, *nln, *nlnm, *p, *pn;
+};
+HostStep save_host(const lsb_handle* h) {
+    HostStep s{h->t, h->dt, h->dt2, h->dt3, {h->abfac[0], h->abfac[1], h->abfac[2]}, {h->bdf[0], h->bdf[1], h->bdf[2]},
+               h->bdfv, h->istep, h->vel, h->veln, h->velnm, h->nlc, h->nln, h->nlnm, h->p, h->pn};
+    return s;
+}
+void restore_host(lsb_handle* h, const HostStep& s) {
+    h->t = s.t; h->dt = s.dt; h->dt2 = s.dt2; h->dt3 = s.dt3;
+    for (int k = 0; k < 3; ++k) { h->abfac[k] = s.abfac[k]; h->bdf[k] = s.bdf[k]; }
+    h->bdfv = s.bdfv; h->istep = s.istep;
+    h->vel = s.vel; h->veln = s.veln; h->velnm = s.velnm; h->nlc = s.nlc; h->nln = s.nln; h->nlnm = s.nlnm;
+    h->p = s.p; h->pn = s.pn;
+}
+
+// the host side of one step, as step_one leaves it (the replayed graph does the device side)
+void replay_advance(lsb_handle* h) {
+    h->istep += 1;
+    coefficients(h);
+    double* t1 = h->nlnm;
+    h->nlnm = h->nln;
+    h->nln = h->nlc;
+    h->nlc = t1;
+    double* t2 = h->velnm;
+    h->velnm = h->veln;
+    h->veln = h->vel;
+    h->vel = t2;
+    std::swap(h->p, h->pn);
+    h->t = h->t + h->dt;
+    h->dt3 = h->dt2;
+    h->dt2 = h->dt;
+}
+
+// runs one step from a graph (replayed, or captured now and launched); false: not eligible
+// or capture unavailable, and the caller runs the step with ordinary launches
+template <class Body>
+bool graph_step(lsb_handle* h, Body&& body) {
+    if (!graph_eligible(h)) return false;
+    double ctop = 0, cwa = 0, cwb = 0;
+    bound_coeffs(h, h->t, ctop, cwa, cwb);
+    const void* key[8] = {h->vel, h->veln, h->velnm, h->nlc, h->nln, h->nlnm, h->p, h->pn};
+    for (auto& g : h->graphs) {
+        if (std::memcmp(g.key, key, sizeof(key)) != 0 || g.dt != h->dt || g.ctop != ctop || g.cwa != cwa || g.cwb != cwb)
+            continue;
+        CK(cudaGraphLaunch(g.exec, h->stream));
+        lsb::note_launches((long long)g.kernels);
+        replay_advance(h);
+        return true;
+    }
+    if (h->graphs.size() >= 6) return false;
+    const HostStep snap = save_host(h);
+    const unsigned long long k0 = lsb::launches_so_far();
+    if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        h->graphs_on = false;
+        return false;
+    }
+    bool ok = true;
+    try {
+        body();
+    } catch (...) {
+        ok = false;
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+    cudaGraphExec_t exec = nullptr;
+    if (ok && e == cudaSuccess && graph != nullptr && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
+        cudaGraphDestroy(graph);
+        lsb_handle::StepGraph g;
+        std::memcpy(g.key, key, sizeof(key));
+        g.dt = snap.dt;
+        g.ctop = ctop;
+        g.cwa = cwa;
+        g.cwb = cwb;
+        g.kernels = lsb::launches_so_far() - k0;
+        g.exec = exec;
+        h->graphs.push_back(g);
+        CK(cudaGraphLaunch(exec, h->stream));  // the captured step has not run yet
+        return true;
+    }
+    // capture did not work here: undo the host side of the captured step, run it plainly
+    cudaGetLastError();
+    if (graph) cudaGraphDestroy(graph);
+    restore_host(h, snap);
+    lsb::note_launches(-(long long)(lsb::launches_so_far() - k0));
+    h->graphs_on = false;
+    return false;
+}
+
 }  // namespace
 
 namespace lsb {
@@ -747,6 +858,8 @@ void set_last_error(const std::string& m) { g_err = m; }
 // kernels launched by this library since it was loaded (all handles, all threads)
 static std::atomic<unsigned long long> g_kernel_launches{0};
 void note_launch() { g_kernel_launches.fetch_add(1, std::memory_order_relaxed); }
+void note_launches(long long n) { g_kernel_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
+unsigned long long launches_so_far() { return g_kernel_launches.load(); }
 
 static std::mutex g_occ_mu;
 static std::map<std::tuple<int, const void*, int, size_t>, int> g_occ;
@@ -1066,7 +1179,7 @@ int lsb_step(lsb_handle* h, int nsteps) {
         if (!(h->dt > 0.0) || !std::isfinite(h->dt)) fail(LSB_ERR_STATE, "dt must be finite and > 0");
         const lsb_config& c = h->cfg;
         const long long S = h->d.S();
-        for (int i = 0; i < nsteps; ++i) {
+        auto body = [&] {
             step_one(h);
             check_launch();
             // adaptive dt: NaN check + maxcalc every 5 steps and every iomod steps
@@ -1087,7 +1200,20 @@ int lsb_step(lsb_handle* h, int nsteps) {
                 const double* q[4] = {h->vel, h->vel + S, h->vel + 2 * S, h->p};
                 for (int k = 0; k < 4; ++k) launch_tavg_add(h->tavg + k * S, q[k], (double)c.iomod, S, h->stream);
             }
+        };
+        for (int i = 0; i < nsteps; ++i) {
+            if (graph_step(h, body)) continue;
+            body();
         }
+    });
+}
+
+int lsb_graphs(lsb_handle* h, int enable) {
+    return guard([&] {
+        if (!h) fail(LSB_ERR_ARG, "null handle");
+        CK(cudaStreamSynchronize(h->stream));
+        h->drop_graphs();
+        h->graphs_on = enable != 0;
     });
 }
 

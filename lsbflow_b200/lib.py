@@ -27,7 +27,7 @@ EXPORTS = [
     "lsb_synchronize", "lsb_horfft", "lsb_dealias_product", "lsb_dfdx", "lsb_dfdy", "lsb_dfdz", "lsb_d2fdz2",
     "lsb_lapl", "lsb_divuv", "lsb_solve_helmholtz", "lsb_solve_nhom_helmholtz", "lsb_nlterm", "lsb_tau_sgs",
     "lsb_upload_velocity", "lsb_download_velocity", "lsb_timers", "lsb_timer_report",
-    "lsb_solve_helmholtz_noalloc", "lsb_tavg", "lsb_spanwise_stats", "lsb_kernel_launches", "lsb_device_bytes",
+    "lsb_solve_helmholtz_noalloc", "lsb_tavg", "lsb_spanwise_stats", "lsb_graphs", "lsb_kernel_launches", "lsb_device_bytes",
 ]
 
 
@@ -207,6 +207,10 @@ class Solver:
 
     def step(self, n: int = 1):
         _ck(self._lib.lsb_step(self._h, C.c_int(n)))
+
+    def graphs(self, enable: bool):
+        """Replay steady steps from CUDA graphs (default) or launch every kernel."""
+        _ck(self._lib.lsb_graphs(self._h, C.c_int(1 if enable else 0)))
 
     def synchronize(self):
         _ck(self._lib.lsb_synchronize(self._h))
