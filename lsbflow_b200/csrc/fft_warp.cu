@@ -427,6 +427,73 @@ __global__ void __launch_bounds__(256) k_row_r2c_w(RowJobList jobs, RowArgs a) {
     }
 }
 
+// r2c row pass for full-warp plans (G = 32, N = 32 R): one warp per row, the physical row
+// staged in shared memory under an XOR swizzle, so that both its natural-order writes
+// (lane-contiguous) and its slot-order reads (stride R, lanes bit-reversed) are free of
+// bank conflicts; the decimation-in-time network then ends in natural order, where the
+// (k, N - k) pairs of the real-to-complex split are one shuffle apart: no lane bit
+// reversal, no second staging.  (The same scheme for c2r measured slower than
+// k_row_c2r_w: its register footprint cost a block per SM.)
+__device__ __forceinline__ int rsw(int n) { return n ^ ((n >> 4) & 7); }  // stays in n's block of 8
+
+template <int R, class V>
+__global__ void __launch_bounds__(256) k_row_r2c_s(RowJobList jobs, RowArgs a) {
+    using S = typename CT<V>::S;
+    constexpr int N = 32 * R, LS = N + 8;
+    extern __shared__ unsigned char rsm_raw[];
+    const V* twr = sizeof(S) == 4 ? reinterpret_cast<const V*>(a.rp.twrf) : reinterpret_cast<const V*>(a.rp.twr);
+    const V* tw = sizeof(S) == 4 ? reinterpret_cast<const V*>(a.rp.half.twf) : reinterpret_cast<const V*>(a.rp.half.tw);
+    const int g = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    V* Z = reinterpret_cast<V*>(rsm_raw) + warp * LS;
+    const int K = a.kxc, mb = R * brev(g, 5);
+    const int nrows = a.nyl * a.nzp;
+    const int nunits = jobs.n * nrows;
+    const int gw = blockIdx.x * 8 + warp, TW = gridDim.x * 8;
+    const int src = (32 - g) & 31;
+    const S h = (S)0.5;
+    auto load_unit = [&](int u, V (&v_)[R]) {
+        const int jbb = u / nrows, roww = u - jbb * nrows;
+        const V* in = reinterpret_cast<const V*>(reinterpret_cast<const S*>(jobs.j[jbb].yin) + (long long)roww * a.row_pitch);
+#pragma unroll
+        for (int r = 0; r < R; ++r) v_[r] = in[g + 32 * r];
+    };
+    V nx_v[R];
+    if (gw < nunits) load_unit(gw, nx_v);
+    (void)N;
+    for (int u = gw; u < nunits; u += TW) {
+        const int jb = u / nrows, row = u - jb * nrows;
+        const RowIO job = jobs.j[jb];
+        V v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) Z[rsw(g + 32 * r)] = nx_v[r];
+        if (u + TW < nunits) load_unit(u + TW, nx_v);
+        __syncwarp();
+#pragma unroll
+        for (int k1 = 0; k1 < R; ++k1) v[k1] = Z[rsw(k1 + mb)];
+        __syncwarp();  // the row buffer is free for the next row
+        wfft_dit<R, -1>(v, 32, g, tw);
+        // natural order: lane g register rr holds Z[g + 32 rr]; Z[N-k] for k = g + 32 rr is
+        // lane (32-g) register R-1-rr (g > 0), or lane 0 register R-rr (g = 0, rr > 0)
+        V* yrow = reinterpret_cast<V*>(reinterpret_cast<S*>(job.out) + (long long)row * 2 * K);
+#pragma unroll
+        for (int rr = 0; rr < R; ++rr) {
+            V zb;
+            zb.x = __shfl_sync(0xffffffffu, v[R - 1 - rr].x, src);
+            zb.y = __shfl_sync(0xffffffffu, v[R - 1 - rr].y, src);
+            if (g == 0) zb = v[rr == 0 ? 0 : R - rr];
+            const int k = g + 32 * rr;
+            if (k < K) {
+                const V za = v[rr];
+                zb = cconj(zb);
+                const V e = CT<V>::make(h * (za.x + zb.x), h * (za.y + zb.y));
+                const V o = CT<V>::make(h * (za.x - zb.x), h * (za.y - zb.y));
+                const V tt = cmul(__ldg(&twr[k]), o);
+                yrow[k] = CT<V>::make(e.x + tt.y, e.y - tt.x);
+            }
+        }
+    }
+}
+
 // The fused nonlinear-product row: 12 c2r (u_l, du_l/dx, du_l/dy, du_l/dz), the skew-
 // symmetric products and fringe of nlterm_skewsym (src/navierstokes.f90:725-769), 9 r2c.
 // A block owns one (z, y) row at a time; the 9 input rows of the next row are staged with
@@ -920,8 +987,15 @@ void rowlaunch_t(const RowJobList& jobs, const RowArgs& a, cudaStream_t s, bool 
     const size_t sm = (size_t)8 * 32 * (N + 1) * sizeof(V) / a.rp.half.g;
     const long long units = (long long)jobs.n * a.nyl * a.nzp;
     const long long blocks = (units + 8 * 32 / a.rp.half.g - 1) / (8 * 32 / a.rp.half.g);
-    lsb::note_launch();
     const bool g32 = a.rp.half.g == 32;
+    if (!c2r && g32 && N == 32 * R) {
+        const size_t ss = (size_t)8 * (N + 8) * sizeof(V);
+        const long long b32 = (units + 7) / 8;
+        lsb::note_launch();
+        k_row_r2c_s<R, V><<<persistent_grid_w(k_row_r2c_s<R, V>, ss, b32), 256, ss, s>>>(jobs, a);
+        return;
+    }
+    lsb::note_launch();
     if (c2r) {
         if (g32) k_row_c2r_w<R, V, 32><<<persistent_grid_w(k_row_c2r_w<R, V, 32>, sm, blocks), 256, sm, s>>>(jobs, a);
         else k_row_c2r_w<R, V><<<persistent_grid_w(k_row_c2r_w<R, V>, sm, blocks), 256, sm, s>>>(jobs, a);
