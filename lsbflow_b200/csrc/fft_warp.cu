@@ -154,6 +154,21 @@ __device__ __forceinline__ int unpad_row(int n, int ny, int nyl, int layout) {
     return -1;
 }
 
+// FP64 spanwise tile [nyl][WKC] (16-byte elements, no padding): the column of a row is
+// XOR-swizzled by a function of the row, chosen per R so that the 8 lanes of a quarter warp
+// hit 8 distinct banks both when a lane group reads a column in natural row order
+// (rows g + G r) and when it writes it back after the lane bit reversal (rows R g + k1);
+// lane-contiguous row accesses only permute a row's columns.
+template <int R>
+__device__ __forceinline__ int yswz(int row) {
+    if (R == 2 || R == 4) return row ^ (row >> 1) ^ (row >> 2);
+    if (R == 6) return row ^ (row >> 1) ^ (row << 1);
+    if (R == 8) return row ^ (row >> 1) ^ (row >> 3);
+    return row;
+}
+template <int R>
+__device__ __forceinline__ int ytix(int row, int col) { return row * WKC + (col ^ (yswz<R>(row) & 7)); }
+
 // ----------------------------------------------------------------------------- spanwise
 // One kernel for both directions.  Work item = (job, z, chunk of WKC kx columns); the tile
 // [nyl][WKC+1] is staged with cp.async (double-buffered), each column is transformed by a
@@ -165,8 +180,7 @@ template <int R, bool INV, int GC = 0>
 __global__ void __launch_bounds__(256, 4) k_ywarp(YInvJobList ij, YFwdJobList fj, YPassArgs a, int nch) {
     extern __shared__ double2 smem[];
     const int ny = a.ny, nyl = a.nyl, G = GC ? GC : a.plan.g, lgg = GC ? ilog2c(GC) : a.plan.lgg;
-    constexpr int TS = WKC + 1;  // tile row stride (complex)
-    double2* Buf[2] = {smem, smem + nyl * TS};
+    double2* Buf[2] = {smem, smem + nyl * WKC};
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int njobs = INV ? ij.n : fj.n;
     const int nitems = njobs * a.nzp * nch;
@@ -179,7 +193,7 @@ __global__ void __launch_bounds__(256, 4) k_ywarp(YInvJobList ij, YFwdJobList fj
             const double* in = ij.j[jb].in;
             for (int idx = tid; idx < ny * WKC; idx += 256) {
                 const int j = idx / WKC, cc = idx - j * WKC, c = c0 + cc;
-                double2* d = &T[pad_row_w(j, ny, nyl, a.layout) * TS + cc];
+                double2* d = &T[ytix<R>(pad_row_w(j, ny, nyl, a.layout), cc)];
                 if (c < a.kxc) cpa16(d, in + ((long long)z * ny + j) * a.nx + 2 * c);
                 else *d = make_double2(0.0, 0.0);
             }
@@ -187,13 +201,13 @@ __global__ void __launch_bounds__(256, 4) k_ywarp(YInvJobList ij, YFwdJobList fj
             for (int idx = tid; idx < npad * WKC; idx += 256) {
                 const int r = idx / WKC, cc = idx - r * WKC;
                 const int jl = (a.layout == 0 || nyl == ny) ? ny + r : ny / 2 + r;
-                T[jl * TS + cc] = make_double2(0.0, 0.0);
+                T[ytix<R>(jl, cc)] = make_double2(0.0, 0.0);
             }
         } else {
             const double* in = fj.j[jb].in;
             for (int idx = tid; idx < nyl * WKC; idx += 256) {
                 const int jl = idx / WKC, cc = idx - jl * WKC, c = c0 + cc;
-                double2* d = &T[jl * TS + cc];
+                double2* d = &T[ytix<R>(jl, cc)];
                 if (c < a.kxc) cpa16(d, in + ((long long)z * nyl + jl) * a.nx + 2 * c);
                 else *d = make_double2(0.0, 0.0);
             }
@@ -220,7 +234,7 @@ __global__ void __launch_bounds__(256, 4) k_ywarp(YInvJobList ij, YFwdJobList fj
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 const int n = g + G * r;
-                double2 x = T[n * TS + Lc];
+                double2 x = T[ytix<R>(n, Lc)];
                 if (INV && mode != YM_COPY) {
                     double k = 0.0;
                     if (mode == YM_IKY) {
@@ -238,7 +252,7 @@ __global__ void __launch_bounds__(256, 4) k_ywarp(YInvJobList ij, YFwdJobList fj
             lane_bitrev<R>(v, G, lane, g, lgg);
             if (act) {
 #pragma unroll
-                for (int k1 = 0; k1 < R; ++k1) T[(R * g + k1) * TS + L] = v[k1];
+                for (int k1 = 0; k1 < R; ++k1) T[ytix<R>(R * g + k1, L)] = v[k1];
             }
         }
         __syncthreads();
@@ -247,17 +261,17 @@ __global__ void __launch_bounds__(256, 4) k_ywarp(YInvJobList ij, YFwdJobList fj
             for (int idx = tid; idx < nyl * WKC; idx += 256) {
                 const int jl = idx / WKC, cc = idx - jl * WKC, c = c0 + cc;
                 if (c >= a.kxc) continue;
-                *reinterpret_cast<double2*>(out + ((long long)z * nyl + jl) * a.nx + 2 * c) = T[jl * TS + cc];
+                *reinterpret_cast<double2*>(out + ((long long)z * nyl + jl) * a.nx + 2 * c) = T[ytix<R>(jl, cc)];
             }
         } else {
             const YFwdJob job = fj.j[jb];
             for (int idx = tid; idx < ny * WKC; idx += 256) {
                 const int j = idx / WKC, cc = idx - j * WKC, c = c0 + cc;
                 if (c >= a.kxc) continue;
-                double2 v = T[pad_row_w(j, ny, nyl, a.layout) * TS + cc];
+                double2 v = T[ytix<R>(pad_row_w(j, ny, nyl, a.layout), cc)];
                 if (job.sym && c == 0) {
                     const int jm = (ny - j) % ny;
-                    const double2 w = T[pad_row_w(jm, ny, nyl, a.layout) * TS + cc];
+                    const double2 w = T[ytix<R>(pad_row_w(jm, ny, nyl, a.layout), cc)];
                     v = make_double2(0.5 * (v.x + w.x), 0.5 * (v.y - w.y));
                 }
                 v.x *= a.scale;
@@ -281,14 +295,21 @@ __global__ void __launch_bounds__(256, 4) k_ywarp(YInvJobList ij, YFwdJobList fj
 // ----------------------------------------------------------------------------- rows
 // c2r of the modes in X (N+1 entries; zero beyond kxc, DC imaginary part dropped) into
 // registers: lane g returns z[k1 + R*bitrev(g)] in v[k1] (z = x[2m] + i x[2m+1]).
+// row-buffer index under an XOR swizzle within blocks of 8 elements for FP64 rows (16-byte
+// elements): lane-contiguous and stride-4 accesses (the staging of a bit-reversed row,
+// R = 4) both avoid bank conflicts; indices N .. N + 7 stay in their block, so a row needs
+// N + 8 slots.  FP32 rows keep the plain layout (measured faster there).
+template <class V>
+__device__ __forceinline__ int xsw(int n) { return sizeof(V) == 16 ? (n ^ ((n >> 3) & 7)) : n; }
+
 template <int R, class V>
 __device__ __forceinline__ void row_c2r_regs(const V* X, int N, int G, int g, const V* __restrict__ twr,
                                              const V* __restrict__ tw, V (&v)[R]) {
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int n = g + G * r;
-        const V xa = X[n];
-        const V xb = cconj(X[N - n]);
+        const V xa = X[xsw<V>(n)];
+        const V xb = cconj(X[xsw<V>(N - n)]);
         const V e = cadd(xa, xb);
         const V o = cmul(csub(xa, xb), cconj(__ldg(&twr[n])));
         v[r] = CT<V>::make(e.x - o.y, e.y + o.x);
@@ -318,7 +339,7 @@ __global__ void __launch_bounds__(256) k_row_c2r_w(RowJobList jobs, RowArgs a) {
     const int N = a.nxl / 2, G = GC ? GC : a.rp.half.g, lgg = GC ? ilog2c(GC) : a.rp.half.lgg;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int lpw = 32 / G, q = lane / G, g = lane - q * G;
-    V* X = smem + (warp * lpw + q) * (N + 1);
+    V* X = smem + (warp * lpw + q) * (N + 8);
     const int nrows = a.nyl * a.nzp;
     const int nunits = jobs.n * nrows;
     const int gw = blockIdx.x * 8 + warp, TW = gridDim.x * 8;
@@ -357,7 +378,7 @@ __global__ void __launch_bounds__(256) k_row_c2r_w(RowJobList jobs, RowArgs a) {
                 v = CT<V>::make(-kk * v.y, kk * v.x);
             }
             if (k == 0) v.y = (S)0;
-            X[k] = v;
+            X[xsw<V>(k)] = v;
         }
         __syncwarp();
         V v[R];
@@ -368,11 +389,11 @@ __global__ void __launch_bounds__(256) k_row_c2r_w(RowJobList jobs, RowArgs a) {
         lane_bitrev<R>(v, G, lane, g, lgg);
         __syncwarp();
 #pragma unroll
-        for (int k1 = 0; k1 < R; ++k1) X[R * g + k1] = CT<V>::make(sc * v[k1].x + m, sc * v[k1].y + m);
+        for (int k1 = 0; k1 < R; ++k1) X[xsw<V>(R * g + k1)] = CT<V>::make(sc * v[k1].x + m, sc * v[k1].y + m);
         __syncwarp();
         if (act) {
             V* o = reinterpret_cast<V*>(reinterpret_cast<S*>(job.out) + (long long)row * a.row_pitch);
-            for (int k = g; k < N; k += G) o[k] = X[k];
+            for (int k = g; k < N; k += G) o[k] = X[xsw<V>(k)];
         }
         __syncwarp();
     }
@@ -984,7 +1005,7 @@ bool ydispatch(const YInvJobList& ij, const YFwdJobList& fj, const YPassArgs& a,
 template <int R, class V>
 void rowlaunch_t(const RowJobList& jobs, const RowArgs& a, cudaStream_t s, bool c2r) {
     const int N = a.nxl / 2;
-    const size_t sm = (size_t)8 * 32 * (N + 1) * sizeof(V) / a.rp.half.g;
+    const size_t sm = (size_t)8 * 32 * (N + 8) * sizeof(V) / a.rp.half.g;  // row stride N + 8 (swizzle)
     const long long units = (long long)jobs.n * a.nyl * a.nzp;
     const long long blocks = (units + 8 * 32 / a.rp.half.g - 1) / (8 * 32 / a.rp.half.g);
     const bool g32 = a.rp.half.g == 32;
