@@ -207,23 +207,19 @@ __global__ void k_norm(double* f0, double* f1, double* f2, int nx, int ny, int n
     double* f = (blockIdx.y == 0) ? f0 : (blockIdx.y == 1 ? f1 : f2);
     double* pl = f + (long long)k * nx * ny;
     const int nyh = ny / 2;
-    if (threadIdx.x == 0) {
-        pl[1] = 0.0;
-        if (ny > 2) {
-            for (int jj = 1; jj <= nyh - 1; ++jj) {
-                const int jp = ny - jj;
-                pl[jj * nx + 0] = 0.5 * (pl[jj * nx + 0] + pl[jp * nx + 0]);
-                pl[jj * nx + 1] = 0.5 * (pl[jj * nx + 1] - pl[jp * nx + 1]);
-            }
-            for (int jj = 1; jj <= nyh - 1; ++jj) {
-                const int jp = ny - jj;
-                pl[jp * nx + 0] = pl[jj * nx + 0];
-                pl[jp * nx + 1] = -pl[jj * nx + 1];
-            }
-        }
-    }
-    __syncthreads();
+    if (threadIdx.x == 0) pl[1] = 0.0;
     if (ny > 2) {
+        // the pairs (ky, -ky) of the kx = 0 column are disjoint (rows 1..nyh-1 and
+        // nyh+1..ny-1): one thread per pair, the reference's two loops in that order
+        for (int jj = 1 + threadIdx.x; jj <= nyh - 1; jj += blockDim.x) {
+            const int jp = ny - jj;
+            const double re = 0.5 * (pl[jj * nx + 0] + pl[jp * nx + 0]);
+            const double im = 0.5 * (pl[jj * nx + 1] - pl[jp * nx + 1]);
+            pl[jj * nx + 0] = re;
+            pl[jj * nx + 1] = im;
+            pl[jp * nx + 0] = re;
+            pl[jp * nx + 1] = -im;
+        }
         for (int i = threadIdx.x; i < nx; i += blockDim.x) pl[nyh * nx + i] = 0.0;
     }
     __syncthreads();
