@@ -434,6 +434,15 @@ __global__ void __launch_bounds__(256) k_row_r2c_w(RowJobList jobs, RowArgs a) {
 #pragma unroll
         for (int r = 0; r < R; ++r) v[r] = nx_v[r];
         if (u0 + TW * lpw < nunits) load_unit(u0 + TW * lpw, nx_v);
+        if (job.lam != nullptr) {  // fringe forcing lambda(x) (m - q) on the fly
+            const S m = (job.mean != nullptr && job.add_mean != 0.0) ? (S)(job.mean[row / a.nyl] * job.add_mean) : (S)0;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int x = 2 * (g + G * r);
+                const S l0 = (S)job.lam[x], l1 = (S)job.lam[x + 1];
+                v[r] = CT<V>::make(l0 * (m - v[r].x), l1 * (m - v[r].y));
+            }
+        }
         wfft<R, -1>(v, G, g, tw);
         lane_bitrev<R>(v, G, lane, g, lgg);
 #pragma unroll
@@ -485,6 +494,15 @@ __global__ void __launch_bounds__(256) k_row_r2c_s(RowJobList jobs, RowArgs a) {
         const int jb = u / nrows, row = u - jb * nrows;
         const RowIO job = jobs.j[jb];
         V v[R];
+        if (job.lam != nullptr) {  // fringe forcing lambda(x) (m - q) on the fly
+            const S m = (job.mean != nullptr && job.add_mean != 0.0) ? (S)(job.mean[row / a.nyl] * job.add_mean) : (S)0;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int x = 2 * (g + 32 * r);
+                const S l0 = (S)job.lam[x], l1 = (S)job.lam[x + 1];
+                nx_v[r] = CT<V>::make(l0 * (m - nx_v[r].x), l1 * (m - nx_v[r].y));
+            }
+        }
 #pragma unroll
         for (int r = 0; r < R; ++r) Z[rsw(g + 32 * r)] = nx_v[r];
         if (u + TW < nunits) load_unit(u + TW, nx_v);

@@ -157,14 +157,18 @@ void filter_hook(lsb_handle* h);
 // xin/xout: nx further physical fields accumulated into spectral ones by the same forward
 // transform launch (the fringe forcing into N)
 void sgs_add_tau(lsb_handle* h, double* const* ph, bool dealias, const double* const* xin = nullptr,
-                 double* const* xout = nullptr, int nx = 0);
+                 double* const* xout = nullptr, int nx = 0, const double* xlam = nullptr,
+                 const double* const* xmeans = nullptr);
 void sgs_tau_phys(lsb_handle* h, const double* ui, const double* g, const double* uiuj, double* tau);
 void sgs_mul(double* y, const double* x, long long n, cudaStream_t s);
 void diag_compute(lsb_handle* h, lsb_diagnostics* out);
 // lsbgpu.cu helpers used by sgs_kernels.cu
 // f32: physical fields and y-intermediates in FP32 (mixed form); spectral fields are FP64
+// lam / lmeans / nlam: the first nlam fields enter as the fringe forcing lambda(x) (m - q),
+// m = lmeans[i][z] (or 0), formed by the row transform as it reads them
 void phys_to_spec(lsb_handle* h, const double* const* phys, double* const* spec, int nf, int nzp, double alpha,
-                  double beta, double* const* ybuf, bool f32 = false);
+                  double beta, double* const* ybuf, bool f32 = false, const double* lam = nullptr,
+                  const double* const* lmeans = nullptr, int nlam = 0);
 void spec_to_phys(lsb_handle* h, const double* const* spec, double* const* phys, int nf, int nzp,
                   const double* const* means, const int* modes, bool f32 = false, double scale = 1.0);
 void zgemm(lsb_handle* h, const Mat& m, const double* in, double* out, int nf, int epi, double alpha, double beta,

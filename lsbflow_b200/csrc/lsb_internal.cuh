@@ -115,6 +115,8 @@ struct RowIO {
     double add_mean;    // c2r only: 0 or 1 -> add mean[k] to the physical row (u + ubar)
     const double* mean; // [nzp] or nullptr
     double scale;       // c2r only: the physical row is scale * c2r (+ mean)
+    const double* lam;  // r2c only: fringe lambda(x) [nxl] or nullptr; the row read is then
+                        // lambda(x) (m - q(x)), m = mean[z] * add_mean (or 0), before the transform
 };
 struct RowArgs {
     int f32 = 0;                // 1: y-intermediate and physical rows in FP32 (mixed form)

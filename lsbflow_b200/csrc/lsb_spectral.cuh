@@ -72,12 +72,8 @@ void launch_pressure_project(double* u, double* v, double* p, const double* dw, 
                              const double* wavy, int nx, long long S, long long C, double dt, double bdfv,
                              cudaStream_t s);
 void launch_norm(double* f0, double* f1, double* f2, int nx, int ny, int nzp, int ifrz, cudaStream_t s);
-void launch_force_phys(const double* u0, const double* u1, const double* u2, double* f0, double* f1, double* f2,
-                       const double* lamx, const double* ubar, int nx, int ny, long long P, cudaStream_t s);
 void launch_axpby(double* y, const double* x, double a, double b, long long n, cudaStream_t s);
 void launch_tavg_add(double* a, const double* q, double iomod, long long n, cudaStream_t s);
-void launch_force_phys_f32(const double* up, const double* u1, const double* u2, double* f0, double* f1, double* f2,
-                           const double* lamx, int nx, long long P, cudaStream_t s);
 void launch_add_half_sq(double* h11, const double* ubar, long long C, int nzp, cudaStream_t s);
 
 }  // namespace lsb

@@ -278,7 +278,8 @@ RowArgs rowargs(lsb_handle* h, bool padded, int nzp) {
 namespace lsb {
 // horfft(-1): physical (unpadded, [nzp][ny][nx]) -> spectral, nf fields
 void phys_to_spec(lsb_handle* h, const double* const* phys, double* const* spec, int nf, int nzp, double alpha,
-                  double beta, double* const* ybuf, bool f32) {
+                  double beta, double* const* ybuf, bool f32, const double* lam, const double* const* lmeans,
+                  int nlam) {
     for (int f0 = 0; f0 < nf; f0 += kMaxJobs) {
         const int n = std::min(kMaxJobs, nf - f0);
         RowJobList rj{};
@@ -286,7 +287,13 @@ void phys_to_spec(lsb_handle* h, const double* const* phys, double* const* spec,
         rj.n = yj.n = n;
         for (int i = 0; i < n; ++i) {
             double* y = ybuf ? ybuf[f0 + i] : h->Yu + (long long)i * h->Yu1;
-            rj.j[i] = RowIO{phys[f0 + i], y, YM_COPY, 0.0, nullptr, 1.0};
+            rj.j[i] = RowIO{phys[f0 + i], y, YM_COPY, 0.0, nullptr, 1.0, nullptr};
+            if (f0 + i < nlam) {
+                const double* m = lmeans ? lmeans[f0 + i] : nullptr;
+                rj.j[i].lam = lam;
+                rj.j[i].mean = m;
+                rj.j[i].add_mean = m ? 1.0 : 0.0;
+            }
             yj.j[i] = YFwdJob{y, spec[f0 + i], alpha, beta, 0};
         }
         RowArgs ra = rowargs(h, false, nzp);
@@ -415,11 +422,14 @@ void nlterm(lsb_handle* h, const double* uin, double* Nout) {
         means[3 + 2] = h->ubarp;
         const int nphys = (h->cfg.sgsflag == 1) ? 12 : 3;
         { TimerScope ts(h, "phys_fields"); spec_to_phys(h, spec, ph, nphys, d.nzp, means, modes, f32); }
-        // the forcing's physical fields in scratch fields 18..21 (the SGS model uses 12..17);
-        // with SGS they go to spectral space in the same launches as the stresses
-        double* fo[3] = {PH(18), PH(19), PH(20)};
+        // with SGS the forcing goes to spectral space in the same launches as the stresses
+        // (scratch field 21 holds the FP32 u' of the mixed form; the SGS model uses 12..17)
         double* no[3] = {Nout, Nout + S, Nout + 2 * S};
+        // the fringe forcing lambda(x) (ubar - u) (src/navierstokes.f90:191-204) is formed by the
+        // forward row transform as it reads u, v, w (k_row_r2c_*: RowIO::lam)
         const bool forcing = dealias && h->cfg.forcing == 1;
+        const double* fin[3] = {ph[0], ph[1], ph[2]};
+        const double* fmean[3] = {h->ubar, nullptr, nullptr};  // ph[0] holds u + ubar
         if (forcing) {
             TimerScope ts(h, "forcing");
             if (f32) {
@@ -428,15 +438,15 @@ void nlterm(lsb_handle* h, const double* uin, double* Nout) {
                 const double* sp1[1] = {uin};
                 double* pp1[1] = {up};
                 spec_to_phys(h, sp1, pp1, 1, d.nzp, nullptr, nullptr, true);
-                launch_force_phys_f32(up, ph[1], ph[2], fo[0], fo[1], fo[2], h->lamx, d.nx, P, h->stream);
-            } else {
-                launch_force_phys(ph[0], ph[1], ph[2], fo[0], fo[1], fo[2], h->lamx, h->ubar, d.nx, d.ny, P, h->stream);
+                fin[0] = up;
+                fmean[0] = nullptr;
             }
-            if (h->cfg.sgsflag != 1) phys_to_spec(h, fo, no, 3, d.nzp, 1.0, 1.0, nullptr, f32);
+            if (h->cfg.sgsflag != 1) phys_to_spec(h, fin, no, 3, d.nzp, 1.0, 1.0, nullptr, f32, h->lamx, fmean, 3);
         }
         if (h->cfg.sgsflag == 1) {
             TimerScope ts(h, "sgs_total");
-            sgs_add_tau(h, ph, dealias, forcing ? (const double* const*)fo : nullptr, forcing ? no : nullptr, forcing ? 3 : 0);
+            sgs_add_tau(h, ph, dealias, forcing ? fin : nullptr, forcing ? no : nullptr, forcing ? 3 : 0,
+                        forcing ? h->lamx : nullptr, fmean);
         }
     }
     // N_l -= d h_l1/dx + d h_l2/dy + d h_l3/dz

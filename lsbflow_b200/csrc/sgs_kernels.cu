@@ -704,7 +704,8 @@ static void model_tau(lsb_handle* h, const double* const* u, const double* const
 // nlterm hook: ph[0..2] = u_l (+ubar), ph[3+3l+m] = du_l/dx_m (physical fields of the
 // working type: FP32 in the mixed form); adds the forward transform of tau into the
 // spectral h fields.
-void sgs_add_tau(lsb_handle* h, double* const* ph, bool dealias, const double* const* xin, double* const* xout, int nx) {
+void sgs_add_tau(lsb_handle* h, double* const* ph, bool dealias, const double* const* xin, double* const* xout, int nx,
+                 const double* xlam, const double* const* xmeans) {
     const Dims& d = h->d;
     const long long P = h->P, S = d.S();
     SgsWork& s = h->sgs;
@@ -757,7 +758,7 @@ void sgs_add_tau(lsb_handle* h, double* const* ph, bool dealias, const double* c
                 hp[n++] = s.H9 + (3 * l + m) * S;
             }
     }
-    phys_to_spec(h, tp, hp, n, d.nzp, 1.0, 1.0, nullptr, f32);
+    phys_to_spec(h, tp, hp, n, d.nzp, 1.0, 1.0, nullptr, f32, xlam, xmeans, nx);
 }
 
 void sgs_tau_phys(lsb_handle* h, const double* ui, const double* g, const double* uiuj, double* tau) {

@@ -229,21 +229,6 @@ __global__ void k_norm(double* f0, double* f1, double* f2, int nx, int ny, int n
     }
 }
 
-// fringe forcing on the unpadded physical grid (src/navierstokes.f90:191-204); u0 holds u + ubar
-__global__ void k_force_phys(const double* __restrict__ u0, const double* __restrict__ u1,
-                             const double* __restrict__ u2, double* __restrict__ f0, double* __restrict__ f1,
-                             double* __restrict__ f2, const double* __restrict__ lamx,
-                             const double* __restrict__ ubar, int nx, int ny, long long P) {
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < P; e += (long long)gridDim.x * blockDim.x) {
-        const int x = (int)(e % nx);
-        const int k = (int)(e / ((long long)nx * ny));
-        const double l = lamx[x];
-        f0[e] = l * (ubar[k] - u0[e]);
-        f1[e] = l * (0.0 - u1[e]);
-        f2[e] = l * (0.0 - u2[e]);
-    }
-}
-
 __global__ void k_tavg_add(double* __restrict__ a, const double* __restrict__ q, double iomod, long long n) {
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
         a[e] = a[e] + q[e] / iomod;
@@ -308,27 +293,6 @@ void launch_pressure_project(double* u, double* v, double* p, const double* dw, 
 }
 void launch_norm(double* f0, double* f1, double* f2, int nx, int ny, int nzp, int ifrz, cudaStream_t s) {
     { lsb::note_launch(); k_norm<<<dim3(nzp, 3), 128, 0, s>>>(f0, f1, f2, nx, ny, nzp, ifrz); }
-}
-void launch_force_phys(const double* u0, const double* u1, const double* u2, double* f0, double* f1, double* f2,
-                       const double* lamx, const double* ubar, int nx, int ny, long long P, cudaStream_t s) {
-    { lsb::note_launch(); k_force_phys<<<nblk(P), 256, 0, s>>>(u0, u1, u2, f0, f1, f2, lamx, ubar, nx, ny, P); }
-}
-// mixed form: fringe forcing in FP32 from the perturbation u' (field without the mean)
-__global__ void k_force_phys_f32(const float* __restrict__ up, const float* __restrict__ u1,
-                                 const float* __restrict__ u2, float* __restrict__ f0, float* __restrict__ f1,
-                                 float* __restrict__ f2, const double* __restrict__ lamx, int nx, long long P) {
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < P; e += (long long)gridDim.x * blockDim.x) {
-        const float l = (float)lamx[(int)((unsigned)e % (unsigned)nx)];
-        f0[e] = -l * up[e];
-        f1[e] = -l * u1[e];
-        f2[e] = -l * u2[e];
-    }
-}
-void launch_force_phys_f32(const double* up, const double* u1, const double* u2, double* f0, double* f1, double* f2,
-                           const double* lamx, int nx, long long P, cudaStream_t s) {
-    auto c = [](const double* p) { return reinterpret_cast<const float*>(p); };
-    auto w = [](double* p) { return reinterpret_cast<float*>(p); };
-    { lsb::note_launch(); k_force_phys_f32<<<nblk(P), 256, 0, s>>>(c(up), c(u1), c(u2), w(f0), w(f1), w(f2), lamx, nx, P); }
 }
 
 // mixed form: the FP32 product kernel leaves 0.5 ubar(z)^2 out of h_11; its (kx, ky) = (0, 0)
