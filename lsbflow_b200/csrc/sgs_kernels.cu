@@ -248,19 +248,26 @@ void filter3_any(lsb_handle* h, const void* const* in, void* const* out, int n, 
         if (rowtile) {
             const int FJ = FR * 512 / d.nx;  // the thread map's rows (rows past ny are masked)
             const int nyb = (d.ny + FJ - 1) / FJ;
-            // z chunks: about four blocks per SM over the launch, at least 4 planes each
-            int nzc = (4 * 148 + nyb * fl.n - 1) / (nyb * fl.n);
-            nzc = std::max(1, std::min(nzc, (d.nzp + 3) / 4));
-            const int zch = (d.nzp + nzc - 1) / nzc;
-            nzc = (d.nzp + zch - 1) / zch;
-            dim3 grid(nyb, nzc, fl.n);
             const size_t es = f32 ? sizeof(float) : sizeof(double);
             const size_t sm = (size_t)RT_ST * (FJ + 2) * d.nx * es;
+            // z chunks: a block marches zch planes plus the two halo planes; pick the chunk
+            // count with the least (waves of resident blocks) x (planes per block)
+            const void* kf = f32 ? (const void*)k_filter3p<float> : (const void*)k_filter3p<double>;
+            const long long slots = std::max(1LL, (long long)resident_blocks(kf, 256, sm) * sm_count());
+            int zch = d.nzp;
+            double best = -1.0;
+            for (int c = 1; c <= std::max(1, (d.nzp + 3) / 4); ++c) {
+                const int zc = (d.nzp + c - 1) / c;
+                const int nc = (d.nzp + zc - 1) / zc;
+                const long long blocks = (long long)nyb * nc * fl.n;
+                const double cost = (double)((blocks + slots - 1) / slots) * (zc + 2);
+                if (best < 0.0 || cost < best) best = cost, zch = zc;
+            }
+            const int nzc = (d.nzp + zch - 1) / zch;
+            dim3 grid(nyb, nzc, fl.n);
             if (f32) {
-                if (sm > 48 * 1024) resident_blocks((const void*)k_filter3p<float>, 256, sm);  // raises the limit once
                 { lsb::note_launch(); k_filter3p<float><<<grid, 256, sm, h->stream>>>(fl, lgx, d.ny, d.nzp, FJ, zch, (float)a, (float)b, zf, zf + d.nzp, zf + 2 * d.nzp); }
             } else {
-                if (sm > 48 * 1024) resident_blocks((const void*)k_filter3p<double>, 256, sm);  // raises the limit once
                 { lsb::note_launch(); k_filter3p<double><<<grid, 256, sm, h->stream>>>(fl, lgx, d.ny, d.nzp, FJ, zch, a, b, zf, zf + d.nzp, zf + 2 * d.nzp); }
             }
         } else {
