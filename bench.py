@@ -13,6 +13,11 @@ time), inputs resident in HBM (the state, 24 FP64 fields = 405 MB, is larger tha
 
 With N > 1 (torchrun) every rank advances its own independent run (replicas: the
 path has no exchange step), so the job's throughput is the sum over ranks.
+
+Beside the headline the line carries the mixed-precision form of the same workload, a
+Poisson serving stream, and the batched ensemble (64 sigma-model members at 128 x 32 x 65
+with their own Re_delta*, dipole amplitude and position, stepped together with one CUDA
+graph launch per ensemble step) in both precisions.
 """
 from __future__ import annotations
 
@@ -168,6 +173,69 @@ def profiled_traffic(path: str):
     return None
 
 
+def run_ensemble(args, rank, world, stream, max_over_ranks, barrier):
+    """Members of the 128 x 32 x 64 (nzp 65) sigma-model ensemble (Re_delta* ~ U[300, 800],
+    A ~ U[0.1, 0.4], x0 ~ U[60, 100] delta*, noise 1e-3, seeds s0 + m) stepped together
+    through lsb_batch_step, in both precisions; beside it one member stepped alone."""
+    import torch
+    from lsbflow_b200 import lib, replicas
+    from lsbflow_b200.config import ensemble_configs
+
+    out = {"members": 0, "grid": "128x32x65 (ref nx,ny,nzp), padded 192x48", "model": "sigma",
+           "draws": "Re_d* ~ U[300,800], A ~ U[0.1,0.4], x0 ~ U[60,100] d*, noise 1e-3, seeds s0+m"}
+    steps = max(6, min(args.steps, 30))
+    for prec, name in ((0, "fp64"), (1, "mixed")):
+        cfgs = ensemble_configs(args.members, seed=3000 + rank, precision=prec)
+        sols = []
+        free = torch.cuda.mem_get_info()[0]
+        for m, cfg in enumerate(cfgs):
+            st = hs.make_setup(cfg)
+            s = lib.Solver(st)
+            u, v, w = ic.seeded_noise(st, replicas.replica_seed(5000 + m, rank), 1e-3)
+            s.upload(u, v, w, dt=st.dt)
+            sols.append(s)
+            if m == 0 and s.device_bytes() * len(cfgs) > 0.8 * free:
+                raise RuntimeError("ensemble does not fit in device memory")
+        pts_m = cfgs[0].nx * cfgs[0].ny * cfgs[0].nzp
+        b = lib.Batch(sols)
+        b.set_stream(stream.cuda_stream)
+        b.step(max(args.warmup, 3) + 6)  # start-up steps, then the 6 ensemble graphs are captured
+        torch.cuda.synchronize()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        n0 = lib.kernel_launches()
+        e0.record(stream)
+        b.step(steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        launches = lib.kernel_launches() - n0
+        ms = max_over_ranks(e0.elapsed_time(e1))
+        b.close()
+        # one member alone on the same stream (its own step graphs)
+        s0 = sols[0]
+        s0.set_stream(stream.cuda_stream)
+        s0.step(6)  # its own 6 step graphs are captured
+        torch.cuda.synchronize()
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        s0.step(steps)
+        a1.record(stream)
+        torch.cuda.synchronize()
+        ms1 = max_over_ranks(a0.elapsed_time(a1))
+        for s in sols:
+            s.close()
+        agg = replicas.job_throughput(pts_m * len(cfgs), steps, world, ms / 1e3)
+        one = replicas.job_throughput(pts_m, steps, world, ms1 / 1e3)
+        out["members"] = len(cfgs)
+        out[name] = {"value": agg, "unit": UNIT, "ms_per_ensemble_step": ms / steps,
+                     "single_member_value": one, "gain_vs_one_member": agg / one,
+                     "gpu_launches_per_ensemble_step": launches / steps, "timed_steps": steps}
+    out["mixed_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -179,6 +247,8 @@ def main():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--serve-runs", type=int, default=12)
+    ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--members", type=int, default=64)
     args = ap.parse_args()
     cfg = workload(args.workload)
     if args.impl == "reference":
@@ -338,6 +408,12 @@ def main():
                    "arrivals": "Poisson 4/s, seeded", "mix": "ens128 sigma / ens128 dyn-Smagorinsky / dns64",
                    "horizon_steps": [100, 400]}
 
+    # ---- batched ensemble: sigma-model LES members of one grid with their own Re_delta*,
+    # dipole amplitude and position, stepped together (one graph launch per ensemble step)
+    ensemble = None
+    if not args.no_ensemble:
+        ensemble = run_ensemble(args, rank, world, stream, max_over_ranks, barrier)
+
     # ---- the CPU baseline (rank 0, N = 1 only), bounded sample
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -364,6 +440,7 @@ def main():
             "cpu_baseline": cpu,
             "mixed": mixed,
             "serving": serving,
+            "ensemble": ensemble,
         }
         print(json.dumps(line), flush=True)
     sol.close()

@@ -128,6 +128,20 @@ int lsb_step(lsb_handle* h, int nsteps);
 /* enable = 0: drop the step graphs and launch every kernel of every step (no reference
  * counterpart) */
 int lsb_graphs(lsb_handle* h, int enable);
+/* Launch schedule of a handle (no reference counterpart; FFTW's plan search is the nearest
+ * analogue).  Zero fields keep the built-in models; a tuner (lsbflow_b200/autotune.py)
+ * times candidates through lsb_step and persists the fastest per grid as JSON.  Every
+ * schedule gives the same results bit for bit: it moves work between blocks, never the
+ * order of a sum. */
+typedef struct {
+    int gemm_warps;      /* FP64 z contractions: warps (8 columns each) per CTA, 4..8;
+                            0 = the wave-quantization model */
+    int filter_zchunks;  /* 3-point SGS test filter: z chunks a block column is split into,
+                            1..(nzp+3)/4; 0 = the waves x planes-per-block model */
+} lsb_schedule;
+/* out-of-range fields return LSB_ERR_ARG; the step graphs are dropped and re-captured */
+int lsb_set_schedule(lsb_handle* h, const lsb_schedule* s);
+int lsb_get_schedule(lsb_handle* h, lsb_schedule* s);
 int lsb_diag(lsb_handle* h, lsb_diagnostics* out);
 int lsb_synchronize(lsb_handle* h);
 /* asynchronous host<->device copies of u, v, w only (the histories stay resident);
@@ -146,6 +160,28 @@ int lsb_timer_report(lsb_handle* h, char* buf, int buflen);
  * about it, sqrt(mean_y (f - mean_y f)^2); mean and rms are host arrays [4][nzp][nx]
  * (field u, v, w, p; z; x) */
 int lsb_spanwise_stats(lsb_handle* h, double* mean, double* rms);
+
+/* ---------------- Ensembles: runs stepped together ----------------------------------- */
+/* No counterpart in the reference (one run per mpiexec there).  A batch steps several
+ * handles (ensemble members: same or different grids, Re, boundary forcing, precision)
+ * together: lsb_batch_step(b, n) advances every member by n calls of timestep(), with the
+ * results of lsb_step on each member alone, bit for bit.  When every member's step is
+ * steady (the lsb_step graph conditions), the members' steps are captured as parallel
+ * branches of one CUDA graph and each ensemble step is one graph launch on the batch's
+ * own stream; otherwise the members are stepped one by one on their own streams.  The
+ * batch does not own its members: destroy the batch before any member.  Work issued on a
+ * member's stream after lsb_batch_step is ordered after the batch's steps.  Not
+ * thread-safe; a member must not be stepped by another batch or thread meanwhile. */
+typedef struct lsb_batch lsb_batch;
+int lsb_batch_create(lsb_handle* const* members, int nmembers, lsb_batch** out);
+int lsb_batch_destroy(lsb_batch* b);
+int lsb_batch_step(lsb_batch* b, int nsteps);
+int lsb_batch_synchronize(lsb_batch* b);
+/* launch the ensemble graphs on a caller stream (cudaStream_t as void*; NULL restores the
+ * batch's own); an event recorded there after lsb_batch_step follows every member's steps */
+int lsb_batch_set_stream(lsb_batch* b, void* stream);
+/* enable = 0: drop the ensemble graphs and step the members one by one */
+int lsb_batch_graphs(lsb_batch* b, int enable);
 
 /* ---------------- Tier 1: the reference's subroutine interfaces (host arrays) --------- */
 /* horfft(ain, ainf, is)             src/horfft.f90:61      is = -1 phys->spec, +1 spec->phys */

@@ -130,7 +130,8 @@ def delta_star_to_x0(re_dstar: float, xnu: float = 0.001, u0: float = 1.0) -> fl
     return (dstar / 1.72) ** 2 * u0 / xnu
 
 
-def workload(name: str, **over) -> LsbConfig:
+def workload(name: str, re_d: float | None = None, bc_amp: float | None = None, bc_xc: float | None = None,
+             **over) -> LsbConfig:
     """Named workloads in the reference's axes (x stream, y span, z Chebyshev).
 
     dns64   : 64 x 16 x 64 (nzp 65) plain DNS, Re_d*=500, fringe 10%, dipole ceiling BC.
@@ -138,22 +139,27 @@ def workload(name: str, **over) -> LsbConfig:
               thickness), alpha d* = 0.25: the domain is one wavelength (linstab = 1).
     les256  : 256 x 64 x 128 (nzp 129) dynamic-Smagorinsky LES with the 3/2 rule.
     ens128  : 128 x 32 x 64 (nzp 65) sigma-model LES member.
-    Lengths are 200/20/20 displacement thicknesses (xlen/ylen/zlen).
+    Lengths are 200/20/20 displacement thicknesses (xlen/ylen/zlen).  ``re_d``, ``bc_amp``
+    and ``bc_xc`` (dipole centre in displacement thicknesses, default 80) override the
+    workload's Re_delta*, ceiling-dipole amplitude and position.
     """
     if name == "dns64":
-        re_d, amp, nx, ny, nz, sgs, model, dal = 500.0, 0.3, 64, 16, 64, 0, 0, 1
+        re_d_default, amp, nx, ny, nz, sgs, model, dal = 500.0, 0.3, 64, 16, 64, 0, 0, 1
         dt = 0.01
     elif name == "os128":
-        re_d, amp, nx, ny, nz, sgs, model, dal = 1000.0, 0.0, 128, 4, 96, 0, 0, 0
+        re_d_default, amp, nx, ny, nz, sgs, model, dal = 1000.0, 0.0, 128, 4, 96, 0, 0, 0
         dt = 0.005
     elif name == "les256":
-        re_d, amp, nx, ny, nz, sgs, model, dal = 800.0, 0.35, 256, 64, 128, 1, 1, 1
+        re_d_default, amp, nx, ny, nz, sgs, model, dal = 800.0, 0.35, 256, 64, 128, 1, 1, 1
         dt = 0.005
     elif name == "ens128":
-        re_d, amp, nx, ny, nz, sgs, model, dal = 500.0, 0.3, 128, 32, 64, 1, 2, 1
+        re_d_default, amp, nx, ny, nz, sgs, model, dal = 500.0, 0.3, 128, 32, 64, 1, 2, 1
         dt = 0.005
     else:
         raise ValueError(f"unknown workload {name!r}")
+    re_d = re_d if re_d is not None else re_d_default
+    amp = bc_amp if bc_amp is not None else amp
+    xc = bc_xc if bc_xc is not None else 80.0
     xnu, u0 = 0.001, 1.0
     dstar = re_d * xnu / u0
     cfg = LsbConfig(
@@ -161,7 +167,7 @@ def workload(name: str, **over) -> LsbConfig:
         x0=delta_star_to_x0(re_d, xnu, u0),
         xlen=200.0 * dstar, ylen=20.0 * dstar, zlen=20.0 * dstar,
         mapping=2, blfac=8.0, dtadapt=0, dt_fixed=dt,
-        bctype=3 if amp > 0 else 0, bc3_amp=amp, bc3_xc=80.0 * dstar, bc3_s=15.0 * dstar,
+        bctype=3 if amp > 0 else 0, bc3_amp=amp, bc3_xc=xc * dstar, bc3_s=15.0 * dstar,
         forcing=1 if name != "os128" else 0, fsize=0.1, lfsize=0.25, sfsize=0.70,
         sgsflag=sgs, sgsmodel=model, dealiasflag=dal, dealias_layout="correct",
         a=1.0, b=6.0, ic=2,
@@ -172,3 +178,16 @@ def workload(name: str, **over) -> LsbConfig:
         cfg = dataclasses.replace(cfg, linstab=1, astar=alpha * 6.02 * math.sqrt(xnu * cfg.x0 / u0),
                                   cguess=0.36 + 0.0j, zlen=20.0 * dstar, nsteps=500)
     return dataclasses.replace(cfg, **over)
+
+
+def ensemble_configs(n: int, seed: int, base: str = "ens128", **over) -> list:
+    """Ensemble members of one grid: Re_delta* ~ U[300, 800], ceiling-dipole amplitude
+    A ~ U[0.1, 0.4] and centre x0 ~ U[60, 100] displacement thicknesses, drawn from a
+    seeded generator (member m's noise seed is the caller's, e.g. seed + m)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        re_d, amp, xc = rng.uniform(300.0, 800.0), rng.uniform(0.1, 0.4), rng.uniform(60.0, 100.0)
+        out.append(workload(base, re_d=float(re_d), bc_amp=float(amp), bc_xc=float(xc), **over))
+    return out

@@ -228,6 +228,7 @@ void gemm_pick(const GemmArgs& g, cudaStream_t s) {
     if (e6 > best + 0.02) best = e6, nw = 6;
     if (e5 > best + 0.02) best = e5, nw = 5;
     if (e4 > best + 0.02) best = e4, nw = 4;
+    if (g.nw >= 4 && g.nw <= 8) nw = g.nw;  // a tuned schedule overrides the model
     switch (nw) {
         case 8: gemm_launch_t<MT, 8>(g, s); break;
         case 7: gemm_launch_t<MT, 7>(g, s); break;

@@ -100,6 +100,7 @@ struct lsb_handle {
     };
     std::vector<StepGraph> graphs;
     bool graphs_on = true;
+    lsb_schedule sched{};  // launch schedule (lsb_set_schedule); zeros: the built-in models
     void drop_graphs() {
         for (auto& g : graphs)
             if (g.exec) cudaGraphExecDestroy(g.exec);

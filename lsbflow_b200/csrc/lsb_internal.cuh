@@ -187,6 +187,7 @@ struct GemmArgs {
     // optional per-field pointers (fields that are not a fixed stride apart); used when set
     const double* inf[4];
     double* outf[4];
+    int nw;                 // CTA width in warps, 4..8, set by the handle's schedule; 0: wave model
 };
 void launch_gemm(const GemmArgs& g, cudaStream_t s);
 void launch_spanwise_stats(const double* ph, double* mean, double* rms, int nf, int nx, int ny, int nzp, long long P,

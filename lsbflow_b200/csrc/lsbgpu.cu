@@ -188,6 +188,7 @@ GemmArgs gemm_base(lsb_handle* h, const Mat& m) {
     g.ht = h->ht;
     g.d2hb = h->d2hb;
     g.d2ht = h->d2ht;
+    g.nw = h->sched.gemm_warps;
     return g;
 }
 
@@ -860,6 +861,175 @@ bool graph_step(lsb_handle* h, Body&& body) {
     return false;
 }
 
+// one timestep() on the handle's stream with ordinary launches: the update, then dt
+// adaptation (src/navierstokes.f90:78-87) and the on-the-fly averages (src/main.f90:70-76)
+void run_step(lsb_handle* h) {
+    const lsb_config& c = h->cfg;
+    const long long S = h->d.S();
+    step_one(h);
+    check_launch();
+    // adaptive dt: NaN check + maxcalc every 5 steps and every iomod steps
+    if (c.dtadapt == 1 && (h->istep % c.iomod == 0 || h->istep % 5 == 0)) {
+        lsb_diagnostics dg;
+        diag_compute(h, &dg);
+        if (dg.nonfinite) fail(LSB_ERR_NONFINITE, "NaN detected at step " + std::to_string(h->istep));
+        const bool exceed = dg.cflz > 0.45 || dg.cflx > 0.25 || dg.cfly > 0.25;
+        const bool below = dg.cflz < 0.25 && dg.cflx < 0.10 && dg.cfly < 0.12 && h->dt < 1.0;
+        if (exceed || below) {
+            const double cdt = exceed ? 1.25 : 1.0 / 1.25;
+            h->dt2 = h->dt;
+            h->dt = h->dt / cdt;
+        }
+    }
+    // on-the-fly averages: q_tavg += q / iomod
+    if (c.otfavg == 1 && h->istep > c.istartavg) {
+        const double* q[4] = {h->vel, h->vel + S, h->vel + 2 * S, h->p};
+        for (int k = 0; k < 4; ++k) launch_tavg_add(h->tavg + k * S, q[k], (double)c.iomod, S, h->stream);
+    }
+}
+
+// one step of one handle: from its step graphs when steady, else ordinary launches
+void step_once(lsb_handle* h) {
+    if (graph_step(h, [h] { run_step(h); })) return;
+    run_step(h);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- ensembles
+// Runs stepped together (lsb_batch_*): every batch step advances each member by one
+// timestep().  When every member's step is steady (graph_eligible), the members' steps are
+// captured as parallel branches of ONE CUDA graph (fork from the batch stream onto each
+// member's stream, join back) and replayed with one graph launch per ensemble step, so the
+// members' kernels overlap on the device and the host issues one launch instead of one per
+// member kernel.  The ensemble key is every member's step-graph key; the members advance in
+// lockstep, so their history rotations stay in phase and at most 6 ensemble graphs exist.
+struct lsb_batch {
+    std::vector<lsb_handle*> m;
+    cudaStream_t own = nullptr;      // the batch's own stream
+    cudaStream_t stream = nullptr;   // ensemble graphs are launched here (own or the caller's)
+    cudaEvent_t fork = nullptr;      // batch stream -> member streams
+    std::vector<cudaEvent_t> join;   // member stream i -> batch stream
+    struct EnsGraph {
+        cudaGraphExec_t exec = nullptr;
+        std::vector<const void*> key;
+        std::vector<double> sc;      // per member: dt, ctop, cwa, cwb
+        unsigned long long kernels = 0;
+    };
+    std::vector<EnsGraph> graphs;
+    bool graphs_on = true;
+    bool on_batch = false;  // the members' latest work is on the batch stream
+    void drop_graphs() {
+        for (auto& g : graphs)
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+        graphs.clear();
+    }
+    ~lsb_batch() {
+        if (stream) cudaStreamSynchronize(stream);
+        drop_graphs();
+        for (auto e : join)
+            if (e) cudaEventDestroy(e);
+        if (fork) cudaEventDestroy(fork);
+        if (own) cudaStreamDestroy(own);
+    }
+};
+
+namespace {
+
+// member streams wait for the batch stream (after ensemble replays)
+void batch_to_members(lsb_batch* b) {
+    if (!b->on_batch) return;
+    CK(cudaEventRecord(b->fork, b->stream));
+    for (lsb_handle* h : b->m) CK(cudaStreamWaitEvent(h->stream, b->fork, 0));
+    b->on_batch = false;
+}
+
+// the batch stream waits for every member stream (before ensemble replays)
+void members_to_batch(lsb_batch* b) {
+    if (b->on_batch) return;
+    for (size_t i = 0; i < b->m.size(); ++i) {
+        CK(cudaEventRecord(b->join[i], b->m[i]->stream));
+        CK(cudaStreamWaitEvent(b->stream, b->join[i], 0));
+    }
+    b->on_batch = true;
+}
+
+// one ensemble step from an ensemble graph (replayed, or captured now); false: some member
+// is not steady, or capture is unavailable, and the caller steps the members one by one
+bool batch_graph_step(lsb_batch* b) {
+    if (!b->graphs_on) return false;
+    const size_t n = b->m.size();
+    std::vector<const void*> key;
+    std::vector<double> sc;
+    key.reserve(8 * n);
+    sc.reserve(4 * n);
+    for (lsb_handle* h : b->m) {
+        if (!graph_eligible(h)) return false;
+        double ctop = 0, cwa = 0, cwb = 0;
+        bound_coeffs(h, h->t, ctop, cwa, cwb);
+        const void* k[8] = {h->vel, h->veln, h->velnm, h->nlc, h->nln, h->nlnm, h->p, h->pn};
+        key.insert(key.end(), k, k + 8);
+        const double s[4] = {h->dt, ctop, cwa, cwb};
+        sc.insert(sc.end(), s, s + 4);
+    }
+    members_to_batch(b);
+    for (auto& g : b->graphs) {
+        if (g.key != key || g.sc != sc) continue;
+        CK(cudaGraphLaunch(g.exec, b->stream));
+        lsb::note_launches((long long)g.kernels);
+        for (lsb_handle* h : b->m) replay_advance(h);
+        return true;
+    }
+    if (b->graphs.size() >= 6) b->drop_graphs();  // a member's scalars changed
+    std::vector<HostStep> snap;
+    snap.reserve(n);
+    for (lsb_handle* h : b->m) snap.push_back(save_host(h));
+    const unsigned long long k0 = lsb::launches_so_far();
+    if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        b->graphs_on = false;
+        return false;
+    }
+    bool ok = cudaEventRecord(b->fork, b->stream) == cudaSuccess;
+    for (size_t i = 0; ok && i < n; ++i) {
+        lsb_handle* h = b->m[i];
+        if (cudaStreamWaitEvent(h->stream, b->fork, 0) != cudaSuccess) {
+            ok = false;
+            break;
+        }
+        try {
+            run_step(h);
+        } catch (...) {
+            ok = false;
+        }
+        // join this member back even after a failure, so that the capture can end
+        if (cudaEventRecord(b->join[i], h->stream) != cudaSuccess ||
+            cudaStreamWaitEvent(b->stream, b->join[i], 0) != cudaSuccess)
+            ok = false;
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
+    cudaGraphExec_t exec = nullptr;
+    if (ok && e == cudaSuccess && graph != nullptr && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
+        cudaGraphDestroy(graph);
+        lsb_batch::EnsGraph g;
+        g.key = std::move(key);
+        g.sc = std::move(sc);
+        g.kernels = lsb::launches_so_far() - k0;
+        g.exec = exec;
+        b->graphs.push_back(std::move(g));
+        CK(cudaGraphLaunch(exec, b->stream));  // the captured step has not run yet
+        return true;
+    }
+    // capture did not work: undo the members' host side, step them one by one
+    cudaGetLastError();
+    if (graph) cudaGraphDestroy(graph);
+    for (size_t i = 0; i < n; ++i) restore_host(b->m[i], snap[i]);
+    lsb::note_launches(-(long long)(lsb::launches_so_far() - k0));
+    b->graphs_on = false;
+    return false;
+}
+
 }  // namespace
 
 namespace lsb {
@@ -1187,34 +1357,110 @@ int lsb_step(lsb_handle* h, int nsteps) {
         if (!h) fail(LSB_ERR_ARG, "null handle");
         if (nsteps < 0) fail(LSB_ERR_ARG, "nsteps < 0");
         if (!(h->dt > 0.0) || !std::isfinite(h->dt)) fail(LSB_ERR_STATE, "dt must be finite and > 0");
-        const lsb_config& c = h->cfg;
-        const long long S = h->d.S();
-        auto body = [&] {
-            step_one(h);
-            check_launch();
-            // adaptive dt: NaN check + maxcalc every 5 steps and every iomod steps
-            if (c.dtadapt == 1 && (h->istep % c.iomod == 0 || h->istep % 5 == 0)) {
-                lsb_diagnostics dg;
-                diag_compute(h, &dg);
-                if (dg.nonfinite) fail(LSB_ERR_NONFINITE, "NaN detected at step " + std::to_string(h->istep));
-                const bool exceed = dg.cflz > 0.45 || dg.cflx > 0.25 || dg.cfly > 0.25;
-                const bool below = dg.cflz < 0.25 && dg.cflx < 0.10 && dg.cfly < 0.12 && h->dt < 1.0;
-                if (exceed || below) {
-                    const double cdt = exceed ? 1.25 : 1.0 / 1.25;
-                    h->dt2 = h->dt;
-                    h->dt = h->dt / cdt;
-                }
-            }
-            // on-the-fly averages (src/main.f90:70-76): q_tavg += q / iomod
-            if (c.otfavg == 1 && h->istep > c.istartavg) {
-                const double* q[4] = {h->vel, h->vel + S, h->vel + 2 * S, h->p};
-                for (int k = 0; k < 4; ++k) launch_tavg_add(h->tavg + k * S, q[k], (double)c.iomod, S, h->stream);
-            }
-        };
-        for (int i = 0; i < nsteps; ++i) {
-            if (graph_step(h, body)) continue;
-            body();
+        for (int i = 0; i < nsteps; ++i) step_once(h);
+    });
+}
+
+// ---------------------------------------------------------------- ensembles (lsb_batch_*)
+int lsb_batch_create(lsb_handle* const* members, int nmembers, lsb_batch** out) {
+    return guard([&] {
+        if (!members || !out || nmembers < 1) fail(LSB_ERR_ARG, "need an array of at least one member handle");
+        *out = nullptr;
+        for (int i = 0; i < nmembers; ++i) {
+            if (!members[i]) fail(LSB_ERR_ARG, "null member handle " + std::to_string(i));
+            for (int j = 0; j < i; ++j)
+                if (members[j] == members[i]) fail(LSB_ERR_ARG, "member " + std::to_string(i) + " appears twice");
         }
+        std::unique_ptr<lsb_batch> b(new lsb_batch);
+        b->m.assign(members, members + nmembers);
+        CK(cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking));
+        b->stream = b->own;
+        CK(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+        b->join.assign(nmembers, nullptr);
+        for (int i = 0; i < nmembers; ++i) CK(cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming));
+        *out = b.release();
+    });
+}
+
+int lsb_batch_destroy(lsb_batch* b) {
+    return guard([&] { delete b; });
+}
+
+int lsb_batch_step(lsb_batch* b, int nsteps) {
+    return guard([&] {
+        if (!b) fail(LSB_ERR_ARG, "null batch");
+        if (nsteps < 0) fail(LSB_ERR_ARG, "nsteps < 0");
+        for (size_t i = 0; i < b->m.size(); ++i) {
+            const double dt = b->m[i]->dt;
+            if (!(dt > 0.0) || !std::isfinite(dt))
+                fail(LSB_ERR_STATE, "member " + std::to_string(i) + ": dt must be finite and > 0");
+        }
+        try {
+            for (int s = 0; s < nsteps; ++s) {
+                if (batch_graph_step(b)) continue;
+                batch_to_members(b);
+                for (lsb_handle* h : b->m) step_once(h);
+            }
+            // both ways: an event recorded on the batch stream now follows every member's
+            // steps, and work queued on a member's stream follows the ensemble replays
+            members_to_batch(b);
+            batch_to_members(b);
+        } catch (...) {
+            if (b->on_batch) {  // keep the members ordered after the batch's launches
+                cudaEventRecord(b->fork, b->stream);
+                for (lsb_handle* h : b->m) cudaStreamWaitEvent(h->stream, b->fork, 0);
+                b->on_batch = false;
+            }
+            throw;
+        }
+    });
+}
+
+int lsb_batch_set_stream(lsb_batch* b, void* stream) {
+    return guard([&] {
+        if (!b) fail(LSB_ERR_ARG, "null batch");
+        CK(cudaStreamSynchronize(b->stream));
+        b->stream = stream ? (cudaStream_t)stream : b->own;
+    });
+}
+
+int lsb_batch_synchronize(lsb_batch* b) {
+    return guard([&] {
+        if (!b) fail(LSB_ERR_ARG, "null batch");
+        CK(cudaStreamSynchronize(b->stream));
+        for (lsb_handle* h : b->m) CK(cudaStreamSynchronize(h->stream));
+        check_launch();
+        for (lsb_handle* h : b->m) check_uerr(h);
+    });
+}
+
+int lsb_batch_graphs(lsb_batch* b, int enable) {
+    return guard([&] {
+        if (!b) fail(LSB_ERR_ARG, "null batch");
+        CK(cudaStreamSynchronize(b->stream));
+        b->drop_graphs();
+        b->graphs_on = enable != 0;
+    });
+}
+
+int lsb_set_schedule(lsb_handle* h, const lsb_schedule* s) {
+    return guard([&] {
+        if (!h || !s) fail(LSB_ERR_ARG, "null argument");
+        if (s->gemm_warps != 0 && (s->gemm_warps < 4 || s->gemm_warps > 8))
+            fail(LSB_ERR_ARG, "gemm_warps must be 0 or 4..8");
+        const int zmax = std::max(1, (h->d.nzp + 3) / 4);
+        if (s->filter_zchunks < 0 || s->filter_zchunks > zmax)
+            fail(LSB_ERR_ARG, "filter_zchunks must be 0.." + std::to_string(zmax));
+        CK(cudaStreamSynchronize(h->stream));
+        h->drop_graphs();
+        h->sched = *s;
+    });
+}
+
+int lsb_get_schedule(lsb_handle* h, lsb_schedule* s) {
+    return guard([&] {
+        if (!h || !s) fail(LSB_ERR_ARG, "null argument");
+        *s = h->sched;
     });
 }
 

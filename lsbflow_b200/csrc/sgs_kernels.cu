@@ -263,6 +263,8 @@ void filter3_any(lsb_handle* h, const void* const* in, void* const* out, int n, 
                 const double cost = (double)((blocks + slots - 1) / slots) * (zc + 2);
                 if (best < 0.0 || cost < best) best = cost, zch = zc;
             }
+            const int force = h->sched.filter_zchunks;  // a tuned schedule overrides the model
+            if (force >= 1 && force <= std::max(1, (d.nzp + 3) / 4)) zch = (d.nzp + force - 1) / force;
             const int nzc = (d.nzp + zch - 1) / zch;
             dim3 grid(nyb, nzc, fl.n);
             if (f32) {

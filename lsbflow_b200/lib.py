@@ -28,6 +28,8 @@ EXPORTS = [
     "lsb_lapl", "lsb_divuv", "lsb_solve_helmholtz", "lsb_solve_nhom_helmholtz", "lsb_nlterm", "lsb_tau_sgs",
     "lsb_upload_velocity", "lsb_download_velocity", "lsb_timers", "lsb_timer_report",
     "lsb_solve_helmholtz_noalloc", "lsb_tavg", "lsb_spanwise_stats", "lsb_graphs", "lsb_kernel_launches", "lsb_device_bytes",
+    "lsb_batch_create", "lsb_batch_destroy", "lsb_batch_step", "lsb_batch_synchronize", "lsb_batch_graphs",
+    "lsb_batch_set_stream", "lsb_set_schedule", "lsb_get_schedule",
 ]
 
 
@@ -67,6 +69,10 @@ class LsbDiagC(C.Structure):
         ("energy_total", C.c_double), ("energy_pert", C.c_double), ("t", C.c_double), ("dt", C.c_double),
         ("istep", C.c_int), ("nonfinite", C.c_int),
     ]
+
+
+class LsbScheduleC(C.Structure):
+    _fields_ = [("gemm_warps", C.c_int), ("filter_zchunks", C.c_int)]
 
 
 _lib = None
@@ -215,6 +221,18 @@ class Solver:
     def synchronize(self):
         _ck(self._lib.lsb_synchronize(self._h))
 
+    def set_schedule(self, sched: dict | None):
+        """Launch schedule ({"gemm_warps": 0|4..8, "filter_zchunks": 0|1..}); None or zeros:
+        the built-in models.  Results do not depend on it."""
+        sched = sched or {}
+        sc = LsbScheduleC(int(sched.get("gemm_warps", 0)), int(sched.get("filter_zchunks", 0)))
+        _ck(self._lib.lsb_set_schedule(self._h, C.byref(sc)))
+
+    def schedule(self) -> dict:
+        sc = LsbScheduleC()
+        _ck(self._lib.lsb_get_schedule(self._h, C.byref(sc)))
+        return {f: getattr(sc, f) for f, _ in LsbScheduleC._fields_}
+
     def device_bytes(self) -> int:
         b = C.c_ulonglong()
         _ck(self._lib.lsb_device_bytes(self._h, C.byref(b)))
@@ -341,3 +359,45 @@ class Solver:
         out = np.empty((3, 3) + self.phys_shape())
         _ck(self._lib.lsb_tau_sgs(self._h, _ptr(a), _ptr(b), _ptr(g), _ptr(out)))
         return out
+
+
+class Batch:
+    """Ensemble members stepped together (``lsb_batch_*``).
+
+    ``members`` are open ``Solver`` objects; the batch does not own them and must be closed
+    before any of them.  ``step(n)`` advances every member by n time steps, each member's
+    result being the one it reaches when stepped alone.
+    """
+
+    def __init__(self, members):
+        lib = load()
+        self.members = list(members)
+        arr = (C.c_void_p * len(self.members))(*[m._h.value for m in self.members])
+        self._b = C.c_void_p()
+        _ck(lib.lsb_batch_create(arr, C.c_int(len(self.members)), C.byref(self._b)))
+        self._lib = lib
+
+    def close(self):
+        if getattr(self, "_b", None) and self._b.value:
+            self._lib.lsb_batch_destroy(self._b)
+            self._b = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, n: int = 1):
+        _ck(self._lib.lsb_batch_step(self._b, C.c_int(n)))
+
+    def synchronize(self):
+        _ck(self._lib.lsb_batch_synchronize(self._b))
+
+    def set_stream(self, stream_handle: int | None):
+        """Ensemble graphs go to this CUDA stream (raw handle); None restores the batch's own."""
+        _ck(self._lib.lsb_batch_set_stream(self._b, C.c_void_p(stream_handle or 0)))
+
+    def graphs(self, enable: bool):
+        """One graph launch per ensemble step when steady (default), or member by member."""
+        _ck(self._lib.lsb_batch_graphs(self._b, C.c_int(1 if enable else 0)))

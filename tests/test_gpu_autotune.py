@@ -1,0 +1,66 @@
+"""Launch schedules (lsb_set_schedule) change speed only: every schedule gives the results
+of the built-in models bit for bit, and the tuner stores a valid schedule per grid."""
+import numpy as np
+import pytest
+
+from lsbflow_b200 import autotune as A
+from lsbflow_b200 import hostsetup as hs
+from lsbflow_b200 import ic
+from lsbflow_b200.config import workload
+
+pytestmark = pytest.mark.gpu
+
+KEYS = ("uf", "vf", "wf", "pf", "pnf", "unif", "nlnif")
+
+
+def run(st, u, v, w, sched, n=12):
+    from lsbflow_b200 import lib
+    s = lib.Solver(st)
+    try:
+        s.set_schedule(sched)
+        assert s.schedule() == {"gemm_warps": sched.get("gemm_warps", 0),
+                                "filter_zchunks": sched.get("filter_zchunks", 0)}
+        s.upload(u, v, w, dt=st.dt)
+        s.step(n)
+        return s.download()
+    finally:
+        s.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "mixed"])
+def test_schedules_are_bit_identical(precision):
+    cfg = workload("les256", nx=64, ny=16, nz=32, precision=precision)   # dynamic model: filtered
+    st = hs.make_setup(cfg)
+    u, v, w = ic.seeded_noise(st, 8, 1e-2)
+    ref = run(st, u, v, w, {})
+    zmax = max(1, (cfg.nzp + 3) // 4)
+    for sched in ({"gemm_warps": 4}, {"gemm_warps": 7, "filter_zchunks": 1},
+                  {"gemm_warps": 8, "filter_zchunks": zmax}, {"filter_zchunks": 2}):
+        got = run(st, u, v, w, sched)
+        for k in KEYS:
+            assert np.array_equal(got[k], ref[k]), (sched, k)
+
+
+def test_set_schedule_rejects_out_of_range():
+    from lsbflow_b200 import lib
+    st = hs.make_setup(workload("dns64", nx=32, ny=8, nz=32))
+    s = lib.Solver(st)
+    try:
+        for bad in ({"gemm_warps": 3}, {"gemm_warps": 9}, {"filter_zchunks": -1},
+                    {"filter_zchunks": (st.cfg.nzp + 3) // 4 + 1}):
+            with pytest.raises(lib.LsbError):
+                s.set_schedule(bad)
+        assert s.schedule() == {"gemm_warps": 0, "filter_zchunks": 0}
+    finally:
+        s.close()
+
+
+def test_tune_and_store(tmp_path):
+    st = hs.make_setup(workload("les256", nx=64, ny=16, nz=32))
+    path = str(tmp_path / "schedules.json")
+    res = A.tune_and_store(st, path, steps=3, reps=1)
+    got = A.lookup(st.cfg, path, res["device"])
+    assert got == res["schedule"]
+    c = A.candidates(st.cfg)
+    assert got["gemm_warps"] in c["gemm_warps"] and got["filter_zchunks"] in c["filter_zchunks"]
+    assert res["ms_per_step"] <= res["model_ms_per_step"] and res["ms_per_step"] > 0
