@@ -412,7 +412,10 @@ def main():
     # dipole amplitude and position, stepped together (one graph launch per ensemble step)
     ensemble = None
     if not args.no_ensemble:
-        ensemble = run_ensemble(args, rank, world, stream, max_over_ranks, barrier)
+        try:
+            ensemble = run_ensemble(args, rank, world, stream, max_over_ranks, barrier)
+        except Exception as e:  # reported in the line; the headline above stands on its own
+            ensemble = {"error": f"{type(e).__name__}: {e}"}
 
     # ---- the CPU baseline (rank 0, N = 1 only), bounded sample
     cpu = None

@@ -20,7 +20,8 @@ KEYS = ("uf", "vf", "wf", "pf", "pnf", "unif", "unmif", "nlnif", "nlnmif")
 
 
 def members():
-    cfgs = ensemble_configs(3, seed=5, nx=64, ny=16, nz=32)           # sigma-model LES draws
+    # the mixed form needs register-plan transform lengths: padded x/2 = 96 = 32 x 3
+    cfgs = ensemble_configs(3, seed=5, nx=128, ny=16, nz=32)          # sigma-model LES draws
     cfgs.append(cfgs[0].replace(precision=1))                         # mixed form of member 0
     cfgs.append(workload("dns64", nx=32, ny=8, nz=32, dealiasflag=1))  # another grid
     out = []
