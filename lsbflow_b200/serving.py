@@ -13,6 +13,13 @@ HBM from admission to result.  The loop works at step boundaries:
 * completion -- a run that has done its steps is downloaded, its handle freed, and its
   slot and memory go to the next arrival.
 
+With ``group=True`` the runs of one shape (grid, model, dealiasing, averaging) form a
+cohort stepped through one ensemble batch (``lsb_batch_step``: one CUDA graph launch per
+ensemble step once the members are steady): at each cohort boundary finished runs leave,
+newly admitted runs of that shape join, and the cohort advances by the smallest of the
+chunk and its members' remaining steps.  A change of membership makes a new batch, whose
+ensemble graphs are captured over its next steps.
+
 Results do not depend on what else runs: handles share no device memory and every kernel
 of a run is on that run's stream.  ``percentiles`` gives p50/p99 of time-to-result
 (completion minus arrival) and the loop reports runs per hour and grid-point-steps/s.
@@ -93,6 +100,32 @@ class DeviceBackend:
     def ready(self, run) -> bool:
         return run["event"] is None or run["event"].query()
 
+    # ---- cohorts of same-shape runs stepped as one ensemble batch
+    def new_group(self):
+        return {"batch": None, "members": (), "event": None, "stream": self.torch.cuda.Stream()}
+
+    def launch_group(self, g, runs, nsteps: int):
+        ids = tuple(id(r) for r in runs)
+        if g["members"] != ids:
+            self.close_group(g)
+            g["batch"] = self.lib.Batch([r["solver"] for r in runs])
+            g["batch"].set_stream(g["stream"].cuda_stream)
+            g["members"] = ids
+        g["batch"].step(nsteps)
+        ev = self.torch.cuda.Event()
+        ev.record(g["stream"])
+        g["event"] = ev
+
+    def group_ready(self, g) -> bool:
+        return g["event"] is None or g["event"].query()
+
+    def close_group(self, g):
+        """Release the cohort's batch (before any member is finished and freed)."""
+        if g["batch"] is not None:
+            g["batch"].close()
+            g["batch"] = None
+            g["members"] = ()
+
     def finish(self, run) -> dict:
         run["stream"].synchronize()
         state = run["solver"].download()
@@ -116,6 +149,7 @@ class Server:
     max_active: int = 32
     chunk: int = 10
     footprints: dict = field(default_factory=dict)
+    group: bool = False                  # step same-shape runs as one ensemble batch
 
     def __post_init__(self):
         if self.backend is None:
@@ -132,7 +166,83 @@ class Server:
             raise ValueError(f"run {req.rid} needs {need} bytes, more than the budget {self.memory_budget}")
         self.queue.append(req)
 
+    def _admit(self, queue, now, n_active, used, t0, clock):
+        """Admits arrived requests, oldest first, no overtaking; yields (request, run, bytes)."""
+        while queue and queue[0].arrival <= now and n_active < self.max_active:
+            req = queue[0]
+            need = self.footprints.get(shape_key(req.cfg), estimate_bytes(req.cfg))
+            if used + need > self.memory_budget and n_active:
+                break
+            queue.pop(0)
+            run = self.backend.start(req)
+            nb = int(run.get("bytes") or need)
+            self.footprints[shape_key(req.cfg)] = nb
+            used += nb
+            n_active += 1
+            yield _Active(req, run, clock() - t0, req.nsteps, nb)
+
+    def _result(self, a: _Active, state: dict, done: float) -> RunResult:
+        c = a.req.cfg
+        return RunResult(a.req.rid, state, a.req.arrival, a.admitted, done, a.req.nsteps, c.nx * c.ny * c.nzp)
+
+    def _wait(self, progressed, busy, queue, clock, t0, idle_sleep):
+        if progressed:
+            return
+        if not busy and queue:
+            wait = queue[0].arrival - (clock() - t0)
+            if wait > 0:
+                time.sleep(min(wait, 0.05))
+        else:
+            time.sleep(idle_sleep)
+
+    def _run_grouped(self, clock, idle_sleep) -> list:
+        queue = sorted(self.queue, key=lambda r: (r.arrival, r.rid))
+        self.queue = []
+        cohorts: dict = {}   # shape -> {"runs": [...], "joining": [...], "g": backend group}
+        results = []
+        used = 0
+        t0 = clock()
+
+        def n_active():
+            return sum(len(c["runs"]) + len(c["joining"]) for c in cohorts.values())
+
+        try:
+            while queue or n_active():
+                for a in self._admit(queue, clock() - t0, n_active(), used, t0, clock):
+                    used += a.nbytes
+                    key = shape_key(a.req.cfg)
+                    if key not in cohorts:
+                        cohorts[key] = {"runs": [], "joining": [], "g": self.backend.new_group()}
+                    cohorts[key]["joining"].append(a)
+                progressed = False
+                for c in cohorts.values():
+                    if not (c["runs"] or c["joining"]) or not self.backend.group_ready(c["g"]):
+                        continue
+                    done = [a for a in c["runs"] if a.remaining == 0]
+                    if done:
+                        self.backend.close_group(c["g"])
+                        for a in done:
+                            results.append(self._result(a, self.backend.finish(a.run), clock() - t0))
+                            c["runs"].remove(a)
+                            used -= a.nbytes
+                    c["runs"] += c["joining"]
+                    c["joining"] = []
+                    if c["runs"]:
+                        k = min(self.chunk, min(a.remaining for a in c["runs"]))
+                        self.backend.launch_group(c["g"], [a.run for a in c["runs"]], k)
+                        for a in c["runs"]:
+                            a.remaining -= k
+                    progressed = progressed or bool(done) or bool(c["runs"])
+                self._wait(progressed, n_active() > 0, queue, clock, t0, idle_sleep)
+        finally:
+            for c in cohorts.values():
+                self.backend.close_group(c["g"])
+        self.elapsed = clock() - t0
+        return sorted(results, key=lambda r: r.rid)
+
     def run(self, clock=time.perf_counter, idle_sleep: float = 1e-4) -> list:
+        if self.group:
+            return self._run_grouped(clock, idle_sleep)
         queue = sorted(self.queue, key=lambda r: (r.arrival, r.rid))
         self.queue = []
         active: list = []

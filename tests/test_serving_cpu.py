@@ -15,6 +15,7 @@ class FakeBackend:
         self.in_use = 0
         self.peak = 0
         self.log = []
+        self.runs_by_rid = {}
 
     def free_bytes(self):
         return self.free
@@ -24,7 +25,9 @@ class FakeBackend:
         self.in_use += b
         self.peak = max(self.peak, self.in_use)
         self.log.append(("start", req.rid))
-        return {"rid": req.rid, "steps": 0, "polls": 0, "bytes": b}
+        run = {"rid": req.rid, "steps": 0, "polls": 0, "bytes": b}
+        self.runs_by_rid[req.rid] = run
+        return run
 
     def launch(self, run, n):
         run["steps"] += n
@@ -37,9 +40,41 @@ class FakeBackend:
         return True
 
     def finish(self, run):
+        assert not run.get("in_group"), "a run was finished while its cohort's batch held it"
         self.in_use -= run["bytes"]
         self.log.append(("finish", run["rid"]))
         return {"steps": run["steps"]}
+
+    # cohorts (Server(group=True)): one launch advances every member
+    def new_group(self):
+        return {"members": (), "polls": 0, "batches": 0}
+
+    def launch_group(self, g, runs, n):
+        ids = tuple(r["rid"] for r in runs)
+        if g["members"] != ids:
+            self.close_group(g)
+            g["members"] = ids
+            g["batches"] += 1
+            for r in runs:
+                r["in_group"] = True
+        for r in runs:
+            assert "polls" not in r or r["polls"] == 0
+            r["steps"] += n
+        g["polls"] = self.lag
+        self.log.append(("group", ids, n))
+
+    def group_ready(self, g):
+        if g["polls"] > 0:
+            g["polls"] -= 1
+            return False
+        return True
+
+    def close_group(self, g):
+        self.log.append(("close", g["members"]))
+        g["members"] = ()
+        # members of a closed batch may be finished
+        for r in self.runs_by_rid.values():
+            r["in_group"] = False
 
 
 def cfg(nx):
@@ -90,3 +125,44 @@ def test_poisson_requests_are_seeded():
     b = S.poisson_requests(8, 4.0, 7, shapes)
     assert [(r.arrival, r.nsteps, r.cfg.nx) for r in a] == [(r.arrival, r.nsteps, r.cfg.nx) for r in b]
     assert all(x.arrival < y.arrival for x, y in zip(a, a[1:]))
+
+
+def test_grouped_cohorts_step_together_and_finish_after_their_batch():
+    be = FakeBackend()
+    srv = S.Server(backend=be, memory_budget=100_000_000, chunk=7, group=True)
+    horizons = [10, 16, 13, 9, 20]
+    shapes = [cfg(32), cfg(32), cfg(64), cfg(32), cfg(64)]
+    for i, (n, c) in enumerate(zip(horizons, shapes)):
+        srv.submit(S.RunRequest(i, c, nsteps=n, arrival=0.0))
+    res = srv.run()
+    assert [r.rid for r in res] == list(range(5))
+    assert [r.state["steps"] for r in res] == horizons          # each run does exactly its steps
+    groups = [e for e in be.log if e[0] == "group"]
+    # runs of one shape advance together; the two shapes never share a launch
+    assert any(set(ids) == {0, 1, 3} for _, ids, _ in groups)
+    assert any(set(ids) == {2, 4} for _, ids, _ in groups)
+    assert all(set(ids) <= {0, 1, 3} or set(ids) <= {2, 4} for _, ids, _ in groups)
+    # a chunk never overshoots a member's horizon
+    assert all(n <= 7 for _, _, n in groups)
+    assert be.in_use == 0
+
+
+def test_grouped_admission_respects_budget_and_late_arrivals_join():
+    one = S.estimate_bytes(cfg(32))
+    be = FakeBackend()
+    t = [0.0]
+
+    def clock():
+        t[0] += 0.001
+        return t[0]
+
+    srv = S.Server(backend=be, memory_budget=int(2.5 * one), chunk=5, group=True)
+    for i in range(5):
+        srv.submit(S.RunRequest(i, cfg(32), nsteps=12, arrival=0.004 * i))
+    res = srv.run(clock=clock, idle_sleep=0.0)
+    assert [r.state["steps"] for r in res] == [12] * 5
+    assert be.peak <= 2 * one
+    starts = [rid for ev, rid, *_ in be.log if ev == "start"]
+    assert starts == sorted(starts)
+    sizes = {len(ids) for ev, ids, *_ in be.log if ev == "group"}
+    assert 2 in sizes                                  # a later arrival joined a running cohort
