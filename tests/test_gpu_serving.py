@@ -36,3 +36,21 @@ def test_results_same_alone_and_in_the_mix():
         assert got["istep"] == r.nsteps
         for k in ("uf", "vf", "wf", "pf"):
             assert np.array_equal(got[k], ref[k]), (r.rid, k, np.abs(got[k] - ref[k]).max())
+
+
+def test_grouped_cohorts_same_as_alone():
+    """Same-shape runs stepped as one ensemble batch (runs 0 and 3 share a grid; 3 joins
+    while 0 is stepping) reach the results they reach alone."""
+    reqs = requests()
+    srv = S.Server(chunk=5, group=True)
+    for r in reqs:
+        srv.submit(r)
+    grouped = {r.rid: r for r in srv.run()}
+    for r in reqs:
+        alone = S.Server(chunk=r.nsteps)
+        alone.submit(S.RunRequest(r.rid, r.cfg, r.nsteps, r.seed, r.amp, 0.0))
+        ref = alone.run()[0].state
+        got = grouped[r.rid].state
+        assert got["istep"] == r.nsteps
+        for k in ("uf", "vf", "wf", "pf"):
+            assert np.array_equal(got[k], ref[k]), (r.rid, k, np.abs(got[k] - ref[k]).max())
