@@ -173,6 +173,47 @@ def profiled_traffic(path: str):
     return None
 
 
+def run_profiles(args, st, u, v, w, stream):
+    """Spanwise mean and rms profiles of u + ubar, v, w, p (per z and x, as run/spanwiseavg.m
+    averages q snapshots over y), averaged in time over the second half of a long run, for
+    the FP64 and the mixed form from the same initial field; the relative L2 difference of
+    the mixed form's profiles from the FP64 ones per field."""
+    from lsbflow_b200 import lib
+
+    nsteps = max(20, args.profile_steps)
+    every = 20
+    out = {}
+    for prec in (0, 1):
+        s = lib.Solver(hs.make_setup(st.cfg.replace(precision=prec)) if prec else st)
+        s.set_stream(stream.cuda_stream)
+        s.upload(u, v, w, dt=st.dt)
+        acc_m = acc_r = None
+        n = 0
+        done = 0
+        while done < nsteps:
+            s.step(every)
+            done += every
+            if done > nsteps // 2:
+                m, r = s.spanwise_stats()
+                acc_m = m if acc_m is None else acc_m + m
+                acc_r = r if acc_r is None else acc_r + r
+                n += 1
+        s.close()
+        out[prec] = (acc_m / n, acc_r / n, n)
+    (m0, r0, n), (m1, r1, _) = out[0], out[1]
+    names = ("u", "v", "w", "p")
+
+    def rel(a, b):
+        return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+    em = {names[k]: rel(m1[k], m0[k]) for k in range(4)}
+    er = {names[k]: rel(r1[k], r0[k]) for k in range(4)}
+    return {"steps": nsteps, "average": f"steps {nsteps // 2 + every}..{nsteps}, every {every} ({n} samples)",
+            "rel_err_mean": em, "rel_err_rms": er,
+            "max_rel_err_mean_velocity": max(em[k] for k in "uvw"),
+            "max_rel_err_rms_velocity": max(er[k] for k in "uvw"), "target": 1e-4}
+
+
 def run_ensemble(args, rank, world, stream, max_over_ranks, barrier):
     """Members of the 128 x 32 x 64 (nzp 65) sigma-model ensemble (Re_delta* ~ U[300, 800],
     A ~ U[0.1, 0.4], x0 ~ U[60, 100] delta*, noise 1e-3, seeds s0 + m) stepped together
@@ -248,6 +289,8 @@ def main():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--serve-runs", type=int, default=12)
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-profiles", action="store_true")
+    ap.add_argument("--profile-steps", type=int, default=2000)
     ap.add_argument("--members", type=int, default=64)
     args = ap.parse_args()
     cfg = workload(args.workload)
@@ -391,6 +434,14 @@ def main():
                  "form": "FP32 transforms, products, physical fields and SGS; FP64 state, time integration, "
                          "boundary conditions, Chebyshev derivatives and eigenbasis solves"}
 
+    # ---- mean / rms profiles of the mixed form against FP64 after a long run
+    profiles = None
+    if not args.no_mixed and not args.no_profiles:
+        try:
+            profiles = run_profiles(args, st, u, v, w, stream)
+        except Exception as e:  # reported in the line; the headline stands on its own
+            profiles = {"error": f"{type(e).__name__}: {e}"}
+
     # ---- serving: a Poisson stream of ensemble runs (continuous batching on this GPU)
     serving = None
     if not args.no_serving:
@@ -457,6 +508,7 @@ def main():
             "mixed": mixed,
             "serving": serving,
             "ensemble": ensemble,
+            "profiles": profiles,
         }
         print(json.dumps(line), flush=True)
     sol.close()
