@@ -11,7 +11,10 @@
  *                                    ky in FFT order, k = 1 the ceiling, k = nzp the wall
  *      physical  (nx+2, ny, nzp)   : two pad columns per x row (written as 0, never read)
  *    nx, ny, nz are the reference's &dimen values, nzp = nz + 1, nzm = nz - 1.
- *  - Caller-owned host arrays are never retained.  Device state belongs to the handle.
+ *  - Caller-owned host arrays are not retained after a call returns, except by the
+ *    asynchronous copies of lsb_upload_velocity, lsb_download_velocity and
+ *    lsb_snapshot_async, which use them when the handle's stream reaches the copy.
+ *    Device state belongs to the handle.
  *  - A handle is one CUDA stream; it is not thread-safe, distinct handles are.
  *  - Temperature is not carried: the reference's set-up keeps T and its mean at exactly
  *    zero (src/init.f90:353-355,429), which makes every temperature term vanish.
@@ -160,6 +163,13 @@ int lsb_timer_report(lsb_handle* h, char* buf, int buflen);
  * about it, sqrt(mean_y (f - mean_y f)^2); mean and rms are host arrays [4][nzp][nx]
  * (field u, v, w, p; z; x) */
 int lsb_spanwise_stats(lsb_handle* h, double* mean, double* rms);
+/* the fields mpi_snapshot writes to a q file (src/mpi_io.f90:339-497): horfft(+1) of the
+ * current state on the device, u + ubar, v, w, p as q[4][nzp][ny][nx] (x fastest, no pad
+ * columns), copied to the host array q on the handle's stream WITHOUT waiting: q must stay
+ * valid, and is complete only, once the stream has passed this point (an event recorded on
+ * the stream set by lsb_set_stream, or lsb_synchronize).  Pinned memory lets the copies
+ * overlap; steps queued afterwards run after them. */
+int lsb_snapshot_async(lsb_handle* h, double* q);
 
 /* ---------------- Ensembles: runs stepped together ----------------------------------- */
 /* No counterpart in the reference (one run per mpiexec there).  A batch steps several

@@ -1715,6 +1715,24 @@ int lsb_spanwise_stats(lsb_handle* h, double* mean, double* rms) {
     });
 }
 
+int lsb_snapshot_async(lsb_handle* h, double* q) {
+    return guard([&] {
+        if (!h || !q) fail(LSB_ERR_ARG, "null argument");
+        const Dims& d = h->d;
+        const long long S = d.S(), P = h->P;
+        // the fields of spanwise_stats: u + ubar, v, w, p on the physical grid (FP64 in both
+        // precisions) in the first four scratch fields, then copied out without waiting
+        double* ph[4] = {h->phys, h->phys + P, h->phys + 2 * P, h->phys + 3 * P};
+        const double* spec[4] = {h->vel, h->vel + S, h->vel + 2 * S, h->p};
+        const double* means[4] = {h->ubar, nullptr, nullptr, nullptr};
+        spec_to_phys(h, spec, ph, 4, d.nzp, means, nullptr, false);
+        check_launch();
+        const long long n = (long long)d.nzp * d.ny * d.nx;
+        for (int k = 0; k < 4; ++k)
+            CK(cudaMemcpyAsync(q + k * n, ph[k], n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    });
+}
+
 int lsb_timers(lsb_handle* h, int enable) {
     return guard([&] {
         if (!h) fail(LSB_ERR_ARG, "null handle");

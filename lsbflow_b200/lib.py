@@ -30,6 +30,7 @@ EXPORTS = [
     "lsb_solve_helmholtz_noalloc", "lsb_tavg", "lsb_spanwise_stats", "lsb_graphs", "lsb_kernel_launches", "lsb_device_bytes",
     "lsb_batch_create", "lsb_batch_destroy", "lsb_batch_step", "lsb_batch_synchronize", "lsb_batch_graphs",
     "lsb_batch_set_stream", "lsb_set_schedule", "lsb_get_schedule",
+    "lsb_snapshot_async",
 ]
 
 
@@ -268,6 +269,11 @@ class Solver:
         rms = np.empty((4, c.nzp, c.nx))
         _ck(self._lib.lsb_spanwise_stats(self._h, _ptr(mean), _ptr(rms)))
         return mean, rms
+
+    def snapshot_async(self, q_ptr: int):
+        """q-file fields (u + ubar, v, w, p; physical, [4][nzp][ny][nx]) copied to the host
+        address q_ptr on the handle's stream without waiting (lsb_snapshot_async)."""
+        _ck(self._lib.lsb_snapshot_async(self._h, C.c_void_p(q_ptr)))
 
     def timers(self, enable: bool):
         _ck(self._lib.lsb_timers(self._h, C.c_int(1 if enable else 0)))
