@@ -36,3 +36,27 @@ def test_create_fails_loudly_without_device():
     from lsbflow_b200.config import workload
     with pytest.raises(lib.LsbError):
         lib.Solver(hs.make_setup(workload("dns64", nx=16, ny=8, nz=16)))
+
+
+def test_new_entry_points_reject_null_arguments_before_any_device_work():
+    """Argument checks of the ensemble, schedule and snapshot calls need no device."""
+    import ctypes as C
+    if not os.path.exists(lib.LIBPATH):
+        pytest.skip("library not built")
+    l = lib.load()
+    b = C.c_void_p()
+    assert l.lsb_batch_create(None, C.c_int(2), C.byref(b)) == -1
+    arr = (C.c_void_p * 2)(None, None)
+    assert l.lsb_batch_create(arr, C.c_int(2), C.byref(b)) == -1
+    assert b"null member" in l.lsb_last_error()
+    assert l.lsb_batch_create(arr, C.c_int(0), C.byref(b)) == -1
+    assert l.lsb_batch_step(None, C.c_int(1)) == -1
+    assert l.lsb_batch_synchronize(None) == -1
+    assert l.lsb_batch_graphs(None, C.c_int(0)) == -1
+    assert l.lsb_batch_set_stream(None, None) == -1
+    assert l.lsb_batch_destroy(None) == 0          # like free(NULL)
+    sc = lib.LsbScheduleC(4, 0)
+    assert l.lsb_set_schedule(None, C.byref(sc)) == -1
+    assert l.lsb_get_schedule(None, C.byref(sc)) == -1
+    assert l.lsb_snapshot_async(None, None) == -1
+    assert l.lsb_step(None, C.c_int(1)) == -1
