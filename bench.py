@@ -375,6 +375,22 @@ def main():
                 "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": round(per_launch_ms, 4),
                 "share_of_step": round(ms_nl / tot, 4)}
 
+    # ---- step-level rooflines (the survey's per-grid-point-step figures): compulsory state
+    # traffic, 24 FP64 spectral fields read or written once per step (u, v, w, p, p^{n-1},
+    # 2 velocity and 2 nonlinear histories read, u, v, w, p, N^n written), and the
+    # contraction work, 11 nzp x nzp derivative and 10 nzm x nzm eigenbasis applications per
+    # column, against the step time
+    nzm = nzp - 2
+    state_b = 24 * 8
+    flop_c = 2.0 * (11 * nzp + 10 * nzm * nzm / nzp)
+    t_step = ms / args.steps / 1e3
+    step_roofline = {"state_bytes_per_pt_step": state_b, "contraction_flop_per_pt_step": round(flop_c, 1),
+                     "achieved_state_GBs": round(state_b * pts / t_step / 1e9, 1),
+                     "state_frac_of_hbm": round(state_b * pts / t_step / 1e9 / hbm, 4),
+                     "achieved_contraction_TFLOPs": round(flop_c * pts / t_step / 1e12, 3),
+                     "note": "the step moves far more than its state: the padded-grid transforms and "
+                             "SGS fields are intermediate traffic; the kernel rooflines explain the time"}
+
     # ---- end-to-end through the C ABI with host buffers (pinned): per step the velocity
     # (u, v, w) goes host->device, one time step runs, the new velocity comes back.
     hb = [torch.empty(pts, dtype=torch.float64, pin_memory=True) for _ in range(3)]
@@ -500,6 +516,7 @@ def main():
                        "global_batch": world, "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (resident state 24 fields x 17 MB = 405 MB)"},
             "roofline": roofline,
+            "step_roofline": step_roofline,
             "kernel_groups": groups,
             "clocks": clocks,
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": 3 * S8, "d2h_bytes_per_step": 3 * S8},
