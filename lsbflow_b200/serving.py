@@ -12,6 +12,10 @@ HBM from admission to result.  The loop works at step boundaries:
   different sizes advance concurrently and kernels of different streams overlap.
 * completion -- a run that has done its steps is downloaded, its handle freed, and its
   slot and memory go to the next arrival.
+* set-up ahead of admission -- when a backend has ``prepare`` (the host-only part of
+  starting a run: grid, matrices, base flow, initial field), arrived requests are prepared
+  on helper threads while the loop keeps stepping, so admission only creates the handle
+  and uploads the state.
 
 With ``group=True`` the runs of one shape (grid, model, dealiasing, averaging) form a
 cohort stepped through one ensemble batch (``lsb_batch_step``: one CUDA graph launch per
@@ -80,14 +84,20 @@ class DeviceBackend:
     def free_bytes(self) -> int:
         return int(self._free)
 
-    def start(self, req: RunRequest):
+    @staticmethod
+    def prepare(req: RunRequest):
+        """Host-only set-up of a run (grid, matrices, base flow, initial field); no device
+        work, so it can run on a helper thread while the loop steps other runs."""
         from . import hostsetup as hs
         from . import ic
         st = hs.make_setup(req.cfg)
+        return st, ic.seeded_noise(st, req.seed, req.amp)
+
+    def start(self, req: RunRequest, prepared=None):
+        st, (u, v, w) = prepared if prepared is not None else self.prepare(req)
         s = self.lib.Solver(st)
         stream = self.torch.cuda.Stream()
         s.set_stream(stream.cuda_stream)
-        u, v, w = ic.seeded_noise(st, req.seed, req.amp)
         s.upload(u, v, w, dt=st.dt)
         return {"solver": s, "stream": stream, "event": None, "bytes": s.device_bytes()}
 
@@ -150,6 +160,7 @@ class Server:
     chunk: int = 10
     footprints: dict = field(default_factory=dict)
     group: bool = False                  # step same-shape runs as one ensemble batch
+    prefetch: int = 2                    # helper threads preparing arrived runs (0: none)
 
     def __post_init__(self):
         if self.backend is None:
@@ -166,15 +177,32 @@ class Server:
             raise ValueError(f"run {req.rid} needs {need} bytes, more than the budget {self.memory_budget}")
         self.queue.append(req)
 
+    def _prefetch(self, queue, now):
+        """Queue the host set-up of every arrived request not yet being prepared."""
+        if self._pool is None:
+            return
+        for req in queue:
+            if req.arrival > now:
+                break
+            if req.rid not in self._prepared:
+                self._prepared[req.rid] = self._pool.submit(self.backend.prepare, req)
+
+    def _start(self, req):
+        fut = self._prepared.pop(req.rid, None)
+        if fut is None:
+            return self.backend.start(req)
+        return self.backend.start(req, fut.result())
+
     def _admit(self, queue, now, n_active, used, t0, clock):
         """Admits arrived requests, oldest first, no overtaking; yields (request, run, bytes)."""
+        self._prefetch(queue, now)
         while queue and queue[0].arrival <= now and n_active < self.max_active:
             req = queue[0]
             need = self.footprints.get(shape_key(req.cfg), estimate_bytes(req.cfg))
             if used + need > self.memory_budget and n_active:
                 break
             queue.pop(0)
-            run = self.backend.start(req)
+            run = self._start(req)
             nb = int(run.get("bytes") or need)
             self.footprints[shape_key(req.cfg)] = nb
             used += nb
@@ -241,8 +269,21 @@ class Server:
         return sorted(results, key=lambda r: r.rid)
 
     def run(self, clock=time.perf_counter, idle_sleep: float = 1e-4) -> list:
-        if self.group:
-            return self._run_grouped(clock, idle_sleep)
+        self._prepared = {}
+        self._pool = None
+        if self.prefetch > 0 and hasattr(self.backend, "prepare"):
+            from concurrent.futures import ThreadPoolExecutor
+            self._pool = ThreadPoolExecutor(max_workers=self.prefetch)
+        try:
+            if self.group:
+                return self._run_grouped(clock, idle_sleep)
+            return self._run_plain(clock, idle_sleep)
+        finally:
+            if self._pool is not None:
+                self._pool.shutdown(wait=True)
+            self._pool = None
+
+    def _run_plain(self, clock, idle_sleep) -> list:
         queue = sorted(self.queue, key=lambda r: (r.arrival, r.rid))
         self.queue = []
         active: list = []
@@ -250,19 +291,10 @@ class Server:
         used = 0
         t0 = clock()
         while queue or active:
-            now = clock() - t0
             # admission at a step boundary, oldest arrival first, no overtaking
-            while queue and queue[0].arrival <= now and len(active) < self.max_active:
-                req = queue[0]
-                need = self.footprints.get(shape_key(req.cfg), estimate_bytes(req.cfg))
-                if used + need > self.memory_budget and active:
-                    break
-                queue.pop(0)
-                run = self.backend.start(req)
-                nb = int(run.get("bytes") or need)
-                self.footprints[shape_key(req.cfg)] = nb
-                used += nb
-                active.append(_Active(req, run, clock() - t0, req.nsteps, nb))
+            for a in self._admit(queue, clock() - t0, len(active), used, t0, clock):
+                used += a.nbytes
+                active.append(a)
             progressed = False
             for a in list(active):
                 if not self.backend.ready(a.run):
@@ -273,20 +305,11 @@ class Server:
                     a.remaining -= k
                     progressed = True
                 else:
-                    state = self.backend.finish(a.run)
-                    c = a.req.cfg
-                    results.append(RunResult(a.req.rid, state, a.req.arrival, a.admitted, clock() - t0,
-                                             a.req.nsteps, c.nx * c.ny * c.nzp))
+                    results.append(self._result(a, self.backend.finish(a.run), clock() - t0))
                     active.remove(a)
                     used -= a.nbytes
                     progressed = True
-            if not progressed:
-                if not active and queue:
-                    wait = queue[0].arrival - (clock() - t0)
-                    if wait > 0:
-                        time.sleep(min(wait, 0.05))
-                else:
-                    time.sleep(idle_sleep)
+            self._wait(progressed, bool(active), queue, clock, t0, idle_sleep)
         self.elapsed = clock() - t0
         return sorted(results, key=lambda r: r.rid)
 

@@ -1,4 +1,6 @@
 """The serving loop's admission and scheduling, with a fake device backend."""
+import threading
+
 import pytest
 
 from lsbflow_b200 import serving as S
@@ -166,3 +168,33 @@ def test_grouped_admission_respects_budget_and_late_arrivals_join():
     assert starts == sorted(starts)
     sizes = {len(ids) for ev, ids, *_ in be.log if ev == "group"}
     assert 2 in sizes                                  # a later arrival joined a running cohort
+
+
+class PreparingBackend(FakeBackend):
+    """A backend whose host set-up runs ahead of admission on helper threads."""
+
+    def __init__(self, **kw):
+        super().__init__(**kw)
+        self.prepared = []
+        self.lock = threading.Lock()
+
+    def prepare(self, req):
+        with self.lock:
+            self.prepared.append((req.rid, threading.current_thread() is threading.main_thread()))
+        return ("setup", req.rid)
+
+    def start(self, req, prepared=None):
+        assert prepared == ("setup", req.rid)
+        return super().start(req)
+
+
+@pytest.mark.parametrize("group", [False, True])
+def test_host_setup_runs_ahead_on_helper_threads(group):
+    be = PreparingBackend()
+    srv = S.Server(backend=be, memory_budget=100_000_000, chunk=4, group=group)
+    for i in range(6):
+        srv.submit(S.RunRequest(i, cfg(32), nsteps=9, arrival=0.002 * i))
+    res = srv.run()
+    assert [r.state["steps"] for r in res] == [9] * 6
+    assert sorted(rid for rid, _ in be.prepared) == list(range(6))   # each prepared once
+    assert not any(on_main for _, on_main in be.prepared)             # never on the loop's thread
