@@ -173,6 +173,39 @@ def profiled_traffic(path: str):
     return None
 
 
+def run_serving(args, rank):
+    """A seeded Poisson stream (4/s) of ensemble runs through the request loop, first with
+    every run on its own stream, then with same-shape runs stepped as one ensemble batch."""
+    from lsbflow_b200 import serving as S
+
+    shapes = [workload("ens128"), workload("ens128", sgsmodel=1), workload("dns64", dealiasflag=1)]
+    reqs = S.poisson_requests(args.serve_runs, 4.0, 11 + rank, shapes, steps_range=(100, 400))
+    srv = S.Server(chunk=20)
+    for r in reqs:
+        srv.submit(r)
+    res = srv.run()
+    summ = S.summary(res, srv.elapsed)
+    serving = {"runs": summ["runs"], "runs_per_hour": round(summ["runs_per_hour"], 1),
+               "p50_s": round(summ["p50"], 4), "p99_s": round(summ["p99"], 4),
+               "pt_steps_per_s": summ["pt_steps_per_s"], "elapsed_s": round(summ["elapsed_s"], 3),
+               "arrivals": "Poisson 4/s, seeded", "mix": "ens128 sigma / ens128 dyn-Smagorinsky / dns64",
+               "horizon_steps": [100, 400]}
+    # the same stream with same-shape runs stepped as one ensemble batch per shape
+    try:
+        srv = S.Server(chunk=20, group=True)
+        for r in reqs:
+            srv.submit(r)
+        res = srv.run()
+        summ = S.summary(res, srv.elapsed)
+        serving["grouped"] = {"runs_per_hour": round(summ["runs_per_hour"], 1),
+                              "p50_s": round(summ["p50"], 4), "p99_s": round(summ["p99"], 4),
+                              "pt_steps_per_s": summ["pt_steps_per_s"],
+                              "elapsed_s": round(summ["elapsed_s"], 3)}
+    except Exception as e:  # reported in the line; the ungrouped numbers above stand
+        serving["grouped"] = {"error": f"{type(e).__name__}: {e}"}
+    return serving
+
+
 def run_profiles(args, st, u, v, w, stream):
     """Spanwise mean and rms profiles of u + ubar, v, w, p (per z and x, as run/spanwiseavg.m
     averages q snapshots over y), averaged in time over the second half of a long run, for
@@ -461,32 +494,10 @@ def main():
     # ---- serving: a Poisson stream of ensemble runs (continuous batching on this GPU)
     serving = None
     if not args.no_serving:
-        from lsbflow_b200 import serving as S
-        shapes = [workload("ens128"), workload("ens128", sgsmodel=1), workload("dns64", dealiasflag=1)]
-        reqs = S.poisson_requests(args.serve_runs, 4.0, 11 + rank, shapes, steps_range=(100, 400))
-        srv = S.Server(chunk=20)
-        for r in reqs:
-            srv.submit(r)
-        res = srv.run()
-        summ = S.summary(res, srv.elapsed)
-        serving = {"runs": summ["runs"], "runs_per_hour": round(summ["runs_per_hour"], 1),
-                   "p50_s": round(summ["p50"], 4), "p99_s": round(summ["p99"], 4),
-                   "pt_steps_per_s": summ["pt_steps_per_s"], "elapsed_s": round(summ["elapsed_s"], 3),
-                   "arrivals": "Poisson 4/s, seeded", "mix": "ens128 sigma / ens128 dyn-Smagorinsky / dns64",
-                   "horizon_steps": [100, 400]}
-        # the same stream with same-shape runs stepped as one ensemble batch per shape
         try:
-            srv = S.Server(chunk=20, group=True)
-            for r in reqs:
-                srv.submit(r)
-            res = srv.run()
-            summ = S.summary(res, srv.elapsed)
-            serving["grouped"] = {"runs_per_hour": round(summ["runs_per_hour"], 1),
-                                  "p50_s": round(summ["p50"], 4), "p99_s": round(summ["p99"], 4),
-                                  "pt_steps_per_s": summ["pt_steps_per_s"],
-                                  "elapsed_s": round(summ["elapsed_s"], 3)}
-        except Exception as e:  # reported in the line; the ungrouped numbers above stand
-            serving["grouped"] = {"error": f"{type(e).__name__}: {e}"}
+            serving = run_serving(args, rank)
+        except Exception as e:  # reported in the line; the headline stands on its own
+            serving = {"error": f"{type(e).__name__}: {e}"}
 
     # ---- batched ensemble: sigma-model LES members of one grid with their own Re_delta*,
     # dipole amplitude and position, stepped together (one graph launch per ensemble step)
