@@ -173,6 +173,25 @@ def profiled_traffic(path: str):
     return None
 
 
+def tune_schedule(args, st, sol):
+    """Times the launch-schedule candidates on this GPU (lsbflow_b200.autotune) and applies
+    the fastest to ``sol``; returns what was found, or why not."""
+    if args.no_tune:
+        return None
+    try:
+        from lsbflow_b200 import autotune as A
+        measure, close = A.gpu_measurer(st, steps=10, reps=2)
+        try:
+            res = A.tune(st.cfg, measure)
+        finally:
+            close()
+        sol.set_schedule(res["schedule"])
+        return {"schedule": res["schedule"], "model_ms_per_step": round(res["model_ms_per_step"], 4),
+                "tuned_ms_per_step": round(res["ms_per_step"], 4), "trials": len(res["trials"])}
+    except Exception as e:  # the models' schedule stays
+        return {"error": f"{type(e).__name__}: {e}"}
+
+
 def run_serving(args, rank):
     """A seeded Poisson stream (4/s) of ensemble runs through the request loop, first with
     every run on its own stream, then with same-shape runs stepped as one ensemble batch."""
@@ -323,6 +342,7 @@ def main():
     ap.add_argument("--serve-runs", type=int, default=12)
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-profiles", action="store_true")
+    ap.add_argument("--no-tune", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=2000)
     ap.add_argument("--members", type=int, default=64)
     args = ap.parse_args()
@@ -355,6 +375,9 @@ def main():
     sol.set_stream(stream.cuda_stream)
     sol.upload(u, v, w, dt=st.dt)
     pts = cfg.nx * cfg.ny * cfg.nzp
+    # launch schedule picked by the tuner (part of set-up, like an FFT planner; every
+    # schedule gives the same results); the models' choice if tuning is off or fails
+    schedules = {"fp64": tune_schedule(args, st, sol)}
 
     # ---- warm-up
     sol.step(args.warmup)
@@ -446,7 +469,9 @@ def main():
     mixed = None
     if not args.no_mixed:
         cfg_m = cfg.replace(precision=1)
-        sm = lib.Solver(hs.make_setup(cfg_m))
+        st_m = hs.make_setup(cfg_m)
+        sm = lib.Solver(st_m)
+        schedules["mixed"] = tune_schedule(args, st_m, sm)
         sm.set_stream(stream.cuda_stream)
         sm.upload(u, v, w, dt=st.dt)
         sm.step(args.warmup)
@@ -528,6 +553,7 @@ def main():
                        "l2": "inputs larger than L2 (resident state 24 fields x 17 MB = 405 MB)"},
             "roofline": roofline,
             "step_roofline": step_roofline,
+            "schedules": schedules,
             "kernel_groups": groups,
             "clocks": clocks,
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": 3 * S8, "d2h_bytes_per_step": 3 * S8},
