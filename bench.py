@@ -173,9 +173,29 @@ def profiled_traffic(path: str):
     return None
 
 
+def same_results(st, sched, nsteps=4):
+    """Whether ``sched`` and the built-in models give identical states after a few steps from
+    the same seeded field on this grid (every schedule should: none reorders a sum)."""
+    from lsbflow_b200 import lib
+
+    u, v, w = ic.seeded_noise(st, 99, 5e-3)
+    out = []
+    for s_ in ({}, sched):
+        s = lib.Solver(st)
+        try:
+            s.set_schedule(s_)
+            s.upload(u, v, w, dt=st.dt)
+            s.step(nsteps)
+            out.append(s.download())
+        finally:
+            s.close()
+    return all(np.array_equal(out[0][k], out[1][k]) for k in ("uf", "vf", "wf", "pf"))
+
+
 def tune_schedule(args, st, sol):
     """Times the launch-schedule candidates on this GPU (lsbflow_b200.autotune) and applies
-    the fastest to ``sol``; returns what was found, or why not."""
+    the fastest to ``sol`` once it is shown to give the models' results bit for bit on this
+    grid; returns what was found, or why not."""
     if args.no_tune:
         return None
     try:
@@ -185,9 +205,16 @@ def tune_schedule(args, st, sol):
             res = A.tune(st.cfg, measure)
         finally:
             close()
+        out = {"schedule": res["schedule"], "model_ms_per_step": round(res["model_ms_per_step"], 4),
+               "tuned_ms_per_step": round(res["ms_per_step"], 4), "trials": len(res["trials"])}
+        if any(res["schedule"].values()):
+            out["bit_identical_to_model"] = same_results(st, res["schedule"])
+            if not out["bit_identical_to_model"]:
+                out["applied"] = False
+                return out
         sol.set_schedule(res["schedule"])
-        return {"schedule": res["schedule"], "model_ms_per_step": round(res["model_ms_per_step"], 4),
-                "tuned_ms_per_step": round(res["ms_per_step"], 4), "trials": len(res["trials"])}
+        out["applied"] = True
+        return out
     except Exception as e:  # the models' schedule stays
         return {"error": f"{type(e).__name__}: {e}"}
 
