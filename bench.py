@@ -308,10 +308,15 @@ def run_ensemble(args, rank, world, stream, max_over_ranks, barrier):
         cfgs = ensemble_configs(args.members, seed=3000 + rank, precision=prec)
         sols = []
         free = torch.cuda.mem_get_info()[0]
-        for m, cfg in enumerate(cfgs):
-            st = hs.make_setup(cfg)
+        def prep(m):  # host-only set-up and initial field, on helper threads
+            st = hs.make_setup(cfgs[m])
+            return st, ic.seeded_noise(st, replicas.replica_seed(5000 + m, rank), 1e-3)
+
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as pool:
+            prepared = list(pool.map(prep, range(len(cfgs))))
+        for m, (st, (u, v, w)) in enumerate(prepared):
             s = lib.Solver(st)
-            u, v, w = ic.seeded_noise(st, replicas.replica_seed(5000 + m, rank), 1e-3)
             s.upload(u, v, w, dt=st.dt)
             sols.append(s)
             if m == 0 and s.device_bytes() * len(cfgs) > 0.8 * free:
