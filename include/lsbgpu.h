@@ -178,9 +178,10 @@ int lsb_snapshot_async(lsb_handle* h, double* q);
  * results of lsb_step on each member alone, bit for bit.  When every member's step is
  * steady (the lsb_step graph conditions), the members' steps are captured as parallel
  * branches of one CUDA graph and each ensemble step is one graph launch on the batch's
- * own stream; otherwise the members are stepped one by one on their own streams.  The
- * batch does not own its members: destroy the batch before any member.  Work issued on a
- * member's stream after lsb_batch_step is ordered after the batch's steps.  Not
+ * stream; otherwise the members are stepped one by one on their own streams.  The batch
+ * does not own its members: destroy the batch before any member.  The batch's steps
+ * follow the work already queued on the members' streams, and work queued on a member's
+ * stream after lsb_batch_step follows them.  Not
  * thread-safe; a member must not be stepped by another batch or thread meanwhile. */
 typedef struct lsb_batch lsb_batch;
 int lsb_batch_create(lsb_handle* const* members, int nmembers, lsb_batch** out);
