@@ -1,0 +1,127 @@
+"""The bench's side sections (tuned schedule, long-run profiles, serving, ensemble) run their
+host logic end to end with stand-ins for the device, so a slip in them shows here and not
+first in a GPU run."""
+import types
+
+import numpy as np
+import pytest
+
+import bench
+from lsbflow_b200 import autotune as A
+from lsbflow_b200 import hostsetup as hs
+from lsbflow_b200 import lib
+from lsbflow_b200 import serving as S
+from lsbflow_b200.config import workload
+
+
+class FakeSolver:
+    def __init__(self, st):
+        self.st = st
+        self.cfg = st.cfg
+        self.sched = {}
+
+    def set_stream(self, s):
+        pass
+
+    def set_schedule(self, s):
+        self.sched = dict(s)
+
+    def upload(self, *a, **k):
+        pass
+
+    def step(self, n):
+        pass
+
+    def download(self):
+        c = self.cfg
+        return {k: np.zeros((c.nzp, c.ny, c.nx)) for k in ("uf", "vf", "wf", "pf")}
+
+    def device_bytes(self):
+        return 1 << 20
+
+    def spanwise_stats(self):
+        c = self.cfg
+        m = np.ones((4, c.nzp, c.nx)) * (1.0 + 1e-7 * c.precision)
+        return m, 2.0 * m
+
+    def close(self):
+        pass
+
+
+class FakeBatch:
+    def __init__(self, members):
+        self.members = members
+
+    def set_stream(self, s):
+        pass
+
+    def step(self, n):
+        pass
+
+    def close(self):
+        pass
+
+
+class FakeEvent:
+    def __init__(self, enable_timing=False):
+        pass
+
+    def record(self, s=None):
+        pass
+
+    def elapsed_time(self, other):
+        return 10.0
+
+
+@pytest.fixture
+def small_st():
+    return hs.make_setup(workload("dns64", nx=32, ny=8, nz=16))
+
+
+def test_tune_schedule_applies_only_checked_schedules(monkeypatch, small_st):
+    monkeypatch.setattr(lib, "Solver", FakeSolver)
+    faster = {"gemm_warps": 6, "filter_zchunks": 0}
+    monkeypatch.setattr(A, "gpu_measurer",
+                        lambda st, steps, reps: (lambda s: 1.0 if s == faster else 2.0, lambda: None))
+    sol = FakeSolver(small_st)
+    out = bench.tune_schedule(types.SimpleNamespace(no_tune=False), small_st, sol)
+    assert out["schedule"] == faster and out["applied"] and out["bit_identical_to_model"]
+    assert sol.sched == faster
+    assert bench.tune_schedule(types.SimpleNamespace(no_tune=True), small_st, sol) is None
+
+
+def test_profiles_compare_the_two_forms(monkeypatch, small_st):
+    monkeypatch.setattr(lib, "Solver", FakeSolver)
+    out = bench.run_profiles(types.SimpleNamespace(profile_steps=100), small_st, None, None, None,
+                             types.SimpleNamespace(cuda_stream=0))
+    assert out["steps"] == 100 and out["target"] == 1e-4
+    assert out["max_rel_err_mean_velocity"] == pytest.approx(1e-7, rel=1e-3)
+    assert set(out["rel_err_rms"]) == set("uvwp")
+
+
+def test_serving_section(monkeypatch):
+    from test_serving_cpu import PreparingBackend
+
+    class Backend(PreparingBackend):
+        def __init__(self):
+            super().__init__(free=10 ** 12, lag=1)
+
+    monkeypatch.setattr(S, "DeviceBackend", Backend)
+    out = bench.run_serving(types.SimpleNamespace(serve_runs=4), 0)
+    assert out["runs"] == 4 and "error" not in out["grouped"]
+    assert out["p99_s"] >= out["p50_s"] > 0
+
+
+def test_ensemble_section(monkeypatch):
+    import torch
+    monkeypatch.setattr(lib, "Solver", FakeSolver)
+    monkeypatch.setattr(lib, "Batch", FakeBatch)
+    monkeypatch.setattr(torch.cuda, "mem_get_info", lambda: (100 << 30, 180 << 30))
+    monkeypatch.setattr(torch.cuda, "Event", FakeEvent)
+    monkeypatch.setattr(torch.cuda, "synchronize", lambda: None)
+    args = types.SimpleNamespace(members=3, steps=300, warmup=5)
+    out = bench.run_ensemble(args, 0, 1, types.SimpleNamespace(cuda_stream=0), lambda x: x, lambda: None)
+    assert out["members"] == 3
+    for form in ("fp64", "mixed"):
+        assert out[form]["gain_vs_one_member"] == pytest.approx(3.0)
+        assert out[form]["timed_steps"] == 30
