@@ -194,7 +194,9 @@ class Server:
         return self.backend.start(req, fut.result())
 
     def _admit(self, queue, now, n_active, used, t0, clock):
-        """Admits arrived requests, oldest first, no overtaking; yields (request, run, bytes)."""
+        """Admits arrived requests, oldest first, no overtaking, while a slot and the memory
+        budget allow (one run is always admitted when none is active); yields each admitted
+        run as an _Active.  ``used`` and ``n_active`` are the caller's totals on entry."""
         self._prefetch(queue, now)
         while queue and queue[0].arrival <= now and n_active < self.max_active:
             req = queue[0]
