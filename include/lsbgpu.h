@@ -181,7 +181,8 @@ int lsb_snapshot_async(lsb_handle* h, double* q);
  * stream; otherwise the members are stepped one by one on their own streams.  The batch
  * does not own its members: destroy the batch before any member.  The batch's steps
  * follow the work already queued on the members' streams, and work queued on a member's
- * stream after lsb_batch_step follows them.  Not
+ * stream after lsb_batch_step follows them.  All members and the batch belong to the
+ * device that is current at lsb_batch_create.  Not
  * thread-safe; a member must not be stepped by another batch or thread meanwhile. */
 typedef struct lsb_batch lsb_batch;
 int lsb_batch_create(lsb_handle* const* members, int nmembers, lsb_batch** out);
