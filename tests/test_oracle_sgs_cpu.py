@@ -1,0 +1,68 @@
+"""Properties of the oracle's SGS pieces that hold whatever the implementation: they check
+the restatement of src/sgsterm.f90 and src/filters.f90 where no golden data exists.
+
+* sigma model (src/sgsterm.f90:283-423): its differential operator
+  D_sigma = s3 (s1 - s2)(s2 - s3) / s1^2 of the singular values of the velocity gradient
+  vanishes for every two-dimensional gradient (s3 = 0: pure shear, solid-body rotation)
+  and for isotropic expansion (s1 = s2 = s3), and is positive otherwise; tau is
+  -2 nu_t S_ij, symmetric.
+* 3-point filter (src/filters.f90:363-613): the (a, b, a) / (2a + b) weights in x and y
+  and the interpolating non-uniform weights in z keep a constant field constant.
+"""
+import numpy as np
+import pytest
+
+from lsbflow_b200 import hostsetup as hs
+from lsbflow_b200.config import workload
+from oracle import lsb_oracle as O
+
+
+@pytest.fixture(scope="module")
+def st():
+    return hs.make_setup(workload("dns64", nx=16, ny=8, nz=16))
+
+
+def gradient(st, g):
+    """duidxj[l][m] = g[l][m] everywhere on the physical grid (nzp, ny, nx + 2)."""
+    c = st.cfg
+    shape = (c.nzp, c.ny, c.nx + 2)
+    return [[np.full(shape, float(g[l][m])) for m in range(3)] for l in range(3)]
+
+
+def smag_scale(st, g):
+    return float(np.max((1.35 * st.grid.dx) ** 2) * np.sum(np.asarray(g, float) ** 2) + 1e-300)
+
+
+@pytest.mark.parametrize("g", [
+    [[0, 0, 2.0], [0, 0, 0], [0, 0, 0]],          # pure shear du/dz
+    [[0, -1.5, 0], [1.5, 0, 0], [0, 0, 0]],       # solid-body rotation about z
+    [[0.3, 1.0, 0], [-0.4, -0.3, 0], [0, 0, 0]],  # any two-dimensional gradient
+    [[0.7, 0, 0], [0, 0.7, 0], [0, 0, 0.7]],      # isotropic expansion
+])
+def test_sigma_model_vanishes_where_it_should(st, g):
+    tau = O.sigma_model(st, gradient(st, g))
+    nx = st.cfg.nx
+    big = max(float(np.abs(tau[l][m][..., :nx]).max()) for l in range(3) for m in range(3))
+    assert big <= 1e-6 * smag_scale(st, g)
+
+
+def test_sigma_model_generic_gradient(st):
+    g = np.array([[0.2, 1.1, -0.3], [0.4, -0.5, 0.8], [-0.6, 0.1, 0.3]])
+    tau = O.sigma_model(st, gradient(st, g))
+    nx = st.cfg.nx
+    S = 0.5 * (g + g.T)
+    t = np.array([[tau[l][m][3, 2, 5] for m in range(3)] for l in range(3)])
+    assert np.allclose(t, t.T, rtol=0, atol=1e-15 * np.abs(t).max())
+    # tau = -2 nu_t S with nu_t > 0: the same ratio in every component, negative
+    ratio = t[np.abs(S) > 1e-12] / S[np.abs(S) > 1e-12]
+    assert np.all(ratio < 0) and np.ptp(ratio) <= 1e-12 * np.abs(ratio).max()
+    assert all(np.all(tau[l][m][..., nx:] == 0) for l in range(3) for m in range(3))
+
+
+@pytest.mark.parametrize("a,b", [(1.0, 1.0), (1.0, 6.0), (1.0, 2.0)])
+def test_three_point_filter_keeps_constants(st, a, b):
+    c = st.cfg
+    q = np.full((c.nzp, c.ny, c.nx + 2), 1.7)
+    out = O.filter_q_3pt(st, q, a, b)
+    assert np.allclose(out[..., : c.nx], 1.7, rtol=0, atol=1e-14)
+    assert np.all(out[..., c.nx:] == 0)
