@@ -11,6 +11,8 @@ restatement where no golden data exists.
 * horfft (src/horfft.f90:61-150): forward after inverse is the identity on normed spectra.
 * solve_helmholtz (src/helmholtz.f90:130-208): the eigenbasis solution satisfies the
   Chebyshev Helmholtz equation at the interior points with q = 0 on both walls.
+* dealiasing_2d_fftw (src/dealiasing.f90:262-447), textbook 3/2 layout: products of two
+  x modes carry no alias of an unresolved sum wavenumber.
 """
 import numpy as np
 import pytest
@@ -98,3 +100,23 @@ def test_helmholtz_solve_satisfies_its_equation(st):
     lhs = np.einsum("km,mji->kji", st.d2, q) - (O.wav2(st)[None] + sigma) * q
     err = np.abs(lhs[1:nz] - rhs[1:nz]).max()
     assert err <= 1e-9 * np.abs(rhs).max()
+
+
+@pytest.mark.parametrize("k1,k2", [(5, 4), (7, 6), (3, 2)])
+def test_padded_product_has_no_aliases_in_x(k1, k2):
+    """The 3/2-rule product (src/dealiasing.f90:262-447, textbook layout) of cos(k1 x) and
+    cos(k2 x) is 1/2 cos((k1 - k2) x) plus 1/2 cos((k1 + k2) x) when k1 + k2 is resolved,
+    and has nothing at the alias nx - (k1 + k2) when it is not."""
+    st = hs.make_setup(workload("dns64", nx=16, ny=8, nz=8, dealiasflag=1))
+    c = st.cfg
+    x = 2.0 * np.pi * np.arange(c.nx) / c.nx
+    a = np.zeros((c.nzp, c.ny, c.nx + 2))
+    b = np.zeros_like(a)
+    a[..., : c.nx] = np.cos(k1 * x)
+    b[..., : c.nx] = np.cos(k2 * x)
+    f = O.to_complex(O.horfft_fwd(O.dealias_product(st, a, b, "correct"), c.nx, c.ny))[2, 0, :]
+    expect = np.zeros(c.nx // 2)
+    expect[k1 - k2] += 0.25
+    if k1 + k2 < c.nx // 2:
+        expect[k1 + k2] += 0.25
+    assert np.allclose(f, expect, rtol=0, atol=1e-14)
