@@ -13,6 +13,7 @@ restatement where no golden data exists.
   Chebyshev Helmholtz equation at the interior points with q = 0 on both walls.
 * dealiasing_2d_fftw (src/dealiasing.f90:262-447), textbook 3/2 layout: products of two
   x modes carry no alias of an unresolved sum wavenumber.
+* timestep (src/navierstokes.f90:10-90): the velocity stays divergence-free to round-off.
 """
 import numpy as np
 import pytest
@@ -120,3 +121,18 @@ def test_padded_product_has_no_aliases_in_x(k1, k2):
     if k1 + k2 < c.nx // 2:
         expect[k1 + k2] += 0.25
     assert np.allclose(f, expect, rtol=0, atol=1e-14)
+
+
+@pytest.mark.parametrize("name,over", [("dns64", dict(nx=32, ny=8, nz=32, dealiasflag=1)),
+                                       ("les256", dict(nx=32, ny=8, nz=32))])
+def test_time_step_keeps_velocity_divergence_free(name, over):
+    """navierstokes_update (src/navierstokes.f90:1157-1496): the pressure correction and
+    the Poisson solve for w leave div u at round-off, walls included."""
+    from lsbflow_b200 import ic
+    st = hs.make_setup(workload(name, **over))
+    u, v, w = ic.seeded_noise(st, 3, 1e-2)
+    s = O.State.zeros_like(st, u, v, w, st.dt)
+    for _ in range(4):
+        O.timestep(st, s)
+        div = O.divuv(st, s.uf, s.vf) + O.dfdz(st, s.wf)
+        assert np.abs(div).max() <= 1e-12 * np.abs(O.dfdx(st, s.uf)).max()
