@@ -192,7 +192,9 @@ int lsb_batch_synchronize(lsb_batch* b);
 /* launch the ensemble graphs on a caller stream (cudaStream_t as void*; NULL restores the
  * batch's own); an event recorded there after lsb_batch_step follows every member's steps */
 int lsb_batch_set_stream(lsb_batch* b, void* stream);
-/* enable = 0: drop the ensemble graphs and step the members one by one */
+/* enable = 0: drop the ensemble graphs and step the members one by one; enable = 1 after
+ * a member's lsb_set_schedule or lsb_graphs makes the batch capture its graphs anew (the
+ * ensemble graphs hold the launches as captured) */
 int lsb_batch_graphs(lsb_batch* b, int enable);
 
 /* ---------------- Tier 1: the reference's subroutine interfaces (host arrays) --------- */
