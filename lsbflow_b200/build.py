@@ -1,4 +1,5 @@
-"""Builds the CUDA library ``liblsbgpu.so`` in-tree for sm_100a with nvcc.
+"""Builds the CUDA library ``liblsbgpu.so`` in-tree for sm_100a with nvcc, and the native
+driver ``lsb_run`` (host C++ over the library's C ABI) with g++.
 
     python -m lsbflow_b200.build          # incremental (object files under _build/)
 """
@@ -14,6 +15,9 @@ CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 BUILD = os.path.join(ROOT, "_build")
 LIB = os.path.join(HERE, "liblsbgpu.so")
+DRIVER_SRC = os.path.join(HERE, "driver", "lsb_run.cpp")
+DRIVER = os.path.join(HERE, "lsb_run")
+CXX = os.environ.get("CXX", "g++")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -49,7 +53,21 @@ def build(verbose: bool = False, force: bool = False) -> str:
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
+    build_driver(verbose=verbose, force=force)
     return LIB
+
+
+def build_driver(verbose: bool = False, force: bool = False) -> str:
+    """lsb_run, linked against the in-tree library (found next to the binary at run time)."""
+    deps = [DRIVER_SRC, LIB] + [os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE) if f.endswith(".h")]
+    if not force and os.path.exists(DRIVER) and os.path.getmtime(DRIVER) >= max(os.path.getmtime(d) for d in deps):
+        return DRIVER
+    cmd = [CXX, "-std=c++17", "-O2", "-Wall", "-Wextra", "-I", INCLUDE, DRIVER_SRC, "-L", HERE, "-llsbgpu",
+           "-Wl,-rpath,$ORIGIN", "-o", DRIVER]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return DRIVER
 
 
 if __name__ == "__main__":

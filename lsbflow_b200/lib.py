@@ -137,6 +137,35 @@ def solve_helmholtz_noalloc(nx, ny, nz, rhs_ptr, out_ptr, lam_ptr, e_ptr, ei_ptr
                                         C.c_double(dtnui), C.c_void_p(stream_ptr)))
 
 
+SETUP_MAGIC = b"LSBSETUP"
+SETUP_VERSION = 1
+
+
+def setup_arrays(st: Setup) -> list:
+    """The lsb_setup arrays in the struct's order, as (name, float64 array) pairs."""
+    g = st.grid
+    return [("xpts", g.xpts), ("ypts", g.ypts), ("zpts", g.zpts), ("wavx", g.wavx), ("wavy", g.wavy),
+            ("dz1", st.dz1), ("dz2", st.dz2), ("lam", st.lam), ("e", st.E), ("ei", st.Ei),
+            ("ubar", st.ubar), ("ubarp", st.ubarp), ("ubarpp", st.ubarpp), ("hbot", st.hbot),
+            ("htop", st.htop), ("d2hbot", st.d2hbot), ("d2htop", st.d2htop), ("lamx", st.lam_x)]
+
+
+def write_setup_file(path: str, st: Setup) -> None:
+    """The inputs of lsb_create in one file for a native driver (lsb_run): the magic
+    ``LSBSETUP``, int32 version, int32 sizeof(lsb_config) and the struct's bytes, dx and
+    dy, then each set-up array as an int64 count and that many little-endian float64."""
+    cs = config_struct(st.cfg)
+    with open(path, "wb") as f:
+        f.write(SETUP_MAGIC)
+        f.write(np.array([SETUP_VERSION, C.sizeof(cs)], dtype="<i4").tobytes())
+        f.write(bytes(cs))
+        f.write(np.array([st.grid.dx, st.grid.dy], dtype="<f8").tobytes())
+        for _, a in setup_arrays(st):
+            a = np.ascontiguousarray(np.asarray(a, dtype="<f8")).ravel()
+            f.write(np.array([a.size], dtype="<i8").tobytes())
+            f.write(a.tobytes())
+
+
 class Solver:
     """One device-resident LSBFLOW run (a library handle)."""
 
