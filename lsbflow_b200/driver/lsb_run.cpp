@@ -1,7 +1,8 @@
 // lsb_run -- the reference's time loop (src/main.f90:62-111) as a native driver over the C
 // ABI of include/lsbgpu.h: read the run's set-up and a restart file, advance the resident
-// state with lsb_step, write a q snapshot every iomod steps and a restart file at the end,
-// in the reference's float32 layouts (src/mpi_io.f90:9-161 restart, :339-497 snapshot).
+// state with lsb_step, write a q snapshot every iomod steps (and after the last step when
+// NSTEPS is not a multiple of IOMOD) and a restart file at the end, in the reference's
+// float32 layouts (src/mpi_io.f90:9-161 restart, :339-497 snapshot).
 //
 //   lsb_run SETUP START NSTEPS IOMOD OUTDIR [--no-ref-bug]
 //   lsb_run --check-setup SETUP            counts and sums of the set-up arrays (no device)
