@@ -14,6 +14,8 @@ same results bit for bit; the tuner changes speed only.
     sched = autotune.lookup(cfg, path, device)            # None if never tuned
     sched = autotune.tune_and_store(st, path)["schedule"]  # times candidates on the GPU
     solver.set_schedule(sched)
+
+    python -m lsbflow_b200.autotune --workload les256 --out schedules.json   # on a GPU
 """
 from __future__ import annotations
 
@@ -140,3 +142,26 @@ def tune_and_store(st, path: str, device: str | None = None, steps: int = 20, re
     save_cache(path, cache)
     res["device"] = device
     return res
+
+
+def main(argv=None) -> int:
+    """python -m lsbflow_b200.autotune --workload les256 [--precision 1] --out schedules.json"""
+    import argparse
+
+    from . import hostsetup as hs
+    from .config import workload
+
+    ap = argparse.ArgumentParser(description="Tune the launch schedule of a workload on this GPU and store it.")
+    ap.add_argument("--workload", default="les256", help="dns64, os128, les256 or ens128")
+    ap.add_argument("--precision", type=int, default=0, choices=[0, 1])
+    ap.add_argument("--steps", type=int, default=20, help="timed steps per candidate and repetition")
+    ap.add_argument("--out", required=True, help="JSON file the schedule is added to")
+    args = ap.parse_args(argv)
+    st = hs.make_setup(workload(args.workload, precision=args.precision))
+    res = tune_and_store(st, args.out, steps=args.steps)
+    print(json.dumps({k: res[k] for k in ("device", "schedule", "ms_per_step", "model_ms_per_step")}))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -62,3 +62,11 @@ def test_store_round_trip_and_keys(tmp_path):
     A.save_cache(p, cache)
     assert A.lookup(a, p, "B200") == {"gemm_warps": 5, "filter_zchunks": 2}
     assert A.lookup(b, p, "B200") is None
+
+
+def test_command_line_help():
+    import subprocess
+    import sys
+    out = subprocess.run([sys.executable, "-m", "lsbflow_b200.autotune", "--help"], capture_output=True, text=True,
+                         timeout=120)
+    assert out.returncode == 0 and "--workload" in out.stdout and "--out" in out.stdout
