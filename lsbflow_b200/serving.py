@@ -72,14 +72,24 @@ def estimate_bytes(cfg: LsbConfig) -> int:
 
 
 class DeviceBackend:
-    """Handles and streams on the current CUDA device (the library's C ABI)."""
+    """Handles and streams on the current CUDA device (the library's C ABI).  With
+    ``schedules`` (a JSON file of lsbflow_b200.autotune) each run gets the launch schedule
+    tuned for its shape on this device, if there is one."""
 
-    def __init__(self):
+    def __init__(self, schedules: str | None = None):
         import torch  # device plumbing: streams and events
         from . import lib
         self.torch = torch
         self.lib = lib
         self._free, _ = torch.cuda.mem_get_info()
+        self.schedules = schedules
+        self.device = torch.cuda.get_device_name() if schedules else None
+
+    def schedule_for(self, cfg):
+        if not self.schedules:
+            return None
+        from . import autotune
+        return autotune.lookup(cfg, self.schedules, self.device)
 
     def free_bytes(self) -> int:
         return int(self._free)
@@ -96,6 +106,9 @@ class DeviceBackend:
     def start(self, req: RunRequest, prepared=None):
         st, (u, v, w) = prepared if prepared is not None else self.prepare(req)
         s = self.lib.Solver(st)
+        sched = self.schedule_for(req.cfg)
+        if sched:
+            s.set_schedule(sched)
         stream = self.torch.cuda.Stream()
         s.set_stream(stream.cuda_stream)
         s.upload(u, v, w, dt=st.dt)
@@ -161,10 +174,11 @@ class Server:
     footprints: dict = field(default_factory=dict)
     group: bool = False                  # step same-shape runs as one ensemble batch
     prefetch: int = 2                    # helper threads preparing arrived runs (0: none)
+    schedules: str | None = None         # tuned launch schedules (autotune JSON) for new runs
 
     def __post_init__(self):
         if self.backend is None:
-            self.backend = DeviceBackend()
+            self.backend = DeviceBackend(schedules=self.schedules)
         if self.memory_budget is None:
             self.memory_budget = int(0.9 * self.backend.free_bytes())
         self.queue: list = []

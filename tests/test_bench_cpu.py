@@ -103,7 +103,8 @@ def test_serving_section(monkeypatch):
     from test_serving_cpu import PreparingBackend
 
     class Backend(PreparingBackend):
-        def __init__(self):
+        def __init__(self, schedules=None):
+            assert schedules is None
             super().__init__(free=10 ** 12, lag=1)
 
     monkeypatch.setattr(S, "DeviceBackend", Backend)
