@@ -86,3 +86,12 @@ def test_run_fails_loudly_without_device(driver, tmp_path):
     assert out.returncode == 1 and "lsb_create failed" in out.stderr
     out = run(driver, tmp_path / "setup.bin", tmp_path / "start.dat", 4)
     assert out.returncode == 2 and "usage" in out.stderr
+
+
+def test_restart_dimension_mismatch_stops_the_run(driver, tmp_path):
+    """As src/mpi_io.f90:233-242, a restart of another grid stops the run before any device work."""
+    st = hs.make_setup(workload("dns64", nx=16, ny=6, nz=8))
+    lib.write_setup_file(str(tmp_path / "setup.bin"), st)
+    F.write_restart(str(tmp_path / "start.dat"), random_restart(workload("dns64", nx=16, ny=8, nz=8), 5))
+    out = run(driver, tmp_path / "setup.bin", tmp_path / "start.dat", 4, 2, tmp_path)
+    assert out.returncode == 1 and "differ from the run's" in out.stderr
