@@ -30,6 +30,7 @@ of a run is on that run's stream.  ``percentiles`` gives p50/p99 of time-to-resu
 """
 from __future__ import annotations
 
+import threading
 import time
 from dataclasses import dataclass, field
 
@@ -55,8 +56,9 @@ class RunResult:
     arrival: float
     admitted: float
     done: float
-    nsteps: int
+    nsteps: int                 # steps done (fewer than requested for a cancelled run)
     points: int
+    cancelled: bool = False     # stopped by Server.cancel; state is None
 
     @property
     def time_to_result(self) -> float:
@@ -149,6 +151,11 @@ class DeviceBackend:
             g["batch"] = None
             g["members"] = ()
 
+    def abort(self, run):
+        """Free a cancelled run's handle without downloading its state."""
+        run["stream"].synchronize()
+        run["solver"].close()
+
     def finish(self, run) -> dict:
         run["stream"].synchronize()
         state = run["solver"].download()
@@ -182,6 +189,35 @@ class Server:
         if self.memory_budget is None:
             self.memory_budget = int(0.9 * self.backend.free_bytes())
         self.queue: list = []
+        self._cancel: set = set()
+        self._cancel_lock = threading.Lock()
+
+    def cancel(self, rid: int):
+        """Stop run ``rid`` (safe from another thread): a queued run is dropped, an active
+        one leaves at its next step boundary and its handle is freed without a download.
+        Its result has ``cancelled`` set, ``state`` None and the steps it did."""
+        with self._cancel_lock:
+            self._cancel.add(rid)
+
+    def _cancelled(self, rid: int) -> bool:
+        with self._cancel_lock:
+            return rid in self._cancel
+
+    def _drop_cancelled(self, queue, results, now):
+        """Cancelled requests still waiting leave the queue with an empty result."""
+        for req in [r for r in queue if self._cancelled(r.rid)]:
+            queue.remove(req)
+            fut = self._prepared.pop(req.rid, None)
+            if fut is not None:
+                fut.cancel()
+            c = req.cfg
+            results.append(RunResult(req.rid, None, req.arrival, now, now, 0, c.nx * c.ny * c.nzp, True))
+
+    def _abort(self, a, results, now):
+        self.backend.abort(a.run)
+        c = a.req.cfg
+        results.append(RunResult(a.req.rid, None, a.req.arrival, a.admitted, now, a.req.nsteps - a.remaining,
+                                 c.nx * c.ny * c.nzp, True))
 
     def submit(self, req: RunRequest):
         if req.nsteps <= 0:
@@ -252,6 +288,7 @@ class Server:
 
         try:
             while queue or n_active():
+                self._drop_cancelled(queue, results, clock() - t0)
                 for a in self._admit(queue, clock() - t0, n_active(), used, t0, clock):
                     used += a.nbytes
                     key = shape_key(a.req.cfg)
@@ -262,12 +299,16 @@ class Server:
                 for c in cohorts.values():
                     if not (c["runs"] or c["joining"]) or not self.backend.group_ready(c["g"]):
                         continue
-                    done = [a for a in c["runs"] if a.remaining == 0]
-                    if done:
+                    stop = [a for a in c["runs"] + c["joining"] if self._cancelled(a.req.rid)]
+                    done = [a for a in c["runs"] if a.remaining == 0 and a not in stop]
+                    if done or stop:
                         self.backend.close_group(c["g"])
                         for a in done:
                             results.append(self._result(a, self.backend.finish(a.run), clock() - t0))
-                            c["runs"].remove(a)
+                        for a in stop:
+                            self._abort(a, results, clock() - t0)
+                        for a in done + stop:
+                            (c["runs"] if a in c["runs"] else c["joining"]).remove(a)
                             used -= a.nbytes
                     c["runs"] += c["joining"]
                     c["joining"] = []
@@ -276,7 +317,7 @@ class Server:
                         self.backend.launch_group(c["g"], [a.run for a in c["runs"]], k)
                         for a in c["runs"]:
                             a.remaining -= k
-                    progressed = progressed or bool(done) or bool(c["runs"])
+                    progressed = progressed or bool(done) or bool(stop) or bool(c["runs"])
                 self._wait(progressed, n_active() > 0, queue, clock, t0, idle_sleep)
         finally:
             for c in cohorts.values():
@@ -307,6 +348,7 @@ class Server:
         used = 0
         t0 = clock()
         while queue or active:
+            self._drop_cancelled(queue, results, clock() - t0)
             # admission at a step boundary, oldest arrival first, no overtaking
             for a in self._admit(queue, clock() - t0, len(active), used, t0, clock):
                 used += a.nbytes
@@ -315,7 +357,12 @@ class Server:
             for a in list(active):
                 if not self.backend.ready(a.run):
                     continue
-                if a.remaining > 0:
+                if self._cancelled(a.req.rid):
+                    self._abort(a, results, clock() - t0)
+                    active.remove(a)
+                    used -= a.nbytes
+                    progressed = True
+                elif a.remaining > 0:
                     k = min(self.chunk, a.remaining)
                     self.backend.launch(a.run, k)
                     a.remaining -= k
@@ -331,14 +378,19 @@ class Server:
 
 
 def percentiles(results, qs=(50, 99)) -> dict:
-    ttr = np.array([r.time_to_result for r in results])
+    """p50/p99 of time-to-result over the runs that completed (cancelled runs excluded)."""
+    ttr = np.array([r.time_to_result for r in results if not r.cancelled])
+    if ttr.size == 0:
+        return {f"p{q}": float("nan") for q in qs}
     return {f"p{q}": float(np.percentile(ttr, q)) for q in qs}
 
 
 def summary(results, elapsed: float) -> dict:
     out = percentiles(results)
-    out["runs"] = len(results)
-    out["runs_per_hour"] = len(results) / elapsed * 3600.0
+    done = [r for r in results if not r.cancelled]
+    out["runs"] = len(done)
+    out["cancelled"] = len(results) - len(done)
+    out["runs_per_hour"] = len(done) / elapsed * 3600.0
     out["pt_steps_per_s"] = sum(r.points * r.nsteps for r in results) / elapsed
     out["elapsed_s"] = elapsed
     return out

@@ -41,6 +41,11 @@ class FakeBackend:
             return False
         return True
 
+    def abort(self, run):
+        assert not run.get("in_group"), "a run was freed while its cohort's batch held it"
+        self.in_use -= run["bytes"]
+        self.log.append(("abort", run["rid"]))
+
     def finish(self, run):
         assert not run.get("in_group"), "a run was finished while its cohort's batch held it"
         self.in_use -= run["bytes"]
@@ -198,3 +203,28 @@ def test_host_setup_runs_ahead_on_helper_threads(group):
     assert [r.state["steps"] for r in res] == [9] * 6
     assert sorted(rid for rid, _ in be.prepared) == list(range(6))   # each prepared once
     assert not any(on_main for _, on_main in be.prepared)             # never on the loop's thread
+
+
+@pytest.mark.parametrize("group", [False, True])
+def test_cancelled_runs_leave_at_a_step_boundary(group):
+    be = FakeBackend(lag=1)
+    t = [0.0]
+    srv = S.Server(backend=be, memory_budget=100_000_000, chunk=3, group=group)
+
+    def clock():
+        t[0] += 0.001
+        if abs(t[0] - 0.010) < 5e-4:
+            srv.cancel(1)            # active by now: leaves at its next boundary
+        return t[0]
+
+    for i in range(4):
+        srv.submit(S.RunRequest(i, cfg(32), nsteps=30, arrival=0.0 if i < 3 else 0.5))
+    srv.cancel(3)                    # still queued: never started
+    res = {r.rid: r for r in srv.run(clock=clock, idle_sleep=0.0)}
+    assert res[3].cancelled and res[3].nsteps == 0 and res[3].state is None
+    assert ("start", 3) not in be.log
+    assert res[1].cancelled and 0 < res[1].nsteps < 30 and ("abort", 1) in be.log
+    assert [res[i].state["steps"] for i in (0, 2)] == [30, 30] and not res[0].cancelled
+    assert be.in_use == 0
+    s = S.summary(list(res.values()), srv.elapsed)
+    assert s["runs"] == 2 and s["cancelled"] == 2
