@@ -1,6 +1,7 @@
 // The library handle (shared by lsbgpu.cu and sgs_kernels.cu).
 #pragma once
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <map>
 #include <string>
@@ -131,12 +132,23 @@ struct lsb_handle {
 
 
 namespace lsb {
-// records CUDA events around the launches of one kernel group when timing is on
+// an NVTX range around a piece of host code that launches work (seen by profilers that
+// attach an NVTX tool; without one the calls return at once)
+struct NvtxRange {
+    explicit NvtxRange(const char* n) { nvtxRangePushA(n); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
+// records CUDA events around the launches of one kernel group when timing is on, and an
+// NVTX range of the group's name around them always.  Steps replayed from a CUDA graph run
+// no host code, so their groups show inside the graph launch only.
 struct TimerScope {
     lsb_handle* h;
     const char* name;
     cudaEvent_t a = nullptr, b = nullptr;
     TimerScope(lsb_handle* h_, const char* n) : h(h_), name(n) {
+        nvtxRangePushA(n);
         if (h->timing) {
             cudaEventCreate(&a);
             cudaEventCreate(&b);
@@ -148,6 +160,7 @@ struct TimerScope {
             cudaEventRecord(b, h->stream);
             h->timers[name].emplace_back(a, b);
         }
+        nvtxRangePop();
     }
 };
 // sgs_kernels.cu

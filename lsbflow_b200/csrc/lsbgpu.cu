@@ -890,6 +890,7 @@ void run_step(lsb_handle* h) {
 
 // one step of one handle: from its step graphs when steady, else ordinary launches
 void step_once(lsb_handle* h) {
+    NvtxRange r("timestep");
     if (graph_step(h, [h] { run_step(h); })) return;
     run_step(h);
 }
@@ -1397,6 +1398,7 @@ int lsb_batch_step(lsb_batch* b, int nsteps) {
         }
         try {
             for (int s = 0; s < nsteps; ++s) {
+                NvtxRange r("ensemble_step");
                 if (batch_graph_step(b)) continue;
                 batch_to_members(b);
                 for (lsb_handle* h : b->m) step_once(h);
