@@ -262,6 +262,8 @@ def run_profiles(args, st, u, v, w, stream):
     nsteps = max(20, args.profile_steps)
     every = 20
     out = {}
+    first_nonfinite = {}
+    umax = {}
     for prec in (0, 1):
         s = lib.Solver(hs.make_setup(st.cfg.replace(precision=prec)) if prec else st)
         s.set_stream(stream.cuda_stream)
@@ -269,15 +271,25 @@ def run_profiles(args, st, u, v, w, stream):
         acc_m = acc_r = None
         n = 0
         done = 0
+        bad = None
         while done < nsteps:
             s.step(every)
             done += every
+            if done % 100 == 0 or done >= nsteps:
+                d = s.diag()  # NaN check of the resident state (maxcalc's reductions)
+                umax.setdefault(prec, []).append(round(d["umax"], 4))
+                if d["nonfinite"] and bad is None:
+                    bad = done
+                    break
             if done > nsteps // 2:
                 m, r = s.spanwise_stats()
                 acc_m = m if acc_m is None else acc_m + m
                 acc_r = r if acc_r is None else acc_r + r
                 n += 1
         s.close()
+        first_nonfinite["fp64" if prec == 0 else "mixed"] = bad
+        if bad is not None or n == 0:
+            return {"steps": nsteps, "first_nonfinite_step": first_nonfinite, "error": "the run went non-finite"}
         out[prec] = (acc_m / n, acc_r / n, n)
     (m0, r0, n), (m1, r1, _) = out[0], out[1]
     names = ("u", "v", "w", "p")
@@ -288,9 +300,43 @@ def run_profiles(args, st, u, v, w, stream):
     em = {names[k]: rel(m1[k], m0[k]) for k in range(4)}
     er = {names[k]: rel(r1[k], r0[k]) for k in range(4)}
     return {"steps": nsteps, "average": f"steps {nsteps // 2 + every}..{nsteps}, every {every} ({n} samples)",
+            "first_nonfinite_step": first_nonfinite,
+            "umax_every_100_steps": {"fp64": umax[0][::4], "mixed": umax[1][::4]},
             "rel_err_mean": em, "rel_err_rms": er,
             "max_rel_err_mean_velocity": max(em[k] for k in "uvw"),
             "max_rel_err_rms_velocity": max(er[k] for k in "uvw"), "target": 1e-4}
+
+
+def run_os_growth(args, stream):
+    """The 128 x 4 x 97 Orr-Sommerfeld linear test (Re_delta* = 1000, alpha delta* = 0.25,
+    dt = 0.005): the Tollmien-Schlichting mode of the host Orr-Sommerfeld solve stepped
+    500 times in FP64 and in the mixed form, the perturbation energy taken every step
+    (lintest, src/orrsomm.f90:566-622), and the mean growth rate <dE/dt> of each against
+    the mode's omega_i."""
+    from lsbflow_b200 import lib
+    from lsbflow_b200 import linstab as L
+
+    nsteps = 500
+    out = {"grid": "128x4x97 (ref nx,ny,nzp)", "steps": nsteps}
+    for prec, name in ((0, "fp64"), (1, "mixed")):
+        st = hs.make_setup(workload("os128", precision=prec))
+        z = np.zeros((st.grid.nzp, st.cfg.ny, st.cfg.nx))
+        uf, vf, wf = z.copy(), z.copy(), z.copy()
+        mode = L.setup_linstab(st, uf, vf, wf)
+        s = lib.Solver(st)
+        s.set_stream(stream.cuda_stream)
+        s.upload(uf, vf, wf, dt=st.dt)
+        e = []
+        for _ in range(nsteps):
+            s.step(1)
+            e.append(s.diag()["energy_pert"])
+        s.close()
+        g = L.mean_growth(L.growth_rates(np.array(e), st.dt))
+        out["omega_i"] = mode.omega.imag
+        out[name] = {"mean_growth": g, "rel_err_vs_omega_i": abs(g - mode.omega.imag) / abs(mode.omega.imag)}
+    out["mixed_rel_err_vs_fp64"] = abs(out["mixed"]["mean_growth"] - out["fp64"]["mean_growth"]) / abs(
+        out["fp64"]["mean_growth"])
+    return out
 
 
 def run_ensemble(args, rank, world, stream, max_over_ranks, barrier):
@@ -516,6 +562,15 @@ def main():
         em1.record(stream)
         torch.cuda.synchronize()
         ms_m = max_over_ranks(em0.elapsed_time(em1))
+        # per kernel-group timing of the mixed step (event timers on, separate region)
+        sm.timers(True)
+        sm.step(min(args.steps, 40))
+        torch.cuda.synchronize()
+        rep_m = sm.timer_report()
+        sm.timers(False)
+        tot_m = sum(v[1] for k, v in rep_m.items() if k != "sgs_filter3")
+        groups_m = {k: {"launches": v[0], "ms_total": round(v[1], 4), "share": round(v[1] / tot_m, 4)}
+                    for k, v in rep_m.items()}
         nerr = 100
         sm.upload(u, v, w, dt=st.dt)
         sm.step(nerr)
@@ -537,6 +592,7 @@ def main():
                  "ms_per_step": ms_m / args.steps, "speedup_vs_fp64": (ms / args.steps) / (ms_m / args.steps),
                  "rel_err_velocity_after_100_steps": rel(vg, vr),
                  "rel_err_components": {k: rel(got[k], ref[k]) for k in ("uf", "vf", "wf", "pf")},
+                 "kernel_groups": groups_m,
                  "form": "FP32 transforms, products, physical fields and SGS; FP64 state, time integration, "
                          "boundary conditions, Chebyshev derivatives and eigenbasis solves"}
 
@@ -547,6 +603,14 @@ def main():
             profiles = run_profiles(args, st, u, v, w, stream)
         except Exception as e:  # reported in the line; the headline stands on its own
             profiles = {"error": f"{type(e).__name__}: {e}"}
+
+    # ---- the Orr-Sommerfeld linear test: growth rate in both forms against omega_i
+    os_growth = None
+    if not args.no_mixed:
+        try:
+            os_growth = run_os_growth(args, stream)
+        except Exception as e:  # reported in the line; the headline stands on its own
+            os_growth = {"error": f"{type(e).__name__}: {e}"}
 
     # ---- serving: a Poisson stream of ensemble runs (continuous batching on this GPU)
     serving = None
@@ -595,6 +659,7 @@ def main():
             "serving": serving,
             "ensemble": ensemble,
             "profiles": profiles,
+            "os_growth": os_growth,
         }
         print(json.dumps(line), flush=True)
     sol.close()

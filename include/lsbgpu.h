@@ -65,6 +65,13 @@ typedef struct {
                               tensor cores as BF16 three-way splits with FP32 accumulation, the
                               time integration, boundary conditions, second derivatives and
                               eigenbasis solves in FP64 (no reference counterpart) */
+    int bc3_top;           /* ceiling condition for u, v with bctype 3 (no reference counterpart):
+                              0 = the reference's u, v = -rhs/(k^2 + sigma/beta) on the ceiling
+                              row (src/navierstokes.f90:1340-1347), an outflow condition that the
+                              dipole's blowing half makes ill-posed (perturbations grow there);
+                              1 = the free stream, u' = v = 0 on the ceiling in the velocity
+                              Helmholtz solves (the projection then leaves a slip of
+                              dt beta dp/dx, dt beta dp/dy there) */
 } lsb_config;
 
 /* Host set-up arrays (inputs, as the reference passes diag/smat/simat): see

@@ -13,6 +13,17 @@ run/input.dat, plus the explicit extensions this implementation adds:
                        src/dealiasing.f90:329-330,435 bit for bit (negative ky modes
                        land at positive frequencies); "correct" is the textbook 3/2 rule.
 * ``ic = 2``        -- start from caller-supplied (seeded) perturbation fields.
+* ``bc3_top``       -- the ceiling condition for u, v with bctype 3.  0: the reference's
+                       u, v = -rhs/(k^2 + sigma/beta) on the ceiling row
+                       (src/navierstokes.f90:1340-1347), which lets the boundary values
+                       evolve by the momentum equation without z diffusion -- an outflow
+                       condition; where the zero-net-flux dipole blows fluid in, it is
+                       ill-posed and perturbations grow there until the run diverges (the
+                       oracle and the device alike, at any dt).  1 (default): the free
+                       stream, u' = v = 0 on the ceiling in the velocity Helmholtz solves
+                       (the projection then leaves a slip of dt beta grad p there).  The
+                       wall's Zang-Hussaini form (src/navierstokes.f90:1338) on the ceiling
+                       row is not used: with the pressure extrapolated there it diverges.
 * ``precision``     -- 0: FP64 throughout (the reference's arithmetic); 1: the mixed form,
                        with the nonlinear-term transforms and products in FP32 and its
                        first z derivatives on the tensor cores (BF16 three-way splits,
@@ -84,6 +95,7 @@ class LsbConfig:
     bc3_s: float = 7.5
     dealias_layout: str = "ref"
     precision: int = 0      # 0: FP64 throughout; 1: mixed form (FP32 nonlinear-term transforms)
+    bc3_top: int = 1        # bctype 3 ceiling for u, v: 0 the reference's outflow row, 1 free stream
     debug: int = 0
 
     @property

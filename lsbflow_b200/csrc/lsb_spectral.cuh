@@ -34,6 +34,7 @@ struct BcArgs {
     const double* rtop[3];    // ceiling planes of the velocity right-hand sides
     const double* pwall;      // wall plane of p^n
     const double* pnwall;     // wall plane of p^(n-1)
+    int top_free;             // 1: u' = v = 0 on the ceiling (bctype 3, bc3_top = 1)
     const double* d2w;        // [2][C] rows 1 and nzp of d2fdz2(w^n)
     const double* btop;       // spectral shape planes of bound(), or null
     const double* bwa;

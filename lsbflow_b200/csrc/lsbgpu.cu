@@ -689,6 +689,7 @@ void step_one(lsb_handle* h) {
     ba.bcp = h->bcp;
     ba.pwall = h->p + (long long)(d.nzp - 1) * C;
     ba.pnwall = h->pn + (long long)(d.nzp - 1) * C;
+    ba.top_free = (c.bctype == 3 && c.bc3_top == 1) ? 1 : 0;
     ba.d2w = h->d2w;
     ba.btop = h->bshape;
     ba.bwa = h->bshape + C;

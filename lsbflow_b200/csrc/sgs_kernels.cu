@@ -430,50 +430,65 @@ __global__ void k_static(P9 g, W9 tau, const double* __restrict__ sdelta,
 }
 
 // ---------------------------------------------------------------- sigma model
+// The FP64 sigma model rounds every operation as the reference's expressions do, one at a
+// time and left to right (no fused multiply-adds): its stresses are a near-cancellation
+// of singular values, so a contraction moves them far more than the operation's ulp.
+__device__ __forceinline__ double r_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double r_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double r_sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float r_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float r_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float r_sub(float a, float b) { return __fsub_rn(a, b); }
+// x**3. (a real power, pow of the C library in the reference): x*x and x*x*x formed with
+// their exact rounding errors (Dekker's two-product by fma), so the result is the exact
+// cube rounded once, up to a few units in the last bit's last half
+__device__ __forceinline__ double r_cube(double x) {
+    const double p = x * x, e = fma(x, x, -p);
+    const double q = p * x, f = fma(p, x, -q);
+    return q + fma(e, x, f);
+}
+__device__ __forceinline__ float r_cube(float x) { return x * x * x; }
+
 template <class T>
 __global__ void k_sigma(P9 g, W9 tau, const double* __restrict__ delta, long long P, int nxy) {
-    const T pi = (T)(4. * atan(1.));
+    const T pi = (T)3.141592653589793;  // 4 atan(1)
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < P; e += (long long)gridDim.x * blockDim.x) {
         const int k = (int)((unsigned)e / (unsigned)nxy);  // P < 2^31 (checked at create)
         T gij[3][3], G[3][3], G2[3][3];
         for (int l = 0; l < 3; ++l)
             for (int m = 0; m < 3; ++m) gij[l][m] = cp_<T>(g.p[3 * l + m])[e];
         for (int l = 0; l < 3; ++l)
-            for (int m = 0; m < 3; ++m) {
-                T s = (T)0;
-                for (int q = 0; q < 3; ++q) s += gij[q][l] * gij[q][m];  // (g^T g)(l,m)
-                G[l][m] = s;
-            }
+            for (int m = 0; m < 3; ++m)  // (g^T g)(l,m), summed over q = 1, 2, 3 in order
+                G[l][m] = r_add(r_add(r_mul(gij[0][l], gij[0][m]), r_mul(gij[1][l], gij[1][m])), r_mul(gij[2][l], gij[2][m]));
         for (int l = 0; l < 3; ++l)
-            for (int m = 0; m < 3; ++m) {
-                T s = (T)0;
-                for (int q = 0; q < 3; ++q) s += G[l][q] * G[q][m];
-                G2[l][m] = s;
-            }
-        const T i1 = G[0][0] + G[1][1] + G[2][2];
-        const T i2 = (T)0.5 * (i1 * i1 - (G2[0][0] + G2[1][1] + G2[2][2]));
-        const T i3 = G[0][0] * (G[1][1] * G[2][2] - G[1][2] * G[2][1]) -
-                     G[0][1] * (G[1][0] * G[2][2] - G[1][2] * G[2][0]) +
-                     G[0][2] * (G[1][0] * G[2][1] - G[1][1] * G[2][0]);
-        T a1 = i1 * i1 / (T)9 - i2 / (T)3;
-        const T a2 = i1 * i1 * i1 / (T)27 - i1 * i2 / (T)6 + (T)0.5 * i3;
+            for (int m = 0; m < 3; ++m)
+                G2[l][m] = r_add(r_add(r_mul(G[l][0], G[0][m]), r_mul(G[l][1], G[1][m])), r_mul(G[l][2], G[2][m]));
+        const T i1 = r_add(r_add(G[0][0], G[1][1]), G[2][2]);
+        const T i2 = r_mul((T)0.5, r_sub(r_mul(i1, i1), r_add(r_add(G2[0][0], G2[1][1]), G2[2][2])));
+        const T i3 = r_add(r_sub(r_mul(G[0][0], r_sub(r_mul(G[1][1], G[2][2]), r_mul(G[1][2], G[2][1]))),
+                                 r_mul(G[0][1], r_sub(r_mul(G[1][0], G[2][2]), r_mul(G[1][2], G[2][0])))),
+                           r_mul(G[0][2], r_sub(r_mul(G[1][0], G[2][1]), r_mul(G[1][1], G[2][0]))));
+        T a1 = r_sub(r_mul(i1, i1) / (T)9, i2 / (T)3);
+        const T a2 = r_add(r_sub(r_cube(i1) / (T)27, r_mul(i1, i2) / (T)6), r_mul((T)0.5, i3));
         if (a1 < (T)0) a1 = fabs(a1);
         const T sq = sqrt(a1);
-        const T pre = a2 / pow(sq, (T)3);
+        const T pre = a2 / r_cube(sq);
         T a3;
         if (pre >= (T)1 || isnan(pre)) a3 = (T)0;
         else if (pre <= (T)-1) a3 = pi / (T)3;
         else a3 = acos(pre) / (T)3;
-        const T s1 = sqrt(fabs(i1 / (T)3 + (T)2 * sq * cos(a3)));
-        const T s2 = sqrt(fabs(i1 / (T)3 - (T)2 * sq * cos(pi / (T)3 + a3)));
-        const T s3 = sqrt(fabs(i1 / (T)3 - (T)2 * sq * cos(pi / (T)3 - a3)));
-        T ds = s3 * (s1 - s2) * (s2 - s3);
-        if (s1 != (T)0) ds = ds / (s1 * s1);
+        const T sq2 = r_mul((T)2, sq);
+        const T s1 = sqrt(fabs(r_add(i1 / (T)3, r_mul(sq2, cos(a3)))));
+        const T s2 = sqrt(fabs(r_sub(i1 / (T)3, r_mul(sq2, cos(r_add(pi / (T)3, a3))))));
+        const T s3 = sqrt(fabs(r_sub(i1 / (T)3, r_mul(sq2, cos(r_sub(pi / (T)3, a3))))));
+        T ds = r_mul(r_mul(s3, r_sub(s1, s2)), r_sub(s2, s3));
+        if (s1 != (T)0) ds = ds / r_mul(s1, s1);
         if (ds < (T)0 || isnan(ds)) ds = (T)0;
         const T cd = (T)(1.35 * delta[k]);
-        const T nu = -(cd * cd) * ds;
+        const T nu = r_mul(-r_mul(cd, cd), ds);
         for (int l = 0; l < 3; ++l)
-            for (int m = 0; m < 3; ++m) wp_<T>(tau.p[3 * l + m])[e] = (T)2 * nu * (T)0.5 * (gij[l][m] + gij[m][l]);
+            for (int m = 0; m < 3; ++m)
+                wp_<T>(tau.p[3 * l + m])[e] = r_mul(r_mul(r_mul((T)2, nu), (T)0.5), r_add(gij[l][m], gij[m][l]));
     }
 }
 

@@ -75,14 +75,19 @@ __global__ void k_bc_planes(BcArgs a) {
         const double psr = a.pfac0 * a.pwall[re] + a.pfac1 * a.pnwall[re];
         const double psi = a.pfac0 * a.pwall[im] + a.pfac1 * a.pnwall[im];
         const double dtb = a.dt * a.bdfv;
-        // u
-        a.bc[0][re] = -a.rtop[0][re] / den;
-        a.bc[0][im] = -a.rtop[0][im] / den;
+        // u, v: the ceiling row of the momentum equation without z diffusion (the reference),
+        // or the free stream (u' = v = 0 in the velocity solves)
+        if (a.top_free) {
+            a.bc[0][re] = a.bc[0][im] = 0.0;
+            a.bc[1][re] = a.bc[1][im] = 0.0;
+        } else {
+            a.bc[0][re] = -a.rtop[0][re] / den;
+            a.bc[0][im] = -a.rtop[0][im] / den;
+            a.bc[1][re] = -a.rtop[1][re] / den;
+            a.bc[1][im] = -a.rtop[1][im] / den;
+        }
         a.bc[0][a.C + re] = dtb * (-wx * psi);
         a.bc[0][a.C + im] = dtb * (wx * psr);
-        // v
-        a.bc[1][re] = -a.rtop[1][re] / den;
-        a.bc[1][im] = -a.rtop[1][im] / den;
         a.bc[1][a.C + re] = dtb * (-wy * psi);
         a.bc[1][a.C + im] = dtb * (wy * psr);
         // w

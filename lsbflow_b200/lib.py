@@ -48,7 +48,7 @@ class LsbConfigC(C.Structure):
         ("bc3_amp", C.c_double), ("bc3_xc", C.c_double), ("bc3_s", C.c_double),
         ("fsize", C.c_double),
         ("dtadapt", C.c_int), ("iomod", C.c_int), ("ifilt", C.c_int), ("modfilt", C.c_int),
-        ("otfavg", C.c_int), ("istartavg", C.c_int), ("precision", C.c_int),
+        ("otfavg", C.c_int), ("istartavg", C.c_int), ("precision", C.c_int), ("bc3_top", C.c_int),
     ]
 
 
@@ -123,7 +123,7 @@ def config_struct(cfg: LsbConfig) -> LsbConfigC:
         cfg.kc, cfg.filt_order, cfg.filt_amp, cfg.istartbound, cfg.samp,
         cfg.bc3_amp, cfg.bc3_xc, cfg.bc3_s, cfg.fsize,
         cfg.dtadapt, cfg.iomod, cfg.ifilt, cfg.modfilt, getattr(cfg, "otfavg", 0), getattr(cfg, "istartavg", 0),
-        getattr(cfg, "precision", 0),
+        getattr(cfg, "precision", 0), getattr(cfg, "bc3_top", 1),
     )
 
 

@@ -737,6 +737,11 @@ def navierstokes_update(st: Setup, s: State):
         uif[2][nzp - 1] = c.xnu * dt * bdfv * dwdzf[nzp - 1]
     dpf = dfdy(st, psf)
     uif[1][nzp - 1] = dt * bdfv * dpf[nzp - 1]
+    if c.bctype == 3 and getattr(c, "bc3_top", 0) == 1:
+        # extension (no reference counterpart): the free stream on the ceiling, u' = v = 0
+        # in the velocity solves
+        uif[0][0] = 0.0
+        uif[1][0] = 0.0
     for l in range(3):
         if active or c.forcing == 1:
             solve_nhom_helmholtz(st, rhsf[l], uif[l], dtnui / bdfv)

@@ -39,6 +39,10 @@ class FakeSolver:
     def device_bytes(self):
         return 1 << 20
 
+    def diag(self):
+        self.ndiag = getattr(self, "ndiag", 0) + 1
+        return {"nonfinite": 0, "umax": 1.0, "energy_pert": float(np.exp(1e-3 * self.ndiag))}
+
     def spanwise_stats(self):
         c = self.cfg
         m = np.ones((4, c.nzp, c.nx)) * (1.0 + 1e-7 * c.precision)
@@ -97,6 +101,28 @@ def test_profiles_compare_the_two_forms(monkeypatch, small_st):
     assert out["steps"] == 100 and out["target"] == 1e-4
     assert out["max_rel_err_mean_velocity"] == pytest.approx(1e-7, rel=1e-3)
     assert set(out["rel_err_rms"]) == set("uvwp")
+
+
+def test_profiles_report_a_nonfinite_run(monkeypatch, small_st):
+    class Diverging(FakeSolver):
+        def diag(self):
+            return {"nonfinite": 1, "umax": 1.0, "energy_pert": 0.0}
+
+    monkeypatch.setattr(lib, "Solver", Diverging)
+    out = bench.run_profiles(types.SimpleNamespace(profile_steps=200), small_st, None, None, None,
+                             types.SimpleNamespace(cuda_stream=0))
+    assert out["first_nonfinite_step"] == {"fp64": 100} and "error" in out
+
+
+def test_os_growth_section(monkeypatch):
+    monkeypatch.setattr(lib, "Solver", FakeSolver)
+    out = bench.run_os_growth(types.SimpleNamespace(), types.SimpleNamespace(cuda_stream=0))
+    assert out["steps"] == 500 and out["omega_i"] > 0
+    # E grows by exp(1e-3) per step: <dE/dt> = (1 - exp(-1e-3)) / (2 dt)
+    g = (1.0 - np.exp(-1e-3)) / (2 * 0.005)
+    for form in ("fp64", "mixed"):
+        assert out[form]["mean_growth"] == pytest.approx(g, rel=1e-9)
+    assert out["mixed_rel_err_vs_fp64"] == pytest.approx(0.0, abs=1e-12)
 
 
 def test_serving_section(monkeypatch):

@@ -173,6 +173,7 @@ STEP_CASES = [
     ("bctype0-hom", dict(dealiasflag=0, bctype=0, forcing=0)),
     ("bctype1", dict(dealiasflag=2, bctype=1, samp=0.3)),
     ("bctype2", dict(dealiasflag=2, bctype=2)),
+    ("dipole-ref-ceiling", dict(dealiasflag=1, dealias_layout="correct", bc3_top=0)),
 ]
 
 
@@ -205,8 +206,12 @@ def test_steps_match_dense_oracle(name, over):
 # The sigma model's singular values come from a trigonometric solution of the
 # characteristic cubic (src/sgsterm.f90:334-364); a 1e-16 relative perturbation of
 # the velocity gradient moves its tau by 1e-7 (diagonal) to 1e-5 (small off-diagonal
-# components) relative on these fields, so whole sigma-model steps are held to 2e-6.
-TOL_SIGMA_STEP = 2e-6
+# components) relative on these fields.  The device evaluates the reference's
+# expressions one rounding at a time (no fused multiply-adds, x**3. as a once-rounded
+# cube), which leaves the 1-ulp differences of acos and cos between CUDA and the C
+# library: on identical gradients tau then differs by 2e-8 (diagonal) to 3e-6 (small
+# off-diagonal components), and five whole steps by 1.6e-7; they are held to 5e-7.
+TOL_SIGMA_STEP = 5e-7
 
 
 @pytest.mark.parametrize("model", [0, 1, 2, 3, 4])
