@@ -53,24 +53,58 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle samples during the timed region."""
+    """SM clock and throttle-reason samples taken during the timed region: NVML read every
+    5 ms from a helper thread when the library is there, else nvidia-smi every 20 ms.  Both
+    only read the GPU's state."""
+
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    # NVML clock-event reason bits of those names
+    BITS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20, "sw_power_cap": 0x4}
 
     def __init__(self, index: int):
         self.index = index
-        self.samples = []
+        self.samples = []  # (time, sm_mhz, sm_max_mhz, set of active reason names)
         self._stop = threading.Event()
         self._proc = None
+        self._t = None
+        self.source = None
 
     def __enter__(self):
+        try:
+            import pynvml as N
+            N.nvmlInit()
+            h = N.nvmlDeviceGetHandleByIndex(self.index)
+            mx = float(N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM))
+            get_reasons = getattr(N, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                N.nvmlDeviceGetCurrentClocksThrottleReasons
+
+            def poll():
+                while not self._stop.is_set():
+                    try:
+                        sm = float(N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM))
+                        bits = int(get_reasons(h))
+                        act = {n for n, b in self.BITS.items() if bits & b}
+                        self.samples.append((time.perf_counter(), sm, mx, act))
+                    except Exception:
+                        pass
+                    time.sleep(0.005)
+
+            self._t = threading.Thread(target=poll, daemon=True)
+            self._t.start()
+            self.source = "nvml, every 5 ms"
+            return self
+        except Exception:
+            pass
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self._proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "20"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self._t = threading.Thread(target=self._read, daemon=True)
             self._t.start()
+            self.source = "nvidia-smi, every 20 ms"
         except Exception:
             self._proc = None
         return self
@@ -79,13 +113,18 @@ class ClockSampler:
         for line in self._proc.stdout:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) >= 9:
-                self.samples.append((time.perf_counter(), parts))
+                try:
+                    sm, mx = float(parts[1]), float(parts[2])
+                except ValueError:
+                    continue
+                act = {n for n, v in zip(self.NAMES, parts[5:9]) if v.lower() == "active"}
+                self.samples.append((time.perf_counter(), sm, mx, act))
 
     def wait_first(self, timeout_s: float = 5.0):
-        """Block until nvidia-smi delivered its first sample, so the timed region is covered."""
+        """Block until the first sample arrived, so the timed region is covered."""
         t0 = time.perf_counter()
-        while self._proc is not None and not self.samples and time.perf_counter() - t0 < timeout_s:
-            time.sleep(0.01)
+        while self._t is not None and not self.samples and time.perf_counter() - t0 < timeout_s:
+            time.sleep(0.002)
 
     def mark(self, start: bool):
         if start:
@@ -94,45 +133,44 @@ class ClockSampler:
             self.t_end = time.perf_counter()
 
     def __exit__(self, *exc):
+        self._stop.set()
         if self._proc is not None:
             self._proc.terminate()
             try:
                 self._proc.wait(timeout=5)
             except Exception:
                 self._proc.kill()
+        if self._t is not None:
+            self._t.join(timeout=2)
 
     def summary(self):
         t0, t1 = getattr(self, "t_start", 0.0), getattr(self, "t_end", float("inf"))
-        inside = [s for ts, s in self.samples if t0 <= ts <= t1 + 0.25]
+        inside = [s for s in self.samples if t0 <= s[0] <= t1]
         if not inside:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        self_samples = inside
-        sm = [float(s[1]) for s in self_samples if s[1].replace(".", "").isdigit()]
-        mx = [float(s[2]) for s in self_samples if s[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({n for s in self_samples for n, v in zip(names, s[5:9]) if v.lower() == "active"})
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self_samples)}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "source": self.source}
+        sm = [s[1] for s in inside]
+        reasons = sorted(set().union(*[s[3] for s in inside]))
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(s[2] for s in inside), "reasons": reasons,
+                "samples": len(inside), "source": self.source}
+
+
+CPU_KIND = "port"
+CPU_WHAT = "the C++/OpenMP restatement of the reference's FP64 step (oracle/cpu_step.cpp)"
 
 
 def cpu_reference_step_time(cfg, max_steps: int, budget_s: float, warmup: int, threads: int):
-    """The FP64 oracle (a NumPy restatement of the reference's step) on the host cores."""
-    from oracle import lsb_oracle as O
-    O.WORKERS = threads
+    """Seconds per step of the C++/OpenMP restatement of the reference's FP64 step
+    (oracle/cpu_step.cpp, parity-tested against the NumPy oracle) on ``threads`` host
+    threads, and the steps timed: a bounded sample of at most ``max_steps`` steps, fewer
+    when a probe step says they would take longer than ``budget_s``."""
+    from oracle import cpu_baseline as CB
     st = hs.make_setup(cfg)
     u, v, w = ic.seeded_noise(st, 0, 5e-3)
-    s = O.State.zeros_like(st, u, v, w, st.dt)
-    for _ in range(warmup):
-        O.timestep(st, s)
-    times = []
-    t_all = time.perf_counter()
-    for _ in range(max_steps):
-        t0 = time.perf_counter()
-        O.timestep(st, s)
-        times.append(time.perf_counter() - t0)
-        if time.perf_counter() - t_all > budget_s:
-            break
-    return float(np.mean(times)), len(times)
+    probe, _ = CB.run(st, u, v, w, max(1, warmup), threads, want_state=False)
+    per = probe / max(1, warmup)
+    n = int(max(1, min(max_steps, budget_s / max(per, 1e-9))))
+    sec, _ = CB.run(st, u, v, w, n, threads, want_state=False)
+    return sec / n, n
 
 
 def run_reference(args, cfg):
@@ -141,19 +179,19 @@ def run_reference(args, cfg):
         return
     threads = os.cpu_count() or 1
     pts = cfg.nx * cfg.ny * cfg.nzp
-    warm = min(args.warmup, 1)
-    t_step, n = cpu_reference_step_time(cfg, args.steps, 150.0, warm, threads)
+    warm = max(1, min(args.warmup, 3))
+    t_step, n = cpu_reference_step_time(cfg, args.steps, 120.0, warm, threads)
     val = pts / t_step
     line = {
         "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
         "steps": n, "warmup": warm, "ms_per_step": t_step * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"{WORKLOAD}: 256x64x129 (ref nx,ny,nzp) dyn-Smagorinsky LES, 3/2 dealias"},
-        "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{n} full time steps of the same workload (FP64 NumPy/SciPy oracle, "
-                                   f"scipy.fft with {threads} workers, BLAS contractions)"},
+        "config": {"workload": f"{WORKLOAD}: 256x64x129 (ref nx,ny,nzp), padded 384x96, dyn-Smagorinsky LES, "
+                               f"dealias 3/2, fringe, dipole BC, dt={cfg.dt_fixed}"},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": CPU_KIND,
+                         "sample": f"{n} full time steps of the same workload with {CPU_WHAT} on {threads} threads"},
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "the reference (Fortran+MPI+FFTW+LAPACK) cannot be built here; its restatement is timed",
+        "note": "the reference (Fortran + MPI + FFTW + LAPACK) cannot be built here; its restatement is timed",
     }
     print(json.dumps(line), flush=True)
 
@@ -220,35 +258,38 @@ def tune_schedule(args, st, sol):
 
 
 def run_serving(args, rank):
-    """A seeded Poisson stream (4/s) of ensemble runs through the request loop, first with
-    every run on its own stream, then with same-shape runs stepped as one ensemble batch."""
+    """The survey's serving stream through the request loop: Poisson arrivals (4/s) of runs
+    on 64x16x65, 128x32x97 and 256x64x129 grids with no SGS model or the static, dynamic,
+    sigma or interscale model, Re_delta*, dipole amplitude and position drawn per run, and
+    horizons of 300-3000 steps; the same stream in FP64 and in the mixed form, each run on
+    its own stream, and the FP64 stream again with same-shape runs stepped as one ensemble
+    batch."""
     from lsbflow_b200 import serving as S
 
-    shapes = [workload("ens128"), workload("ens128", sgsmodel=1), workload("dns64", dealiasflag=1)]
-    reqs = S.poisson_requests(args.serve_runs, 4.0, 11 + rank, shapes, steps_range=(100, 400))
-    srv = S.Server(chunk=20)
-    for r in reqs:
-        srv.submit(r)
-    res = srv.run()
-    summ = S.summary(res, srv.elapsed)
-    serving = {"runs": summ["runs"], "runs_per_hour": round(summ["runs_per_hour"], 1),
-               "p50_s": round(summ["p50"], 4), "p99_s": round(summ["p99"], 4),
-               "pt_steps_per_s": summ["pt_steps_per_s"], "elapsed_s": round(summ["elapsed_s"], 3),
-               "arrivals": "Poisson 4/s, seeded", "mix": "ens128 sigma / ens128 dyn-Smagorinsky / dns64",
-               "horizon_steps": [100, 400]}
-    # the same stream with same-shape runs stepped as one ensemble batch per shape
-    try:
-        srv = S.Server(chunk=20, group=True)
+    def one(precision, group=False):
+        reqs = S.stream_requests(args.serve_runs, 4.0, 11 + rank, precision=precision)
+        srv = S.Server(chunk=50, group=group)
         for r in reqs:
             srv.submit(r)
         res = srv.run()
         summ = S.summary(res, srv.elapsed)
-        serving["grouped"] = {"runs_per_hour": round(summ["runs_per_hour"], 1),
-                              "p50_s": round(summ["p50"], 4), "p99_s": round(summ["p99"], 4),
-                              "pt_steps_per_s": summ["pt_steps_per_s"],
-                              "elapsed_s": round(summ["elapsed_s"], 3)}
-    except Exception as e:  # reported in the line; the ungrouped numbers above stand
-        serving["grouped"] = {"error": f"{type(e).__name__}: {e}"}
+        return {"runs": summ["runs"], "runs_per_hour": round(summ["runs_per_hour"], 1),
+                "p50_s": round(summ["p50"], 4), "p99_s": round(summ["p99"], 4),
+                "pt_steps_per_s": summ["pt_steps_per_s"], "elapsed_s": round(summ["elapsed_s"], 3)}
+
+    serving = {"arrivals": "Poisson 4/s, seeded",
+               "mix": "grids 64x16x65 / 128x32x97 / 256x64x129 (ref nx,ny,nzp) x SGS none / static / dynamic / "
+                      "sigma / interscale, Re_d* ~ U[300,800], A ~ U[0.1,0.4], x0 ~ U[60,100] d*",
+               "horizon_steps": [300, 3000]}
+    serving["fp64"] = one(0)
+    try:
+        serving["mixed"] = one(1)
+    except Exception as e:  # reported in the line; the FP64 numbers above stand
+        serving["mixed"] = {"error": f"{type(e).__name__}: {e}"}
+    try:
+        serving["fp64_grouped"] = one(0, group=True)
+    except Exception as e:
+        serving["fp64_grouped"] = {"error": f"{type(e).__name__}: {e}"}
     return serving
 
 
@@ -383,6 +424,18 @@ def run_ensemble(args, rank, world, stream, max_over_ranks, barrier):
         launches = lib.kernel_launches() - n0
         ms = max_over_ranks(e0.elapsed_time(e1))
         b.close()
+        # every member's velocity after the batch's steps, for the mixed form's error per member
+        finals = [s_.download() for s_ in sols]
+        vel = [np.concatenate([o_[k].ravel() for k in ("uf", "vf", "wf")]) for o_ in finals]
+        if prec == 0:
+            ref_vel = vel
+        else:
+            errs = [float(np.linalg.norm(a - b_) / np.linalg.norm(b_)) for a, b_ in zip(vel, ref_vel)]
+            out["mixed_rel_err_velocity_per_member"] = {
+                "steps": max(args.warmup, 3) + 6 + steps, "max": max(errs), "median": float(np.median(errs)),
+                "min": min(errs), "members": [round(e_, 9) for e_ in errs],
+                "note": "sigma-model members: the model's trigonometric singular values are ill-conditioned "
+                        "near equal singular values, so FP32 inputs move them far more than FP32 rounding"}
         # one member alone on the same stream (its own step graphs)
         s0 = sols[0]
         s0.set_stream(stream.cuda_stream)
@@ -593,8 +646,10 @@ def main():
                  "rel_err_velocity_after_100_steps": rel(vg, vr),
                  "rel_err_components": {k: rel(got[k], ref[k]) for k in ("uf", "vf", "wf", "pf")},
                  "kernel_groups": groups_m,
-                 "form": "FP32 transforms, products, physical fields and SGS; FP64 state, time integration, "
-                         "boundary conditions, Chebyshev derivatives and eigenbasis solves"}
+                 "form": "FP32 transforms, products, physical fields and SGS; z derivatives of the nonlinear "
+                         "term and velocity Helmholtz solves on the int8 tensor cores (5 digits per operand, "
+                         "exact int32 accumulation); FP64 state, time integration, boundary conditions, "
+                         "Poisson solve, pressure and projection"}
 
     # ---- mean / rms profiles of the mixed form against FP64 after a long run
     profiles = None
@@ -633,10 +688,10 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        t_step, n = cpu_reference_step_time(cfg, 2, 40.0, 0, threads)
-        cpu = {"value": pts / t_step, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"{n} time step(s) of the same {nx}x{ny}x{nzp} workload with the FP64 NumPy oracle "
-                         f"(scipy.fft with {threads} workers)"}
+        t_step, n = cpu_reference_step_time(cfg, 10, 20.0, 1, threads)
+        cpu = {"value": pts / t_step, "unit": UNIT, "cores": threads, "kind": CPU_KIND,
+               "sample": f"{n} time step(s) of the same {nx}x{ny}x{nzp} workload with {CPU_WHAT} on "
+                         f"{threads} threads"}
 
     if rank == 0:
         line = {

@@ -60,11 +60,14 @@ typedef struct {
                               TNS automatic filtering when sgsmodel = 4, else filterall3pt */
     int otfavg, istartavg; /* on-the-fly time averages of u, v, w, p (src/main.f90:70-76) */
     int precision;         /* 0: FP64 throughout (the reference's arithmetic); 1: mixed form --
-                              the nonlinear-term transforms and products in FP32 with FP32
-                              y-intermediates, the nonlinear term's first z derivatives on the
-                              tensor cores as BF16 three-way splits with FP32 accumulation, the
-                              time integration, boundary conditions, second derivatives and
-                              eigenbasis solves in FP64 (no reference counterpart) */
+                              the nonlinear-term transforms, products and SGS model in FP32
+                              with FP32 y-intermediates (the padded passes in FP64 when the
+                              3/2-rule x length has no full-warp register plan), the nonlinear
+                              term's z derivatives and the three velocity Helmholtz solves on
+                              the int8 tensor cores (five int8 digits per operand with power-
+                              of-two scales, exact int32 accumulation); the state, time
+                              integration, boundary conditions, Poisson solve, pressure and
+                              projection in FP64 (no reference counterpart) */
     int bc3_top;           /* ceiling condition for u, v with bctype 3 (no reference counterpart):
                               0 = the reference's u, v = -rhs/(k^2 + sigma/beta) on the ceiling
                               row (src/navierstokes.f90:1340-1347), an outflow condition that the
@@ -199,9 +202,11 @@ int lsb_batch_synchronize(lsb_batch* b);
 /* launch the ensemble graphs on a caller stream (cudaStream_t as void*; NULL restores the
  * batch's own); an event recorded there after lsb_batch_step follows every member's steps */
 int lsb_batch_set_stream(lsb_batch* b, void* stream);
-/* enable = 0: drop the ensemble graphs and step the members one by one; enable = 1 after
- * a member's lsb_set_schedule or lsb_graphs makes the batch capture its graphs anew (the
- * ensemble graphs hold the launches as captured) */
+/* enable = 0: drop the ensemble graphs and step the members one by one; enable = 1 (the
+ * default) captures them again when needed.  A member's lsb_set_schedule or lsb_graphs
+ * changes its graph generation, which is part of the ensemble graphs' key: the batch then
+ * captures new ensemble graphs by itself (or steps members one by one while that member's
+ * graphs are off) */
 int lsb_batch_graphs(lsb_batch* b, int enable);
 
 /* ---------------- Tier 1: the reference's subroutine interfaces (host arrays) --------- */
@@ -240,7 +245,11 @@ int lsb_tau_sgs(lsb_handle* h, const double* ui, const double* uiuj, const doubl
  * columns are processed in chunks that fit the array); larger nz returns
  * LSB_ERR_UNSUPPORTED.  The first call on a device looks up the array's address, so make
  * it before any stream capture.  Calls share the array: calls that overlap on the GPU
- * race and must be serialised by the caller.  stream is a cudaStream_t (NULL = default). */
+ * race and must be serialised by the caller.  stream is a cudaStream_t of the current
+ * device (NULL = default); a stream of another device returns LSB_ERR_ARG.  The address
+ * found on the first call is kept for the life of the process: a device reset
+ * (cudaDeviceReset, or the primary context destroyed and made again) is not supported
+ * afterwards. */
 #define LSB_NOALLOC_SCRATCH_BYTES (8u << 20)
 int lsb_solve_helmholtz_noalloc(int nx, int ny, int nz, const double* rhs, double* out, const double* lam,
                                 const double* e, const double* ei, const double* wavx, const double* wavy,

@@ -25,9 +25,11 @@ run/input.dat, plus the explicit extensions this implementation adds:
                        wall's Zang-Hussaini form (src/navierstokes.f90:1338) on the ceiling
                        row is not used: with the pressure extrapolated there it diverges.
 * ``precision``     -- 0: FP64 throughout (the reference's arithmetic); 1: the mixed form,
-                       with the nonlinear-term transforms and products in FP32 and its
-                       first z derivatives on the tensor cores (BF16 three-way splits,
-                       FP32 accumulation).
+                       with the nonlinear-term transforms, products and SGS model in FP32
+                       and the z derivatives of the nonlinear term and the velocity
+                       Helmholtz solves on the int8 tensor cores (five int8 digits per
+                       operand, exact int32 accumulation); the Poisson solve, the pressure
+                       and the state stay FP64.
 
 Sizes follow the reference's axes: x streamwise Fourier (nx), y spanwise Fourier
 (ny), z vertical Chebyshev with nzp = nz+1 points, k=1 the ceiling, k=nzp the wall.

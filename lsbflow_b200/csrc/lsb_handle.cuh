@@ -67,7 +67,7 @@ struct lsb_handle {
     double *p = nullptr, *pn = nullptr;                       // S each
     // scratch
     double *filt = nullptr, *dz = nullptr, *H = nullptr, *rhs = nullptr, *T = nullptr, *divf = nullptr;
-    lsb::UmmaMat u_dz1;          // mixed form: split dz1 for the tcgen05 z derivatives
+    lsb::OzMat oz_dz1, oz_ei, oz_eext;  // mixed form: int8 digits of D, E^-1, E (tensor cores)
     int* uerr = nullptr;         // device word raised by a tensor-core kernel whose wait timed out
     double *Y = nullptr;     // 18 y-intermediates on the (padded) transform grid
     double *Yu = nullptr;    // 12 y-intermediates on the unpadded grid
@@ -82,6 +82,9 @@ struct lsb_handle {
     int sgs_nwall = 0;
     // per kernel-group CUDA-event timers (lsb_timers / lsb_timer_report)
     bool timing = false;
+    // mixed form: the nonlinear term's padded-grid transforms and products in FP32 (false when
+    // the padded x length has no full-warp register plan: those passes then run in FP64)
+    bool nl_f32 = false;
     std::map<std::string, std::vector<std::pair<cudaEvent_t, cudaEvent_t>>> timers;
     static constexpr int kPhys = 24;
     long long Yl = 0, Yu1 = 0, P = 0;
@@ -102,10 +105,14 @@ struct lsb_handle {
     std::vector<StepGraph> graphs;
     bool graphs_on = true;
     lsb_schedule sched{};  // launch schedule (lsb_set_schedule); zeros: the built-in models
+    // bumped whenever the step graphs are dropped (a new schedule, graphs switched): the
+    // ensemble graphs that captured this member's launches carry it in their key
+    unsigned long long graph_gen = 0;
     void drop_graphs() {
         for (auto& g : graphs)
             if (g.exec) cudaGraphExecDestroy(g.exec);
         graphs.clear();
+        ++graph_gen;
     }
 
     size_t device_bytes = 0;  // sum of this handle's device allocations

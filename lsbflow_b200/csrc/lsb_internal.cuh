@@ -193,15 +193,25 @@ void launch_gemm(const GemmArgs& g, cudaStream_t s);
 void launch_spanwise_stats(const double* ph, double* mean, double* rms, int nf, int nx, int ny, int nzp, long long P,
                            cudaStream_t s);
 
-// mixed form: the z derivative as BF16-split tcgen05 MMAs (umma_kernels.cu)
-struct UmmaMat {
-    const uint16_t* img = nullptr;  // device: the three BF16 splits in the shared-memory image
+// mixed form: z contractions on the int8 tensor cores, operands split into int8 digits with
+// power-of-two scales (ozaki_kernels.cu)
+struct OzMat {
+    const uint8_t* img = nullptr;   // device: matrix digits in the shared-memory image
+    const double* rscale = nullptr; // device [nmma]: 2^e_r per row
+    const double* arow = nullptr;   // device [K]: FP64 row 128 (M == 129), or null
+    const double* acol = nullptr;   // device [128]: FP64 column 128 (K == 129), or null
     unsigned img_bytes = 0;
-    int M = 0, K = 0, npad = 0, nsteps = 0;
+    int M = 0, K = 0, nmma = 0, kin = 0, ksteps = 0;
+    int digits = 0;                 // int8 digits per operand (5)
 };
-UmmaMat make_umma_mat(const double* A, int M, int K, std::vector<uint16_t>& img);
-// false when it does not apply (epilogue other than store / axpby, N > 256, limits)
-bool launch_umma_dz(const GemmArgs& g, const UmmaMat& um, int* err, cudaStream_t s);
-
+struct OzHost {                     // the host side of an OzMat, before upload
+    OzMat mat;
+    std::vector<uint8_t> img;
+    std::vector<double> rscale, arow, acol;
+};
+// false when M or K is above 129 or S is not 5
+bool make_ozaki_mat(const double* A, int M, int K, int S, OzHost& out);
+// false when it does not apply (matrix sizes, shared memory refused)
+bool launch_ozaki(const GemmArgs& g, const OzMat& om, int* err, cudaStream_t s);
 
 }  // namespace lsb

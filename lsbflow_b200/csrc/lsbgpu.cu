@@ -192,6 +192,27 @@ GemmArgs gemm_base(lsb_handle* h, const Mat& m) {
     return g;
 }
 
+// a matrix's int8 digits for the mixed form's tensor-core contractions, on the device (an
+// empty OzMat when the sizes do not apply: those contractions stay FP64)
+OzMat upload_ozaki(lsb_handle* h, const double* A, int M, int K, int S) {
+    OzHost oh;
+    if (!make_ozaki_mat(A, M, K, S, oh)) return OzMat{};
+    OzMat om = oh.mat;
+    om.img = reinterpret_cast<const uint8_t*>(
+        h->upload(reinterpret_cast<const double*>(oh.img.data()), (oh.img.size() + 7) / 8));
+    om.rscale = h->upload(oh.rscale.data(), oh.rscale.size());
+    if (!oh.arow.empty()) om.arow = h->upload(oh.arow.data(), oh.arow.size());
+    if (!oh.acol.empty()) om.acol = h->upload(oh.acol.data(), oh.acol.size());
+    return om;
+}
+
+// a z contraction: on the int8 tensor cores in the mixed form when the matrix has digits
+// there, else the FP64 tensor-core MMA
+void contract(lsb_handle* h, const GemmArgs& g, const OzMat& om) {
+    if (h->cfg.precision == 1 && om.img && launch_ozaki(g, om, h->uerr, h->stream)) return;
+    launch_gemm(g, h->stream);
+}
+
 }  // namespace
 
 namespace lsb {
@@ -216,8 +237,13 @@ void zgemm1(lsb_handle* h, const Mat& m, const double* in, double* out, int nf) 
 }
 
 // Helmholtz / Poisson solve of nf fields (stride S): out = solve(rhs, sigma) with the
-// lifting functions of solve_nhom_helmholtz when bc != null (bc: [nf][2][C], ceiling first)
-void helmholtz(lsb_handle* h, const double* rhs, double* out, int nf, double sigma, const double* bc) {
+// lifting functions of solve_nhom_helmholtz when bc != null (bc: [nf][2][C], ceiling first).
+// tc: the mixed form's int8 tensor-core contractions where the handle has them (the
+// velocity solves); the Poisson solve keeps FP64 contractions in both forms, because the
+// pressure -(Dw + div)/(k^2 dt bdfv) is a near-cancellation that turns their error into
+// pressure error a thousandfold and more.
+void helmholtz(lsb_handle* h, const double* rhs, double* out, int nf, double sigma, const double* bc,
+               bool tc = true) {
     const long long C = h->d.C();
     GemmArgs g1 = gemm_base(h, h->m_ei);
     g1.in = rhs;
@@ -233,7 +259,7 @@ void helmholtz(lsb_handle* h, const double* rhs, double* out, int nf, double sig
         g1.bc_fstride = 2 * C;
         g1.lift_sigma = sigma;
     }
-    launch_gemm(g1, h->stream);
+    contract(h, g1, tc ? h->oz_ei : OzMat{});
     GemmArgs g2 = gemm_base(h, h->m_eext);
     g2.in = h->T;
     g2.out = out;
@@ -244,7 +270,7 @@ void helmholtz(lsb_handle* h, const double* rhs, double* out, int nf, double sig
         g2.bct = bc;
         g2.bc_fstride = 2 * C;
     }
-    launch_gemm(g2, h->stream);
+    contract(h, g2, tc ? h->oz_eext : OzMat{});
 }
 
 YPassArgs ypass(lsb_handle* h, bool padded, int nzp) {
@@ -352,16 +378,12 @@ void nlterm(lsb_handle* h, const double* uin, double* Nout) {
     // du_l/dz
     {
         TimerScope ts(h, "gemm_dz");
-        bool done = false;
-        if (h->cfg.precision == 1) {
-            GemmArgs g = gemm_base(h, h->m_dz1);
-            g.in = uin;
-            g.out = h->dz;
-            g.nfields = 3;
-            g.epi = EPI_STORE;
-            done = launch_umma_dz(g, h->u_dz1, h->uerr, h->stream);
-        }
-        if (!done) zgemm1(h, h->m_dz1, uin, h->dz, 3);
+        GemmArgs g = gemm_base(h, h->m_dz1);
+        g.in = uin;
+        g.out = h->dz;
+        g.nfields = 3;
+        g.epi = EPI_STORE;
+        contract(h, g, h->oz_dz1);
     }
     // spanwise inverse: u_l, du_l/dy, du_l/dz  -> Y[0..8]
     YInvJobList yj{};
@@ -371,13 +393,14 @@ void nlterm(lsb_handle* h, const double* uin, double* Nout) {
         yj.j[3 + l] = YInvJob{uin + l * S, h->Y + (long long)(3 + l) * h->Yl, YM_IKY};
         yj.j[6 + l] = YInvJob{h->dz + l * S, h->Y + (long long)(6 + l) * h->Yl, YM_COPY};
     }
-    const int f32 = h->cfg.precision == 1 ? 1 : 0;
+    const int f32 = h->cfg.precision == 1 ? 1 : 0;  // the physical (unpadded) fields
+    const int f32nl = (f32 && h->nl_f32) ? 1 : 0;     // the padded product passes
     YPassArgs ya = ypass(h, dealias, d.nzp);
-    ya.f32 = f32;
+    ya.f32 = f32nl;
     { TimerScope ts(h, "yinv_nl"); launch_yinv(yj, ya, h->stream); }
     NlRowArgs na{};
     na.r = rowargs(h, dealias, d.nzp);
-    na.r.f32 = f32;
+    na.r.f32 = f32nl;
     for (int l = 0; l < 3; ++l) {
         na.U[l] = h->Y + (long long)l * h->Yl;
         na.DY[l] = h->Y + (long long)(3 + l) * h->Yl;
@@ -394,7 +417,7 @@ void nlterm(lsb_handle* h, const double* uin, double* Nout) {
     for (int l = 0; l < 3; ++l) yf.j[l] = YFwdJob{na.N[l], Nout + l * S, 1.0, 0.0, dealias ? 1 : 0};
     for (int m = 0; m < 6; ++m) yf.j[3 + m] = YFwdJob{na.H[m], h->H + m * S, 1.0, 0.0, dealias ? 1 : 0};
     { TimerScope ts(h, "yfwd_nl"); launch_yfwd(yf, ya, h->stream); }
-    if (f32) launch_add_half_sq(h->H, h->ubar, d.C(), d.nzp, h->stream);
+    if (f32nl) launch_add_half_sq(h->H, h->ubar, d.C(), d.nzp, h->stream);
 
     const bool need_phys = (dealias && h->cfg.forcing == 1) || h->cfg.sgsflag == 1;
     if (need_phys) {
@@ -476,7 +499,7 @@ void nlterm(lsb_handle* h, const double* uin, double* Nout) {
     gz.out = gz.outf[0];
     gz.nfields = 3;
     gz.epi = EPI_STORE;
-    if (!(h->cfg.precision == 1 && launch_umma_dz(gz, h->u_dz1, h->uerr, h->stream))) launch_gemm(gz, h->stream);
+    contract(h, gz, h->oz_dz1);
     launch_nl_div_xy(nd, h->stream);
 }
 
@@ -714,9 +737,10 @@ void step_one(lsb_handle* h) {
     {
         TimerScope ts(h, "poisson");
         launch_divuv(h->vel, h->vel + S, h->divf, h->wavx, h->wavy, d.nx, S, C, st);
+        // (FP64 contractions in both forms: see helmholtz())
         zgemm(h, h->m_dz1, h->divf, h->rhs, 1, EPI_POISSON_RHS, 1.0, 0.0, h->vel + 2 * S);
         // 8-9. Poisson solve for w^{n+1}
-        helmholtz(h, h->rhs, h->vel + 2 * S, 1, 0.0, h->bcp);
+        helmholtz(h, h->rhs, h->vel + 2 * S, 1, 0.0, h->bcp, false);
     }
     // 10. Dw^{n+1} (the eigenbasis temporary is free again)
     {
@@ -964,15 +988,16 @@ bool batch_graph_step(lsb_batch* b) {
     std::vector<const void*> key;
     std::vector<double> sc;
     key.reserve(8 * n);
-    sc.reserve(4 * n);
+    sc.reserve(5 * n);
     for (lsb_handle* h : b->m) {
         if (!graph_eligible(h)) return false;
         double ctop = 0, cwa = 0, cwb = 0;
         bound_coeffs(h, h->t, ctop, cwa, cwb);
         const void* k[8] = {h->vel, h->veln, h->velnm, h->nlc, h->nln, h->nlnm, h->p, h->pn};
         key.insert(key.end(), k, k + 8);
-        const double s[4] = {h->dt, ctop, cwa, cwb};
-        sc.insert(sc.end(), s, s + 4);
+        // the member's graph generation: a schedule set on it since makes a new capture
+        const double s[5] = {h->dt, ctop, cwa, cwb, (double)h->graph_gen};
+        sc.insert(sc.end(), s, s + 5);
     }
     members_to_batch(b);
     for (auto& g : b->graphs) {
@@ -1186,12 +1211,6 @@ int lsb_create(const lsb_config* cfg, const lsb_setup* su, lsb_handle** out) {
         h->lamx = h->upload(su->lamx, nx);
         h->m_dz1 = make_mat(h.get(), su->dz1, nzp, nzp);
         h->uerr = reinterpret_cast<int*>(h->alloc(1));
-        if (cfg->precision == 1 && nzp <= 256) {
-            std::vector<uint16_t> img;
-            h->u_dz1 = make_umma_mat(su->dz1, nzp, nzp, img);
-            h->u_dz1.img = reinterpret_cast<const uint16_t*>(
-                h->upload(reinterpret_cast<const double*>(img.data()), (img.size() * sizeof(uint16_t) + 7) / 8));
-        }
         h->m_dz2 = make_mat(h.get(), su->dz2, nzp, nzp);
         {
             std::vector<double> rows(2 * (size_t)nzp);
@@ -1203,6 +1222,16 @@ int lsb_create(const lsb_config* cfg, const lsb_setup* su, lsb_handle** out) {
         }
         h->m_ei = make_mat(h.get(), su->ei, nzm, nzm);
         h->m_eext = make_mat(h.get(), su->e, nzm, nzm, 0, nzm, 1, nzp);  // zero ceiling / wall rows
+        if (cfg->precision == 1) {
+            // the mixed form's contractions on the int8 tensor cores: D, E^-1 and E (the latter
+            // with its zero ceiling and wall rows, as m_eext)
+            std::vector<double> eext((size_t)nzp * nzm, 0.0);
+            for (int r = 0; r < nzm; ++r)
+                for (int k = 0; k < nzm; ++k) eext[(size_t)(r + 1) * nzm + k] = su->e[(size_t)r * nzm + k];
+            h->oz_dz1 = upload_ozaki(h.get(), su->dz1, nzp, nzp, 5);
+            h->oz_ei = upload_ozaki(h.get(), su->ei, nzm, nzm, 5);
+            h->oz_eext = upload_ozaki(h.get(), eext.data(), nzp, nzm, 5);
+        }
         make_plan(h.get(), ny, h->py, 16);
         make_plan(h.get(), d.nyl, h->pyl, 16);
         make_real_plan(h.get(), nx, h->rx);
@@ -1211,8 +1240,10 @@ int lsb_create(const lsb_config* cfg, const lsb_setup* su, lsb_handle** out) {
         if (cfg->precision == 1) {
             const bool dl = cfg->dealiasflag == 1;
             const bool phys = cfg->sgsflag == 1 || (dl && cfg->forcing == 1);
-            if ((dl ? h->pyl : h->py).g == 0 || (dl ? h->rxl : h->rx).half.g != 32 ||
-                (phys && (h->py.g == 0 || h->rx.half.g == 0)))
+            // the nonlinear term's (padded) passes in FP32 where their lengths have full-warp
+            // register plans, else in FP64 (the 3/2-rule x length 48 of a 64-point grid)
+            h->nl_f32 = (dl ? h->pyl : h->py).g != 0 && (dl ? h->rxl : h->rx).half.g == 32;
+            if ((!dl && !h->nl_f32) || (phys && (h->py.g == 0 || h->rx.half.g == 0)))
                 fail(LSB_ERR_ARG, "mixed precision needs transform lengths with register plans: x/2 a multiple of "
                                   "32 (32 R, R in 1,2,3,4,6,8) and y a power of two times 1,2,3,4,6,8");
         }
@@ -1503,6 +1534,7 @@ void from_dev(lsb_handle* h, const double* src, double* dst, long long n) {
     CK(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     check_launch();
+    check_uerr(h);
 }
 }  // namespace
 
@@ -1554,7 +1586,12 @@ int lsb_dfdz(lsb_handle* h, const double* uf, double* out) {
     return guard([&] {
         const long long S = h->d.S();
         to_dev(h, uf, h->io, S);
-        zgemm1(h, h->m_dz1, h->io, h->io + S, 1);
+        // the contraction of the handle's form (int8 tensor cores in the mixed form)
+        GemmArgs g = gemm_base(h, h->m_dz1);
+        g.in = h->io;
+        g.out = h->io + S;
+        g.epi = EPI_STORE;
+        contract(h, g, h->oz_dz1);
         from_dev(h, h->io + S, out, S);
     });
 }

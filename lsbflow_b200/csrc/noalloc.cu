@@ -184,6 +184,15 @@ extern "C" int lsb_solve_helmholtz_noalloc(int nx, int ny, int nz, const double*
         base = g_scratch_ptr[dev];
     }
     cudaStream_t s = (cudaStream_t)stream;
+    if (s != nullptr) {
+        // the scratch address above belongs to the current device: the stream must too
+        int sdev = -1;
+        ce = cudaStreamGetDevice(s, &sdev);
+        if (ce != cudaSuccess) return fail(LSB_ERR_CUDA, std::string("cudaStreamGetDevice: ") + cudaGetErrorString(ce));
+        if (sdev != dev)
+            return fail(LSB_ERR_ARG, "the stream belongs to device " + std::to_string(sdev) + ", not the current device " +
+                                         std::to_string(dev));
+    }
     double* a1 = base;                        // padded E^-1
     double* a2 = base + (long long)kMaxMp * kMaxKp;  // padded E with zero ceiling / wall rows
     double* tmp = base + kMatDoubles;         // nzm x chunk intermediate

@@ -386,13 +386,45 @@ def percentiles(results, qs=(50, 99)) -> dict:
 
 
 def summary(results, elapsed: float) -> dict:
+    """runs, runs/h, p50/p99 and pt_steps_per_s count completed runs only; the grid-point
+    steps that cancelled runs took before they stopped are reported apart
+    (cancelled_pt_steps_per_s)."""
     out = percentiles(results)
     done = [r for r in results if not r.cancelled]
     out["runs"] = len(done)
     out["cancelled"] = len(results) - len(done)
     out["runs_per_hour"] = len(done) / elapsed * 3600.0
-    out["pt_steps_per_s"] = sum(r.points * r.nsteps for r in results) / elapsed
+    out["pt_steps_per_s"] = sum(r.points * r.nsteps for r in done) / elapsed
+    out["cancelled_pt_steps_per_s"] = sum(r.points * r.nsteps for r in results if r.cancelled) / elapsed
     out["elapsed_s"] = elapsed
+    return out
+
+
+# the serving mix of the survey's stream: grids (reference nx x ny x nzp) and SGS models
+STREAM_GRIDS = (("dns64", {}), ("ens128", {"nz": 96}), ("les256", {}))   # 64x16x65, 128x32x97, 256x64x129
+STREAM_MODELS = ((0, 0), (1, 0), (1, 1), (1, 2), (1, 3))  # (sgsflag, sgsmodel): none, static, dynamic, sigma,
+                                                          # interscale (src/sgsterm.f90:21-35)
+
+
+def stream_requests(n: int, rate: float, seed: int, precision: int = 0, steps_range=(300, 3000)) -> list:
+    """Poisson arrivals at ``rate`` per second of runs with the grid drawn uniformly from
+    64 x 16 x 65, 128 x 32 x 97 and 256 x 64 x 129, the SGS model from none, static and
+    dynamic Smagorinsky, sigma and interscale, Re_delta* ~ U[300, 800], ceiling-dipole
+    amplitude A ~ U[0.1, 0.4] and centre x0 ~ U[60, 100] displacement thicknesses, and a
+    horizon drawn uniformly from ``steps_range``; every run in ``precision`` (0 FP64, 1 mixed)."""
+    from .config import workload
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for i in range(n):
+        t += rng.exponential(1.0 / rate)
+        base, over = STREAM_GRIDS[int(rng.integers(len(STREAM_GRIDS)))]
+        sgsflag, sgsmodel = STREAM_MODELS[int(rng.integers(len(STREAM_MODELS)))]
+        re_d, amp, xc = rng.uniform(300.0, 800.0), rng.uniform(0.1, 0.4), rng.uniform(60.0, 100.0)
+        nsteps = int(rng.integers(steps_range[0], steps_range[1] + 1))
+        cfg = workload(base, re_d=float(re_d), bc_amp=float(amp), bc_xc=float(xc), sgsflag=sgsflag,
+                       sgsmodel=sgsmodel, precision=precision, **over)
+        out.append(RunRequest(i, cfg, nsteps, seed=1000 + i, amp=1e-3, arrival=t))
     return out
 
 

@@ -34,7 +34,7 @@ class FakeSolver:
 
     def download(self):
         c = self.cfg
-        return {k: np.zeros((c.nzp, c.ny, c.nx)) for k in ("uf", "vf", "wf", "pf")}
+        return {k: np.ones((c.nzp, c.ny, c.nx)) * (1.0 + 1e-7 * c.precision) for k in ("uf", "vf", "wf", "pf")}
 
     def device_bytes(self):
         return 1 << 20
@@ -135,8 +135,22 @@ def test_serving_section(monkeypatch):
 
     monkeypatch.setattr(S, "DeviceBackend", Backend)
     out = bench.run_serving(types.SimpleNamespace(serve_runs=4), 0)
-    assert out["runs"] == 4 and "error" not in out["grouped"]
-    assert out["p99_s"] >= out["p50_s"] > 0
+    for form in ("fp64", "mixed", "fp64_grouped"):
+        assert out[form]["runs"] == 4 and "error" not in out[form]
+        assert out[form]["p99_s"] >= out[form]["p50_s"] > 0
+    assert out["horizon_steps"] == [300, 3000]
+
+
+def test_stream_requests_draw_the_survey_mix():
+    reqs = S.stream_requests(300, 4.0, 5, precision=1)
+    grids = {(r.cfg.nx, r.cfg.ny, r.cfg.nzp) for r in reqs}
+    assert grids == {(64, 16, 65), (128, 32, 97), (256, 64, 129)}
+    models = {(r.cfg.sgsflag, r.cfg.sgsmodel if r.cfg.sgsflag else None) for r in reqs}
+    assert models == {(0, None), (1, 0), (1, 1), (1, 2), (1, 3)}
+    assert all(r.cfg.precision == 1 for r in reqs)
+    assert min(r.nsteps for r in reqs) >= 300 and max(r.nsteps for r in reqs) <= 3000
+    t = [r.arrival for r in reqs]
+    assert all(b > a for a, b in zip(t, t[1:])) and 50 < t[-1] < 100  # about 300 / 4 s
 
 
 def test_ensemble_section(monkeypatch):
@@ -152,3 +166,16 @@ def test_ensemble_section(monkeypatch):
     for form in ("fp64", "mixed"):
         assert out[form]["gain_vs_one_member"] == pytest.approx(3.0)
         assert out[form]["timed_steps"] == 30
+    per = out["mixed_rel_err_velocity_per_member"]
+    assert len(per["members"]) == 3 and per["max"] == pytest.approx(1e-7, rel=1e-6)
+
+
+def test_clock_sampler_summary_inside_the_timed_region():
+    c = bench.ClockSampler(0)
+    c.samples = [(0.5, 1000.0, 1965.0, set()), (1.5, 1960.0, 1965.0, {"sw_power_cap"}),
+                 (2.5, 1965.0, 1965.0, set()), (9.0, 500.0, 1965.0, {"hw_slowdown"})]
+    c.t_start, c.t_end = 1.0, 3.0
+    s = c.summary()
+    assert s["samples"] == 2 and s["sm_mhz"] == 1962.5 and s["reasons"] == ["sw_power_cap"]
+    c.t_start, c.t_end = 3.0, 4.0
+    assert c.summary()["reasons"] == ["unsampled"]

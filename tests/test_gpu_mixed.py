@@ -72,6 +72,17 @@ def test_mixed_les256_within_1e6():
         assert rel(got[k], ref[k]) < 2 * TOL_MIXED, (k, rel(got[k], ref[k]))
 
 
+def test_mixed_dns64_padded_rows_in_fp64():
+    # the 64 x 16 x 65 DNS of the serving mix: its 3/2-rule x length (96 reals, 48 complex)
+    # has no full-warp register plan, so the mixed form runs the nonlinear term's padded
+    # passes in FP64 and the rest (contractions, unpadded fields) in its own precision
+    cfg = workload("dns64")
+    ref = run(cfg, 100, seed=21, amp=1e-2)
+    got = run(cfg.replace(precision=1), 100, seed=21, amp=1e-2)
+    for k in ("uf", "vf", "wf"):
+        assert rel(got[k], ref[k]) < TOL_MIXED, (k, rel(got[k], ref[k]))
+
+
 def test_mixed_nlterm_against_oracle():
     from lsbflow_b200 import lib
     cfg = workload("les256", nx=128, ny=16, nz=32, sgsflag=0, precision=1)
@@ -91,3 +102,36 @@ def test_mixed_rejects_lengths_without_register_plans():
     cfg = workload("dns64", nx=40, ny=10, nz=8, dealiasflag=0, precision=1)
     with pytest.raises(lib.LsbError, match="mixed precision"):
         lib.Solver(hs.make_setup(cfg))
+
+
+# The mixed form's z contractions run on the int8 tensor cores with five digits per
+# operand (exact int32 accumulation): measured in an emulation of the split at 3e-10 ..
+# 7e-10 relative on random columns; the single operators through the C ABI are held to
+# 1e-8 against the FP64 oracle.
+TOL_INT8 = 1e-8
+
+
+@pytest.mark.parametrize("grid", [dict(nx=64, ny=8, nz=32), dict(nx=128, ny=32, nz=64), dict(nx=256, ny=64, nz=128),
+                                  dict(nx=64, ny=16, nz=16)])
+def test_mixed_contractions_on_int8_tensor_cores(grid):
+    from lsbflow_b200 import lib
+    cfg = workload("les256", sgsflag=0, dealiasflag=0, precision=1, **grid)
+    st = hs.make_setup(cfg)
+    s = lib.Solver(st)
+    try:
+        rng = np.random.default_rng(4)
+        u = rng.standard_normal((cfg.nzp, cfg.ny, cfg.nx))
+        O.norm([u], cfg.ny)
+        assert rel(s.dfdz(u), O.dfdz(st, u)) < TOL_INT8
+        dtnui = 1.0 / (cfg.xnu * st.dt) / (6.0 / 11.0)
+        rhs = rng.standard_normal((cfg.nzp, cfg.ny, cfg.nx)) * 1e5
+        assert rel(s.solve_helmholtz(rhs, dtnui), O.solve_helmholtz(st, rhs.copy(), dtnui)) < TOL_INT8
+        bc = np.zeros_like(rhs)
+        bc[0] = rng.standard_normal((cfg.ny, cfg.nx))
+        bc[-1] = rng.standard_normal((cfg.ny, cfg.nx))
+        assert rel(s.solve_nhom_helmholtz(rhs, bc, dtnui),
+                   O.solve_nhom_helmholtz(st, rhs.copy(), bc, dtnui)) < TOL_INT8
+        # the Poisson solve (sigma = 0)
+        assert rel(s.solve_nhom_helmholtz(rhs, bc, 0.0), O.solve_nhom_helmholtz(st, rhs.copy(), bc, 0.0)) < TOL_INT8
+    finally:
+        s.close()

@@ -228,3 +228,7 @@ def test_cancelled_runs_leave_at_a_step_boundary(group):
     assert be.in_use == 0
     s = S.summary(list(res.values()), srv.elapsed)
     assert s["runs"] == 2 and s["cancelled"] == 2
+    pts = [r.points for r in res.values()][0]
+    # throughput of completed runs only; the cancelled run's partial steps apart
+    assert s["pt_steps_per_s"] * srv.elapsed == pytest.approx(pts * 60)
+    assert s["cancelled_pt_steps_per_s"] * srv.elapsed == pytest.approx(pts * res[1].nsteps)

@@ -23,10 +23,17 @@ def rel(a, b):
     return np.linalg.norm(a - b) / np.linalg.norm(b)
 
 
-def test_noalloc_matches_handle_entry_point_twice():
+# nx*ny = 16384 columns at nzp = 129 (three chunks of whole 64-column tiles); 17500 columns
+# (two full chunks and a tail of 1628, a partly filled last tile); 288 columns at nzp = 33
+# (one chunk, a partly filled last tile)
+GRIDS = [dict(), dict(nx=250, ny=70), dict(nx=48, ny=6, nz=32)]
+
+
+@pytest.mark.parametrize("grid", GRIDS, ids=["256x64x129", "250x70x129", "48x6x33"])
+def test_noalloc_matches_handle_entry_point_twice(grid):
     import torch
     from lsbflow_b200 import lib
-    cfg = workload("les256", dealiasflag=0, sgsflag=0)  # nx*ny = 16384 columns, nzp = 129
+    cfg = workload("les256", dealiasflag=0, sgsflag=0, **grid)
     st = hs.make_setup(cfg)
     s = lib.Solver(st)
     dev = torch.device("cuda")
