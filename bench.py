@@ -467,6 +467,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=WORKLOAD)
+    ap.add_argument("--precision", type=int, default=0, choices=[0, 1],
+                    help="form of the headline handle: 0 FP64 (the benchmark), 1 the mixed form (for "
+                         "profiling the mixed step alone)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
@@ -477,7 +480,7 @@ def main():
     ap.add_argument("--profile-steps", type=int, default=2000)
     ap.add_argument("--members", type=int, default=64)
     args = ap.parse_args()
-    cfg = workload(args.workload)
+    cfg = workload(args.workload, precision=args.precision) if args.impl != "reference" else workload(args.workload)
     if args.impl == "reference":
         run_reference(args, cfg)
         return
@@ -697,7 +700,8 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "vs_baseline": None, "dtype": "f64" if args.precision == 0 else "mixed (f32 / int8 tensor cores / f64)",
+            "data": "synthetic",
             "config": {"workload": f"{args.workload}: {nx}x{ny}x{nzp} (ref nx,ny,nzp), padded {nxl}x{nyl}, "
                                    f"dyn-Smagorinsky LES, dealias 3/2, fringe, dipole BC, dt={st.dt}",
                        "global_batch": world, "parallelism": f"replicas x{world}",

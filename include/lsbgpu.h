@@ -151,6 +151,9 @@ typedef struct {
                             0 = the wave-quantization model */
     int filter_zchunks;  /* 3-point SGS test filter: z chunks a block column is split into,
                             1..(nzp+3)/4; 0 = the waves x planes-per-block model */
+    int y_staging;       /* FP64 spanwise passes: tiles staged by cp.async (1) or by TMA tile
+                            loads (2); 0 = the built-in choice (TMA on the padded grid,
+                            cp.async on the unpadded one) */
 } lsb_schedule;
 /* out-of-range fields return LSB_ERR_ARG; the step graphs are dropped and re-captured */
 int lsb_set_schedule(lsb_handle* h, const lsb_schedule* s);

@@ -10,8 +10,11 @@
 // inside a transform.  Lengths whose R is not in {1,2,3,4,6,8} use fft_kernels.cu.
 #include <stdexcept>
 
+#include <cstring>
+
 #include "lsb_fftdev.cuh"
 #include "lsb_internal.cuh"
+#include "lsb_tma.cuh"
 
 namespace lsb {
 namespace {
@@ -169,31 +172,92 @@ __device__ __forceinline__ int yswz(int row) {
 template <int R>
 __device__ __forceinline__ int ytix(int row, int col) { return row * WKC + (col ^ (yswz<R>(row) & 7)); }
 
+// FP64 spanwise tile staged by TMA: the two 8-column halves of a row are 128-byte lines of
+// two regions [nyl][8], each 1024-byte aligned, under the TMA's 128-byte swizzle (16-byte
+// chunk c of line r at c ^ (r & 7)): a lane group reading a column in natural row order hits
+// 8 distinct banks per quarter warp
+__device__ __forceinline__ int ytix_tma(int row, int col, int nyl) {
+    return (col >> 3) * (nyl * 8) + row * 8 + ((col & 7) ^ (row & 7));
+}
+
+// tensor maps of a launch's input fields (one per job), passed as a grid constant
+struct alignas(64) YTmaMaps {
+    CUtensorMap m[kMaxJobs];
+};
+
 // ----------------------------------------------------------------------------- spanwise
 // One kernel for both directions.  Work item = (job, z, chunk of WKC kx columns); the tile
-// [nyl][WKC+1] is staged with cp.async (double-buffered), each column is transformed by a
-// lane group, and the tile is written back in coalesced rows.
+// [nyl][WKC] is staged double-buffered -- by cp.async (TMA = false) or by TMA tile loads that
+// complete on an mbarrier per buffer (TMA = true, 2 or 4 box loads issued by one thread) --,
+// each column is transformed by a lane group, and the tile is written back in coalesced rows.
 // GC: the lane-group width as a compile-time constant (0: the plan's, at run time), so that
 // the transform's cross-lane stages unroll and their twiddle loads are issued up front;
 // 64 registers (4 blocks per SM) fit the unrolled FP64 form without spills
-template <int R, bool INV, int GC = 0>
-__global__ void __launch_bounds__(256, 4) k_ywarp(YInvJobList ij, YFwdJobList fj, YPassArgs a, int nch) {
-    extern __shared__ double2 smem[];
+template <int R, bool INV, int GC = 0, bool TMA = false>
+__global__ void __launch_bounds__(256, 4) k_ywarp(YInvJobList ij, YFwdJobList fj, YPassArgs a, int nch,
+                                                  const __grid_constant__ YTmaMaps tm) {
+    extern __shared__ __align__(1024) unsigned char ysm_raw[];
+    // the TMA's 128-byte swizzle wants 1024-byte aligned destinations
+    double2* smem = reinterpret_cast<double2*>(
+        ysm_raw + ((1024u - (unsigned)(__cvta_generic_to_shared(ysm_raw) & 1023u)) & 1023u));
     const int ny = a.ny, nyl = a.nyl, G = GC ? GC : a.plan.g, lgg = GC ? ilog2c(GC) : a.plan.lgg;
     double2* Buf[2] = {smem, smem + nyl * WKC};
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * nyl * WKC);  // [2] (TMA)
+    int* sabort = reinterpret_cast<int*>(bar + 2);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int njobs = INV ? ij.n : fj.n;
     const int nitems = njobs * a.nzp * nch;
     const int lpw = 32 / G;              // lines per warp per pass
     const int q = lane / G, g = lane - q * G;
-    auto issue = [&](int item, double2* T) {
+    auto IX = [&](int row, int col) { return TMA ? ytix_tma(row, col, nyl) : ytix<R>(row, col); };
+    // TMA: the input rows of a tile land in tile rows [0, h0) and [nyl - (ny - h0), nyl) when
+    // the padded tile splits the spectrum (the textbook 3/2 layout), else in rows [0, rows)
+    const bool split = INV && a.layout != 0 && nyl != ny;
+    const int h0 = split ? ny / 2 : (INV ? ny : nyl);
+    const uint32_t tile_bytes = 2u * (uint32_t)(INV ? ny : nyl) * 128u;
+    uint32_t ph[2] = {0u, 0u};
+    bool inflight[2] = {false, false};
+    if (TMA) {
+        if (tid == 0) {
+            tma::mbar_init(&bar[0], 1);
+            tma::mbar_init(&bar[1], 1);
+            tma::fence_init();
+            *sabort = 0;
+        }
+        __syncthreads();
+    }
+    auto issue = [&](int item, int b) {
+        double2* T = Buf[b];
         const int ch = item % nch, rest = item / nch, z = rest % a.nzp, jb = rest / a.nzp;
         const int c0 = ch * WKC;
+        if (TMA) {
+            if (INV && nyl != ny) {  // the padded rows hold zeros (generic stores, rows the TMA does not write)
+                const int r0 = split ? h0 : ny;
+                for (int idx = tid; idx < (nyl - ny) * WKC; idx += 256) {
+                    const int r = idx / WKC, cc = idx - r * WKC;
+                    T[IX(r0 + r, cc)] = make_double2(0.0, 0.0);
+                }
+            }
+            if (tid == 0) {
+                // the block's earlier generic accesses of this buffer (ordered by the barrier
+                // before this call) come before the TMA's writes
+                tma::fence_proxy_async();
+                tma::mbar_expect_tx(&bar[b], tile_bytes);
+                const CUtensorMap* map = &tm.m[jb];
+                for (int hf = 0; hf < 2; ++hf) {
+                    double2* dst = T + hf * (nyl * 8);
+                    tma::load_3d(dst, map, 2 * c0 + 16 * hf, 0, z, &bar[b]);
+                    if (split) tma::load_3d(dst + (nyl - (ny - h0)) * 8, map, 2 * c0 + 16 * hf, h0, z, &bar[b]);
+                }
+            }
+            inflight[b] = true;
+            return;
+        }
         if (INV) {
             const double* in = ij.j[jb].in;
             for (int idx = tid; idx < ny * WKC; idx += 256) {
                 const int j = idx / WKC, cc = idx - j * WKC, c = c0 + cc;
-                double2* d = &T[ytix<R>(pad_row_w(j, ny, nyl, a.layout), cc)];
+                double2* d = &T[IX(pad_row_w(j, ny, nyl, a.layout), cc)];
                 if (c < a.kxc) cpa16(d, in + ((long long)z * ny + j) * a.nx + 2 * c);
                 else *d = make_double2(0.0, 0.0);
             }
@@ -201,13 +265,13 @@ __global__ void __launch_bounds__(256, 4) k_ywarp(YInvJobList ij, YFwdJobList fj
             for (int idx = tid; idx < npad * WKC; idx += 256) {
                 const int r = idx / WKC, cc = idx - r * WKC;
                 const int jl = (a.layout == 0 || nyl == ny) ? ny + r : ny / 2 + r;
-                T[ytix<R>(jl, cc)] = make_double2(0.0, 0.0);
+                T[IX(jl, cc)] = make_double2(0.0, 0.0);
             }
         } else {
             const double* in = fj.j[jb].in;
             for (int idx = tid; idx < nyl * WKC; idx += 256) {
                 const int jl = idx / WKC, cc = idx - jl * WKC, c = c0 + cc;
-                double2* d = &T[ytix<R>(jl, cc)];
+                double2* d = &T[IX(jl, cc)];
                 if (c < a.kxc) cpa16(d, in + ((long long)z * nyl + jl) * a.nx + 2 * c);
                 else *d = make_double2(0.0, 0.0);
             }
@@ -216,15 +280,22 @@ __global__ void __launch_bounds__(256, 4) k_ywarp(YInvJobList ij, YFwdJobList fj
     };
     int cur = 0;
     int item = blockIdx.x;
-    if (item < nitems) issue(item, Buf[0]);
+    if (item < nitems) issue(item, 0);
     for (; item < nitems; item += gridDim.x) {
         const int ch = item % nch, rest = item / nch, z = rest % a.nzp, jb = rest / a.nzp;
         const int c0 = ch * WKC;
         double2* T = Buf[cur];
-        cpa_wait_all();
+        if (TMA) {
+            if (!tma::mbar_wait(&bar[cur], ph[cur])) *sabort = 1;
+            ph[cur] ^= 1u;
+            inflight[cur] = false;
+        } else {
+            cpa_wait_all();
+        }
         __syncthreads();
+        if (TMA && *sabort != 0) break;
         const int next = item + gridDim.x;
-        if (next < nitems) issue(next, Buf[cur ^ 1]);
+        if (next < nitems) issue(next, cur ^ 1);
         const int mode = INV ? ij.j[jb].mode : YM_COPY;
         for (int L0 = warp * lpw; L0 < WKC; L0 += 8 * lpw) {
             const int L = L0 + q;
@@ -234,7 +305,7 @@ __global__ void __launch_bounds__(256, 4) k_ywarp(YInvJobList ij, YFwdJobList fj
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 const int n = g + G * r;
-                double2 x = T[ytix<R>(n, Lc)];
+                double2 x = T[IX(n, Lc)];
                 if (INV && mode != YM_COPY) {
                     double k = 0.0;
                     if (mode == YM_IKY) {
@@ -252,7 +323,7 @@ __global__ void __launch_bounds__(256, 4) k_ywarp(YInvJobList ij, YFwdJobList fj
             lane_bitrev<R>(v, G, lane, g, lgg);
             if (act) {
 #pragma unroll
-                for (int k1 = 0; k1 < R; ++k1) T[ytix<R>(R * g + k1, L)] = v[k1];
+                for (int k1 = 0; k1 < R; ++k1) T[IX(R * g + k1, L)] = v[k1];
             }
         }
         __syncthreads();
@@ -261,17 +332,17 @@ __global__ void __launch_bounds__(256, 4) k_ywarp(YInvJobList ij, YFwdJobList fj
             for (int idx = tid; idx < nyl * WKC; idx += 256) {
                 const int jl = idx / WKC, cc = idx - jl * WKC, c = c0 + cc;
                 if (c >= a.kxc) continue;
-                *reinterpret_cast<double2*>(out + ((long long)z * nyl + jl) * a.nx + 2 * c) = T[ytix<R>(jl, cc)];
+                *reinterpret_cast<double2*>(out + ((long long)z * nyl + jl) * a.nx + 2 * c) = T[IX(jl, cc)];
             }
         } else {
             const YFwdJob job = fj.j[jb];
             for (int idx = tid; idx < ny * WKC; idx += 256) {
                 const int j = idx / WKC, cc = idx - j * WKC, c = c0 + cc;
                 if (c >= a.kxc) continue;
-                double2 v = T[ytix<R>(pad_row_w(j, ny, nyl, a.layout), cc)];
+                double2 v = T[IX(pad_row_w(j, ny, nyl, a.layout), cc)];
                 if (job.sym && c == 0) {
                     const int jm = (ny - j) % ny;
-                    const double2 w = T[ytix<R>(pad_row_w(jm, ny, nyl, a.layout), cc)];
+                    const double2 w = T[IX(pad_row_w(jm, ny, nyl, a.layout), cc)];
                     v = make_double2(0.5 * (v.x + w.x), 0.5 * (v.y - w.y));
                 }
                 v.x *= a.scale;
@@ -289,6 +360,17 @@ __global__ void __launch_bounds__(256, 4) k_ywarp(YInvJobList ij, YFwdJobList fj
         }
         __syncthreads();
         cur ^= 1;
+    }
+    if (TMA) {
+        // after a time-out: the loads this block still has in flight end before it exits (a
+        // bounded wait again), and the launch's error word is raised
+        if (*sabort != 0) {
+            for (int b = 0; b < 2; ++b)
+                if (inflight[b]) tma::mbar_wait(&bar[b], ph[b]);
+            if (tid == 0 && a.err) atomicExch(a.err, 1);
+        }
+    } else {
+        cpa_wait_all();
     }
 }
 
@@ -1001,10 +1083,35 @@ void ylaunch(const YInvJobList& ij, const YFwdJobList& fj, const YPassArgs& a, c
         else k_ywarp_f<R, INV><<<persistent_grid_w(k_ywarp_f<R, INV>, smf, nitems), 256, smf, s>>>(ij, fj, a, nch);
         return;
     }
-    const size_t sm = (size_t)2 * a.nyl * (WKC + 1) * sizeof(double2);
+    YTmaMaps tm;
+    std::memset(&tm, 0, sizeof(tm));
+    // TMA staging (the handle's schedule): one tensor map per job's input field; a grid or
+    // field the maps do not fit (tile rows not a multiple of 8, a box over 256 rows, the
+    // driver call missing) takes the cp.async staging
+    const int njobs = INV ? ij.n : fj.n;
+    const bool split = INV && a.layout != 0 && a.nyl != a.ny;
+    // every box lands on a 1024-byte boundary (the swizzle's atom): tile rows, and the row at
+    // which the split's second box starts, multiples of 8
+    bool use_tma = a.y_tma == 1 && a.nyl % 8 == 0 && a.nyl <= 256 && a.ny % 2 == 0 &&
+                   (!split || (a.nyl - a.ny / 2) % 8 == 0);
+    for (int jb = 0; use_tma && jb < njobs; ++jb) {
+        const double* in = INV ? ij.j[jb].in : fj.j[jb].in;
+        const uint64_t rows = INV ? (uint64_t)a.ny : (uint64_t)a.nyl;
+        const uint32_t box_rows = split ? (uint32_t)(a.ny / 2) : (uint32_t)rows;
+        use_tma = tmap_f64_3d(&tm.m[jb], in, (uint64_t)a.nx, rows, (uint64_t)a.nzp, 16, box_rows);
+    }
+    const size_t base = (size_t)2 * a.nyl * (WKC + 1) * sizeof(double2);
+    const size_t smt = (size_t)2 * a.nyl * WKC * sizeof(double2) + 64 + 1024;
     lsb::note_launch();
-    if (a.plan.g == 16) k_ywarp<R, INV, 16><<<persistent_grid_w(k_ywarp<R, INV, 16>, sm, nitems), 256, sm, s>>>(ij, fj, a, nch);
-    else k_ywarp<R, INV><<<persistent_grid_w(k_ywarp<R, INV>, sm, nitems), 256, sm, s>>>(ij, fj, a, nch);
+    if (use_tma) {
+        if (a.plan.g == 16)
+            k_ywarp<R, INV, 16, true><<<persistent_grid_w(k_ywarp<R, INV, 16, true>, smt, nitems), 256, smt, s>>>(ij, fj, a, nch, tm);
+        else
+            k_ywarp<R, INV, 0, true><<<persistent_grid_w(k_ywarp<R, INV, 0, true>, smt, nitems), 256, smt, s>>>(ij, fj, a, nch, tm);
+        return;
+    }
+    if (a.plan.g == 16) k_ywarp<R, INV, 16><<<persistent_grid_w(k_ywarp<R, INV, 16>, base, nitems), 256, base, s>>>(ij, fj, a, nch, tm);
+    else k_ywarp<R, INV><<<persistent_grid_w(k_ywarp<R, INV>, base, nitems), 256, base, s>>>(ij, fj, a, nch, tm);
 }
 
 template <bool INV>

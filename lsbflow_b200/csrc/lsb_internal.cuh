@@ -99,6 +99,8 @@ struct YPassArgs {
     const double* wavx;         // [nx] device
     FftPlan plan;               // length nyl
     int f32 = 0;                // 1: y-intermediates in FP32, transforms in FP32 (mixed form)
+    int y_tma = 0;              // FP64 tiles staged by TMA tile loads (1) or by cp.async (0)
+    int* err = nullptr;         // raised when a bounded wait of a TMA-staged pass timed out
 };
 
 constexpr int kMaxJobs = 12;

@@ -73,7 +73,7 @@ class LsbDiagC(C.Structure):
 
 
 class LsbScheduleC(C.Structure):
-    _fields_ = [("gemm_warps", C.c_int), ("filter_zchunks", C.c_int)]
+    _fields_ = [("gemm_warps", C.c_int), ("filter_zchunks", C.c_int), ("y_staging", C.c_int)]
 
 
 _lib = None
@@ -255,7 +255,8 @@ class Solver:
         """Launch schedule ({"gemm_warps": 0|4..8, "filter_zchunks": 0|1..}); None or zeros:
         the built-in models.  Results do not depend on it."""
         sched = sched or {}
-        sc = LsbScheduleC(int(sched.get("gemm_warps", 0)), int(sched.get("filter_zchunks", 0)))
+        sc = LsbScheduleC(int(sched.get("gemm_warps", 0)), int(sched.get("filter_zchunks", 0)),
+                          int(sched.get("y_staging", 0)))
         _ck(self._lib.lsb_set_schedule(self._h, C.byref(sc)))
 
     def schedule(self) -> dict:

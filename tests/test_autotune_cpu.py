@@ -5,12 +5,14 @@ from lsbflow_b200 import autotune as A
 from lsbflow_b200.config import workload
 
 
-def surface(best_w=6, best_z=3, floor=1.0):
-    """ms per step: separable, minimal at (best_w, best_z); 0 (the models) is 5% off."""
+def surface(best_w=6, best_z=3, tma_gain=0.03, floor=1.0):
+    """ms per step: separable, minimal at (best_w, best_z) with TMA staging of the spanwise
+    passes (y_staging 2) ``tma_gain`` faster; 0 (the models) is a few % off."""
     def ms(s):
         w = s["gemm_warps"] or 8
         z = s["filter_zchunks"] or 1
-        return floor * (1.0 + 0.01 * abs(w - best_w) + 0.02 * abs(z - best_z))
+        y = -tma_gain if s.get("y_staging", 0) == 2 else 0.0
+        return floor * (1.0 + 0.01 * abs(w - best_w) + 0.02 * abs(z - best_z) + y + tma_gain)
     return ms
 
 
@@ -23,6 +25,7 @@ def test_candidates_are_within_the_c_abi_limits():
         zmax = max(1, (cfg.nzp + 3) // 4)
         assert all(0 <= v <= zmax for v in c["filter_zchunks"])
         assert 0 in c["gemm_warps"] and 0 in c["filter_zchunks"]
+        assert c["y_staging"] == ([0, 1, 2] if cfg.precision == 0 else [0])
     assert A.candidates(workload("ens128"))["filter_zchunks"] == [0]     # sigma: no test filter
     assert len(A.candidates(workload("les256"))["filter_zchunks"]) > 4  # dynamic: filtered
 
@@ -37,17 +40,17 @@ def test_search_finds_the_minimum_and_counts_trials():
         return m(s)
 
     res = A.tune(cfg, measure)
-    assert res["schedule"] == {"gemm_warps": 6, "filter_zchunks": 3}
+    assert res["schedule"] == {"gemm_warps": 6, "filter_zchunks": 3, "y_staging": 2}
     assert res["ms_per_step"] == pytest.approx(1.0)
-    assert res["model_ms_per_step"] == m({"gemm_warps": 0, "filter_zchunks": 0})
+    assert res["model_ms_per_step"] == m({"gemm_warps": 0, "filter_zchunks": 0, "y_staging": 0})
     c = A.candidates(cfg)
-    assert len(calls) == 1 + (len(c["gemm_warps"]) - 1) + (len(c["filter_zchunks"]) - 1)
+    assert len(calls) == 1 + sum(len(c[k]) - 1 for k in A.KNOBS)
     assert len(res["trials"]) == len(calls)
 
 
 def test_ties_keep_the_model():
     res = A.tune(workload("les256"), lambda s: 1.0 if s["gemm_warps"] else 1.001)
-    assert res["schedule"] == {"gemm_warps": 0, "filter_zchunks": 0}
+    assert res["schedule"] == {"gemm_warps": 0, "filter_zchunks": 0, "y_staging": 0}
 
 
 def test_store_round_trip_and_keys(tmp_path):

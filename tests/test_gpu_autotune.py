@@ -19,7 +19,8 @@ def run(st, u, v, w, sched, n=12):
     try:
         s.set_schedule(sched)
         assert s.schedule() == {"gemm_warps": sched.get("gemm_warps", 0),
-                                "filter_zchunks": sched.get("filter_zchunks", 0)}
+                                "filter_zchunks": sched.get("filter_zchunks", 0),
+                                "y_staging": sched.get("y_staging", 0)}
         s.upload(u, v, w, dt=st.dt)
         s.step(n)
         return s.download()
@@ -36,7 +37,8 @@ def test_schedules_are_bit_identical(precision):
     ref = run(st, u, v, w, {})
     zmax = max(1, (cfg.nzp + 3) // 4)
     for sched in ({"gemm_warps": 4}, {"gemm_warps": 7, "filter_zchunks": 1},
-                  {"gemm_warps": 8, "filter_zchunks": zmax}, {"filter_zchunks": 2}):
+                  {"gemm_warps": 8, "filter_zchunks": zmax}, {"filter_zchunks": 2},
+                  {"y_staging": 2}, {"y_staging": 1, "gemm_warps": 5}):
         got = run(st, u, v, w, sched)
         for k in KEYS:
             assert np.array_equal(got[k], ref[k]), (sched, k)
@@ -48,10 +50,10 @@ def test_set_schedule_rejects_out_of_range():
     s = lib.Solver(st)
     try:
         for bad in ({"gemm_warps": 3}, {"gemm_warps": 9}, {"filter_zchunks": -1},
-                    {"filter_zchunks": (st.cfg.nzp + 3) // 4 + 1}):
+                    {"filter_zchunks": (st.cfg.nzp + 3) // 4 + 1}, {"y_staging": 3}):
             with pytest.raises(lib.LsbError):
                 s.set_schedule(bad)
-        assert s.schedule() == {"gemm_warps": 0, "filter_zchunks": 0}
+        assert s.schedule() == {"gemm_warps": 0, "filter_zchunks": 0, "y_staging": 0}
     finally:
         s.close()
 
@@ -64,4 +66,21 @@ def test_tune_and_store(tmp_path):
     assert got == res["schedule"]
     c = A.candidates(st.cfg)
     assert got["gemm_warps"] in c["gemm_warps"] and got["filter_zchunks"] in c["filter_zchunks"]
+    assert got["y_staging"] in c["y_staging"]
     assert res["ms_per_step"] <= res["model_ms_per_step"] and res["ms_per_step"] > 0
+
+
+@pytest.mark.parametrize("grid", [dict(nx=256, ny=64, nz=128), dict(nx=64, ny=16, nz=64, sgsflag=0),
+                                  dict(nx=64, ny=16, nz=16, dealias_layout="ref"), dict(nx=64, ny=16, nz=32, dealiasflag=0)],
+                         ids=["les256", "dns64", "ref-layout", "no-dealias"])
+def test_tma_staged_spanwise_passes_are_bit_identical(grid):
+    # the FP64 spanwise tiles staged by TMA tile loads (y_staging 2): the same arithmetic as
+    # the cp.async staging, so the same state bit for bit, on the padded textbook layout (the
+    # two-box split), the reference's padded layout, and the unpadded grid
+    cfg = workload("les256", **grid)
+    st = hs.make_setup(cfg)
+    u, v, w = ic.seeded_noise(st, 9, 5e-3)
+    ref = run(st, u, v, w, {"y_staging": 1}, n=6)
+    got = run(st, u, v, w, {"y_staging": 2}, n=6)
+    for k in KEYS:
+        assert np.array_equal(got[k], ref[k]), k
