@@ -758,7 +758,13 @@ __global__ void __launch_bounds__(256, 2) k_row_nl_w(NlRowArgs a) {
 // products are lane-local, and the r2c (decimation in time from that layout) ends in
 // natural order, where the pair Z[k], Z[N-k] of the real-to-complex split is one shuffle
 // apart.  No shared memory and no block barrier.
-template <int R, class S, class V, bool SEL = (sizeof(S) == 8)>
+#ifndef NLR_MINB
+#define NLR_MINB 4
+#endif
+#ifndef NLR_SEL
+#define NLR_SEL 1
+#endif
+template <int R, class S, class V, bool SEL = (sizeof(S) == 8 && NLR_SEL)>
 __device__ __forceinline__ void nl_c2r_r(const S* __restrict__ src, bool ikx, int K, int N, int g,
                                          const double* __restrict__ wavx, const V* __restrict__ twr,
                                          const V* __restrict__ tw, V (&v)[R]) {
@@ -785,7 +791,7 @@ __device__ __forceinline__ void nl_c2r_r(const S* __restrict__ src, bool ikx, in
 }
 
 // r2c of a slot-layout row; writes the K stored modes of the row at dst
-template <int R, class S, class V, bool SEL = (sizeof(S) == 8)>
+template <int R, class S, class V, bool SEL = (sizeof(S) == 8 && NLR_SEL)>
 __device__ __forceinline__ void nl_r2c_r(V (&v)[R], S* __restrict__ dst, int K, int g, const V* __restrict__ twr,
                                          const V* __restrict__ tw) {
     wfft_dit<R, -1, SEL>(v, 32, g, tw);
@@ -811,72 +817,87 @@ __device__ __forceinline__ void nl_r2c_r(V (&v)[R], S* __restrict__ dst, int K, 
     }
 }
 
+// shared memory of k_row_nl_r: per warp, the three velocity rows and the convective sum
 template <int R>
-__global__ void __launch_bounds__(128, 3) k_row_nl_r(NlRowArgs a) {
+constexpr size_t nl_r_smem() { return (size_t)4 * 4 * R * 32 * sizeof(double2); }
+
+template <int R>
+__global__ void __launch_bounds__(128, (R <= 6 ? NLR_MINB : 3)) k_row_nl_r(NlRowArgs a) {
     const RowArgs& r = a.r;
     const int N = 32 * R, K = r.kxc, lgg = r.rp.half.lgg;
     const int g = threadIdx.x & 31;
     const int nitems = r.nyl * r.nzp;
     const int W = gridDim.x * (blockDim.x >> 5);
+    // the physical velocity rows of this warp's row, lane-private slots [l][k1][lane]: kept
+    // in shared memory rather than registers, so that more warps fit per SM
+    extern __shared__ double2 nl_r_sm[];
+    double2* us = nl_r_sm + (threadIdx.x >> 5) * (4 * R * 32);
+    auto U = [&](int l, int k1) -> double2& { return us[(l * R + k1) * 32 + g]; };
     // physical x of the pair held in register k1: 2m, 2m+1 with m = k1 + R*bitrev(g)
     const int mb = R * brev(g, lgg);
     for (int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); row < nitems; row += W) {
         const int z = row / r.nyl;
         const long long off = (long long)row * 2 * K;
         const double ub = a.ubar[z], ubp = a.ubarp[z];
-        double2 u[3][R];
+#pragma unroll 1
+        for (int l = 0; l < 3; ++l) {
+            double2 t[R];
+            nl_c2r_r<R>(a.U[l] + off, false, K, N, g, r.wavx, r.rp.twr, r.rp.half.tw, t);
+            const double add = (l == 0) ? ub : 0.0;
 #pragma unroll
-        for (int l = 0; l < 3; ++l) nl_c2r_r<R>(a.U[l] + off, false, K, N, g, r.wavx, r.rp.twr, r.rp.half.tw, u[l]);
-#pragma unroll
-        for (int k1 = 0; k1 < R; ++k1) {
-            u[0][k1].x += ub;
-            u[0][k1].y += ub;
+            for (int k1 = 0; k1 < R; ++k1) U(l, k1) = make_double2(t[k1].x + add, t[k1].y + add);
         }
         // fluxes 0.5 u_l u_m for (11, 12, 13, 22, 23, 33)
-#pragma unroll
+#pragma unroll 1
         for (int p = 0; p < 6; ++p) {
             const int l = (p < 3) ? 0 : (p < 5 ? 1 : 2);
             const int m = (p < 3) ? p : (p < 5 ? p - 2 : 2);
             double2 f[R];
 #pragma unroll
-            for (int k1 = 0; k1 < R; ++k1)
-                f[k1] = make_double2(0.5 * (u[l][k1].x * u[m][k1].x), 0.5 * (u[l][k1].y * u[m][k1].y));
+            for (int k1 = 0; k1 < R; ++k1) {
+                const double2 ul = U(l, k1), um = U(m, k1);
+                f[k1] = make_double2(0.5 * (ul.x * um.x), 0.5 * (ul.y * um.y));
+            }
             nl_r2c_r<R>(f, a.H[p] + off, K, g, r.rp.twr, r.rp.half.tw);
         }
         // convective terms -0.5 u_m d_m u_l, plus the fringe
 #pragma unroll 1
         for (int l = 0; l < 3; ++l) {
-            double2 acc[R], d[R];
+            double2 d[R];
             nl_c2r_r<R>(a.U[l] + off, true, K, N, g, r.wavx, r.rp.twr, r.rp.half.tw, d);
 #pragma unroll
-            for (int k1 = 0; k1 < R; ++k1)
-                acc[k1] = make_double2(0.0 - 0.5 * (u[0][k1].x * d[k1].x), 0.0 - 0.5 * (u[0][k1].y * d[k1].y));
+            for (int k1 = 0; k1 < R; ++k1) {
+                const double2 u0 = U(0, k1);
+                U(3, k1) = make_double2(0.0 - 0.5 * (u0.x * d[k1].x), 0.0 - 0.5 * (u0.y * d[k1].y));
+            }
             nl_c2r_r<R>(a.DY[l] + off, false, K, N, g, r.wavx, r.rp.twr, r.rp.half.tw, d);
 #pragma unroll
             for (int k1 = 0; k1 < R; ++k1) {
-                acc[k1].x = acc[k1].x - 0.5 * (u[1][k1].x * d[k1].x);
-                acc[k1].y = acc[k1].y - 0.5 * (u[1][k1].y * d[k1].y);
+                const double2 u1 = U(1, k1);
+                double2 c = U(3, k1);
+                c.x = c.x - 0.5 * (u1.x * d[k1].x);
+                c.y = c.y - 0.5 * (u1.y * d[k1].y);
+                U(3, k1) = c;
             }
             nl_c2r_r<R>(a.DZ[l] + off, false, K, N, g, r.wavx, r.rp.twr, r.rp.half.tw, d);
             const double dzb = (l == 0) ? ubp : 0.0;
+            const double ut = (l == 0) ? ub : 0.0;
 #pragma unroll
             for (int k1 = 0; k1 < R; ++k1) {
-                acc[k1].x = acc[k1].x - 0.5 * (u[2][k1].x * (d[k1].x + dzb));
-                acc[k1].y = acc[k1].y - 0.5 * (u[2][k1].y * (d[k1].y + dzb));
-            }
-            if (a.lamx != nullptr) {
-                const double ut = (l == 0) ? ub : 0.0;
-#pragma unroll
-                for (int k1 = 0; k1 < R; ++k1) {
+                const double2 u2 = U(2, k1);
+                double2 c = U(3, k1);
+                c.x = c.x - 0.5 * (u2.x * (d[k1].x + dzb));
+                c.y = c.y - 0.5 * (u2.y * (d[k1].y + dzb));
+                if (a.lamx != nullptr) {
                     const int x = 2 * (k1 + mb);
                     const double lx0 = __ldg(&a.lamx[x]), lx1 = __ldg(&a.lamx[x + 1]);
-                    const double ua = (l == 0) ? u[0][k1].x : (l == 1 ? u[1][k1].x : u[2][k1].x);
-                    const double ubb = (l == 0) ? u[0][k1].y : (l == 1 ? u[1][k1].y : u[2][k1].y);
-                    acc[k1].x = acc[k1].x + lx0 * (ut - ua);
-                    acc[k1].y = acc[k1].y + lx1 * (ut - ubb);
+                    const double2 ul = U(l, k1);
+                    c.x = c.x + lx0 * (ut - ul.x);
+                    c.y = c.y + lx1 * (ut - ul.y);
                 }
+                d[k1] = c;
             }
-            nl_r2c_r<R>(acc, a.N[l] + off, K, g, r.rp.twr, r.rp.half.tw);
+            nl_r2c_r<R>(d, a.N[l] + off, K, g, r.rp.twr, r.rp.half.tw);
         }
     }
 }
@@ -995,8 +1016,15 @@ __global__ void __launch_bounds__(256) k_ywarp_f(YInvJobList ij, YFwdJobList fj,
 //   h_11 = u'(ubar + u'/2)   (0.5 ubar^2 dropped: a kx = 0 function of z that only ever
 //                              enters the step through d/dx, where it vanishes)
 //   h_1m = (ubar + u') u_m / 2,  fringe lambda (ubar - u) = -lambda u'.
+#ifndef NLF_MINB
+#define NLF_MINB 6
+#endif
+// shared memory of k_row_nl_f: per warp, u', v, w and the convective sum (FP32)
 template <int R>
-__global__ void __launch_bounds__(128, 4) k_row_nl_f(NlRowArgs a) {
+constexpr size_t nl_f_smem() { return (size_t)4 * 4 * R * 32 * sizeof(float2); }
+
+template <int R>
+__global__ void __launch_bounds__(128, NLF_MINB) k_row_nl_f(NlRowArgs a) {
     const RowArgs& r = a.r;
     const int N = 32 * R, K = r.kxc, lgg = r.rp.half.lgg;
     const int g = threadIdx.x & 31;
@@ -1004,64 +1032,77 @@ __global__ void __launch_bounds__(128, 4) k_row_nl_f(NlRowArgs a) {
     const int W = gridDim.x * (blockDim.x >> 5);
     const int mb = R * brev(g, lgg);
     auto F = [](const double* p) { return reinterpret_cast<const float*>(p); };
+    // lane-private slots [l][k1][lane] of u', v, w (l = 0..2) and the convective sum (l = 3)
+    extern __shared__ float2 nl_f_sm[];
+    float2* us = nl_f_sm + (threadIdx.x >> 5) * (4 * R * 32);
+    auto U = [&](int l, int k1) -> float2& { return us[(l * R + k1) * 32 + g]; };
     for (int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); row < nitems; row += W) {
         const int z = row / r.nyl;
         const long long off = (long long)row * 2 * K;
         const float ub = (float)a.ubar[z], ubp = (float)a.ubarp[z];
-        float2 u[3][R];  // u', v, w
+#pragma unroll 1
+        for (int l = 0; l < 3; ++l) {
+            float2 t[R];
+            nl_c2r_r<R>(F(a.U[l]) + off, false, K, N, g, r.wavx, r.rp.twrf, r.rp.half.twf, t);
 #pragma unroll
-        for (int l = 0; l < 3; ++l) nl_c2r_r<R>(F(a.U[l]) + off, false, K, N, g, r.wavx, r.rp.twrf, r.rp.half.twf, u[l]);
-#pragma unroll
+            for (int k1 = 0; k1 < R; ++k1) U(l, k1) = t[k1];
+        }
+#pragma unroll 1
         for (int p = 0; p < 6; ++p) {
             float2 f[R];
 #pragma unroll
             for (int k1 = 0; k1 < R; ++k1) {
-                const float2 up = u[0][k1];
+                const float2 up = U(0, k1);
                 if (p == 0) {
                     f[k1] = make_float2(up.x * (ub + 0.5f * up.x), up.y * (ub + 0.5f * up.y));
                 } else if (p < 3) {
-                    const float2 um = u[p][k1];
+                    const float2 um = U(p, k1);
                     f[k1] = make_float2(0.5f * ((ub + up.x) * um.x), 0.5f * ((ub + up.y) * um.y));
                 } else {
                     const int l = (p < 5) ? 1 : 2;
                     const int m = (p < 5) ? p - 2 : 2;
-                    f[k1] = make_float2(0.5f * (u[l][k1].x * u[m][k1].x), 0.5f * (u[l][k1].y * u[m][k1].y));
+                    const float2 ul = U(l, k1), um = U(m, k1);
+                    f[k1] = make_float2(0.5f * (ul.x * um.x), 0.5f * (ul.y * um.y));
                 }
             }
             nl_r2c_r<R>(f, reinterpret_cast<float*>(a.H[p]) + off, K, g, r.rp.twrf, r.rp.half.twf);
         }
 #pragma unroll 1
         for (int l = 0; l < 3; ++l) {
-            float2 acc[R], d[R];
+            float2 d[R];
             nl_c2r_r<R>(F(a.U[l]) + off, true, K, N, g, r.wavx, r.rp.twrf, r.rp.half.twf, d);
 #pragma unroll
-            for (int k1 = 0; k1 < R; ++k1)
-                acc[k1] = make_float2(0.f - 0.5f * ((ub + u[0][k1].x) * d[k1].x),
-                                      0.f - 0.5f * ((ub + u[0][k1].y) * d[k1].y));
+            for (int k1 = 0; k1 < R; ++k1) {
+                const float2 u0 = U(0, k1);
+                U(3, k1) = make_float2(0.f - 0.5f * ((ub + u0.x) * d[k1].x), 0.f - 0.5f * ((ub + u0.y) * d[k1].y));
+            }
             nl_c2r_r<R>(F(a.DY[l]) + off, false, K, N, g, r.wavx, r.rp.twrf, r.rp.half.twf, d);
 #pragma unroll
             for (int k1 = 0; k1 < R; ++k1) {
-                acc[k1].x = acc[k1].x - 0.5f * (u[1][k1].x * d[k1].x);
-                acc[k1].y = acc[k1].y - 0.5f * (u[1][k1].y * d[k1].y);
+                const float2 u1 = U(1, k1);
+                float2 c = U(3, k1);
+                c.x = c.x - 0.5f * (u1.x * d[k1].x);
+                c.y = c.y - 0.5f * (u1.y * d[k1].y);
+                U(3, k1) = c;
             }
             nl_c2r_r<R>(F(a.DZ[l]) + off, false, K, N, g, r.wavx, r.rp.twrf, r.rp.half.twf, d);
             const float dzb = (l == 0) ? ubp : 0.f;
 #pragma unroll
             for (int k1 = 0; k1 < R; ++k1) {
-                acc[k1].x = acc[k1].x - 0.5f * (u[2][k1].x * (d[k1].x + dzb));
-                acc[k1].y = acc[k1].y - 0.5f * (u[2][k1].y * (d[k1].y + dzb));
-            }
-            if (a.lamx != nullptr) {
-#pragma unroll
-                for (int k1 = 0; k1 < R; ++k1) {
+                const float2 u2 = U(2, k1);
+                float2 c = U(3, k1);
+                c.x = c.x - 0.5f * (u2.x * (d[k1].x + dzb));
+                c.y = c.y - 0.5f * (u2.y * (d[k1].y + dzb));
+                if (a.lamx != nullptr) {
                     const int x = 2 * (k1 + mb);
                     const float lx0 = (float)__ldg(&a.lamx[x]), lx1 = (float)__ldg(&a.lamx[x + 1]);
-                    const float2 ul = (l == 0) ? u[0][k1] : (l == 1 ? u[1][k1] : u[2][k1]);
-                    acc[k1].x = acc[k1].x - lx0 * ul.x;
-                    acc[k1].y = acc[k1].y - lx1 * ul.y;
+                    const float2 ul = U(l, k1);
+                    c.x = c.x - lx0 * ul.x;
+                    c.y = c.y - lx1 * ul.y;
                 }
+                d[k1] = c;
             }
-            nl_r2c_r<R>(acc, reinterpret_cast<float*>(a.N[l]) + off, K, g, r.rp.twrf, r.rp.half.twf);
+            nl_r2c_r<R>(d, reinterpret_cast<float*>(a.N[l]) + off, K, g, r.rp.twrf, r.rp.half.twf);
         }
     }
 }
@@ -1175,17 +1216,23 @@ void nllaunch(const NlRowArgs& a, cudaStream_t s) {
     const int nitems = a.r.nyl * a.r.nzp;
     if (a.r.f32) {
         if (a.r.rp.half.g != 32) throw std::runtime_error("mixed precision: x transform length has no full-warp plan");
-        const int occ = resident_blocks((const void*)k_row_nl_f<R>, 128, 0);
+        constexpr size_t sm = nl_f_smem<R>();
+        if (!allow_smem((const void*)k_row_nl_f<R>, sm))
+            throw std::runtime_error("product rows: shared memory of the register plan refused");
+        const int occ = resident_blocks((const void*)k_row_nl_f<R>, 128, sm);
         long long blocks = (long long)occ * sm_count(), need = (nitems + 3) / 4;
         if (blocks > need) blocks = need > 0 ? need : 1;
-        { lsb::note_launch(); k_row_nl_f<R><<<(int)blocks, 128, 0, s>>>(a); }
+        { lsb::note_launch(); k_row_nl_f<R><<<(int)blocks, 128, sm, s>>>(a); }
         return;
     }
     if (a.r.rp.half.g == 32) {
-        const int occ = resident_blocks((const void*)k_row_nl_r<R>, 128, 0);
+        constexpr size_t sm = nl_r_smem<R>();
+        if (!allow_smem((const void*)k_row_nl_r<R>, sm))
+            throw std::runtime_error("product rows: shared memory of the register plan refused");
+        const int occ = resident_blocks((const void*)k_row_nl_r<R>, 128, sm);
         long long blocks = (long long)occ * sm_count(), need = (nitems + 3) / 4;
         if (blocks > need) blocks = need > 0 ? need : 1;
-        { lsb::note_launch(); k_row_nl_r<R><<<(int)blocks, 128, 0, s>>>(a); }
+        { lsb::note_launch(); k_row_nl_r<R><<<(int)blocks, 128, sm, s>>>(a); }
         return;
     }
     const size_t sm =
