@@ -154,6 +154,10 @@ typedef struct {
     int y_staging;       /* FP64 spanwise passes: tiles staged by cp.async (1) or by TMA tile
                             loads (2); 0 = the built-in choice (TMA on the padded grid,
                             cp.async on the unpadded one) */
+    int filter_staging;  /* 3-point SGS test filter: plane ring filled by cp.async (1) or by TMA
+                            row loads (2, rows of a multiple of 128 bytes); 0 = the built-in
+                            choice (TMA for FP64 rows, cp.async for the FP32 rows of the mixed
+                            form) */
 } lsb_schedule;
 /* out-of-range fields return LSB_ERR_ARG; the step graphs are dropped and re-captured */
 int lsb_set_schedule(lsb_handle* h, const lsb_schedule* s);

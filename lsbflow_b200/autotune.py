@@ -26,7 +26,7 @@ from typing import Callable
 
 from .config import LsbConfig
 
-KNOBS = ("gemm_warps", "filter_zchunks", "y_staging")
+KNOBS = ("gemm_warps", "filter_zchunks", "y_staging", "filter_staging")
 
 
 def uses_filter3(cfg: LsbConfig) -> bool:
@@ -38,13 +38,17 @@ def uses_filter3(cfg: LsbConfig) -> bool:
 def candidates(cfg: LsbConfig) -> dict:
     """Values tried per knob; 0 is the built-in model.  The ranges are the ones
     lsb_set_schedule accepts (gemm_warps 4..8, filter_zchunks 1..(nzp+3)/4, y_staging 1 cp.async
-    or 2 TMA for the FP64 spanwise passes; the built-in choice is TMA on the padded grid and
-    cp.async on the unpadded one)."""
+    or 2 TMA for the FP64 spanwise passes -- the built-in choice is TMA on the padded grid and
+    cp.async on the unpadded one --, filter_staging 1 cp.async or 2 TMA row loads for the SGS
+    filter's plane ring, where a row is a multiple of 128 bytes)."""
     zmax = max(1, (cfg.nzp + 3) // 4)
     zs = [0] + [c for c in (1, 2, 3, 4, 6, 8, 12, 16) if c <= zmax]
+    prec = getattr(cfg, "precision", 0)
+    row_bytes = cfg.nx * (4 if prec == 1 else 8)
     return {"gemm_warps": [0, 4, 5, 6, 7, 8],
             "filter_zchunks": zs if uses_filter3(cfg) else [0],
-            "y_staging": [0, 1, 2] if getattr(cfg, "precision", 0) == 0 else [0]}
+            "y_staging": [0, 1, 2] if prec == 0 else [0],
+            "filter_staging": [0, 1, 2] if uses_filter3(cfg) and row_bytes % 128 == 0 else [0]}
 
 
 def schedule_key(cfg: LsbConfig, device: str) -> str:

@@ -286,9 +286,12 @@ __global__ void __launch_bounds__(256, 4) k_ywarp(YInvJobList ij, YFwdJobList fj
         const int c0 = ch * WKC;
         double2* T = Buf[cur];
         if (TMA) {
-            if (!tma::mbar_wait(&bar[cur], ph[cur])) *sabort = 1;
-            ph[cur] ^= 1u;
-            inflight[cur] = false;
+            if (tma::mbar_wait(&bar[cur], ph[cur])) {
+                ph[cur] ^= 1u;
+                inflight[cur] = false;
+            } else {
+                *sabort = 1;  // the buffer stays in flight for the clean-up at the end
+            }
         } else {
             cpa_wait_all();
         }
@@ -412,7 +415,7 @@ __device__ __forceinline__ V r2c_mode_w(const V* Z, int k, int N, const V* __res
 
 // Generic row transforms: each lane group of each warp owns one row at a time.
 template <int R, class V, int GC = 0>
-__global__ void __launch_bounds__(256) k_row_c2r_w(RowJobList jobs, RowArgs a) {
+__global__ void __launch_bounds__(256, 3) k_row_c2r_w(RowJobList jobs, RowArgs a) {
     using S = typename CT<V>::S;
     extern __shared__ unsigned char rsm_raw[];
     V* smem = reinterpret_cast<V*>(rsm_raw);

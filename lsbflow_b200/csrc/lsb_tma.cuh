@@ -16,6 +16,11 @@ namespace lsb {
 bool tmap_f64_3d(CUtensorMap* out, const void* base, uint64_t nx, uint64_t rows, uint64_t nz, uint32_t box_x,
                  uint32_t box_rows);
 
+// A 2-D tensor [rows][nx] of 4- or 8-byte elements with a box of box_x x 1 (one row piece),
+// no swizzle: box_x <= 256 divides nx and box_x * elem_bytes is a multiple of 16.  Cached
+// like tmap_f64_3d.
+bool tmap_rows(CUtensorMap* out, const void* base, uint32_t elem_bytes, uint64_t nx, uint64_t rows, uint32_t box_x);
+
 namespace tma {
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -55,6 +60,16 @@ __device__ __forceinline__ void load_3d(void* dst, const CUtensorMap* map, int x
         "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
         "[%5];\n" ::"r"(smem_u32(dst)),
         "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// box at (x, y) of a 2-D tensor map into shared memory at dst (128-byte aligned); completes
+// on bar.  x * element size must be a multiple of 16 bytes.
+__device__ __forceinline__ void load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];\n" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
         : "memory");
 }
 

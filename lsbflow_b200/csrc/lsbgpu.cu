@@ -766,14 +766,15 @@ void step_one(lsb_handle* h) {
     h->dt2 = dt;
 }
 
-// a tensor-core kernel raises h->uerr when one of its bounded waits ran out
+// a kernel raises h->uerr when one of its bounded waits ran out (the int8 tensor-core
+// contractions, the TMA-staged spanwise passes and SGS filter)
 void check_uerr(lsb_handle* h) {
     if (!h->uerr) return;
     int e = 0;
     CK(cudaMemcpy(&e, h->uerr, sizeof(int), cudaMemcpyDeviceToHost));
     if (e != 0) {
         CK(cudaMemset(h->uerr, 0, sizeof(int)));
-        fail(LSB_ERR_CUDA, "tensor-core contraction: a completion wait timed out");
+        fail(LSB_ERR_CUDA, "a bounded completion wait timed out (tensor-core contraction or TMA staging)");
     }
 }
 
@@ -1493,6 +1494,9 @@ int lsb_set_schedule(lsb_handle* h, const lsb_schedule* s) {
         if (s->filter_zchunks < 0 || s->filter_zchunks > zmax)
             fail(LSB_ERR_ARG, "filter_zchunks must be 0.." + std::to_string(zmax));
         if (s->y_staging < 0 || s->y_staging > 2) fail(LSB_ERR_ARG, "y_staging must be 0, 1 or 2");
+        if (s->filter_staging < 0 || s->filter_staging > 2) fail(LSB_ERR_ARG, "filter_staging must be 0, 1 or 2");
+        if (s->filter_staging == 2 && (h->d.nx * (h->cfg.precision == 1 ? 4 : 8)) % 128 != 0)
+            fail(LSB_ERR_ARG, "filter_staging 2 needs rows of a multiple of 128 bytes");
         CK(cudaStreamSynchronize(h->stream));
         h->drop_graphs();
         h->sched = *s;

@@ -12,6 +12,7 @@
 
 #include "lsb_handle.cuh"
 #include "lsb_spectral.cuh"
+#include "lsb_tma.cuh"
 
 namespace lsb {
 
@@ -133,16 +134,33 @@ template <> struct Vec2<float> { using type = float2; };
 // from the plane tile and the y and z filters run in registers: one barrier per plane.
 constexpr int FR = 4;
 
-// three blocks per SM fit the FP32 form in 80 registers; the FP64 form would spill there
-template <class T>
+// the input fields' row maps ([nzp * ny][nx], box of min(nx, 256) x 1) for TMA staging
+struct alignas(64) FiltMaps {
+    CUtensorMap m[kFilterFields];
+};
+
+// three blocks per SM fit the FP32 form in 80 registers; the FP64 form would spill there.
+// TMA = true: each plane of the ring (the block's rows and their two periodic y halo rows)
+// is brought in by TMA row loads, one per lane of warp 0 (issued from one thread they
+// serialised and ran slower than cp.async), completing on an mbarrier per ring slot
+// (bounded waits: a time-out raises *err and ends the block after its loads in flight have
+// landed); TMA = false: cp.async by all threads.
+template <class T, bool TMA>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_filter3p(FieldList fl, int lgx, int ny, int nzp, int FJ, int zch, T a, T b,
                                                      const double* __restrict__ az, const double* __restrict__ bz,
-                                                     const double* __restrict__ cz) {
+                                                     const double* __restrict__ cz,
+                                                     const __grid_constant__ FiltMaps tm, int* err) {
     using V2 = typename Vec2<T>::type;
     const int nx = 1 << lgx, NP = nx >> 1;
-    extern __shared__ __align__(16) unsigned char fsm_raw[];
+    extern __shared__ __align__(128) unsigned char fsm_raw[];
+    // TMA destinations are 128-byte aligned: the tiles start on a 128-byte boundary and a
+    // row is a multiple of 128 bytes (checked by the host)
+    unsigned char* sbase = TMA ? fsm_raw + ((128u - (unsigned)(__cvta_generic_to_shared(fsm_raw) & 127u)) & 127u)
+                               : fsm_raw;
     const int tsz = (FJ + 2) * nx;
-    T* tiles = reinterpret_cast<T*>(fsm_raw);  // RT_ST tiles of (FJ + 2) rows
+    T* tiles = reinterpret_cast<T*>(sbase);  // RT_ST tiles of (FJ + 2) rows
+    uint64_t* bar = reinterpret_cast<uint64_t*>(tiles + RT_ST * tsz);  // [RT_ST] (TMA)
+    int* sabort = reinterpret_cast<int*>(bar + RT_ST);
     const int f = blockIdx.z, zc = blockIdx.y;
     const T* q = reinterpret_cast<const T*>(fl.in[f]);
     T* out = reinterpret_cast<T*>(fl.out[f]);
@@ -159,7 +177,40 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_filter3p(FieldL
     const int lgrv = lgx - LGV;                // log2 of the copies per row
     const int nld_v = (rows + 2) << lgrv;
     const long long plane = (long long)ny * nx;
+    const int bx = nx < 256 ? nx : 256;        // TMA box width
+    uint32_t ph[RT_ST] = {0u, 0u, 0u};
+    bool inflight[RT_ST] = {false, false, false};
+    if (TMA) {
+        if (tid == 0) {
+            for (int i = 0; i < RT_ST; ++i) tma::mbar_init(&bar[i], 1);
+            tma::fence_init();
+            *sabort = 0;
+        }
+        __syncthreads();
+    }
     auto issue = [&](int kk) {
+        if (TMA) {
+            if (kk > ke) return;
+            const int sl = kk % RT_ST;
+            if (tid < 32) {
+                // warp 0 issues the plane's row loads, one per lane (lane 0 first announces
+                // their bytes); the block's reads of this slot, ordered before this call by a
+                // barrier, come before the TMA's writes
+                T* dst = tiles + sl * tsz;
+                tma::fence_proxy_async();
+                if (tid == 0) tma::mbar_expect_tx(&bar[sl], (uint32_t)((rows + 2) * nx * (int)sizeof(T)));
+                __syncwarp();
+                const int nb = nx / bx;
+                for (int i = tid; i < (rows + 2) * nb; i += 32) {
+                    const int r = i / nb, x0 = (i - r * nb) * bx;
+                    int j = j0 + r - 1;
+                    j = (j < 0) ? j + ny : (j >= ny ? j - ny : j);
+                    tma::load_2d(dst + (r << lgx) + x0, &tm.m[f], x0, kk * ny + j, &bar[sl]);
+                }
+            }
+            inflight[sl] = true;
+            return;
+        }
         if (kk <= ke) {
             T* dst = tiles + (kk % RT_ST) * tsz;
             const T* src = q + (long long)kk * plane;
@@ -178,8 +229,19 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_filter3p(FieldL
 #pragma unroll
     for (int i = 0; i < FR; ++i) y0[i][0] = y0[i][1] = y1[i][0] = y1[i][1] = y2[i][0] = y2[i][1] = (T)0;
     for (int kk = ks; kk <= ke; ++kk) {
-        cpa_wait_s<1>();
+        if (TMA) {
+            const int sl = kk % RT_ST;
+            if (tma::mbar_wait(&bar[sl], ph[sl])) {
+                ph[sl] ^= 1u;
+                inflight[sl] = false;
+            } else {
+                *sabort = 1;  // the slot stays in flight for the clean-up below
+            }
+        } else {
+            cpa_wait_s<1>();
+        }
         __syncthreads();  // plane kk has landed; every thread is done with plane kk - 1's slot
+        if (TMA && *sabort != 0) break;
         issue(kk + 2);
         const T* tile = tiles + (kk % RT_ST) * tsz;
         // x filter of tile rows r0 .. r0 + FR + 1 (grid rows j0 + r0 - 1 ..), then y filter
@@ -226,7 +288,17 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_filter3p(FieldL
             }
         }
     }
-    cpa_wait_s<0>();
+    if (TMA) {
+        // after a time-out: the loads still in flight land before the block exits (bounded
+        // waits again), and the launch's error word is raised
+        if (*sabort != 0) {
+            for (int i = 0; i < RT_ST; ++i)
+                if (inflight[i]) tma::mbar_wait(&bar[i], ph[i]);
+            if (tid == 0 && err) atomicExch(err, 1);
+        }
+    } else {
+        cpa_wait_s<0>();
+    }
 }
 
 void filter3_any(lsb_handle* h, const void* const* in, void* const* out, int n, double a, double b, int which,
@@ -249,10 +321,24 @@ void filter3_any(lsb_handle* h, const void* const* in, void* const* out, int n, 
             const int FJ = FR * 512 / d.nx;  // the thread map's rows (rows past ny are masked)
             const int nyb = (d.ny + FJ - 1) / FJ;
             const size_t es = f32 ? sizeof(float) : sizeof(double);
-            const size_t sm = (size_t)RT_ST * (FJ + 2) * d.nx * es;
+            // TMA row loads need 128-byte rows (the destinations' alignment); the built-in
+            // choice (filter_staging 0) is TMA for FP64 rows and cp.async for FP32 ones (at
+            // 256 x 64 x 129: FP64 172 -> 167 us per step with TMA; FP32 112 -> 129 us)
+            FiltMaps tm;
+            std::memset(&tm, 0, sizeof(tm));
+            const bool tma_ok = (d.nx * es) % 128 == 0;
+            bool tma = tma_ok && (h->sched.filter_staging == 2 || (h->sched.filter_staging == 0 && !f32));
+            for (int i = 0; tma && i < fl.n; ++i)
+                tma = tmap_rows(&tm.m[i], fl.in[i], (uint32_t)es, (uint64_t)d.nx, (uint64_t)d.nzp * d.ny,
+                                (uint32_t)std::min(d.nx, 256));
+            if (!tma && h->sched.filter_staging == 2) sfail(LSB_ERR_UNSUPPORTED, "filter_staging 2: no TMA row maps for this grid");
+            const size_t tiles = (size_t)RT_ST * (FJ + 2) * d.nx * es;
+            const size_t sm = tma ? 128 + tiles + RT_ST * sizeof(uint64_t) + 16 : tiles;
+            const void* kf = f32 ? (tma ? (const void*)k_filter3p<float, true> : (const void*)k_filter3p<float, false>)
+                                 : (tma ? (const void*)k_filter3p<double, true> : (const void*)k_filter3p<double, false>);
+            if (!allow_smem(kf, sm)) sfail(LSB_ERR_UNSUPPORTED, "SGS filter: shared memory of the plane ring refused");
             // z chunks: a block marches zch planes plus the two halo planes; pick the chunk
             // count with the least (waves of resident blocks) x (planes per block)
-            const void* kf = f32 ? (const void*)k_filter3p<float> : (const void*)k_filter3p<double>;
             const long long slots = std::max(1LL, (long long)resident_blocks(kf, 256, sm) * sm_count());
             int zch = d.nzp;
             double best = -1.0;
@@ -267,10 +353,16 @@ void filter3_any(lsb_handle* h, const void* const* in, void* const* out, int n, 
             if (force >= 1 && force <= std::max(1, (d.nzp + 3) / 4)) zch = (d.nzp + force - 1) / force;
             const int nzc = (d.nzp + zch - 1) / zch;
             dim3 grid(nyb, nzc, fl.n);
+            const double* z0 = zf;
+            const double* z1 = zf + d.nzp;
+            const double* z2 = zf + 2 * d.nzp;
+            lsb::note_launch();
             if (f32) {
-                { lsb::note_launch(); k_filter3p<float><<<grid, 256, sm, h->stream>>>(fl, lgx, d.ny, d.nzp, FJ, zch, (float)a, (float)b, zf, zf + d.nzp, zf + 2 * d.nzp); }
+                if (tma) k_filter3p<float, true><<<grid, 256, sm, h->stream>>>(fl, lgx, d.ny, d.nzp, FJ, zch, (float)a, (float)b, z0, z1, z2, tm, h->uerr);
+                else k_filter3p<float, false><<<grid, 256, sm, h->stream>>>(fl, lgx, d.ny, d.nzp, FJ, zch, (float)a, (float)b, z0, z1, z2, tm, h->uerr);
             } else {
-                { lsb::note_launch(); k_filter3p<double><<<grid, 256, sm, h->stream>>>(fl, lgx, d.ny, d.nzp, FJ, zch, a, b, zf, zf + d.nzp, zf + 2 * d.nzp); }
+                if (tma) k_filter3p<double, true><<<grid, 256, sm, h->stream>>>(fl, lgx, d.ny, d.nzp, FJ, zch, a, b, z0, z1, z2, tm, h->uerr);
+                else k_filter3p<double, false><<<grid, 256, sm, h->stream>>>(fl, lgx, d.ny, d.nzp, FJ, zch, a, b, z0, z1, z2, tm, h->uerr);
             }
         } else {
             const int nzc = (d.nzp + FZC - 1) / FZC;

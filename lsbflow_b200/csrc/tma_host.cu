@@ -64,4 +64,36 @@ bool tmap_f64_3d(CUtensorMap* out, const void* base, uint64_t nx, uint64_t rows,
     return true;
 }
 
+// row maps: [rows][nx] of 4- or 8-byte elements, box of box_x x 1, no swizzle
+using RowKey = std::tuple<const void*, uint64_t, uint64_t, uint32_t, uint32_t>;
+std::map<RowKey, CUtensorMap> g_rowmaps;
+
+bool tmap_rows(CUtensorMap* out, const void* base, uint32_t elem_bytes, uint64_t nx, uint64_t rows, uint32_t box_x) {
+    const RowKey key{base, nx, rows, box_x, elem_bytes};
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = g_rowmaps.find(key);
+    if (it != g_rowmaps.end()) {
+        *out = it->second;
+        return true;
+    }
+    EncodeFn enc = encoder();
+    if (!enc || (elem_bytes != 4 && elem_bytes != 8) || box_x == 0 || box_x > 256 || (box_x * elem_bytes) % 16 ||
+        nx % box_x || (reinterpret_cast<uintptr_t>(base) & 15) || (nx * elem_bytes) % 16)
+        return false;
+    const cuuint64_t dims[2] = {nx, rows};
+    const cuuint64_t strides[1] = {nx * elem_bytes};
+    const cuuint32_t box[2] = {box_x, 1};
+    const cuuint32_t estr[2] = {1, 1};
+    CUtensorMap m;
+    std::memset(&m, 0, sizeof(m));
+    const CUresult r = enc(&m, elem_bytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                           const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return false;
+    g_rowmaps.emplace(key, m);
+    *out = m;
+    return true;
+}
+
 }  // namespace lsb

@@ -73,7 +73,8 @@ class LsbDiagC(C.Structure):
 
 
 class LsbScheduleC(C.Structure):
-    _fields_ = [("gemm_warps", C.c_int), ("filter_zchunks", C.c_int), ("y_staging", C.c_int)]
+    _fields_ = [("gemm_warps", C.c_int), ("filter_zchunks", C.c_int), ("y_staging", C.c_int),
+                ("filter_staging", C.c_int)]
 
 
 _lib = None
@@ -252,11 +253,12 @@ class Solver:
         _ck(self._lib.lsb_synchronize(self._h))
 
     def set_schedule(self, sched: dict | None):
-        """Launch schedule ({"gemm_warps": 0|4..8, "filter_zchunks": 0|1..}); None or zeros:
-        the built-in models.  Results do not depend on it."""
+        """Launch schedule ({"gemm_warps": 0|4..8, "filter_zchunks": 0|1.., "y_staging": 0|1|2,
+        "filter_staging": 0|1|2}); None or zeros: the built-in choices.  Results do not depend
+        on it."""
         sched = sched or {}
         sc = LsbScheduleC(int(sched.get("gemm_warps", 0)), int(sched.get("filter_zchunks", 0)),
-                          int(sched.get("y_staging", 0)))
+                          int(sched.get("y_staging", 0)), int(sched.get("filter_staging", 0)))
         _ck(self._lib.lsb_set_schedule(self._h, C.byref(sc)))
 
     def schedule(self) -> dict:

@@ -26,7 +26,9 @@ def test_candidates_are_within_the_c_abi_limits():
         assert all(0 <= v <= zmax for v in c["filter_zchunks"])
         assert 0 in c["gemm_warps"] and 0 in c["filter_zchunks"]
         assert c["y_staging"] == ([0, 1, 2] if cfg.precision == 0 else [0])
+        assert c["filter_staging"] == ([0, 1, 2] if A.uses_filter3(cfg) else [0])
     assert A.candidates(workload("ens128"))["filter_zchunks"] == [0]     # sigma: no test filter
+    assert A.candidates(workload("les256", nx=8))["filter_staging"] == [0]  # 64-byte rows: no TMA
     assert len(A.candidates(workload("les256"))["filter_zchunks"]) > 4  # dynamic: filtered
 
 
@@ -40,9 +42,9 @@ def test_search_finds_the_minimum_and_counts_trials():
         return m(s)
 
     res = A.tune(cfg, measure)
-    assert res["schedule"] == {"gemm_warps": 6, "filter_zchunks": 3, "y_staging": 2}
+    assert res["schedule"] == {"gemm_warps": 6, "filter_zchunks": 3, "y_staging": 2, "filter_staging": 0}
     assert res["ms_per_step"] == pytest.approx(1.0)
-    assert res["model_ms_per_step"] == m({"gemm_warps": 0, "filter_zchunks": 0, "y_staging": 0})
+    assert res["model_ms_per_step"] == m({"gemm_warps": 0, "filter_zchunks": 0, "y_staging": 0, "filter_staging": 0})
     c = A.candidates(cfg)
     assert len(calls) == 1 + sum(len(c[k]) - 1 for k in A.KNOBS)
     assert len(res["trials"]) == len(calls)
@@ -50,7 +52,7 @@ def test_search_finds_the_minimum_and_counts_trials():
 
 def test_ties_keep_the_model():
     res = A.tune(workload("les256"), lambda s: 1.0 if s["gemm_warps"] else 1.001)
-    assert res["schedule"] == {"gemm_warps": 0, "filter_zchunks": 0, "y_staging": 0}
+    assert res["schedule"] == {"gemm_warps": 0, "filter_zchunks": 0, "y_staging": 0, "filter_staging": 0}
 
 
 def test_store_round_trip_and_keys(tmp_path):

@@ -84,7 +84,7 @@ def small_st():
 
 def test_tune_schedule_applies_only_checked_schedules(monkeypatch, small_st):
     monkeypatch.setattr(lib, "Solver", FakeSolver)
-    faster = {"gemm_warps": 6, "filter_zchunks": 0, "y_staging": 0}
+    faster = {"gemm_warps": 6, "filter_zchunks": 0, "y_staging": 0, "filter_staging": 0}
     monkeypatch.setattr(A, "gpu_measurer",
                         lambda st, steps, reps: (lambda s: 1.0 if s == faster else 2.0, lambda: None))
     sol = FakeSolver(small_st)

@@ -17,7 +17,7 @@ PROGRAM = r"""
 int main(void) {
     lsb_batch* b = 0;
     lsb_handle* h = 0;
-    lsb_schedule s = {4, 0, 0};
+    lsb_schedule s = {4, 0, 0, 0};
     lsb_config cfg = {0};
     lsb_setup su = {0};
     int bad = 0;
