@@ -415,7 +415,7 @@ __device__ __forceinline__ V r2c_mode_w(const V* Z, int k, int N, const V* __res
 
 // Generic row transforms: each lane group of each warp owns one row at a time.
 template <int R, class V, int GC = 0>
-__global__ void __launch_bounds__(256, 3) k_row_c2r_w(RowJobList jobs, RowArgs a) {
+__global__ void __launch_bounds__(256) k_row_c2r_w(RowJobList jobs, RowArgs a) {
     using S = typename CT<V>::S;
     extern __shared__ unsigned char rsm_raw[];
     V* smem = reinterpret_cast<V*>(rsm_raw);
@@ -761,8 +761,116 @@ __global__ void __launch_bounds__(256, 2) k_row_nl_w(NlRowArgs a) {
 // products are lane-local, and the r2c (decimation in time from that layout) ends in
 // natural order, where the pair Z[k], Z[N-k] of the real-to-complex split is one shuffle
 // apart.  No shared memory and no block barrier.
+// Exchange networks for full-warp rows with an even register count R = 2H (the product
+// rows).  In the lane-pair networks above both lanes of a pair evaluate a butterfly branch
+// for every register.  Here, at each stage, a lane sends half of its registers to its partner
+// and receives the partner's matching half, so that it holds H whole butterflies: half the
+// shuffles and half the butterfly arithmetic per stage.  Invariant before the stage on lane
+// bit h: register i (i < H) of the lane with bit h clear and register H + i of its partner
+// hold the two inputs of one butterfly, and the other way round; the upper lane's operand
+// order is reversed, which the twiddle's sign absorbs ((r - k)(-w) = (k - r) w exactly).
+// The outputs are stored in the order the next stage's invariant needs (swapped on lanes
+// whose next bit is set), and lanes with bit 16 set start with their halves rotated.
+// DIF (wfft_x): dft_reg, twiddles, rotation, stages h = 16 .. 1.  Lane g, register k then
+// holds X[m] with m = nl_slot<R>(g, k) = k%H + H*g_4 + R*bitrev4(g mod 16) + (N/2)*(k/H).
+// DIT (wfft_dit_x): the conjugate transpose of that network (stages h = 1 .. 16, the
+// butterfly s +- w d, the data routing inverted), from that layout to natural order.
+template <int R>
+__device__ __forceinline__ int nl_slot(int g, int k) {
+    constexpr int H = R / 2;
+    return (k % H) + H * ((g >> 4) & 1) + R * brev(g & 15, 4) + 16 * R * (k / H);
+}
+
+template <int R, class V>
+__device__ __forceinline__ void rotate_halves(V (&v)[R], bool on) {
+    constexpr int H = R / 2;
+#pragma unroll
+    for (int i = 0; i < H; ++i) {
+        const V a = v[i], b = v[H + i];
+        v[i] = on ? b : a;
+        v[H + i] = on ? a : b;
+    }
+}
+
+template <int R, int SIGN, class V>
+__device__ __forceinline__ void wfft_x(V (&v)[R], int g, const V* __restrict__ tw) {
+    static_assert(R % 2 == 0, "exchange network needs an even register count");
+    constexpr int H = R / 2;
+    dft_reg<R, SIGN>(v);
+    if (g != 0) {
+#pragma unroll
+        for (int k1 = 1; k1 < R; ++k1) {
+            V w = __ldg(&tw[g * k1]);
+            if (SIGN > 0) w.y = -w.y;
+            v[k1] = cmul(v[k1], w);
+        }
+    }
+    rotate_halves<R>(v, (g & 16) != 0);
+    int st = R;
+#pragma unroll
+    for (int h = 16; h >= 1; h >>= 1) {
+        V w = __ldg(&tw[(g & (h - 1)) * st]);
+        if (SIGN > 0) w.y = -w.y;
+        if (g & h) w = CT<V>::make(-w.x, -w.y);
+        const bool sw = (h > 1) && (g & (h >> 1)) != 0;
+#pragma unroll
+        for (int i = 0; i < H; ++i) {
+            V r;
+            r.x = __shfl_xor_sync(0xffffffffu, v[H + i].x, h);
+            r.y = __shfl_xor_sync(0xffffffffu, v[H + i].y, h);
+            const V sm = cadd(v[i], r);
+            const V df = cmul(csub(v[i], r), w);
+            v[i] = sw ? df : sm;
+            v[H + i] = sw ? sm : df;
+        }
+        st <<= 1;
+    }
+}
+
+template <int R, int SIGN, class V>
+__device__ __forceinline__ void wfft_dit_x(V (&v)[R], int g, const V* __restrict__ tw) {
+    static_assert(R % 2 == 0, "exchange network needs an even register count");
+    constexpr int H = R / 2;
+    int st = 16 * R;
+#pragma unroll
+    for (int h = 1; h <= 16; h <<= 1) {
+        V w = __ldg(&tw[(g & (h - 1)) * st]);
+        if (SIGN > 0) w.y = -w.y;
+        if (g & h) w = CT<V>::make(-w.x, -w.y);
+        const bool sw = (h > 1) && (g & (h >> 1)) != 0;
+#pragma unroll
+        for (int i = 0; i < H; ++i) {
+            const V sm = sw ? v[H + i] : v[i];
+            const V df = sw ? v[i] : v[H + i];
+            const V t = cmul(w, df);
+            const V bk = csub(sm, t);
+            v[i] = cadd(sm, t);
+            v[H + i].x = __shfl_xor_sync(0xffffffffu, bk.x, h);
+            v[H + i].y = __shfl_xor_sync(0xffffffffu, bk.y, h);
+        }
+        st >>= 1;
+    }
+    rotate_halves<R>(v, (g & 16) != 0);
+    if (g != 0) {
+#pragma unroll
+        for (int k1 = 1; k1 < R; ++k1) {
+            V w = __ldg(&tw[g * k1]);
+            if (SIGN > 0) w.y = -w.y;
+            v[k1] = cmul(v[k1], w);
+        }
+    }
+    dft_reg<R, SIGN>(v);
+}
+
+// physical pair index of register k of lane g after a product-row c2r (the slot layout)
+template <int R>
+__device__ __forceinline__ int nl_pair(int g, int k) {
+    if constexpr (R % 2 == 0) return nl_slot<R>(g, k);
+    else return k + R * brev(g, 5);
+}
+
 #ifndef NLR_MINB
-#define NLR_MINB 4
+#define NLR_MINB 3
 #endif
 #ifndef NLR_SEL
 #define NLR_SEL 1
@@ -790,14 +898,16 @@ __device__ __forceinline__ void nl_c2r_r(const S* __restrict__ src, bool ikx, in
         const V o = cmul(csub(xa, xb), cconj(__ldg(&twr[n])));
         v[rr] = CT<V>::make(e.x - o.y, e.y + o.x);
     }
-    wfft<R, +1, SEL>(v, 32, g, tw);
+    if constexpr (R % 2 == 0) wfft_x<R, +1>(v, g, tw);
+    else wfft<R, +1, SEL>(v, 32, g, tw);
 }
 
 // r2c of a slot-layout row; writes the K stored modes of the row at dst
 template <int R, class S, class V, bool SEL = (sizeof(S) == 8 && NLR_SEL)>
 __device__ __forceinline__ void nl_r2c_r(V (&v)[R], S* __restrict__ dst, int K, int g, const V* __restrict__ twr,
                                          const V* __restrict__ tw) {
-    wfft_dit<R, -1, SEL>(v, 32, g, tw);
+    if constexpr (R % 2 == 0) wfft_dit_x<R, -1>(v, g, tw);
+    else wfft_dit<R, -1, SEL>(v, 32, g, tw);
     // natural order: lane g register rr holds Z[g + 32 rr]; Z[N-k] for k = g + 32 rr is
     // lane (32-g) register R-1-rr (g > 0), or lane 0 register R-rr (g = 0, rr > 0)
     const int src = (32 - g) & 31;
@@ -827,7 +937,7 @@ constexpr size_t nl_r_smem() { return (size_t)4 * 4 * R * 32 * sizeof(double2); 
 template <int R>
 __global__ void __launch_bounds__(128, (R <= 6 ? NLR_MINB : 3)) k_row_nl_r(NlRowArgs a) {
     const RowArgs& r = a.r;
-    const int N = 32 * R, K = r.kxc, lgg = r.rp.half.lgg;
+    const int N = 32 * R, K = r.kxc;
     const int g = threadIdx.x & 31;
     const int nitems = r.nyl * r.nzp;
     const int W = gridDim.x * (blockDim.x >> 5);
@@ -836,8 +946,6 @@ __global__ void __launch_bounds__(128, (R <= 6 ? NLR_MINB : 3)) k_row_nl_r(NlRow
     extern __shared__ double2 nl_r_sm[];
     double2* us = nl_r_sm + (threadIdx.x >> 5) * (4 * R * 32);
     auto U = [&](int l, int k1) -> double2& { return us[(l * R + k1) * 32 + g]; };
-    // physical x of the pair held in register k1: 2m, 2m+1 with m = k1 + R*bitrev(g)
-    const int mb = R * brev(g, lgg);
     for (int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); row < nitems; row += W) {
         const int z = row / r.nyl;
         const long long off = (long long)row * 2 * K;
@@ -892,7 +1000,7 @@ __global__ void __launch_bounds__(128, (R <= 6 ? NLR_MINB : 3)) k_row_nl_r(NlRow
                 c.x = c.x - 0.5 * (u2.x * (d[k1].x + dzb));
                 c.y = c.y - 0.5 * (u2.y * (d[k1].y + dzb));
                 if (a.lamx != nullptr) {
-                    const int x = 2 * (k1 + mb);
+                    const int x = 2 * nl_pair<R>(g, k1);  // physical x of the pair in register k1
                     const double lx0 = __ldg(&a.lamx[x]), lx1 = __ldg(&a.lamx[x + 1]);
                     const double2 ul = U(l, k1);
                     c.x = c.x + lx0 * (ut - ul.x);
@@ -1029,11 +1137,10 @@ constexpr size_t nl_f_smem() { return (size_t)4 * 4 * R * 32 * sizeof(float2); }
 template <int R>
 __global__ void __launch_bounds__(128, NLF_MINB) k_row_nl_f(NlRowArgs a) {
     const RowArgs& r = a.r;
-    const int N = 32 * R, K = r.kxc, lgg = r.rp.half.lgg;
+    const int N = 32 * R, K = r.kxc;
     const int g = threadIdx.x & 31;
     const int nitems = r.nyl * r.nzp;
     const int W = gridDim.x * (blockDim.x >> 5);
-    const int mb = R * brev(g, lgg);
     auto F = [](const double* p) { return reinterpret_cast<const float*>(p); };
     // lane-private slots [l][k1][lane] of u', v, w (l = 0..2) and the convective sum (l = 3)
     extern __shared__ float2 nl_f_sm[];
@@ -1097,7 +1204,7 @@ __global__ void __launch_bounds__(128, NLF_MINB) k_row_nl_f(NlRowArgs a) {
                 c.x = c.x - 0.5f * (u2.x * (d[k1].x + dzb));
                 c.y = c.y - 0.5f * (u2.y * (d[k1].y + dzb));
                 if (a.lamx != nullptr) {
-                    const int x = 2 * (k1 + mb);
+                    const int x = 2 * nl_pair<R>(g, k1);  // physical x of the pair in register k1
                     const float lx0 = (float)__ldg(&a.lamx[x]), lx1 = (float)__ldg(&a.lamx[x + 1]);
                     const float2 ul = U(l, k1);
                     c.x = c.x - lx0 * ul.x;
