@@ -138,6 +138,115 @@ __device__ __forceinline__ void lane_bitrev(V (&v)[R], int G, int lane, int g, i
     }
 }
 
+// Exchange networks for lane groups of G = 16 or 32 lanes with an even register count
+// R = 2H.  In the lane-pair networks above both lanes of a pair evaluate a butterfly branch
+// for every register.  Here, at each stage, a lane sends half of its registers to its partner
+// and receives the partner's matching half, so that it holds H whole butterflies: half the
+// shuffles and half the butterfly arithmetic per stage.  Invariant before the stage on lane
+// bit h: register i (i < H) of the lane with bit h clear and register H + i of its partner
+// hold the two inputs of one butterfly, and the other way round; the upper lane's operand
+// order is reversed, which the twiddle's sign absorbs ((r - k)(-w) = (k - r) w exactly).
+// The outputs are stored in the order the next stage's invariant needs (swapped on lanes
+// whose next bit is set), and lanes with bit G/2 set start with their halves rotated.
+// DIF (wfft_x): dft_reg, twiddles, rotation, stages h = G/2 .. 1.  Lane g, register k then
+// holds X[m], m = xslot<R, G>(g, k) = k%H + H*g_top + R*bitrev(g mod G/2) + (N/2)*(k/H)
+// with N = R G and g_top the lane's bit G/2 -- the lane bit reversal of wfft is not needed.
+// DIT (wfft_dit_x): the conjugate transpose of that network (stages h = 1 .. G/2, the
+// butterfly s +- w d, the data routing inverted), from that layout to natural order.
+template <int R, int G>
+__device__ __forceinline__ int xslot(int g, int k) {
+    constexpr int H = R / 2, LG = ilog2c(G);
+    return (k % H) + H * ((g >> (LG - 1)) & 1) + R * brev(g & (G / 2 - 1), LG - 1) + (G / 2) * R * (k / H);
+}
+
+template <int R, class V>
+__device__ __forceinline__ void rotate_halves(V (&v)[R], bool on) {
+    constexpr int H = R / 2;
+#pragma unroll
+    for (int i = 0; i < H; ++i) {
+        const V a = v[i], b = v[H + i];
+        v[i] = on ? b : a;
+        v[H + i] = on ? a : b;
+    }
+}
+
+template <int R, int SIGN, int G, class V>
+__device__ __forceinline__ void wfft_x(V (&v)[R], int g, const V* __restrict__ tw) {
+    static_assert(R % 2 == 0 && (G == 16 || G == 32), "exchange network: even R, 16- or 32-lane groups");
+    constexpr int H = R / 2;
+    dft_reg<R, SIGN>(v);
+    if (g != 0) {
+#pragma unroll
+        for (int k1 = 1; k1 < R; ++k1) {
+            V w = __ldg(&tw[g * k1]);
+            if (SIGN > 0) w.y = -w.y;
+            v[k1] = cmul(v[k1], w);
+        }
+    }
+    rotate_halves<R>(v, (g & (G / 2)) != 0);
+    int st = R;
+#pragma unroll
+    for (int h = G / 2; h >= 1; h >>= 1) {
+        V w = __ldg(&tw[(g & (h - 1)) * st]);
+        if (SIGN > 0) w.y = -w.y;
+        if (g & h) w = CT<V>::make(-w.x, -w.y);
+        const bool sw = (h > 1) && (g & (h >> 1)) != 0;
+#pragma unroll
+        for (int i = 0; i < H; ++i) {
+            V r;
+            r.x = __shfl_xor_sync(0xffffffffu, v[H + i].x, h);
+            r.y = __shfl_xor_sync(0xffffffffu, v[H + i].y, h);
+            const V sm = cadd(v[i], r);
+            const V df = cmul(csub(v[i], r), w);
+            v[i] = sw ? df : sm;
+            v[H + i] = sw ? sm : df;
+        }
+        st <<= 1;
+    }
+}
+
+template <int R, int SIGN, int G, class V>
+__device__ __forceinline__ void wfft_dit_x(V (&v)[R], int g, const V* __restrict__ tw) {
+    static_assert(R % 2 == 0 && (G == 16 || G == 32), "exchange network: even R, 16- or 32-lane groups");
+    constexpr int H = R / 2;
+    int st = (G / 2) * R;
+#pragma unroll
+    for (int h = 1; h <= G / 2; h <<= 1) {
+        V w = __ldg(&tw[(g & (h - 1)) * st]);
+        if (SIGN > 0) w.y = -w.y;
+        if (g & h) w = CT<V>::make(-w.x, -w.y);
+        const bool sw = (h > 1) && (g & (h >> 1)) != 0;
+#pragma unroll
+        for (int i = 0; i < H; ++i) {
+            const V sm = sw ? v[H + i] : v[i];
+            const V df = sw ? v[i] : v[H + i];
+            const V t = cmul(w, df);
+            const V bk = csub(sm, t);
+            v[i] = cadd(sm, t);
+            v[H + i].x = __shfl_xor_sync(0xffffffffu, bk.x, h);
+            v[H + i].y = __shfl_xor_sync(0xffffffffu, bk.y, h);
+        }
+        st >>= 1;
+    }
+    rotate_halves<R>(v, (g & (G / 2)) != 0);
+    if (g != 0) {
+#pragma unroll
+        for (int k1 = 1; k1 < R; ++k1) {
+            V w = __ldg(&tw[g * k1]);
+            if (SIGN > 0) w.y = -w.y;
+            v[k1] = cmul(v[k1], w);
+        }
+    }
+    dft_reg<R, SIGN>(v);
+}
+
+// physical pair index of register k of lane g after a product-row c2r (the slot layout)
+template <int R>
+__device__ __forceinline__ int nl_pair(int g, int k) {
+    if constexpr (R % 2 == 0) return xslot<R, 32>(g, k);
+    else return k + R * brev(g, 5);
+}
+
 __device__ __forceinline__ void cpa16(void* sdst, const void* gsrc) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc));
@@ -322,11 +431,20 @@ __global__ void __launch_bounds__(256, 4) k_ywarp(YInvJobList ij, YFwdJobList fj
                 }
                 v[r] = x;
             }
-            wfft<R, INV ? +1 : -1>(v, G, g, a.plan.tw);
-            lane_bitrev<R>(v, G, lane, g, lgg);
-            if (act) {
+            if constexpr (GC == 16 && R % 2 == 0) {
+                // exchange network: register k1 holds output xslot(g, k1)
+                wfft_x<R, INV ? +1 : -1, 16>(v, g, a.plan.tw);
+                if (act) {
 #pragma unroll
-                for (int k1 = 0; k1 < R; ++k1) T[IX(R * g + k1, L)] = v[k1];
+                    for (int k1 = 0; k1 < R; ++k1) T[IX(xslot<R, 16>(g, k1), L)] = v[k1];
+                }
+            } else {
+                wfft<R, INV ? +1 : -1>(v, G, g, a.plan.tw);
+                lane_bitrev<R>(v, G, lane, g, lgg);
+                if (act) {
+#pragma unroll
+                    for (int k1 = 0; k1 < R; ++k1) T[IX(R * g + k1, L)] = v[k1];
+                }
             }
         }
         __syncthreads();
@@ -387,7 +505,7 @@ __global__ void __launch_bounds__(256, 4) k_ywarp(YInvJobList ij, YFwdJobList fj
 template <class V>
 __device__ __forceinline__ int xsw(int n) { return sizeof(V) == 16 ? (n ^ ((n >> 3) & 7)) : n; }
 
-template <int R, class V>
+template <int R, bool XN, class V>
 __device__ __forceinline__ void row_c2r_regs(const V* X, int N, int G, int g, const V* __restrict__ twr,
                                              const V* __restrict__ tw, V (&v)[R]) {
 #pragma unroll
@@ -399,7 +517,8 @@ __device__ __forceinline__ void row_c2r_regs(const V* X, int N, int G, int g, co
         const V o = cmul(csub(xa, xb), cconj(__ldg(&twr[n])));
         v[r] = CT<V>::make(e.x - o.y, e.y + o.x);
     }
-    wfft<R, +1>(v, G, g, tw);
+    if constexpr (XN) wfft_x<R, +1, 32>(v, g, tw);
+    else wfft<R, +1>(v, G, g, tw);
 }
 
 template <class V>
@@ -467,14 +586,18 @@ __global__ void __launch_bounds__(256) k_row_c2r_w(RowJobList jobs, RowArgs a) {
         }
         __syncwarp();
         V v[R];
-        row_c2r_regs<R>(X, N, G, g, twr, tw, v);
+        constexpr bool XN = (GC == 32 && R % 2 == 0);  // exchange network
+        row_c2r_regs<R, XN>(X, N, G, g, twr, tw, v);
         S m = (S)0;
         if (job.mean != nullptr && job.add_mean != 0.0) m = (S)(job.mean[row / a.nyl] * job.add_mean);
         const S sc = (S)job.scale;
-        lane_bitrev<R>(v, G, lane, g, lgg);
+        if constexpr (!XN) lane_bitrev<R>(v, G, lane, g, lgg);
         __syncwarp();
 #pragma unroll
-        for (int k1 = 0; k1 < R; ++k1) X[xsw<V>(R * g + k1)] = CT<V>::make(sc * v[k1].x + m, sc * v[k1].y + m);
+        for (int k1 = 0; k1 < R; ++k1) {
+            const int n = XN ? xslot<R, 32>(g, k1) : R * g + k1;
+            X[xsw<V>(n)] = CT<V>::make(sc * v[k1].x + m, sc * v[k1].y + m);
+        }
         __syncwarp();
         if (act) {
             V* o = reinterpret_cast<V*>(reinterpret_cast<S*>(job.out) + (long long)row * a.row_pitch);
@@ -550,6 +673,14 @@ __global__ void __launch_bounds__(256) k_row_r2c_w(RowJobList jobs, RowArgs a) {
 // reversal, no second staging.  (The same scheme for c2r measured slower than
 // k_row_c2r_w: its register footprint cost a block per SM.)
 __device__ __forceinline__ int rsw(int n) { return n ^ ((n >> 4) & 7); }  // stays in n's block of 8
+// the row buffer's swizzle per register count: conflict-free for the natural-order writes
+// and for the gather in the exchange network's slot order at R = 2, 4, 8 (2-way at R = 6);
+// for odd R the slot order of the lane-pair network (k1 + R bitrev(g))
+template <int R>
+__device__ __forceinline__ int rsw_x(int n) {
+    if constexpr (R % 2 == 1 || R == 8) return rsw(n);
+    else return n ^ ((n >> 3) & 7);
+}
 
 template <int R, class V>
 __global__ void __launch_bounds__(256) k_row_r2c_s(RowJobList jobs, RowArgs a) {
@@ -589,13 +720,20 @@ __global__ void __launch_bounds__(256) k_row_r2c_s(RowJobList jobs, RowArgs a) {
             }
         }
 #pragma unroll
-        for (int r = 0; r < R; ++r) Z[rsw(g + 32 * r)] = nx_v[r];
+        for (int r = 0; r < R; ++r) Z[rsw_x<R>(g + 32 * r)] = nx_v[r];
         if (u + TW < nunits) load_unit(u + TW, nx_v);
         __syncwarp();
+        if constexpr (R % 2 == 0) {
+            // the exchange network's input layout: register k1 holds z[xslot(g, k1)]
 #pragma unroll
-        for (int k1 = 0; k1 < R; ++k1) v[k1] = Z[rsw(k1 + mb)];
+            for (int k1 = 0; k1 < R; ++k1) v[k1] = Z[rsw_x<R>(xslot<R, 32>(g, k1))];
+        } else {
+#pragma unroll
+            for (int k1 = 0; k1 < R; ++k1) v[k1] = Z[rsw_x<R>(k1 + mb)];
+        }
         __syncwarp();  // the row buffer is free for the next row
-        wfft_dit<R, -1>(v, 32, g, tw);
+        if constexpr (R % 2 == 0) wfft_dit_x<R, -1, 32>(v, g, tw);
+        else wfft_dit<R, -1>(v, 32, g, tw);
         // natural order: lane g register rr holds Z[g + 32 rr]; Z[N-k] for k = g + 32 rr is
         // lane (32-g) register R-1-rr (g > 0), or lane 0 register R-rr (g = 0, rr > 0)
         V* yrow = reinterpret_cast<V*>(reinterpret_cast<S*>(job.out) + (long long)row * 2 * K);
@@ -761,114 +899,6 @@ __global__ void __launch_bounds__(256, 2) k_row_nl_w(NlRowArgs a) {
 // products are lane-local, and the r2c (decimation in time from that layout) ends in
 // natural order, where the pair Z[k], Z[N-k] of the real-to-complex split is one shuffle
 // apart.  No shared memory and no block barrier.
-// Exchange networks for full-warp rows with an even register count R = 2H (the product
-// rows).  In the lane-pair networks above both lanes of a pair evaluate a butterfly branch
-// for every register.  Here, at each stage, a lane sends half of its registers to its partner
-// and receives the partner's matching half, so that it holds H whole butterflies: half the
-// shuffles and half the butterfly arithmetic per stage.  Invariant before the stage on lane
-// bit h: register i (i < H) of the lane with bit h clear and register H + i of its partner
-// hold the two inputs of one butterfly, and the other way round; the upper lane's operand
-// order is reversed, which the twiddle's sign absorbs ((r - k)(-w) = (k - r) w exactly).
-// The outputs are stored in the order the next stage's invariant needs (swapped on lanes
-// whose next bit is set), and lanes with bit 16 set start with their halves rotated.
-// DIF (wfft_x): dft_reg, twiddles, rotation, stages h = 16 .. 1.  Lane g, register k then
-// holds X[m] with m = nl_slot<R>(g, k) = k%H + H*g_4 + R*bitrev4(g mod 16) + (N/2)*(k/H).
-// DIT (wfft_dit_x): the conjugate transpose of that network (stages h = 1 .. 16, the
-// butterfly s +- w d, the data routing inverted), from that layout to natural order.
-template <int R>
-__device__ __forceinline__ int nl_slot(int g, int k) {
-    constexpr int H = R / 2;
-    return (k % H) + H * ((g >> 4) & 1) + R * brev(g & 15, 4) + 16 * R * (k / H);
-}
-
-template <int R, class V>
-__device__ __forceinline__ void rotate_halves(V (&v)[R], bool on) {
-    constexpr int H = R / 2;
-#pragma unroll
-    for (int i = 0; i < H; ++i) {
-        const V a = v[i], b = v[H + i];
-        v[i] = on ? b : a;
-        v[H + i] = on ? a : b;
-    }
-}
-
-template <int R, int SIGN, class V>
-__device__ __forceinline__ void wfft_x(V (&v)[R], int g, const V* __restrict__ tw) {
-    static_assert(R % 2 == 0, "exchange network needs an even register count");
-    constexpr int H = R / 2;
-    dft_reg<R, SIGN>(v);
-    if (g != 0) {
-#pragma unroll
-        for (int k1 = 1; k1 < R; ++k1) {
-            V w = __ldg(&tw[g * k1]);
-            if (SIGN > 0) w.y = -w.y;
-            v[k1] = cmul(v[k1], w);
-        }
-    }
-    rotate_halves<R>(v, (g & 16) != 0);
-    int st = R;
-#pragma unroll
-    for (int h = 16; h >= 1; h >>= 1) {
-        V w = __ldg(&tw[(g & (h - 1)) * st]);
-        if (SIGN > 0) w.y = -w.y;
-        if (g & h) w = CT<V>::make(-w.x, -w.y);
-        const bool sw = (h > 1) && (g & (h >> 1)) != 0;
-#pragma unroll
-        for (int i = 0; i < H; ++i) {
-            V r;
-            r.x = __shfl_xor_sync(0xffffffffu, v[H + i].x, h);
-            r.y = __shfl_xor_sync(0xffffffffu, v[H + i].y, h);
-            const V sm = cadd(v[i], r);
-            const V df = cmul(csub(v[i], r), w);
-            v[i] = sw ? df : sm;
-            v[H + i] = sw ? sm : df;
-        }
-        st <<= 1;
-    }
-}
-
-template <int R, int SIGN, class V>
-__device__ __forceinline__ void wfft_dit_x(V (&v)[R], int g, const V* __restrict__ tw) {
-    static_assert(R % 2 == 0, "exchange network needs an even register count");
-    constexpr int H = R / 2;
-    int st = 16 * R;
-#pragma unroll
-    for (int h = 1; h <= 16; h <<= 1) {
-        V w = __ldg(&tw[(g & (h - 1)) * st]);
-        if (SIGN > 0) w.y = -w.y;
-        if (g & h) w = CT<V>::make(-w.x, -w.y);
-        const bool sw = (h > 1) && (g & (h >> 1)) != 0;
-#pragma unroll
-        for (int i = 0; i < H; ++i) {
-            const V sm = sw ? v[H + i] : v[i];
-            const V df = sw ? v[i] : v[H + i];
-            const V t = cmul(w, df);
-            const V bk = csub(sm, t);
-            v[i] = cadd(sm, t);
-            v[H + i].x = __shfl_xor_sync(0xffffffffu, bk.x, h);
-            v[H + i].y = __shfl_xor_sync(0xffffffffu, bk.y, h);
-        }
-        st >>= 1;
-    }
-    rotate_halves<R>(v, (g & 16) != 0);
-    if (g != 0) {
-#pragma unroll
-        for (int k1 = 1; k1 < R; ++k1) {
-            V w = __ldg(&tw[g * k1]);
-            if (SIGN > 0) w.y = -w.y;
-            v[k1] = cmul(v[k1], w);
-        }
-    }
-    dft_reg<R, SIGN>(v);
-}
-
-// physical pair index of register k of lane g after a product-row c2r (the slot layout)
-template <int R>
-__device__ __forceinline__ int nl_pair(int g, int k) {
-    if constexpr (R % 2 == 0) return nl_slot<R>(g, k);
-    else return k + R * brev(g, 5);
-}
-
 #ifndef NLR_MINB
 #define NLR_MINB 3
 #endif
@@ -898,7 +928,7 @@ __device__ __forceinline__ void nl_c2r_r(const S* __restrict__ src, bool ikx, in
         const V o = cmul(csub(xa, xb), cconj(__ldg(&twr[n])));
         v[rr] = CT<V>::make(e.x - o.y, e.y + o.x);
     }
-    if constexpr (R % 2 == 0) wfft_x<R, +1>(v, g, tw);
+    if constexpr (R % 2 == 0) wfft_x<R, +1, 32>(v, g, tw);
     else wfft<R, +1, SEL>(v, 32, g, tw);
 }
 
@@ -906,7 +936,7 @@ __device__ __forceinline__ void nl_c2r_r(const S* __restrict__ src, bool ikx, in
 template <int R, class S, class V, bool SEL = (sizeof(S) == 8 && NLR_SEL)>
 __device__ __forceinline__ void nl_r2c_r(V (&v)[R], S* __restrict__ dst, int K, int g, const V* __restrict__ twr,
                                          const V* __restrict__ tw) {
-    if constexpr (R % 2 == 0) wfft_dit_x<R, -1>(v, g, tw);
+    if constexpr (R % 2 == 0) wfft_dit_x<R, -1, 32>(v, g, tw);
     else wfft_dit<R, -1, SEL>(v, 32, g, tw);
     // natural order: lane g register rr holds Z[g + 32 rr]; Z[N-k] for k = g + 32 rr is
     // lane (32-g) register R-1-rr (g > 0), or lane 0 register R-rr (g = 0, rr > 0)
@@ -1076,12 +1106,21 @@ __global__ void __launch_bounds__(256) k_ywarp_f(YInvJobList ij, YFwdJobList fj,
                 }
                 v[r] = x;
             }
-            wfft<R, INV ? +1 : -1>(v, G, g, a.plan.twf);
-            lane_bitrev<R>(v, G, lane, g, lgg);
-            __syncwarp();
-            if (act) {
+            if constexpr (GC == 16 && R % 2 == 0) {
+                wfft_x<R, INV ? +1 : -1, 16>(v, g, a.plan.twf);
+                __syncwarp();
+                if (act) {
 #pragma unroll
-                for (int k1 = 0; k1 < R; ++k1) T[(R * g + k1) * TS + L] = v[k1];
+                    for (int k1 = 0; k1 < R; ++k1) T[xslot<R, 16>(g, k1) * TS + L] = v[k1];
+                }
+            } else {
+                wfft<R, INV ? +1 : -1>(v, G, g, a.plan.twf);
+                lane_bitrev<R>(v, G, lane, g, lgg);
+                __syncwarp();
+                if (act) {
+#pragma unroll
+                    for (int k1 = 0; k1 < R; ++k1) T[(R * g + k1) * TS + L] = v[k1];
+                }
             }
         }
         __syncthreads();
