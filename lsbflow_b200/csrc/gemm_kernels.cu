@@ -13,6 +13,8 @@
 // (mma.sync m16n8k8 f64: 1024 FMAs per instruction).  One CTA owns all Mp rows of a block
 // of 32..64 columns (8 per warp), A and B staged through shared memory in k-chunks of 16 with
 // conflict-free strides.
+#include <type_traits>
+
 #include "lsb_internal.cuh"
 
 namespace lsb {
@@ -60,6 +62,7 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
     double (*As)[MT * 16][LDA_S] = reinterpret_cast<double (*)[MT * 16][LDA_S]>(gsm);
     double (*Bs)[GBK][LDB_S] = reinterpret_cast<double (*)[GBK][LDB_S]>(gsm + GSTAGES * MT * 16 * LDA_S);
     double* lrow = gsm + GSTAGES * (MT * 16 * LDA_S + GBK * LDB_S);  // [4][Kp]: d2hb, hb, d2ht, ht
+    double* erow = lrow + 4 * g.Kp;  // [2][MT * 16]: the epilogue's row factors (lam, or hb and ht)
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int gq = lane >> 2, tq = lane & 3;
     const int f = blockIdx.y;
@@ -89,6 +92,19 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
             lbcb = bcb[lc];
             lbct = bct[lc];
             lfac = (-w2_of(g, lc)) - g.lift_sigma;
+        }
+    }
+    // the epilogue's row factors, staged once (their global loads would otherwise sit between
+    // the stores of every output element)
+    if (g.epi == EPI_HELM_SCALE || g.epi == EPI_LIFT_ADD) {
+        for (int r = tid; r < MT * 16; r += NT) {
+            const bool ok = r < g.M;
+            if (g.epi == EPI_HELM_SCALE) {
+                erow[r] = ok ? g.lam[r] : 0.0;
+            } else {
+                erow[r] = ok ? g.hb[r + g.roff] : 0.0;
+                erow[MT * 16 + r] = ok ? g.ht[r + g.roff] : 0.0;
+            }
         }
     }
     auto load_chunk = [&](int buf, int kc) {
@@ -149,52 +165,72 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
     }
     cp_async_wait<0>();
 
-    double* out = (f < 4 && g.outf[f]) ? g.outf[f] : g.out + f * g.out_fstride;
-    const double* aux = g.aux ? g.aux + f * g.out_fstride : nullptr;
+    double* __restrict__ out = (f < 4 && g.outf[f]) ? g.outf[f] : g.out + f * g.out_fstride;
+    const double* __restrict__ aux = g.aux ? g.aux + f * g.out_fstride : nullptr;
     const long long cb = c0 + warp * 8 + tq * 2;
-    // the two columns this thread writes, and their k^2 for the epilogues that need it
-    double ew2[2] = {0.0, 0.0};
-    if (g.epi == EPI_HELM_SCALE || g.epi == EPI_POISSON_RHS) {
-        for (int e = 0; e < 2; ++e)
-            if (cb + e < g.C) ew2[e] = w2_of(g, cb + e);
+    // per column of this thread: k^2 for the epilogues that need it, the boundary planes
+    double ew2[2] = {0.0, 0.0}, eb[2] = {0.0, 0.0}, et[2] = {0.0, 0.0};
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+        if (cb + e >= g.C) continue;
+        if (g.epi == EPI_HELM_SCALE || g.epi == EPI_POISSON_RHS) ew2[e] = w2_of(g, cb + e);
+        if (g.epi == EPI_LIFT_ADD && bcb != nullptr) {
+            eb[e] = bcb[cb + e];
+            et[e] = bct[cb + e];
+        }
     }
+    // one unrolled store loop per epilogue kind (the kind is uniform over the launch)
+    auto epilogue = [&](auto kind) {
+        constexpr int E = decltype(kind)::value;
+        constexpr bool RD = (E == EPI_AXPBY || E == EPI_POISSON_RHS);
 #pragma unroll
-    for (int t = 0; t < MT; ++t)
+        for (int t = 0; t < MT; ++t) {
+            // the field values this tile's epilogue reads, loaded together before its stores
+            double old[4] = {0.0, 0.0, 0.0, 0.0};
+            if (RD && (E == EPI_POISSON_RHS || g.beta != 0.0)) {
 #pragma unroll
-    for (int hh = 0; hh < 2; ++hh) {
-        const int r = t * 16 + hh * 8 + gq;
-        if (r >= g.M) continue;
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-            const long long c = cb + e;
-            if (c >= g.C) continue;
-            const long long o = (long long)(r + g.roff) * g.C + c;
-            double v = acc[t][2 * hh + e];
-            switch (g.epi) {
-                case EPI_STORE: break;
-                case EPI_AXPBY: v = g.alpha * v + (g.beta != 0.0 ? g.beta * out[o] : 0.0); break;
-                case EPI_HELM_SCALE: {
-                    const double dfac = (-ew2[e]) - g.sigma;
-                    v = v / (g.lam[r] + dfac);
-                    break;
-                }
-                case EPI_POISSON_RHS: {
-                    v = -v - ew2[e] * aux[o];
-                    break;
-                }
-                default: {  // EPI_LIFT_ADD (5): acc + hb*bcb + ht*bct
-                    if (bcb != nullptr) v = v + g.hb[r + g.roff] * bcb[c] + g.ht[r + g.roff] * bct[c];
-                    break;
+                for (int q = 0; q < 4; ++q) {
+                    const int r = t * 16 + (q >> 1) * 8 + gq;
+                    const long long c = cb + (q & 1);
+                    if (r < g.M && c < g.C) {
+                        const long long o = (long long)(r + g.roff) * g.C + c;
+                        old[q] = (E == EPI_POISSON_RHS) ? aux[o] : out[o];
+                    }
                 }
             }
-            out[o] = v;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int r = t * 16 + (q >> 1) * 8 + gq;
+                const int e = q & 1;
+                const long long c = cb + e;
+                if (r >= g.M || c >= g.C) continue;
+                double v = acc[t][q];
+                if constexpr (E == EPI_AXPBY) {
+                    v = g.alpha * v + (g.beta != 0.0 ? g.beta * old[q] : 0.0);
+                } else if constexpr (E == EPI_HELM_SCALE) {
+                    const double dfac = (-ew2[e]) - g.sigma;
+                    v = v / (erow[r] + dfac);
+                } else if constexpr (E == EPI_POISSON_RHS) {
+                    v = -v - ew2[e] * old[q];
+                } else if constexpr (E == EPI_LIFT_ADD) {  // acc + hb*bcb + ht*bct
+                    if (bcb != nullptr) v = v + erow[r] * eb[e] + erow[MT * 16 + r] * et[e];
+                }
+                out[(long long)(r + g.roff) * g.C + c] = v;
+            }
         }
+    };
+    switch (g.epi) {
+        case EPI_STORE: epilogue(std::integral_constant<int, EPI_STORE>{}); break;
+        case EPI_AXPBY: epilogue(std::integral_constant<int, EPI_AXPBY>{}); break;
+        case EPI_HELM_SCALE: epilogue(std::integral_constant<int, EPI_HELM_SCALE>{}); break;
+        case EPI_POISSON_RHS: epilogue(std::integral_constant<int, EPI_POISSON_RHS>{}); break;
+        default: epilogue(std::integral_constant<int, EPI_LIFT_ADD>{}); break;
     }
 }
 
 template <int MT, int NW>
 size_t gemm_smem(int Kp) {
-    return (size_t)(GSTAGES * (MT * 16 * LDA_S + GBK * (NW * 8 + 4)) + 4 * Kp) * sizeof(double);
+    return (size_t)(GSTAGES * (MT * 16 * LDA_S + GBK * (NW * 8 + 4)) + 4 * Kp + 2 * MT * 16) * sizeof(double);
 }
 
 template <int MT, int NW>
