@@ -14,6 +14,7 @@
 
 #include "lsb_fftdev.cuh"
 #include "lsb_internal.cuh"
+#include "lsb_sgs.cuh"
 #include "lsb_tma.cuh"
 
 namespace lsb {
@@ -604,6 +605,125 @@ __global__ void __launch_bounds__(256) k_row_c2r_w(RowJobList jobs, RowArgs a) {
             for (int k = g; k < N; k += G) o[k] = X[xsw<V>(k)];
         }
         __syncwarp();
+    }
+}
+
+// The dynamic model's physical fields with its first pointwise pass (k_dyn1 in
+// sgs_kernels.cu) fused in, for full-warp row plans with even R: one warp per (z, y) row runs
+// 12 c2r -- u_l, then the gradients in the order g_11, g_22, g_33, (g_12, g_21), (g_13, g_31),
+// (g_23, g_32), so that each off-diagonal S_lm is formed as soon as its pair is in registers
+// -- keeps S_ij in per-warp shared-memory slots of the exchange network's layout, and writes
+// u_l, S_ij and delta^2 |S| S_ij (the same expressions in the same order as k_dyn1, so the
+// same values bit for bit).  The nine gradient rows never go to HBM.
+template <int R>
+__host__ __device__ constexpr int dyn_row_slots() { return 32 * R + 8 + 6 * R * 32; }
+
+template <int R, class V>
+__global__ void __launch_bounds__(128) k_row_c2r_dyn(DynRowArgs a) {
+    using S = typename CT<V>::S;
+    const RowArgs& r = a.r;
+    extern __shared__ unsigned char dsm_raw[];
+    const V* twr = sizeof(S) == 4 ? reinterpret_cast<const V*>(r.rp.twrf) : reinterpret_cast<const V*>(r.rp.twr);
+    const V* tw = sizeof(S) == 4 ? reinterpret_cast<const V*>(r.rp.half.twf) : reinterpret_cast<const V*>(r.rp.half.tw);
+    constexpr int N = 32 * R;
+    const int g = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    V* X = reinterpret_cast<V*>(dsm_raw) + warp * dyn_row_slots<R>();
+    V* Ss = X + N + 8;  // [6][R][32]
+    auto SL = [&](int q, int k1) -> V& { return Ss[(q * R + k1) * 32 + g]; };
+    const int nrows = r.nyl * r.nzp;
+    const int W = gridDim.x * 4;
+    const V zero = CT<V>::make((S)0, (S)0);
+    for (int row = blockIdx.x * 4 + warp; row < nrows; row += W) {
+        const int z = row / r.nyl;
+        const long long in_off = (long long)row * 2 * r.kxc;
+        // c2r of one y-intermediate row into the slot layout (as k_row_c2r_w)
+        auto c2r = [&](const double* yin, bool ikx, V (&v)[R]) {
+            const S* yr = reinterpret_cast<const S*>(yin) + in_off;
+            __syncwarp();  // the row buffer is free
+#pragma unroll
+            for (int it = 0; it <= R; ++it) {
+                const int k = g + 32 * it;
+                if (k > N) break;
+                V x = (k < r.kxc) ? *reinterpret_cast<const V*>(yr + 2 * k) : zero;
+                if (ikx && k < r.kxc) {
+                    const S kk = (S)r.wavx[2 * k];
+                    x = CT<V>::make(-kk * x.y, kk * x.x);
+                }
+                if (k == 0) x.y = (S)0;
+                X[xsw<V>(k)] = x;
+            }
+            __syncwarp();
+            row_c2r_regs<R, true>(X, N, 32, g, twr, tw, v);
+        };
+        // a physical row from the slot layout, written in coalesced order through the buffer
+        auto store = [&](double* out, const V (&v)[R]) {
+            __syncwarp();
+#pragma unroll
+            for (int k1 = 0; k1 < R; ++k1) X[xsw<V>(xslot<R, 32>(g, k1))] = v[k1];
+            __syncwarp();
+            V* o = reinterpret_cast<V*>(reinterpret_cast<S*>(out) + (long long)row * r.row_pitch);
+#pragma unroll
+            for (int k = g; k < N; k += 32) o[k] = X[xsw<V>(k)];
+        };
+        V v[R], w[R];
+        // u_l (u_1 + ubar)
+#pragma unroll 1
+        for (int l = 0; l < 3; ++l) {
+            c2r(a.yu[l], false, v);
+            const S m = (l == 0) ? (S)(a.ubar[z] * 1.0) : (S)0;
+#pragma unroll
+            for (int k1 = 0; k1 < R; ++k1) v[k1] = CT<V>::make(v[k1].x + m, v[k1].y + m);
+            store(a.u[l], v);
+        }
+        // diagonal S_ll from g_ll (du_1/dx, du_2/dy, du_3/dz)
+#pragma unroll 1
+        for (int l = 0; l < 3; ++l) {
+            c2r(l == 0 ? a.yu[0] : (l == 1 ? a.ydy[1] : a.ydz[2]), l == 0, v);
+            const int q = sym6(l, l);
+#pragma unroll
+            for (int k1 = 0; k1 < R; ++k1)
+                SL(q, k1) = CT<V>::make(dyn_sij<S>(v[k1].x, v[k1].x), dyn_sij<S>(v[k1].y, v[k1].y));
+        }
+        // off-diagonal S_lm from (g_lm, g_ml): (du_1/dy, du_2/dx), (du_1/dz + ubarp, du_3/dx),
+        // (du_2/dz, du_3/dy)
+#pragma unroll 1
+        for (int p = 0; p < 3; ++p) {
+            const int l = (p < 2) ? 0 : 1, m = (p == 0) ? 1 : 2;
+            c2r(m == 1 ? a.ydy[l] : a.ydz[l], false, v);
+            if (p == 1) {
+                const S mz = (S)(a.ubarp[z] * 1.0);
+#pragma unroll
+                for (int k1 = 0; k1 < R; ++k1) v[k1] = CT<V>::make(v[k1].x + mz, v[k1].y + mz);
+            }
+            c2r(l == 0 ? a.yu[m] : a.ydy[2], l == 0, w);
+            const int q = sym6(l, m);
+#pragma unroll
+            for (int k1 = 0; k1 < R; ++k1)
+                SL(q, k1) = CT<V>::make(dyn_sij<S>(v[k1].x, w[k1].x), dyn_sij<S>(v[k1].y, w[k1].y));
+        }
+        // |S| per point, then S_ij and delta^2 |S| S_ij
+        const S dl = (S)a.delta[z];
+        V sn[R];
+#pragma unroll
+        for (int k1 = 0; k1 < R; ++k1) {
+            S sx[6], sy[6];
+#pragma unroll
+            for (int q = 0; q < 6; ++q) {
+                sx[q] = SL(q, k1).x;
+                sy[q] = SL(q, k1).y;
+            }
+            sn[k1] = CT<V>::make(snorm6<S>(sx), snorm6<S>(sy));
+        }
+#pragma unroll 1
+        for (int q = 0; q < 6; ++q) {
+#pragma unroll
+            for (int k1 = 0; k1 < R; ++k1) v[k1] = SL(q, k1);
+            store(a.sij[q], v);
+#pragma unroll
+            for (int k1 = 0; k1 < R; ++k1)
+                v[k1] = CT<V>::make(dyn_lij<S>(dl, sn[k1].x, v[k1].x), dyn_lij<S>(dl, sn[k1].y, v[k1].y));
+            store(a.lij[q], v);
+        }
     }
 }
 
@@ -1411,6 +1531,36 @@ bool launch_row_c2r_warp(const RowJobList& jobs, const RowArgs& a, cudaStream_t 
 bool launch_row_r2c_warp(const RowJobList& jobs, const RowArgs& a, cudaStream_t s) {
     if (a.rp.half.g == 0) return false;
     return rowdispatch(jobs, a, s, false);
+}
+
+namespace {
+template <int R>
+void dynlaunch(const DynRowArgs& a, cudaStream_t s) {
+    const size_t sm = (size_t)4 * dyn_row_slots<R>() * (a.r.f32 ? sizeof(float2) : sizeof(double2));
+    const void* k = a.r.f32 ? (const void*)k_row_c2r_dyn<R, float2> : (const void*)k_row_c2r_dyn<R, double2>;
+    if (!allow_smem(k, sm)) throw std::runtime_error("dynamic-model row pass: shared memory refused");
+    const int nrows = a.r.nyl * a.r.nzp;
+    long long blocks = (long long)resident_blocks(k, 128, sm) * sm_count(), need = (nrows + 3) / 4;
+    if (blocks > need) blocks = need > 0 ? need : 1;
+    lsb::note_launch();
+    if (a.r.f32) k_row_c2r_dyn<R, float2><<<(int)blocks, 128, sm, s>>>(a);
+    else k_row_c2r_dyn<R, double2><<<(int)blocks, 128, sm, s>>>(a);
+}
+}  // namespace
+
+bool row_c2r_dyn_plan(const RowArgs& r) {
+    const int R = r.rp.half.r;
+    return r.rp.half.g == 32 && (R == 2 || R == 4 || R == 6 || R == 8);
+}
+
+void launch_row_c2r_dyn(const DynRowArgs& a, cudaStream_t s) {
+    switch (row_c2r_dyn_plan(a.r) ? a.r.rp.half.r : 0) {
+        case 2: dynlaunch<2>(a, s); break;
+        case 4: dynlaunch<4>(a, s); break;
+        case 6: dynlaunch<6>(a, s); break;
+        case 8: dynlaunch<8>(a, s); break;
+        default: throw std::runtime_error("dynamic-model row pass: no fused plan for this length");
+    }
 }
 
 bool launch_row_nl_warp(const NlRowArgs& a, cudaStream_t s) {

@@ -42,6 +42,7 @@ struct SgsWork {
     double* delta = nullptr;    // [nzp] (dx dy dz)^(1/3) of dynamic/sigma
     double* sdelta = nullptr;   // [nzp] static-Smagorinsky delta (its own quirks)
     double* scal = nullptr;     // device scalars (u_tau average)
+    bool dyn1_fused = false;    // this step's row pass already wrote S_ij and delta^2 |S| S_ij
 };
 
 }  // namespace lsb
@@ -181,6 +182,9 @@ void sgs_add_tau(lsb_handle* h, double* const* ph, bool dealias, const double* c
                  double* const* xout = nullptr, int nx = 0, const double* xlam = nullptr,
                  const double* const* xmeans = nullptr);
 void sgs_tau_phys(lsb_handle* h, const double* ui, const double* g, const double* uiuj, double* tau);
+// the dynamic model's work fields S_ij (i = 0..5) and delta^2 |S| S_ij (i = 6..11), in the
+// working type of the handle's precision
+double* sgs_dyn_field(lsb_handle* h, int i);
 void sgs_mul(double* y, const double* x, long long n, cudaStream_t s);
 void diag_compute(lsb_handle* h, lsb_diagnostics* out);
 // lsbgpu.cu helpers used by sgs_kernels.cu

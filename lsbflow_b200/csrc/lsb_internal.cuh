@@ -131,6 +131,24 @@ struct RowJobList { int n; RowIO j[kMaxJobs]; };
 void launch_row_c2r(const RowJobList& jobs, const RowArgs& a, cudaStream_t s);
 void launch_row_r2c(const RowJobList& jobs, const RowArgs& a, cudaStream_t s);
 
+// the unpadded row pass of the dynamic SGS model's physical fields, with the model's first
+// pointwise pass fused in: u_l, S_ij and delta^2 |S| S_ij from the y-intermediates
+struct DynRowArgs {
+    RowArgs r;
+    const double* yu[3];   // y-intermediates of u_l (also the source of du_l/dx, with ikx)
+    const double* ydy[3];  // of du_l/dy
+    const double* ydz[3];  // of du_l/dz
+    double* u[3];          // physical u_l (u_1 + ubar)
+    double* sij[6];        // S_ij for (11, 12, 13, 22, 23, 33)
+    double* lij[6];        // delta^2 |S| S_ij
+    const double* ubar;    // [nzp], added to u_1
+    const double* ubarp;   // [nzp], added to du_1/dz
+    const double* delta;   // [nzp], the model's filter width
+};
+// whether the unpadded row plan has the fused form (full-warp groups, even R)
+bool row_c2r_dyn_plan(const RowArgs& r);
+void launch_row_c2r_dyn(const DynRowArgs& a, cudaStream_t s);
+
 // the fused nonlinear-product row kernel
 struct NlRowArgs {
     RowArgs r;

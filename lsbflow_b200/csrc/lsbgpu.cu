@@ -452,7 +452,46 @@ void nlterm(lsb_handle* h, const double* uin, double* Nout) {
         means[0] = h->ubar;
         means[3 + 2] = h->ubarp;
         const int nphys = (h->cfg.sgsflag == 1) ? 12 : 3;
-        { TimerScope ts(h, "phys_fields"); spec_to_phys(h, spec, ph, nphys, d.nzp, means, modes, f32); }
+        // the dynamic model takes only S_ij and delta^2 |S| S_ij from the gradients: its row
+        // pass forms them in registers (k_row_c2r_dyn) and the nine gradient rows are not stored
+        RowArgs ra = rowargs(h, false, d.nzp);
+        ra.f32 = f32;
+        const bool dynfuse = h->cfg.sgsflag == 1 && h->cfg.sgsmodel == 1 && row_c2r_dyn_plan(ra);
+        {
+            TimerScope ts(h, "phys_fields");
+            if (dynfuse) {
+                YInvJobList yj{};
+                DynRowArgs da{};
+                da.r = ra;
+                yj.n = 9;
+                for (int l = 0; l < 3; ++l) {
+                    double* yu = h->Yu + (long long)l * h->Yu1;
+                    double* ydy = h->Yu + (long long)(3 + l) * h->Yu1;
+                    double* ydz = h->Yu + (long long)(6 + l) * h->Yu1;
+                    yj.j[l] = YInvJob{uin + l * S, yu, YM_COPY};
+                    yj.j[3 + l] = YInvJob{uin + l * S, ydy, YM_IKY};
+                    yj.j[6 + l] = YInvJob{h->dz + l * S, ydz, YM_COPY};
+                    da.yu[l] = yu;
+                    da.ydy[l] = ydy;
+                    da.ydz[l] = ydz;
+                    da.u[l] = ph[l];
+                }
+                for (int q = 0; q < 6; ++q) {
+                    da.sij[q] = sgs_dyn_field(h, q);
+                    da.lij[q] = sgs_dyn_field(h, 6 + q);
+                }
+                da.ubar = h->ubar;
+                da.ubarp = h->ubarp;
+                da.delta = h->sgs.delta;
+                YPassArgs ya = ypass(h, false, d.nzp);
+                ya.f32 = f32;
+                launch_yinv(yj, ya, h->stream);
+                launch_row_c2r_dyn(da, h->stream);
+            } else {
+                spec_to_phys(h, spec, ph, nphys, d.nzp, means, modes, f32);
+            }
+        }
+        h->sgs.dyn1_fused = dynfuse;
         // with SGS the forcing goes to spectral space in the same launches as the stresses
         // (scratch field 21 holds the FP32 u' of the mixed form; the SGS model uses 12..17)
         double* no[3] = {Nout, Nout + S, Nout + 2 * S};
@@ -479,6 +518,7 @@ void nlterm(lsb_handle* h, const double* uin, double* Nout) {
             sgs_add_tau(h, ph, dealias, forcing ? fin : nullptr, forcing ? no : nullptr, forcing ? 3 : 0,
                         forcing ? h->lamx : nullptr, fmean);
         }
+        h->sgs.dyn1_fused = false;
     }
     // N_l -= d h_l1/dx + d h_l2/dy + d h_l3/dz
     NlDivArgs nd{};

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "lsb_handle.cuh"
+#include "lsb_sgs.cuh"
 #include "lsb_spectral.cuh"
 #include "lsb_tma.cuh"
 
@@ -19,11 +20,6 @@ namespace lsb {
 namespace {
 void sfail(int code, const std::string& m) { throw LsbError{code, m}; }
 
-__host__ __device__ __forceinline__ int sym6(int l, int m) {
-    // (1,1)=0 (1,2)=1 (1,3)=2 (2,2)=3 (2,3)=4 (3,3)=5
-    const int a = l < m ? l : m, b = l < m ? m : l;
-    return a == 0 ? b : (a == 1 ? 2 + b : 5);
-}
 
 inline int nblk(long long n) {
     long long b = (n + 255) / 256;
@@ -401,21 +397,6 @@ struct DynArgs {
 template <class T> __device__ __forceinline__ const T* cp_(const double* p) { return reinterpret_cast<const T*>(p); }
 template <class T> __device__ __forceinline__ T* wp_(double* p) { return reinterpret_cast<T*>(p); }
 
-// products rounded one at a time, so that no multiply-add contraction changes them
-__device__ __forceinline__ double mul_rn(double x, double y) { return __dmul_rn(x, y); }
-__device__ __forceinline__ float mul_rn(float x, float y) { return __fmul_rn(x, y); }
-
-// |S| = sqrt(2 S_ij S_ij) from the six independent components
-template <class T>
-__device__ __forceinline__ T snorm6(const T (&s6)[6]) {
-    T sn = (T)0;
-    for (int m = 0; m < 3; ++m)
-        for (int l = 0; l < 3; ++l) {
-            const T v = s6[sym6(l, m)];
-            sn = sn + (T)2 * v * v;
-        }
-    return sqrt(sn);
-}
 
 template <class T>
 __global__ void k_dyn1(DynArgs a) {  // S_ij and L'_ij = delta^2 |S| S_ij
@@ -424,11 +405,11 @@ __global__ void k_dyn1(DynArgs a) {  // S_ij and L'_ij = delta^2 |S| S_ij
         const T dl = (T)a.delta[k];
         T s6[6];
         for (int l = 0; l < 3; ++l)
-            for (int m = l; m < 3; ++m) s6[sym6(l, m)] = (T)0.5 * (cp_<T>(a.g[3 * l + m])[e] + cp_<T>(a.g[3 * m + l])[e]);
+            for (int m = l; m < 3; ++m) s6[sym6(l, m)] = dyn_sij<T>(cp_<T>(a.g[3 * l + m])[e], cp_<T>(a.g[3 * m + l])[e]);
         const T sn = snorm6<T>(s6);
         for (int q = 0; q < 6; ++q) {
             wp_<T>(a.sij[q])[e] = s6[q];
-            wp_<T>(a.lij[q])[e] = mul_rn(mul_rn(mul_rn(dl, dl), sn), s6[q]);
+            wp_<T>(a.lij[q])[e] = dyn_lij<T>(dl, sn, s6[q]);
         }
     }
 }
@@ -746,7 +727,7 @@ static void model_tau(lsb_handle* h, const double* const* u, const double* const
         a.P = P;
         a.nxy = nxy;
         a.full9 = full9 ? 1 : 0;
-        { lsb::note_launch(); k_dyn1<T><<<nblk(P), 256, 0, st>>>(a); }
+        if (!s.dyn1_fused) { lsb::note_launch(); k_dyn1<T><<<nblk(P), 256, 0, st>>>(a); }
         {  // one launch: [S_ij], [delta^2 |S| S_ij], [u_i], [u_i u_j]
             const double* fin[21];
             double* fout[21];
@@ -877,6 +858,11 @@ void sgs_add_tau(lsb_handle* h, double* const* ph, bool dealias, const double* c
     phys_to_spec(h, tp, hp, n, d.nzp, 1.0, 1.0, nullptr, f32, xlam, xmeans, nx);
 }
 
+double* sgs_dyn_field(lsb_handle* h, int i) {
+    const int w = (i < 6) ? i : 12 + (i - 6);  // model_tau's sij (0..5) and lij (12..17)
+    return h->cfg.precision == 1 ? fld<float>(h->sgs.w, w, h->P) : fld<double>(h->sgs.w, w, h->P);
+}
+
 void sgs_tau_phys(lsb_handle* h, const double* ui, const double* g, const double* uiuj, double* tau) {
     const long long P = h->P;
     const double* u3[3] = {ui, ui + P, ui + 2 * P};
@@ -885,6 +871,7 @@ void sgs_tau_phys(lsb_handle* h, const double* ui, const double* g, const double
     const double* uu6[6];
     for (int l = 0; l < 3; ++l)
         for (int m = l; m < 3; ++m) uu6[sym6(l, m)] = uiuj + (3 * l + m) * P;
+    h->sgs.dyn1_fused = false;  // the gradients are the caller's fields
     model_tau<double>(h, u3, g9, uu6, tau);
 }
 
