@@ -876,6 +876,88 @@ __global__ void __launch_bounds__(256) k_row_r2c_s(RowJobList jobs, RowArgs a) {
     }
 }
 
+// The dynamic model's last pointwise pass (k_dyn4 in sgs_kernels.cu) fused into the forward
+// row pass of its stresses, for full-warp row plans with even R: one warp per (z, y) row
+// reads S_ij and the filtered contractions in natural order, forms nu = C delta^2 |S| per
+// point (C = <L M> / <M M> clipped to [0, 0.2^2], NaN to 0) and, per component, tau_ij =
+// -2 nu S_ij -- the same expressions in the same order as k_dyn4 -- which it stages, gathers
+// in the exchange network's slot order and transforms as k_row_r2c_s does.  The six stress
+// fields never go to HBM.
+template <int R, class V>
+__global__ void __launch_bounds__(256) k_row_r2c_tau(TauRowArgs a) {
+    using S = typename CT<V>::S;
+    const RowArgs& r = a.r;
+    constexpr int N = 32 * R, LS = N + 8;
+    extern __shared__ unsigned char rsm_raw[];
+    const V* twr = sizeof(S) == 4 ? reinterpret_cast<const V*>(r.rp.twrf) : reinterpret_cast<const V*>(r.rp.twr);
+    const V* tw = sizeof(S) == 4 ? reinterpret_cast<const V*>(r.rp.half.twf) : reinterpret_cast<const V*>(r.rp.half.tw);
+    const int g = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    V* Z = reinterpret_cast<V*>(rsm_raw) + warp * LS;
+    const int K = r.kxc;
+    const int nrows = r.nyl * r.nzp;
+    const int gw = blockIdx.x * 8 + warp, TW = gridDim.x * 8;
+    const int src = (32 - g) & 31;
+    const S h = (S)0.5;
+    const S cmax = (S)(0.2 * 0.2);
+    for (int row = gw; row < nrows; row += TW) {
+        const int z = row / r.nyl;
+        const S dl = (S)a.delta[z];
+        const long long ro = (long long)row * r.row_pitch;
+        auto at = [&](const double* f) { return reinterpret_cast<const V*>(reinterpret_cast<const S*>(f) + ro); };
+        // nu at the pair g + 32 rr of this lane
+        V nu[R];
+#pragma unroll
+        for (int rr = 0; rr < R; ++rr) {
+            const int m = g + 32 * rr;
+            S sx[6], sy[6];
+#pragma unroll
+            for (int q = 0; q < 6; ++q) {
+                const V sv = at(a.sij[q])[m];
+                sx[q] = sv.x;
+                sy[q] = sv.y;
+            }
+            const V ct = at(a.ctot)[m], cd = at(a.cdd)[m];
+            S cx = ct.x / cd.x, cy = ct.y / cd.y;
+            if (cx < (S)0 || isnan(cx)) cx = (S)0;
+            if (cx > cmax) cx = cmax;
+            if (cy < (S)0 || isnan(cy)) cy = (S)0;
+            if (cy > cmax) cy = cmax;
+            nu[rr] = CT<V>::make(cx * dl * dl * snorm6<S>(sx), cy * dl * dl * snorm6<S>(sy));
+        }
+#pragma unroll 1
+        for (int q = 0; q < 6; ++q) {
+            V v[R];
+            __syncwarp();  // the row buffer is free
+#pragma unroll
+            for (int rr = 0; rr < R; ++rr) {
+                const V sv = at(a.sij[q])[g + 32 * rr];
+                Z[rsw_x<R>(g + 32 * rr)] = CT<V>::make((S)-2 * nu[rr].x * sv.x, (S)-2 * nu[rr].y * sv.y);
+            }
+            __syncwarp();
+#pragma unroll
+            for (int k1 = 0; k1 < R; ++k1) v[k1] = Z[rsw_x<R>(xslot<R, 32>(g, k1))];
+            wfft_dit_x<R, -1, 32>(v, g, tw);
+            V* yrow = reinterpret_cast<V*>(reinterpret_cast<S*>(a.out[q]) + (long long)row * 2 * K);
+#pragma unroll
+            for (int rr = 0; rr < R; ++rr) {
+                V zb;
+                zb.x = __shfl_sync(0xffffffffu, v[R - 1 - rr].x, src);
+                zb.y = __shfl_sync(0xffffffffu, v[R - 1 - rr].y, src);
+                if (g == 0) zb = v[rr == 0 ? 0 : R - rr];
+                const int k = g + 32 * rr;
+                if (k < K) {
+                    const V za = v[rr];
+                    zb = cconj(zb);
+                    const V e = CT<V>::make(h * (za.x + zb.x), h * (za.y + zb.y));
+                    const V o = CT<V>::make(h * (za.x - zb.x), h * (za.y - zb.y));
+                    const V tt = cmul(__ldg(&twr[k]), o);
+                    yrow[k] = CT<V>::make(e.x + tt.y, e.y - tt.x);
+                }
+            }
+        }
+    }
+}
+
 // The fused nonlinear-product row: 12 c2r (u_l, du_l/dx, du_l/dy, du_l/dz), the skew-
 // symmetric products and fringe of nlterm_skewsym (src/navierstokes.f90:725-769), 9 r2c.
 // A block owns one (z, y) row at a time; the 9 input rows of the next row are staged with
@@ -1547,6 +1629,33 @@ void dynlaunch(const DynRowArgs& a, cudaStream_t s) {
     else k_row_c2r_dyn<R, double2><<<(int)blocks, 128, sm, s>>>(a);
 }
 }  // namespace
+
+namespace {
+template <int R>
+void taulaunch(const TauRowArgs& a, cudaStream_t s) {
+    const size_t sm = (size_t)8 * (32 * R + 8) * (a.r.f32 ? sizeof(float2) : sizeof(double2));
+    const void* k = a.r.f32 ? (const void*)k_row_r2c_tau<R, float2> : (const void*)k_row_r2c_tau<R, double2>;
+    if (!allow_smem(k, sm)) throw std::runtime_error("dynamic-model stress row pass: shared memory refused");
+    const int nrows = a.r.nyl * a.r.nzp;
+    long long blocks = (long long)resident_blocks(k, 256, sm) * sm_count(), need = (nrows + 7) / 8;
+    if (blocks > need) blocks = need > 0 ? need : 1;
+    lsb::note_launch();
+    if (a.r.f32) k_row_r2c_tau<R, float2><<<(int)blocks, 256, sm, s>>>(a);
+    else k_row_r2c_tau<R, double2><<<(int)blocks, 256, sm, s>>>(a);
+}
+}  // namespace
+
+bool row_r2c_tau_plan(const RowArgs& r) { return row_c2r_dyn_plan(r); }
+
+void launch_row_r2c_tau(const TauRowArgs& a, cudaStream_t s) {
+    switch (row_r2c_tau_plan(a.r) ? a.r.rp.half.r : 0) {
+        case 2: taulaunch<2>(a, s); break;
+        case 4: taulaunch<4>(a, s); break;
+        case 6: taulaunch<6>(a, s); break;
+        case 8: taulaunch<8>(a, s); break;
+        default: throw std::runtime_error("dynamic-model stress row pass: no fused plan for this length");
+    }
+}
 
 bool row_c2r_dyn_plan(const RowArgs& r) {
     const int R = r.rp.half.r;

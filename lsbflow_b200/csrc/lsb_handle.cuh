@@ -43,6 +43,7 @@ struct SgsWork {
     double* sdelta = nullptr;   // [nzp] static-Smagorinsky delta (its own quirks)
     double* scal = nullptr;     // device scalars (u_tau average)
     bool dyn1_fused = false;    // this step's row pass already wrote S_ij and delta^2 |S| S_ij
+    bool dyn4_fused = false;    // the stresses are formed by the forward row pass (k_dyn4 skipped)
 };
 
 }  // namespace lsb
@@ -190,10 +191,12 @@ void diag_compute(lsb_handle* h, lsb_diagnostics* out);
 // lsbgpu.cu helpers used by sgs_kernels.cu
 // f32: physical fields and y-intermediates in FP32 (mixed form); spectral fields are FP64
 // lam / lmeans / nlam: the first nlam fields enter as the fringe forcing lambda(x) (m - q),
-// m = lmeans[i][z] (or 0), formed by the row transform as it reads them
+// m = lmeans[i][z] (or 0), formed by the row transform as it reads them.  tau: the last six
+// fields are the dynamic model's stresses, formed and transformed by the fused row pass from
+// its inputs (their phys entries are not read)
 void phys_to_spec(lsb_handle* h, const double* const* phys, double* const* spec, int nf, int nzp, double alpha,
                   double beta, double* const* ybuf, bool f32 = false, const double* lam = nullptr,
-                  const double* const* lmeans = nullptr, int nlam = 0);
+                  const double* const* lmeans = nullptr, int nlam = 0, const TauRowArgs* tau = nullptr);
 void spec_to_phys(lsb_handle* h, const double* const* spec, double* const* phys, int nf, int nzp,
                   const double* const* means, const int* modes, bool f32 = false, double scale = 1.0);
 void zgemm(lsb_handle* h, const Mat& m, const double* in, double* out, int nf, int epi, double alpha, double beta,

@@ -149,6 +149,20 @@ struct DynRowArgs {
 bool row_c2r_dyn_plan(const RowArgs& r);
 void launch_row_c2r_dyn(const DynRowArgs& a, cudaStream_t s);
 
+// the forward row pass of the dynamic model's stresses with its last pointwise pass fused in:
+// tau_ij = -2 nu S_ij, nu = C delta^2 |S| with C the clipped ratio of the filtered
+// contractions, transformed straight from S_ij into the y-intermediates
+struct TauRowArgs {
+    RowArgs r;
+    const double* sij[6];  // S_ij for (11, 12, 13, 22, 23, 33)
+    const double* ctot;    // filtered <L M>
+    const double* cdd;     // filtered <M M>
+    const double* delta;   // [nzp]
+    double* out[6];        // y-intermediate rows of tau_ij
+};
+bool row_r2c_tau_plan(const RowArgs& r);
+void launch_row_r2c_tau(const TauRowArgs& a, cudaStream_t s);
+
 // the fused nonlinear-product row kernel
 struct NlRowArgs {
     RowArgs r;

@@ -313,7 +313,8 @@ namespace lsb {
 // horfft(-1): physical (unpadded, [nzp][ny][nx]) -> spectral, nf fields
 void phys_to_spec(lsb_handle* h, const double* const* phys, double* const* spec, int nf, int nzp, double alpha,
                   double beta, double* const* ybuf, bool f32, const double* lam, const double* const* lmeans,
-                  int nlam) {
+                  int nlam, const TauRowArgs* tau) {
+    if (tau && (nf > kMaxJobs || nf < 6)) fail(LSB_ERR_STATE, "fused stress pass: 6..12 fields in one batch");
     for (int f0 = 0; f0 < nf; f0 += kMaxJobs) {
         const int n = std::min(kMaxJobs, nf - f0);
         RowJobList rj{};
@@ -333,7 +334,17 @@ void phys_to_spec(lsb_handle* h, const double* const* phys, double* const* spec,
         RowArgs ra = rowargs(h, false, nzp);
         YPassArgs ya = ypass(h, false, nzp);
         ra.f32 = ya.f32 = f32 ? 1 : 0;
-        launch_row_r2c(rj, ra, h->stream);
+        if (tau) {
+            // the plain rows first, then the stresses from S_ij and the filtered contractions
+            rj.n = n - 6;
+            if (rj.n > 0) launch_row_r2c(rj, ra, h->stream);
+            TauRowArgs t = *tau;
+            t.r = ra;
+            for (int q = 0; q < 6; ++q) t.out[q] = const_cast<double*>(yj.j[n - 6 + q].in);
+            launch_row_r2c_tau(t, h->stream);
+        } else {
+            launch_row_r2c(rj, ra, h->stream);
+        }
         launch_yfwd(yj, ya, h->stream);
     }
 }

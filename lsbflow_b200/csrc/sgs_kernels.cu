@@ -749,7 +749,7 @@ static void model_tau(lsb_handle* h, const double* const* u, const double* const
         const double* nd[2] = {a.numc, a.denomc};
         double* cc[2] = {W(36), W(37)};
         F3(nd, cc, 2, 1.0, 1.0, 1);
-        { lsb::note_launch(); k_dyn4<T><<<nblk(P), 256, 0, st>>>(a); }
+        if (!s.dyn4_fused) { lsb::note_launch(); k_dyn4<T><<<nblk(P), 256, 0, st>>>(a); }
     } else if (c.sgsmodel == 0) {
         P9 gt{};
         W9 tt{};
@@ -829,6 +829,9 @@ void sgs_add_tau(lsb_handle* h, double* const* ph, bool dealias, const double* c
     }
     const double* g[9];
     for (int q = 0; q < 9; ++q) g[q] = ph[3 + q];
+    // with the fused first pass (same row plan), the dynamic model's last pass goes into the
+    // forward row pass of the stresses too
+    s.dyn4_fused = s.dyn1_fused && h->cfg.sgsmodel == 1 && !s.nonsym;
     if (f32) model_tau<float>(h, u3, g, (const double* const*)uu6, s.tau, s.nonsym);
     else model_tau<double>(h, u3, g, (const double* const*)uu6, s.tau, s.nonsym);
     // add T(tau_lm) to h_lm (6 independent components, or all 9 when tau is not symmetric),
@@ -855,7 +858,16 @@ void sgs_add_tau(lsb_handle* h, double* const* ph, bool dealias, const double* c
                 hp[n++] = s.H9 + (3 * l + m) * S;
             }
     }
-    phys_to_spec(h, tp, hp, n, d.nzp, 1.0, 1.0, nullptr, f32, xlam, xmeans, nx);
+    TauRowArgs ta{};
+    if (s.dyn4_fused) {
+        // model_tau's work fields: S_ij, and the filtered contractions (W 36, 37)
+        for (int q = 0; q < 6; ++q) ta.sij[q] = sgs_dyn_field(h, q);
+        ta.ctot = f32 ? fld<float>(s.w, 36, P) : fld<double>(s.w, 36, P);
+        ta.cdd = f32 ? fld<float>(s.w, 37, P) : fld<double>(s.w, 37, P);
+        ta.delta = s.delta;
+    }
+    phys_to_spec(h, tp, hp, n, d.nzp, 1.0, 1.0, nullptr, f32, xlam, xmeans, nx, s.dyn4_fused ? &ta : nullptr);
+    s.dyn4_fused = false;
 }
 
 double* sgs_dyn_field(lsb_handle* h, int i) {
@@ -871,7 +883,7 @@ void sgs_tau_phys(lsb_handle* h, const double* ui, const double* g, const double
     const double* uu6[6];
     for (int l = 0; l < 3; ++l)
         for (int m = l; m < 3; ++m) uu6[sym6(l, m)] = uiuj + (3 * l + m) * P;
-    h->sgs.dyn1_fused = false;  // the gradients are the caller's fields
+    h->sgs.dyn1_fused = h->sgs.dyn4_fused = false;  // the gradients and the stresses are the caller's fields
     model_tau<double>(h, u3, g9, uu6, tau);
 }
 
