@@ -458,26 +458,56 @@ __global__ void __launch_bounds__(256, 4) k_ywarp(YInvJobList ij, YFwdJobList fj
             }
         } else {
             const YFwdJob job = fj.j[jb];
-            for (int idx = tid; idx < ny * WKC; idx += 256) {
-                const int j = idx / WKC, cc = idx - j * WKC, c = c0 + cc;
-                if (c >= a.kxc) continue;
-                double2 v = T[IX(pad_row_w(j, ny, nyl, a.layout), cc)];
-                if (job.sym && c == 0) {
-                    const int jm = (ny - j) % ny;
-                    const double2 w = T[IX(pad_row_w(jm, ny, nyl, a.layout), cc)];
-                    v = make_double2(0.5 * (v.x + w.x), 0.5 * (v.y - w.y));
+            if (job.beta == 0.0) {
+                for (int idx = tid; idx < ny * WKC; idx += 256) {
+                    const int j = idx / WKC, cc = idx - j * WKC, c = c0 + cc;
+                    if (c >= a.kxc) continue;
+                    double2 v = T[IX(pad_row_w(j, ny, nyl, a.layout), cc)];
+                    if (job.sym && c == 0) {
+                        const int jm = (ny - j) % ny;
+                        const double2 w = T[IX(pad_row_w(jm, ny, nyl, a.layout), cc)];
+                        v = make_double2(0.5 * (v.x + w.x), 0.5 * (v.y - w.y));
+                    }
+                    v.x *= a.scale;
+                    v.y *= a.scale;
+                    *reinterpret_cast<double2*>(job.out + ((long long)z * ny + j) * a.nx + 2 * c) =
+                        make_double2(job.alpha * v.x, job.alpha * v.y);
                 }
-                v.x *= a.scale;
-                v.y *= a.scale;
-                double2* o = reinterpret_cast<double2*>(job.out + ((long long)z * ny + j) * a.nx + 2 * c);
-                double2 rr;
-                if (job.beta != 0.0) {
-                    const double2 old = *o;
-                    rr = make_double2(fma(job.alpha, v.x, job.beta * old.x), fma(job.alpha, v.y, job.beta * old.y));
-                } else {
-                    rr = make_double2(job.alpha * v.x, job.alpha * v.y);
+            } else
+            // an accumulating job: groups of four elements per thread, the destination values
+            // loaded together before the group's stores
+            for (int i0 = tid; i0 < ny * WKC; i0 += 4 * 256) {
+                double2 old[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int idx = i0 + e * 256;
+                    const int j = idx / WKC, cc = idx - j * WKC, c = c0 + cc;
+                    old[e] = make_double2(0.0, 0.0);
+                    if (job.beta != 0.0 && idx < ny * WKC && c < a.kxc)
+                        old[e] = *reinterpret_cast<const double2*>(job.out + ((long long)z * ny + j) * a.nx + 2 * c);
                 }
-                *o = rr;
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int idx = i0 + e * 256;
+                    const int j = idx / WKC, cc = idx - j * WKC, c = c0 + cc;
+                    if (idx >= ny * WKC || c >= a.kxc) continue;
+                    double2 v = T[IX(pad_row_w(j, ny, nyl, a.layout), cc)];
+                    if (job.sym && c == 0) {
+                        const int jm = (ny - j) % ny;
+                        const double2 w = T[IX(pad_row_w(jm, ny, nyl, a.layout), cc)];
+                        v = make_double2(0.5 * (v.x + w.x), 0.5 * (v.y - w.y));
+                    }
+                    v.x *= a.scale;
+                    v.y *= a.scale;
+                    double2* o = reinterpret_cast<double2*>(job.out + ((long long)z * ny + j) * a.nx + 2 * c);
+                    double2 rr;
+                    if (job.beta != 0.0) {
+                        rr = make_double2(fma(job.alpha, v.x, job.beta * old[e].x), fma(job.alpha, v.y, job.beta * old[e].y));
+                    } else {
+                        rr = make_double2(job.alpha * v.x, job.alpha * v.y);
+                    }
+                    *o = rr;
+                }
             }
         }
         __syncthreads();
@@ -633,18 +663,46 @@ __global__ void __launch_bounds__(128) k_row_c2r_dyn(DynRowArgs a) {
     const int nrows = r.nyl * r.nzp;
     const int W = gridDim.x * 4;
     const V zero = CT<V>::make((S)0, (S)0);
+    // the 12 input rows of a row in transform order (the order of the c2r calls below):
+    // u_l (3), du_1/dx, du_2/dy, du_3/dz, (du_1/dy, du_2/dx), (du_1/dz, du_3/dx), (du_2/dz, du_3/dy)
+    auto src_of = [&](int rw, int i) -> const S* {
+        if (rw >= nrows) return nullptr;
+        const double* p;
+        switch (i) {
+            case 0: case 3: p = a.yu[0]; break;
+            case 1: case 7: p = a.yu[1]; break;
+            case 2: case 9: p = a.yu[2]; break;
+            case 4: p = a.ydy[1]; break;
+            case 5: p = a.ydz[2]; break;
+            case 6: p = a.ydy[0]; break;
+            case 8: p = a.ydz[0]; break;
+            case 10: p = a.ydz[1]; break;
+            default: p = a.ydy[2]; break;
+        }
+        return reinterpret_cast<const S*>(p) + (long long)rw * 2 * r.kxc;
+    };
+    // the next input row's modes, loaded while the current row is transformed
+    V nx_ld[R + 1];
+    auto load_row = [&](const S* yr) {
+#pragma unroll
+        for (int it = 0; it <= R; ++it) {
+            const int k = g + 32 * it;
+            nx_ld[it] = (yr != nullptr && k < r.kxc) ? *reinterpret_cast<const V*>(yr + 2 * k) : zero;
+        }
+    };
+    load_row(src_of(blockIdx.x * 4 + warp, 0));
     for (int row = blockIdx.x * 4 + warp; row < nrows; row += W) {
         const int z = row / r.nyl;
-        const long long in_off = (long long)row * 2 * r.kxc;
-        // c2r of one y-intermediate row into the slot layout (as k_row_c2r_w)
-        auto c2r = [&](const double* yin, bool ikx, V (&v)[R]) {
-            const S* yr = reinterpret_cast<const S*>(yin) + in_off;
+        // c2r of input i (staged from the prefetched modes) into the slot layout, as
+        // k_row_c2r_w; the next input's loads are issued before the transform
+        auto c2r = [&](int i, V (&v)[R]) {
+            const bool ikx = (i == 3 || i == 7 || i == 9);
             __syncwarp();  // the row buffer is free
 #pragma unroll
             for (int it = 0; it <= R; ++it) {
                 const int k = g + 32 * it;
                 if (k > N) break;
-                V x = (k < r.kxc) ? *reinterpret_cast<const V*>(yr + 2 * k) : zero;
+                V x = nx_ld[it];
                 if (ikx && k < r.kxc) {
                     const S kk = (S)r.wavx[2 * k];
                     x = CT<V>::make(-kk * x.y, kk * x.x);
@@ -652,6 +710,7 @@ __global__ void __launch_bounds__(128) k_row_c2r_dyn(DynRowArgs a) {
                 if (k == 0) x.y = (S)0;
                 X[xsw<V>(k)] = x;
             }
+            load_row(i < 11 ? src_of(row, i + 1) : src_of(row + W, 0));
             __syncwarp();
             row_c2r_regs<R, true>(X, N, 32, g, twr, tw, v);
         };
@@ -669,7 +728,7 @@ __global__ void __launch_bounds__(128) k_row_c2r_dyn(DynRowArgs a) {
         // u_l (u_1 + ubar)
 #pragma unroll 1
         for (int l = 0; l < 3; ++l) {
-            c2r(a.yu[l], false, v);
+            c2r(l, v);
             const S m = (l == 0) ? (S)(a.ubar[z] * 1.0) : (S)0;
 #pragma unroll
             for (int k1 = 0; k1 < R; ++k1) v[k1] = CT<V>::make(v[k1].x + m, v[k1].y + m);
@@ -678,7 +737,7 @@ __global__ void __launch_bounds__(128) k_row_c2r_dyn(DynRowArgs a) {
         // diagonal S_ll from g_ll (du_1/dx, du_2/dy, du_3/dz)
 #pragma unroll 1
         for (int l = 0; l < 3; ++l) {
-            c2r(l == 0 ? a.yu[0] : (l == 1 ? a.ydy[1] : a.ydz[2]), l == 0, v);
+            c2r(3 + l, v);
             const int q = sym6(l, l);
 #pragma unroll
             for (int k1 = 0; k1 < R; ++k1)
@@ -689,13 +748,13 @@ __global__ void __launch_bounds__(128) k_row_c2r_dyn(DynRowArgs a) {
 #pragma unroll 1
         for (int p = 0; p < 3; ++p) {
             const int l = (p < 2) ? 0 : 1, m = (p == 0) ? 1 : 2;
-            c2r(m == 1 ? a.ydy[l] : a.ydz[l], false, v);
+            c2r(6 + 2 * p, v);
             if (p == 1) {
                 const S mz = (S)(a.ubarp[z] * 1.0);
 #pragma unroll
                 for (int k1 = 0; k1 < R; ++k1) v[k1] = CT<V>::make(v[k1].x + mz, v[k1].y + mz);
             }
-            c2r(l == 0 ? a.yu[m] : a.ydy[2], l == 0, w);
+            c2r(7 + 2 * p, w);
             const int q = sym6(l, m);
 #pragma unroll
             for (int k1 = 0; k1 < R; ++k1)
@@ -1335,27 +1394,57 @@ __global__ void __launch_bounds__(256) k_ywarp_f(YInvJobList ij, YFwdJobList fj,
             }
         } else {
             const YFwdJob job = fj.j[jb];
-            for (int idx = tid; idx < ny * WKC; idx += 256) {
-                const int j = idx / WKC, cc = idx - j * WKC, c = c0 + cc;
-                if (c >= a.kxc) continue;
-                const float2 vf = T[pad_row_w(j, ny, nyl, a.layout) * TS + cc];
-                double2 v = make_double2((double)vf.x, (double)vf.y);
-                if (job.sym && c == 0) {
-                    const int jm = (ny - j) % ny;
-                    const float2 wf = T[pad_row_w(jm, ny, nyl, a.layout) * TS + cc];
-                    v = make_double2(0.5 * (v.x + (double)wf.x), 0.5 * (v.y - (double)wf.y));
+            if (job.beta == 0.0) {
+                for (int idx = tid; idx < ny * WKC; idx += 256) {
+                    const int j = idx / WKC, cc = idx - j * WKC, c = c0 + cc;
+                    if (c >= a.kxc) continue;
+                    const float2 vf = T[pad_row_w(j, ny, nyl, a.layout) * TS + cc];
+                    double2 v = make_double2((double)vf.x, (double)vf.y);
+                    if (job.sym && c == 0) {
+                        const int jm = (ny - j) % ny;
+                        const float2 wf = T[pad_row_w(jm, ny, nyl, a.layout) * TS + cc];
+                        v = make_double2(0.5 * (v.x + (double)wf.x), 0.5 * (v.y - (double)wf.y));
+                    }
+                    v.x *= a.scale;
+                    v.y *= a.scale;
+                    *reinterpret_cast<double2*>(job.out + ((long long)z * ny + j) * a.nx + 2 * c) =
+                        make_double2(job.alpha * v.x, job.alpha * v.y);
                 }
-                v.x *= a.scale;
-                v.y *= a.scale;
-                double2* o = reinterpret_cast<double2*>(job.out + ((long long)z * ny + j) * a.nx + 2 * c);
-                double2 rr;
-                if (job.beta != 0.0) {
-                    const double2 old = *o;
-                    rr = make_double2(fma(job.alpha, v.x, job.beta * old.x), fma(job.alpha, v.y, job.beta * old.y));
-                } else {
-                    rr = make_double2(job.alpha * v.x, job.alpha * v.y);
+            } else
+            // as in k_ywarp: an accumulating job's destination values are loaded four at a time
+            for (int i0 = tid; i0 < ny * WKC; i0 += 4 * 256) {
+                double2 old[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int idx = i0 + e * 256;
+                    const int j = idx / WKC, cc = idx - j * WKC, c = c0 + cc;
+                    old[e] = make_double2(0.0, 0.0);
+                    if (job.beta != 0.0 && idx < ny * WKC && c < a.kxc)
+                        old[e] = *reinterpret_cast<const double2*>(job.out + ((long long)z * ny + j) * a.nx + 2 * c);
                 }
-                *o = rr;
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int idx = i0 + e * 256;
+                    const int j = idx / WKC, cc = idx - j * WKC, c = c0 + cc;
+                    if (idx >= ny * WKC || c >= a.kxc) continue;
+                    const float2 vf = T[pad_row_w(j, ny, nyl, a.layout) * TS + cc];
+                    double2 v = make_double2((double)vf.x, (double)vf.y);
+                    if (job.sym && c == 0) {
+                        const int jm = (ny - j) % ny;
+                        const float2 wf = T[pad_row_w(jm, ny, nyl, a.layout) * TS + cc];
+                        v = make_double2(0.5 * (v.x + (double)wf.x), 0.5 * (v.y - (double)wf.y));
+                    }
+                    v.x *= a.scale;
+                    v.y *= a.scale;
+                    double2* o = reinterpret_cast<double2*>(job.out + ((long long)z * ny + j) * a.nx + 2 * c);
+                    double2 rr;
+                    if (job.beta != 0.0) {
+                        rr = make_double2(fma(job.alpha, v.x, job.beta * old[e].x), fma(job.alpha, v.y, job.beta * old[e].y));
+                    } else {
+                        rr = make_double2(job.alpha * v.x, job.alpha * v.y);
+                    }
+                    *o = rr;
+                }
             }
         }
         __syncthreads();
