@@ -1262,34 +1262,27 @@ __global__ void __launch_bounds__(128, (R <= 6 ? NLR_MINB : 3)) k_row_nl_r(NlRow
             }
             nl_r2c_r<R>(f, a.H[p] + off, K, g, r.rp.twr, r.rp.half.tw);
         }
-        // convective terms -0.5 u_m d_m u_l, plus the fringe
+        // convective terms -0.5 u_m d_m u_l, plus the fringe; the three c2r of a component
+        // share one loop body (a third of the code of three inlined copies)
 #pragma unroll 1
         for (int l = 0; l < 3; ++l) {
             double2 d[R];
-            nl_c2r_r<R>(a.U[l] + off, true, K, N, g, r.wavx, r.rp.twr, r.rp.half.tw, d);
+#pragma unroll 1
+            for (int t = 0; t < 3; ++t) {
+                const double* src = (t == 0) ? a.U[l] : (t == 1 ? a.DY[l] : a.DZ[l]);
+                nl_c2r_r<R>(src + off, t == 0, K, N, g, r.wavx, r.rp.twr, r.rp.half.tw, d);
+                const double dzb = (t == 2 && l == 0) ? ubp : 0.0;
 #pragma unroll
-            for (int k1 = 0; k1 < R; ++k1) {
-                const double2 u0 = U(0, k1);
-                U(3, k1) = make_double2(0.0 - 0.5 * (u0.x * d[k1].x), 0.0 - 0.5 * (u0.y * d[k1].y));
+                for (int k1 = 0; k1 < R; ++k1) {
+                    const double2 um = U(t, k1);
+                    const double2 c = (t == 0) ? make_double2(0.0, 0.0) : U(3, k1);
+                    U(3, k1) = make_double2(c.x - 0.5 * (um.x * (d[k1].x + dzb)), c.y - 0.5 * (um.y * (d[k1].y + dzb)));
+                }
             }
-            nl_c2r_r<R>(a.DY[l] + off, false, K, N, g, r.wavx, r.rp.twr, r.rp.half.tw, d);
-#pragma unroll
-            for (int k1 = 0; k1 < R; ++k1) {
-                const double2 u1 = U(1, k1);
-                double2 c = U(3, k1);
-                c.x = c.x - 0.5 * (u1.x * d[k1].x);
-                c.y = c.y - 0.5 * (u1.y * d[k1].y);
-                U(3, k1) = c;
-            }
-            nl_c2r_r<R>(a.DZ[l] + off, false, K, N, g, r.wavx, r.rp.twr, r.rp.half.tw, d);
-            const double dzb = (l == 0) ? ubp : 0.0;
             const double ut = (l == 0) ? ub : 0.0;
 #pragma unroll
             for (int k1 = 0; k1 < R; ++k1) {
-                const double2 u2 = U(2, k1);
                 double2 c = U(3, k1);
-                c.x = c.x - 0.5 * (u2.x * (d[k1].x + dzb));
-                c.y = c.y - 0.5 * (u2.y * (d[k1].y + dzb));
                 if (a.lamx != nullptr) {
                     const int x = 2 * nl_pair<R>(g, k1);  // physical x of the pair in register k1
                     const double lx0 = __ldg(&a.lamx[x]), lx1 = __ldg(&a.lamx[x + 1]);
@@ -1510,29 +1503,24 @@ __global__ void __launch_bounds__(128, NLF_MINB) k_row_nl_f(NlRowArgs a) {
 #pragma unroll 1
         for (int l = 0; l < 3; ++l) {
             float2 d[R];
-            nl_c2r_r<R>(F(a.U[l]) + off, true, K, N, g, r.wavx, r.rp.twrf, r.rp.half.twf, d);
+            // the three c2r of a component share one loop body (as in k_row_nl_r)
+#pragma unroll 1
+            for (int t = 0; t < 3; ++t) {
+                const double* src = (t == 0) ? a.U[l] : (t == 1 ? a.DY[l] : a.DZ[l]);
+                nl_c2r_r<R>(F(src) + off, t == 0, K, N, g, r.wavx, r.rp.twrf, r.rp.half.twf, d);
+                const float dzb = (t == 2 && l == 0) ? ubp : 0.f;
+                const float um0 = (t == 0) ? ub : 0.f;  // u' carries the mean ubar only in u_1
 #pragma unroll
-            for (int k1 = 0; k1 < R; ++k1) {
-                const float2 u0 = U(0, k1);
-                U(3, k1) = make_float2(0.f - 0.5f * ((ub + u0.x) * d[k1].x), 0.f - 0.5f * ((ub + u0.y) * d[k1].y));
+                for (int k1 = 0; k1 < R; ++k1) {
+                    const float2 um = U(t, k1);
+                    const float2 c = (t == 0) ? make_float2(0.f, 0.f) : U(3, k1);
+                    U(3, k1) = make_float2(c.x - 0.5f * ((um0 + um.x) * (d[k1].x + dzb)),
+                                           c.y - 0.5f * ((um0 + um.y) * (d[k1].y + dzb)));
+                }
             }
-            nl_c2r_r<R>(F(a.DY[l]) + off, false, K, N, g, r.wavx, r.rp.twrf, r.rp.half.twf, d);
 #pragma unroll
             for (int k1 = 0; k1 < R; ++k1) {
-                const float2 u1 = U(1, k1);
                 float2 c = U(3, k1);
-                c.x = c.x - 0.5f * (u1.x * d[k1].x);
-                c.y = c.y - 0.5f * (u1.y * d[k1].y);
-                U(3, k1) = c;
-            }
-            nl_c2r_r<R>(F(a.DZ[l]) + off, false, K, N, g, r.wavx, r.rp.twrf, r.rp.half.twf, d);
-            const float dzb = (l == 0) ? ubp : 0.f;
-#pragma unroll
-            for (int k1 = 0; k1 < R; ++k1) {
-                const float2 u2 = U(2, k1);
-                float2 c = U(3, k1);
-                c.x = c.x - 0.5f * (u2.x * (d[k1].x + dzb));
-                c.y = c.y - 0.5f * (u2.y * (d[k1].y + dzb));
                 if (a.lamx != nullptr) {
                     const int x = 2 * nl_pair<R>(g, k1);  // physical x of the pair in register k1
                     const float lx0 = (float)__ldg(&a.lamx[x]), lx1 = (float)__ldg(&a.lamx[x + 1]);
