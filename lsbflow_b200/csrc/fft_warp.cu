@@ -1241,58 +1241,64 @@ __global__ void __launch_bounds__(128, (R <= 6 ? NLR_MINB : 3)) k_row_nl_r(NlRow
         const int z = row / r.nyl;
         const long long off = (long long)row * 2 * K;
         const double ub = a.ubar[z], ubp = a.ubarp[z];
+        // the row's 21 transforms as one loop, so that each direction's code is inlined once
+        // (instruction fetch was a top stall with the transforms inlined per call site):
+        // ops 0..2   c2r of u_l into the slots (u_1 + ubar)
+        // ops 3..8   r2c of the fluxes 0.5 u_l u_m for (11, 12, 13, 22, 23, 33)
+        // ops 9..20  per component l: c2r of du_l/dx, du_l/dy, du_l/dz, accumulating
+        //            -0.5 u_m d_m u_l in slot 3, then the r2c of that sum (+ the fringe)
+        // (the FP32 rows and the dynamic-model row pass measured slower in this form)
 #pragma unroll 1
-        for (int l = 0; l < 3; ++l) {
-            double2 t[R];
-            nl_c2r_r<R>(a.U[l] + off, false, K, N, g, r.wavx, r.rp.twr, r.rp.half.tw, t);
-            const double add = (l == 0) ? ub : 0.0;
+        for (int op = 0; op < 21; ++op) {
+            const int cl = (op - 9) >> 2, ct = (op - 9) & 3;  // component and step of ops 9..20
+            double2 v[R];
+            if (op < 3 || (op >= 9 && ct < 3)) {
+                const double* src = (op < 3) ? a.U[op] : (ct == 0 ? a.U[cl] : (ct == 1 ? a.DY[cl] : a.DZ[cl]));
+                nl_c2r_r<R>(src + off, op >= 9 && ct == 0, K, N, g, r.wavx, r.rp.twr, r.rp.half.tw, v);
+                if (op < 3) {
+                    const double add = (op == 0) ? ub : 0.0;
 #pragma unroll
-            for (int k1 = 0; k1 < R; ++k1) U(l, k1) = make_double2(t[k1].x + add, t[k1].y + add);
-        }
-        // fluxes 0.5 u_l u_m for (11, 12, 13, 22, 23, 33)
-#pragma unroll 1
-        for (int p = 0; p < 6; ++p) {
-            const int l = (p < 3) ? 0 : (p < 5 ? 1 : 2);
-            const int m = (p < 3) ? p : (p < 5 ? p - 2 : 2);
-            double2 f[R];
+                    for (int k1 = 0; k1 < R; ++k1) U(op, k1) = make_double2(v[k1].x + add, v[k1].y + add);
+                } else {
+                    const double dzb = (ct == 2 && cl == 0) ? ubp : 0.0;
 #pragma unroll
-            for (int k1 = 0; k1 < R; ++k1) {
-                const double2 ul = U(l, k1), um = U(m, k1);
-                f[k1] = make_double2(0.5 * (ul.x * um.x), 0.5 * (ul.y * um.y));
-            }
-            nl_r2c_r<R>(f, a.H[p] + off, K, g, r.rp.twr, r.rp.half.tw);
-        }
-        // convective terms -0.5 u_m d_m u_l, plus the fringe; the three c2r of a component
-        // share one loop body (a third of the code of three inlined copies)
-#pragma unroll 1
-        for (int l = 0; l < 3; ++l) {
-            double2 d[R];
-#pragma unroll 1
-            for (int t = 0; t < 3; ++t) {
-                const double* src = (t == 0) ? a.U[l] : (t == 1 ? a.DY[l] : a.DZ[l]);
-                nl_c2r_r<R>(src + off, t == 0, K, N, g, r.wavx, r.rp.twr, r.rp.half.tw, d);
-                const double dzb = (t == 2 && l == 0) ? ubp : 0.0;
-#pragma unroll
-                for (int k1 = 0; k1 < R; ++k1) {
-                    const double2 um = U(t, k1);
-                    const double2 c = (t == 0) ? make_double2(0.0, 0.0) : U(3, k1);
-                    U(3, k1) = make_double2(c.x - 0.5 * (um.x * (d[k1].x + dzb)), c.y - 0.5 * (um.y * (d[k1].y + dzb)));
+                    for (int k1 = 0; k1 < R; ++k1) {
+                        const double2 um = U(ct, k1);
+                        const double2 c = (ct == 0) ? make_double2(0.0, 0.0) : U(3, k1);
+                        U(3, k1) = make_double2(c.x - 0.5 * (um.x * (v[k1].x + dzb)),
+                                                c.y - 0.5 * (um.y * (v[k1].y + dzb)));
+                    }
                 }
-            }
-            const double ut = (l == 0) ? ub : 0.0;
+            } else {
+                double* dst;
+                if (op < 9) {
+                    const int p = op - 3;
+                    const int l = (p < 3) ? 0 : (p < 5 ? 1 : 2);
+                    const int m = (p < 3) ? p : (p < 5 ? p - 2 : 2);
 #pragma unroll
-            for (int k1 = 0; k1 < R; ++k1) {
-                double2 c = U(3, k1);
-                if (a.lamx != nullptr) {
-                    const int x = 2 * nl_pair<R>(g, k1);  // physical x of the pair in register k1
-                    const double lx0 = __ldg(&a.lamx[x]), lx1 = __ldg(&a.lamx[x + 1]);
-                    const double2 ul = U(l, k1);
-                    c.x = c.x + lx0 * (ut - ul.x);
-                    c.y = c.y + lx1 * (ut - ul.y);
+                    for (int k1 = 0; k1 < R; ++k1) {
+                        const double2 ul = U(l, k1), um = U(m, k1);
+                        v[k1] = make_double2(0.5 * (ul.x * um.x), 0.5 * (ul.y * um.y));
+                    }
+                    dst = a.H[p];
+                } else {
+                    const double ut = (cl == 0) ? ub : 0.0;
+#pragma unroll
+                    for (int k1 = 0; k1 < R; ++k1) {
+                        double2 c = U(3, k1);
+                        if (a.lamx != nullptr) {
+                            const int x = 2 * nl_pair<R>(g, k1);  // physical x of the pair in register k1
+                            const double lx0 = __ldg(&a.lamx[x]), lx1 = __ldg(&a.lamx[x + 1]);
+                            const double2 ul = U(cl, k1);
+                            c.x = c.x + lx0 * (ut - ul.x);
+                            c.y = c.y + lx1 * (ut - ul.y);
+                        }
+                        v[k1] = c;
+                    }
+                    dst = a.N[cl];
                 }
-                d[k1] = c;
+                nl_r2c_r<R>(v, dst + off, K, g, r.rp.twr, r.rp.half.tw);
             }
-            nl_r2c_r<R>(d, a.N[l] + off, K, g, r.rp.twr, r.rp.half.tw);
         }
     }
 }
