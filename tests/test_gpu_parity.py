@@ -127,10 +127,11 @@ def test_nlterm_production_sizes(nx, ny, nz, layout):
         assert rel(got[l], ref[l]) < TOL_OP, (l, rel(got[l], ref[l]))
 
 
-@pytest.mark.parametrize("nx,ny,nz", [(64, 8, 16), (128, 8, 16), (256, 16, 32), (384, 8, 16)])
+@pytest.mark.parametrize("nx,ny,nz", [(64, 8, 16), (128, 8, 16), (256, 16, 32), (384, 8, 16), (512, 8, 16)])
 def test_nlterm_fringe_full_warp(nx, ny, nz):
-    # unpadded rows of 32 R complex (R = 1, 2, 4, 6) with the fringe term: the
-    # register-resident product kernel, one warp per row
+    # unpadded rows of 32 R complex (R = 1, 2, 4, 6, 8) with the fringe term: the
+    # register-resident product kernel, one warp per row (exchange networks for even R, whose
+    # slot layout the fringe factor is read in)
     st, s = solver(workload("dns64", nx=nx, ny=ny, nz=nz, dealiasflag=0, forcing=1))
     u, v, w = ic.seeded_noise(st, 13, 1e-2)
     ref = O.nlterm_skewsym(st, [u, v, w])
@@ -139,8 +140,10 @@ def test_nlterm_fringe_full_warp(nx, ny, nz):
         assert rel(got[l], ref[l]) < TOL_OP, (l, rel(got[l], ref[l]))
 
 
-@pytest.mark.parametrize("nx,ny,nz", [(128, 32, 64), (256, 64, 128), (64, 48, 16)])
+@pytest.mark.parametrize("nx,ny,nz", [(128, 32, 64), (256, 64, 128), (64, 48, 16), (512, 8, 16), (64, 128, 16)])
 def test_horfft_production_sizes(nx, ny, nz):
+    # x rows of R = 2, 4, 1, 8 and spanwise 16-lane groups of R = 2, 4, 3, 8 (the exchange
+    # networks for even R)
     st, s = solver(workload("les256", nx=nx, ny=ny, nz=nz, sgsflag=0, dealiasflag=0))
     a = rand_phys(st, 21)
     assert rel(s.horfft(a, None, -1), O.horfft_fwd(a, nx, ny)) < TOL_OP
@@ -223,6 +226,16 @@ def test_sgs_steps_match_oracle(model, dealias):
     tol = TOL_SIGMA_STEP if model == 2 else TOL_STEP
     for key, ref in (("uf", ost.uf), ("vf", ost.vf), ("wf", ost.wf), ("pf", ost.pf)):
         assert rel(got[key], ref) < tol, (key, rel(got[key], ref))
+
+
+@pytest.mark.parametrize("nx", [128, 256, 512])
+def test_dynamic_fused_rows_match_oracle(nx):
+    # the dynamic model's first and last pointwise passes fused into the row transforms
+    # (full-warp rows of R = 2, 4, 8) over whole steps against the oracle
+    cfg = workload("les256", nx=nx, ny=8, nz=16)
+    st, ost, got = run_both(cfg, 4, amp=2e-2, zder="dense")
+    for key, ref in (("uf", ost.uf), ("vf", ost.vf), ("wf", ost.wf), ("pf", ost.pf)):
+        assert rel(got[key], ref) < TOL_STEP, (key, rel(got[key], ref))
 
 
 @pytest.mark.parametrize("model", [0, 1, 2, 3])
