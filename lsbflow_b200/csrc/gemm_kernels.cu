@@ -183,6 +183,45 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
     auto epilogue = [&](auto kind) {
         constexpr int E = decltype(kind)::value;
         constexpr bool RD = (E == EPI_AXPBY || E == EPI_POISSON_RHS);
+        if constexpr (E == EPI_NLDIV) {
+            // the thread's two columns (cb, cb + 1) are the real and imaginary parts of one
+            // mode: N_l -= i kx h_l1 + i ky h_l2 + d h_l3/dz in the order of k_nl_div_xy
+            if (cb >= g.C) return;
+            double* __restrict__ Nl = g.nd_N[f];
+            const double* __restrict__ hx = g.nd_hx[f];
+            const double* __restrict__ hy = g.nd_hy[f];
+            const double wx = g.wavx[(int)((unsigned)cb % (unsigned)g.nx)];
+            const double wy = g.wavy[(int)((unsigned)cb / (unsigned)g.nx)];
+#pragma unroll
+            for (int t = 0; t < MT; ++t) {
+                double2 nv[2], xv[2], yv[2];
+#pragma unroll
+                for (int hh = 0; hh < 2; ++hh) {
+                    const int r = t * 16 + hh * 8 + gq;
+                    nv[hh] = xv[hh] = yv[hh] = make_double2(0.0, 0.0);
+                    if (r < g.M) {
+                        const long long o = (long long)(r + g.roff) * g.C + cb;
+                        nv[hh] = *reinterpret_cast<const double2*>(Nl + o);
+                        xv[hh] = *reinterpret_cast<const double2*>(hx + o);
+                        yv[hh] = *reinterpret_cast<const double2*>(hy + o);
+                    }
+                }
+#pragma unroll
+                for (int hh = 0; hh < 2; ++hh) {
+                    const int r = t * 16 + hh * 8 + gq;
+                    if (r >= g.M) continue;
+                    double nr = nv[hh].x, ni = nv[hh].y;
+                    nr = nr - (-wx * xv[hh].y);
+                    ni = ni - (wx * xv[hh].x);
+                    nr = nr - (-wy * yv[hh].y);
+                    ni = ni - (wy * yv[hh].x);
+                    nr = nr - acc[t][2 * hh];
+                    ni = ni - acc[t][2 * hh + 1];
+                    *reinterpret_cast<double2*>(Nl + (long long)(r + g.roff) * g.C + cb) = make_double2(nr, ni);
+                }
+            }
+            return;
+        }
 #pragma unroll
         for (int t = 0; t < MT; ++t) {
             // the field values this tile's epilogue reads, loaded together before its stores
@@ -224,6 +263,7 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
         case EPI_AXPBY: epilogue(std::integral_constant<int, EPI_AXPBY>{}); break;
         case EPI_HELM_SCALE: epilogue(std::integral_constant<int, EPI_HELM_SCALE>{}); break;
         case EPI_POISSON_RHS: epilogue(std::integral_constant<int, EPI_POISSON_RHS>{}); break;
+        case EPI_NLDIV: epilogue(std::integral_constant<int, EPI_NLDIV>{}); break;
         default: epilogue(std::integral_constant<int, EPI_LIFT_ADD>{}); break;
     }
 }

@@ -193,6 +193,8 @@ enum GemmEpi {
     EPI_HELM_SCALE = 2,     // out = acc / (lam[r] - w2(c) - sigma)
     EPI_POISSON_RHS = 4,    // out = -acc - w2(c)*aux
     EPI_LIFT_ADD = 5,       // out = acc + hb[row]*bcb(c) + ht[row]*bct(c)   (bcb may be null)
+    EPI_NLDIV = 6,          // acc = d h_l3/dz is not stored: N_l -= d h_l1/dx + d h_l2/dy + acc
+                            // (field f = l; nd_N, nd_hx, nd_hy; the elementwise divergence pass)
 };
 struct GemmArgs {
     const double* A;        // device, [Mp][Kp] zero padded
@@ -222,6 +224,10 @@ struct GemmArgs {
     const double* inf[4];
     double* outf[4];
     int nw;                 // CTA width in warps, 4..8, set by the handle's schedule; 0: wave model
+    // EPI_NLDIV: per field l, the nonlinear term updated in place and the fluxes h_l1, h_l2
+    double* nd_N[3];
+    const double* nd_hx[3];
+    const double* nd_hy[3];
 };
 void launch_gemm(const GemmArgs& g, cudaStream_t s);
 void launch_spanwise_stats(const double* ph, double* mean, double* rms, int nf, int nx, int ny, int nzp, long long P,

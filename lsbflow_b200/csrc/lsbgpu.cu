@@ -557,6 +557,17 @@ void nlterm(lsb_handle* h, const double* uin, double* Nout) {
     gz.out = gz.outf[0];
     gz.nfields = 3;
     gz.epi = EPI_STORE;
+    if (h->cfg.precision == 0) {
+        // FP64: the contraction's epilogue applies the whole divergence (d h_l3/dz is not stored)
+        gz.epi = EPI_NLDIV;
+        for (int l = 0; l < 3; ++l) {
+            gz.nd_N[l] = nd.N[l];
+            gz.nd_hx[l] = nd.hx[l];
+            gz.nd_hy[l] = nd.hy[l];
+        }
+        contract(h, gz, h->oz_dz1);
+        return;
+    }
     contract(h, gz, h->oz_dz1);
     launch_nl_div_xy(nd, h->stream);
 }
