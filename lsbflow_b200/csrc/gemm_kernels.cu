@@ -222,6 +222,48 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
             }
             return;
         }
+        if constexpr (E == EPI_PRESSURE) {
+            // the pressure and projection of k_pressure_project, for the thread's mode
+            if (cb >= g.C) return;
+            double* __restrict__ pu = g.pp_u;
+            double* __restrict__ pv = g.pp_v;
+            double* __restrict__ pp = g.pp_p;
+            const double* __restrict__ pdiv = g.pp_div;
+            const double wx = g.wavx[(int)((unsigned)cb % (unsigned)g.nx)];
+            const double wy = g.wavy[(int)((unsigned)cb / (unsigned)g.nx)];
+            const double w2 = wx * wx + wy * wy;
+            const double dt = g.pp_dt, bdfv = g.pp_bdfv;
+            const double dtb = dt * bdfv;
+#pragma unroll
+            for (int t = 0; t < MT; ++t) {
+                double2 dv[2], uv[2], vv[2];
+#pragma unroll
+                for (int hh = 0; hh < 2; ++hh) {
+                    const int r = t * 16 + hh * 8 + gq;
+                    dv[hh] = uv[hh] = vv[hh] = make_double2(0.0, 0.0);
+                    if (r < g.M) {
+                        const long long o = (long long)(r + g.roff) * g.C + cb;
+                        dv[hh] = *reinterpret_cast<const double2*>(pdiv + o);
+                        uv[hh] = *reinterpret_cast<const double2*>(pu + o);
+                        vv[hh] = *reinterpret_cast<const double2*>(pv + o);
+                    }
+                }
+#pragma unroll
+                for (int hh = 0; hh < 2; ++hh) {
+                    const int r = t * 16 + hh * 8 + gq;
+                    if (r >= g.M) continue;
+                    const long long o = (long long)(r + g.roff) * g.C + cb;
+                    const double pr = (w2 == 0.0) ? 0.0 : -(acc[t][2 * hh] + dv[hh].x) / (w2 * dt * bdfv);
+                    const double pi = (w2 == 0.0) ? 0.0 : -(acc[t][2 * hh + 1] + dv[hh].y) / (w2 * dt * bdfv);
+                    *reinterpret_cast<double2*>(pp + o) = make_double2(pr, pi);
+                    *reinterpret_cast<double2*>(pu + o) =
+                        make_double2(uv[hh].x - dtb * (-wx * pi), uv[hh].y - dtb * (wx * pr));
+                    *reinterpret_cast<double2*>(pv + o) =
+                        make_double2(vv[hh].x - dtb * (-wy * pi), vv[hh].y - dtb * (wy * pr));
+                }
+            }
+            return;
+        }
 #pragma unroll
         for (int t = 0; t < MT; ++t) {
             // the field values this tile's epilogue reads, loaded together before its stores
@@ -264,6 +306,7 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
         case EPI_HELM_SCALE: epilogue(std::integral_constant<int, EPI_HELM_SCALE>{}); break;
         case EPI_POISSON_RHS: epilogue(std::integral_constant<int, EPI_POISSON_RHS>{}); break;
         case EPI_NLDIV: epilogue(std::integral_constant<int, EPI_NLDIV>{}); break;
+        case EPI_PRESSURE: epilogue(std::integral_constant<int, EPI_PRESSURE>{}); break;
         default: epilogue(std::integral_constant<int, EPI_LIFT_ADD>{}); break;
     }
 }

@@ -195,6 +195,8 @@ enum GemmEpi {
     EPI_LIFT_ADD = 5,       // out = acc + hb[row]*bcb(c) + ht[row]*bct(c)   (bcb may be null)
     EPI_NLDIV = 6,          // acc = d h_l3/dz is not stored: N_l -= d h_l1/dx + d h_l2/dy + acc
                             // (field f = l; nd_N, nd_hx, nd_hy; the elementwise divergence pass)
+    EPI_PRESSURE = 7,       // acc = Dw is not stored: pressure phi = -(acc + div)/(k^2 dt bdfv)
+                            // into pp_p, u -= dt bdfv dphi/dx, v -= dt bdfv dphi/dy (one field)
 };
 struct GemmArgs {
     const double* A;        // device, [Mp][Kp] zero padded
@@ -228,6 +230,12 @@ struct GemmArgs {
     double* nd_N[3];
     const double* nd_hx[3];
     const double* nd_hy[3];
+    // EPI_PRESSURE: the velocity updated in place, the pressure written, the divergence read
+    double* pp_u;
+    double* pp_v;
+    double* pp_p;
+    const double* pp_div;
+    double pp_dt, pp_bdfv;
 };
 void launch_gemm(const GemmArgs& g, cudaStream_t s);
 void launch_spanwise_stats(const double* ph, double* mean, double* rms, int nf, int nx, int ny, int nzp, long long P,

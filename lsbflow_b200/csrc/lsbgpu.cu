@@ -811,15 +811,25 @@ void step_one(lsb_handle* h) {
         // 8-9. Poisson solve for w^{n+1}
         helmholtz(h, h->rhs, h->vel + 2 * S, 1, 0.0, h->bcp, false);
     }
-    // 10. Dw^{n+1} (the eigenbasis temporary is free again)
+    // 10-11. Dw^{n+1}, the pressure phi = -(Dw + div)/(k^2 dt bdfv) into pn (then swapped into
+    // p) and the projection of u, v: one contraction whose epilogue does the last two
     {
         TimerScope ts(h, "pressure");
-        zgemm1(h, h->m_dz1, h->vel + 2 * S, h->T, 1);
+        GemmArgs g = gemm_base(h, h->m_dz1);
+        g.in = h->vel + 2 * S;
+        g.out = h->T;  // not written
+        g.nfields = 1;
+        g.epi = EPI_PRESSURE;
+        g.pp_u = h->vel;
+        g.pp_v = h->vel + S;
+        g.pp_p = h->pn;
+        g.pp_div = h->divf;
+        g.pp_dt = dt;
+        g.pp_bdfv = h->bdfv;
+        launch_gemm(g, st);
     }
-    // 11. pressure phi = -(Dw + div)/(k^2 dt bdfv) into pn (then swapped into p) and the
-    // projection of u, v in one pass; norm; ifrz
+    // norm; ifrz
     TimerScope ts(h, "projection_norm");
-    launch_pressure_project(h->vel, h->vel + S, h->pn, h->T, h->divf, h->wavx, h->wavy, d.nx, S, C, dt, h->bdfv, st);
     std::swap(h->p, h->pn);
     launch_norm(h->vel, h->vel + S, h->vel + 2 * S, d.nx, d.ny, d.nzp, c.ifrz, st);
     // 12. time
