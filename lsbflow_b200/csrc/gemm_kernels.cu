@@ -223,7 +223,9 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
             return;
         }
         if constexpr (E == EPI_PRESSURE) {
-            // the pressure and projection of k_pressure_project, for the thread's mode
+            // the pressure phi = -(Dw + div)/(k^2 dt bdfv) (0 at k = 0; src/navierstokes.f90:
+            // 1466-1476) and the projection u -= dt bdfv dphi/dx, v -= dt bdfv dphi/dy
+            // (:1478-1488), for the thread's mode
             if (cb >= g.C) return;
             double* __restrict__ pu = g.pp_u;
             double* __restrict__ pv = g.pp_v;

@@ -69,9 +69,6 @@ void launch_dxy(const double* in, double* out, const double* wavx, const double*
 void launch_lapl_xy(const double* u, double* d2, const double* wavx, const double* wavy, int nx, long long S,
                     long long C, cudaStream_t s);
 void launch_nl_div_xy(const NlDivArgs& a, cudaStream_t s);
-void launch_pressure_project(double* u, double* v, double* p, const double* dw, const double* div, const double* wavx,
-                             const double* wavy, int nx, long long S, long long C, double dt, double bdfv,
-                             cudaStream_t s);
 void launch_norm(double* f0, double* f1, double* f2, int nx, int ny, int nzp, int ifrz, cudaStream_t s);
 void launch_axpby(double* y, const double* x, double a, double b, long long n, cudaStream_t s);
 void launch_tavg_add(double* a, const double* q, double iomod, long long n, cudaStream_t s);

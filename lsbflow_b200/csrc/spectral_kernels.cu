@@ -182,29 +182,6 @@ __global__ void k_nl_div_xy(NlDivArgs a) {
     }
 }
 
-// pressure phi = -(Dw + div)/(k^2 dt bdfv) (0 at k = 0; src/navierstokes.f90:1466-1476) into
-// p, then u -= dt*bdfv*dfdx(phi), v -= dt*bdfv*dfdy(phi) (:1478-1488), in one pass
-__global__ void k_pressure_project(double* __restrict__ u, double* __restrict__ v, double* __restrict__ p,
-                                   const double* __restrict__ dw, const double* __restrict__ div,
-                                   const double* __restrict__ wavx, const double* __restrict__ wavy, int nx,
-                                   long long S, long long C, double dt, double bdfv) {
-    const long long n2 = S / 2;
-    const double dtb = dt * bdfv;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n2; e += (long long)gridDim.x * blockDim.x) {
-        int i, j;
-        ij_of(e % (C / 2), nx, i, j);
-        const double wx = wavx[i], wy = wavy[j];
-        const double w2 = wx * wx + wy * wy;
-        const double pr = (w2 == 0.0) ? 0.0 : -(dw[2 * e] + div[2 * e]) / (w2 * dt * bdfv);
-        const double pi = (w2 == 0.0) ? 0.0 : -(dw[2 * e + 1] + div[2 * e + 1]) / (w2 * dt * bdfv);
-        p[2 * e] = pr;
-        p[2 * e + 1] = pi;
-        u[2 * e] = u[2 * e] - dtb * (-wx * pi);
-        u[2 * e + 1] = u[2 * e + 1] - dtb * (wx * pr);
-        v[2 * e] = v[2 * e] - dtb * (-wy * pi);
-        v[2 * e + 1] = v[2 * e + 1] - dtb * (wy * pr);
-    }
-}
 
 // norm (src/horfft.f90:153-224) on 3 fields + the ifrz mean removal (src/navierstokes.f90:53-59)
 __global__ void k_norm(double* f0, double* f1, double* f2, int nx, int ny, int nzp, int ifrz) {
@@ -291,11 +268,6 @@ void launch_lapl_xy(const double* u, double* d2, const double* wavx, const doubl
     { lsb::note_launch(); k_lapl_xy<<<nblk(S), 256, 0, s>>>(u, d2, wavx, wavy, nx, S, C); }
 }
 void launch_nl_div_xy(const NlDivArgs& a, cudaStream_t s) { lsb::note_launch(); k_nl_div_xy<<<nblk(3 * a.S / 2), 256, 0, s>>>(a); }
-void launch_pressure_project(double* u, double* v, double* p, const double* dw, const double* div, const double* wavx,
-                             const double* wavy, int nx, long long S, long long C, double dt, double bdfv,
-                             cudaStream_t s) {
-    { lsb::note_launch(); k_pressure_project<<<nblk(S / 2), 256, 0, s>>>(u, v, p, dw, div, wavx, wavy, nx, S, C, dt, bdfv); }
-}
 void launch_norm(double* f0, double* f1, double* f2, int nx, int ny, int nzp, int ifrz, cudaStream_t s) {
     { lsb::note_launch(); k_norm<<<dim3(nzp, 3), 128, 0, s>>>(f0, f1, f2, nx, ny, nzp, ifrz); }
 }
