@@ -626,7 +626,8 @@ __global__ void __launch_bounds__(256) k_row_c2r_w(RowJobList jobs, RowArgs a) {
         __syncwarp();
 #pragma unroll
         for (int k1 = 0; k1 < R; ++k1) {
-            const int n = XN ? xslot<R, 32>(g, k1) : R * g + k1;
+            int n = R * g + k1;
+            if constexpr (XN) n = xslot<R, 32>(g, k1);
             X[xsw<V>(n)] = CT<V>::make(sc * v[k1].x + m, sc * v[k1].y + m);
         }
         __syncwarp();

@@ -185,7 +185,8 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
         constexpr bool RD = (E == EPI_AXPBY || E == EPI_POISSON_RHS);
         if constexpr (E == EPI_NLDIV) {
             // the thread's two columns (cb, cb + 1) are the real and imaginary parts of one
-            // mode: N_l -= i kx h_l1 + i ky h_l2 + d h_l3/dz in the order of k_nl_div_xy
+            // mode: N_l -= i kx h_l1 + i ky h_l2 + d h_l3/dz (src/navierstokes.f90:789-795),
+            // the real part first taking -(-kx Im h_l1), then -(-ky Im h_l2), then Re d h_l3/dz
             if (cb >= g.C) return;
             double* __restrict__ Nl = g.nd_N[f];
             const double* __restrict__ hx = g.nd_hx[f];
@@ -220,9 +221,7 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
                     *reinterpret_cast<double2*>(Nl + (long long)(r + g.roff) * g.C + cb) = make_double2(nr, ni);
                 }
             }
-            return;
-        }
-        if constexpr (E == EPI_PRESSURE) {
+        } else if constexpr (E == EPI_PRESSURE) {
             // the pressure phi = -(Dw + div)/(k^2 dt bdfv) (0 at k = 0; src/navierstokes.f90:
             // 1466-1476) and the projection u -= dt bdfv dphi/dx, v -= dt bdfv dphi/dy
             // (:1478-1488), for the thread's mode
@@ -264,8 +263,7 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
                         make_double2(vv[hh].x - dtb * (-wy * pi), vv[hh].y - dtb * (wy * pr));
                 }
             }
-            return;
-        }
+        } else {
 #pragma unroll
         for (int t = 0; t < MT; ++t) {
             // the field values this tile's epilogue reads, loaded together before its stores
@@ -300,6 +298,7 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
                 }
                 out[(long long)(r + g.roff) * g.C + c] = v;
             }
+        }
         }
     };
     switch (g.epi) {

@@ -48,15 +48,12 @@ struct BcArgs {
     long long C;
 };
 
+// the nonlinear term's divergence operands: N_l and the fluxes h_l1, h_l2 (d h_l3/dz is
+// formed and subtracted by the contraction's EPI_NLDIV epilogue)
 struct NlDivArgs {
     double* N[3];
     const double* hx[3];
     const double* hy[3];
-    const double* hz[3];  // d h_l3 / dz, already formed (subtracted after the x and y terms)
-    const double* wavx;
-    const double* wavy;
-    int nx;
-    long long S, C;
 };
 
 void launch_specfilter(const SpecFilterArgs& a, cudaStream_t s);
@@ -68,7 +65,6 @@ void launch_dxy(const double* in, double* out, const double* wavx, const double*
                 long long C, int mode, cudaStream_t s);
 void launch_lapl_xy(const double* u, double* d2, const double* wavx, const double* wavy, int nx, long long S,
                     long long C, cudaStream_t s);
-void launch_nl_div_xy(const NlDivArgs& a, cudaStream_t s);
 void launch_norm(double* f0, double* f1, double* f2, int nx, int ny, int nzp, int ifrz, cudaStream_t s);
 void launch_axpby(double* y, const double* x, double a, double b, long long n, cudaStream_t s);
 void launch_tavg_add(double* a, const double* q, double iomod, long long n, cudaStream_t s);

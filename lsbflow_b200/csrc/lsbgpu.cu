@@ -539,37 +539,23 @@ void nlterm(lsb_handle* h, const double* uin, double* Nout) {
         nd.hx[l] = full9 ? h->sgs.H9 + (l * 3 + 0) * S : Hsym(h, l, 0);
         nd.hy[l] = full9 ? h->sgs.H9 + (l * 3 + 1) * S : Hsym(h, l, 1);
     }
-    nd.wavx = h->wavx;
-    nd.wavy = h->wavy;
-    nd.nx = d.nx;
-    nd.S = S;
-    nd.C = d.C();
     TimerScope ts(h, "nl_divergence");
-    // d h_l3 / dz for the three components in one launch, into the du/dz buffer (free by
-    // now); the elementwise pass then subtracts all three derivatives from N_l
+    // d h_l3 / dz for the three components in one FP64 contraction whose epilogue applies the
+    // whole divergence (d h_l3/dz is not stored).  The mixed form uses it too: its int8
+    // contraction followed by an elementwise divergence pass took longer (73 + 44 us against
+    // 111 us at 256x64x129), and this derivative is then exact
     GemmArgs gz = gemm_base(h, h->m_dz1);
-    for (int l = 0; l < 3; ++l) {
-        gz.inf[l] = full9 ? h->sgs.H9 + (l * 3 + 2) * S : Hsym(h, l, 2);
-        gz.outf[l] = h->dz + l * S;
-        nd.hz[l] = h->dz + l * S;
-    }
+    for (int l = 0; l < 3; ++l) gz.inf[l] = full9 ? h->sgs.H9 + (l * 3 + 2) * S : Hsym(h, l, 2);
     gz.in = gz.inf[0];
-    gz.out = gz.outf[0];
+    gz.out = h->dz;  // not written
     gz.nfields = 3;
-    gz.epi = EPI_STORE;
-    if (h->cfg.precision == 0) {
-        // FP64: the contraction's epilogue applies the whole divergence (d h_l3/dz is not stored)
-        gz.epi = EPI_NLDIV;
-        for (int l = 0; l < 3; ++l) {
-            gz.nd_N[l] = nd.N[l];
-            gz.nd_hx[l] = nd.hx[l];
-            gz.nd_hy[l] = nd.hy[l];
-        }
-        contract(h, gz, h->oz_dz1);
-        return;
+    gz.epi = EPI_NLDIV;
+    for (int l = 0; l < 3; ++l) {
+        gz.nd_N[l] = nd.N[l];
+        gz.nd_hx[l] = nd.hx[l];
+        gz.nd_hy[l] = nd.hy[l];
     }
-    contract(h, gz, h->oz_dz1);
-    launch_nl_div_xy(nd, h->stream);
+    launch_gemm(gz, h->stream);
 }
 
 void coefficients(lsb_handle* h) {

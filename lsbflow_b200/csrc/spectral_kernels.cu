@@ -159,30 +159,6 @@ __global__ void k_lapl_xy(const double* __restrict__ u, double* __restrict__ d2,
     }
 }
 
-// N_l = (N_l - dfdx(h_l1)) - dfdy(h_l2)   (src/navierstokes.f90:789-795, x and y parts)
-__global__ void k_nl_div_xy(NlDivArgs a) {
-    const long long n2 = a.S / 2;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < 3 * n2; e += (long long)gridDim.x * blockDim.x) {
-        const int l = (int)(e / n2);
-        const long long ce = e % n2;
-        int i, j;
-        ij_of(ce % (a.C / 2), a.nx, i, j);
-        const double wx = a.wavx[i], wy = a.wavy[j];
-        const double* hx = a.hx[l];
-        const double* hy = a.hy[l];
-        double nr = a.N[l][2 * ce], ni = a.N[l][2 * ce + 1];
-        nr = nr - (-wx * hx[2 * ce + 1]);
-        ni = ni - (wx * hx[2 * ce]);
-        nr = nr - (-wy * hy[2 * ce + 1]);
-        ni = ni - (wy * hy[2 * ce]);
-        nr = nr - a.hz[l][2 * ce];
-        ni = ni - a.hz[l][2 * ce + 1];
-        a.N[l][2 * ce] = nr;
-        a.N[l][2 * ce + 1] = ni;
-    }
-}
-
-
 // norm (src/horfft.f90:153-224) on 3 fields + the ifrz mean removal (src/navierstokes.f90:53-59)
 __global__ void k_norm(double* f0, double* f1, double* f2, int nx, int ny, int nzp, int ifrz) {
     const int k = blockIdx.x;
@@ -267,7 +243,6 @@ void launch_lapl_xy(const double* u, double* d2, const double* wavx, const doubl
                     long long C, cudaStream_t s) {
     { lsb::note_launch(); k_lapl_xy<<<nblk(S), 256, 0, s>>>(u, d2, wavx, wavy, nx, S, C); }
 }
-void launch_nl_div_xy(const NlDivArgs& a, cudaStream_t s) { lsb::note_launch(); k_nl_div_xy<<<nblk(3 * a.S / 2), 256, 0, s>>>(a); }
 void launch_norm(double* f0, double* f1, double* f2, int nx, int ny, int nzp, int ifrz, cudaStream_t s) {
     { lsb::note_launch(); k_norm<<<dim3(nzp, 3), 128, 0, s>>>(f0, f1, f2, nx, ny, nzp, ifrz); }
 }
