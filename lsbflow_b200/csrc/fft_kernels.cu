@@ -403,7 +403,6 @@ __device__ double2* rows_c2r(double2* X, double2* Z, int L, const RealPlan& rp, 
 // line l is then made by r2c_mode().
 template <bool WIDE>
 __device__ double2* rows_r2c(double2* Z, double2* X, int L, const RealPlan& rp, int tid, int nthr) {
-    const int N = rp.nr / 2;
     const bool inZ = fft_batch<-1, WIDE>(Z, X, L, rp.half.ls, rp.half, tid, nthr);
     return inZ ? Z : X;
 }

@@ -730,6 +730,7 @@ __global__ void __launch_bounds__(128) k_row_c2r_dyn(DynRowArgs a) {
 #pragma unroll 1
         for (int l = 0; l < 3; ++l) {
             c2r(l, v);
+            if (l == 0 && a.uprime != nullptr) store(a.uprime, v);
             const S m = (l == 0) ? (S)(a.ubar[z] * 1.0) : (S)0;
 #pragma unroll
             for (int k1 = 0; k1 < R; ++k1) v[k1] = CT<V>::make(v[k1].x + m, v[k1].y + m);

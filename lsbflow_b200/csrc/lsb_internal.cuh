@@ -139,6 +139,7 @@ struct DynRowArgs {
     const double* ydy[3];  // of du_l/dy
     const double* ydz[3];  // of du_l/dz
     double* u[3];          // physical u_l (u_1 + ubar)
+    double* uprime;        // or null: u_1 without the mean as well (the mixed form's forcing)
     double* sij[6];        // S_ij for (11, 12, 13, 22, 23, 33)
     double* lij[6];        // delta^2 |S| S_ij
     const double* ubar;    // [nzp], added to u_1

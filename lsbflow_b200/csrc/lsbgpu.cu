@@ -494,6 +494,8 @@ void nlterm(lsb_handle* h, const double* uin, double* Nout) {
                 da.ubar = h->ubar;
                 da.ubarp = h->ubarp;
                 da.delta = h->sgs.delta;
+                // the mixed form's forcing reads an FP32 u' without the mean (scratch field 21)
+                if (f32 && dealias && h->cfg.forcing == 1) da.uprime = PH(21);
                 YPassArgs ya = ypass(h, false, d.nzp);
                 ya.f32 = f32;
                 launch_yinv(yj, ya, h->stream);
@@ -514,11 +516,12 @@ void nlterm(lsb_handle* h, const double* uin, double* Nout) {
         if (forcing) {
             TimerScope ts(h, "forcing");
             if (f32) {
-                // lambda (ubar - u) = -lambda u' from an FP32 u' without the mean (no cancellation)
+                // lambda (ubar - u) = -lambda u' from an FP32 u' without the mean (no cancellation;
+                // the dynamic model's fused row pass has written it already)
                 double* up = PH(21);
                 const double* sp1[1] = {uin};
                 double* pp1[1] = {up};
-                spec_to_phys(h, sp1, pp1, 1, d.nzp, nullptr, nullptr, true);
+                if (!dynfuse) spec_to_phys(h, sp1, pp1, 1, d.nzp, nullptr, nullptr, true);
                 fin[0] = up;
                 fmean[0] = nullptr;
             }

@@ -68,8 +68,8 @@ def test_mixed_les256_within_1e6():
     ref = run(cfg, 100, seed=1000, amp=5e-3)
     got = run(cfg.replace(precision=1), 100, seed=1000, amp=5e-3)
     assert rel(vec(got), vec(ref)) < TOL_MIXED
-    for k in ("uf", "vf", "wf"):
-        assert rel(got[k], ref[k]) < 2 * TOL_MIXED, (k, rel(got[k], ref[k]))
+    for k in ("uf", "vf", "wf"):  # each component within 1e-6 (measured: 1.5e-7, 8.0e-7, 1.3e-7)
+        assert rel(got[k], ref[k]) < TOL_MIXED, (k, rel(got[k], ref[k]))
 
 
 def test_mixed_dns64_padded_rows_in_fp64():
