@@ -945,7 +945,7 @@ __global__ void __launch_bounds__(256) k_row_r2c_s(RowJobList jobs, RowArgs a) {
 // in the exchange network's slot order and transforms as k_row_r2c_s does.  The six stress
 // fields never go to HBM.
 template <int R, class V>
-__global__ void __launch_bounds__(256) k_row_r2c_tau(TauRowArgs a) {
+__global__ void __launch_bounds__(128, 5) k_row_r2c_tau(TauRowArgs a) {
     using S = typename CT<V>::S;
     const RowArgs& r = a.r;
     constexpr int N = 32 * R, LS = N + 8;
@@ -956,7 +956,7 @@ __global__ void __launch_bounds__(256) k_row_r2c_tau(TauRowArgs a) {
     V* Z = reinterpret_cast<V*>(rsm_raw) + warp * LS;
     const int K = r.kxc;
     const int nrows = r.nyl * r.nzp;
-    const int gw = blockIdx.x * 8 + warp, TW = gridDim.x * 8;
+    const int gw = blockIdx.x * 4 + warp, TW = gridDim.x * 4;  // 4 warps per block
     const int src = (32 - g) & 31;
     const S h = (S)0.5;
     const S cmax = (S)(0.2 * 0.2);
@@ -1718,15 +1718,16 @@ void dynlaunch(const DynRowArgs& a, cudaStream_t s) {
 namespace {
 template <int R>
 void taulaunch(const TauRowArgs& a, cudaStream_t s) {
-    const size_t sm = (size_t)8 * (32 * R + 8) * (a.r.f32 ? sizeof(float2) : sizeof(double2));
+    // 4-warp blocks: at ~100 registers, 5 blocks (20 warps) fit an SM where 8-warp blocks fit 2
+    const size_t sm = (size_t)4 * (32 * R + 8) * (a.r.f32 ? sizeof(float2) : sizeof(double2));
     const void* k = a.r.f32 ? (const void*)k_row_r2c_tau<R, float2> : (const void*)k_row_r2c_tau<R, double2>;
     if (!allow_smem(k, sm)) throw std::runtime_error("dynamic-model stress row pass: shared memory refused");
     const int nrows = a.r.nyl * a.r.nzp;
-    long long blocks = (long long)resident_blocks(k, 256, sm) * sm_count(), need = (nrows + 7) / 8;
+    long long blocks = (long long)resident_blocks(k, 128, sm) * sm_count(), need = (nrows + 3) / 4;
     if (blocks > need) blocks = need > 0 ? need : 1;
     lsb::note_launch();
-    if (a.r.f32) k_row_r2c_tau<R, float2><<<(int)blocks, 256, sm, s>>>(a);
-    else k_row_r2c_tau<R, double2><<<(int)blocks, 256, sm, s>>>(a);
+    if (a.r.f32) k_row_r2c_tau<R, float2><<<(int)blocks, 128, sm, s>>>(a);
+    else k_row_r2c_tau<R, double2><<<(int)blocks, 128, sm, s>>>(a);
 }
 }  // namespace
 
