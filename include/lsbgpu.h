@@ -148,7 +148,9 @@ int lsb_graphs(lsb_handle* h, int enable);
  * order of a sum. */
 typedef struct {
     int gemm_warps;      /* FP64 z contractions: warps (8 columns each) per CTA, 4..8;
-                            0 = the wave-quantization model */
+                            0 = the wave-quantization model.  The Helmholtz / Poisson
+                            solves run as one fused launch at 0, 4 and 6, as their two
+                            contractions at 5, 7 and 8 */
     int filter_zchunks;  /* 3-point SGS test filter: z chunks a block column is split into,
                             1..(nzp+3)/4; 0 = the waves x planes-per-block model */
     int y_staging;       /* FP64 spanwise passes: tiles staged by cp.async (1) or by TMA tile

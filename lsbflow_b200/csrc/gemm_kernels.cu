@@ -53,16 +53,28 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // chunk; the lifted right-hand side of the non-homogeneous solve is formed from the raw
 // input as the B fragments are read (the lane's column is fixed, the row factors sit in
 // shared memory), so the lifted contractions stream like the plain ones.
+//
+// Odd Chebyshev sizes (nzp = 2^n + 1) leave one row and one column past a multiple of 16.
+// The row (M = 16 MT + 1) is not a 16-row tile of mostly zeros: each lane accumulates it on
+// the FP64 pipe from the B values it already holds (its k subset of its fragment column),
+// the four lanes of a column are summed at the end, and the epilogue stores it as one more
+// tile.  The column (K = 16 (chunks - 1) + 1, no lift) is not a chunk of mostly zeros: it
+// is a rank-1 update acc += A[:, K-1] B[K-1, :] after the last chunk.  Both belong to the
+// EDGE instantiations (M = 16 MT + 1); the others compile without them.
 constexpr int GSTAGES = 3;
 
-template <int MT, int NW>
+template <int MT, int NW, bool EDGE>
 __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
     constexpr int NT = NW * 32, GBN = NW * 8, LDB_S = GBN + 4;  // GBN + 4 = 4 or 12 mod 16: conflict-free
+    constexpr int NTL = MT + (EDGE ? 1 : 0);                     // accumulator tiles (+ the edge row)
+    constexpr int AR = MT * 16 + (EDGE ? 1 : 0), ER = NTL * 16;  // A rows staged, epilogue row stride
     extern __shared__ double gsm[];
-    double (*As)[MT * 16][LDA_S] = reinterpret_cast<double (*)[MT * 16][LDA_S]>(gsm);
-    double (*Bs)[GBK][LDB_S] = reinterpret_cast<double (*)[GBK][LDB_S]>(gsm + GSTAGES * MT * 16 * LDA_S);
-    double* lrow = gsm + GSTAGES * (MT * 16 * LDA_S + GBK * LDB_S);  // [4][Kp]: d2hb, hb, d2ht, ht
-    double* erow = lrow + 4 * g.Kp;  // [2][MT * 16]: the epilogue's row factors (lam, or hb and ht)
+    double (*As)[AR][LDA_S] = reinterpret_cast<double (*)[AR][LDA_S]>(gsm);
+    double (*Bs)[GBK][LDB_S] = reinterpret_cast<double (*)[GBK][LDB_S]>(gsm + GSTAGES * AR * LDA_S);
+    double* lrow = gsm + GSTAGES * (AR * LDA_S + GBK * LDB_S);  // [4][Kp]: d2hb, hb, d2ht, ht
+    double* erow = lrow + 4 * g.Kp;  // [2][ER]: the epilogue's row factors (lam, or hb and ht)
+    double* kcol = erow + 2 * ER;    // [AR][2]: A[r][K-1], A[r][K] of the rank-1 update
+    double* krow = kcol + 2 * AR;    // [GBN]: B[K-1][c0 ..] of the rank-1 update
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int gq = lane >> 2, tq = lane & 3;
     const int f = blockIdx.y;
@@ -71,9 +83,15 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
     const double* bcb = g.bcb ? g.bcb + f * g.bc_fstride : nullptr;
     const double* bct = g.bct ? g.bct + f * g.bc_fstride : nullptr;
     const bool lift = (g.epi != 5) && (bcb != nullptr);
-    double acc[MT][4];
+    const int nchunks = g.Kp / GBK;
+    const bool edge_k = EDGE && !lift && nchunks > 1 && g.K == (nchunks - 1) * GBK + 1;
+    const int nmma = edge_k ? nchunks - 1 : nchunks;
+    // tile MT of the EDGE form (the launcher guarantees M == 16 MT + 1): the edge row, row
+    // MT*16 in its first two entries
+    double acc[NTL][4];
 #pragma unroll
-    for (int t = 0; t < MT; ++t) acc[t][0] = acc[t][1] = acc[t][2] = acc[t][3] = 0.0;
+    for (int t = 0; t < NTL; ++t) acc[t][0] = acc[t][1] = acc[t][2] = acc[t][3] = 0.0;
+    double pe = 0.0;  // the edge row: this lane's partial sum for column warp*8 + gq
 
     // lifting: per-column factors of this lane's B column, per-row factors in shared memory
     // (zero past K, so the padded rows stay zero)
@@ -97,19 +115,20 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
     // the epilogue's row factors, staged once (their global loads would otherwise sit between
     // the stores of every output element)
     if (g.epi == EPI_HELM_SCALE || g.epi == EPI_LIFT_ADD) {
-        for (int r = tid; r < MT * 16; r += NT) {
+        for (int r = tid; r < ER; r += NT) {
             const bool ok = r < g.M;
             if (g.epi == EPI_HELM_SCALE) {
                 erow[r] = ok ? g.lam[r] : 0.0;
             } else {
                 erow[r] = ok ? g.hb[r + g.roff] : 0.0;
-                erow[MT * 16 + r] = ok ? g.ht[r + g.roff] : 0.0;
+                erow[ER + r] = ok ? g.ht[r + g.roff] : 0.0;
             }
         }
     }
+    constexpr int arows = AR;
     auto load_chunk = [&](int buf, int kc) {
         // A: 16-byte copies (Kp and the chunk start are multiples of 16 doubles)
-        for (int idx = tid; idx < MT * 16 * (GBK / 2); idx += NT) {
+        for (int idx = tid; idx < arows * (GBK / 2); idx += NT) {
             const int r = idx / (GBK / 2), cp = idx % (GBK / 2);
             cp_async16(&As[buf][r][2 * cp], &g.A[(long long)r * g.Kp + kc + 2 * cp], 16);
         }
@@ -135,18 +154,29 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
         return v;
     };
 
-    const int nchunks = g.Kp / GBK;
+    // the rank-1 update's operands ride with the first chunk (16-byte pairs: K - 1, Kp and C
+    // are even)
+    const int kl = g.K - 1;
+    if (EDGE && edge_k) {
+        for (int r = tid; r < arows; r += NT) cp_async16(&kcol[2 * r], &g.A[(long long)r * g.Kp + kl], 16);
+        for (int n2 = tid; n2 < GBN / 2; n2 += NT) {
+            const long long c = c0 + 2 * n2;
+            const bool ok = c < g.C;
+            cp_async16(&krow[2 * n2], ok ? (const void*)&in[(long long)(kl + g.koff) * g.C + c] : (const void*)in,
+                       ok ? 16 : 0);
+        }
+    }
 #pragma unroll
     for (int st = 0; st < GSTAGES - 1; ++st) {
-        if (st < nchunks) load_chunk(st, st * GBK);
+        if (st < nmma) load_chunk(st, st * GBK);
         cp_async_commit();
     }
-    for (int ch = 0; ch < nchunks; ++ch) {
+    for (int ch = 0; ch < nmma; ++ch) {
         const int buf = ch % GSTAGES;
         cp_async_wait<GSTAGES - 2>();
         __syncthreads();
         // the ring slot refilled here was read in iteration ch - 1, before the barrier
-        if (ch + GSTAGES - 1 < nchunks) load_chunk((ch + GSTAGES - 1) % GSTAGES, (ch + GSTAGES - 1) * GBK);
+        if (ch + GSTAGES - 1 < nmma) load_chunk((ch + GSTAGES - 1) % GSTAGES, (ch + GSTAGES - 1) * GBK);
         cp_async_commit();
 #pragma unroll
         for (int k8 = 0; k8 < GBK / 8; ++k8) {
@@ -161,13 +191,38 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
                 const double a3 = As[buf][t * 16 + gq + 8][k8 * 8 + tq + 4];
                 dmma16(acc[t], a0, a1, a2, a3, b0, b1);
             }
+            if constexpr (EDGE) {
+                pe = fma(As[buf][AR - 1][kk], b0, pe);
+                pe = fma(As[buf][AR - 1][kk + 4], b1, pe);
+            }
         }
     }
     cp_async_wait<0>();
+    const long long cb = c0 + warp * 8 + tq * 2;
+    if (EDGE && edge_k) {
+        // the last column of A against the last row of B (the lanes' own columns; zero-filled
+        // past C)
+        const double bq0 = krow[warp * 8 + 2 * tq], bq1 = krow[warp * 8 + 2 * tq + 1];
+#pragma unroll
+        for (int t = 0; t < MT; ++t) {
+#pragma unroll
+            for (int hh = 0; hh < 2; ++hh) {
+                const double a = kcol[2 * (t * 16 + hh * 8 + gq)];
+                acc[t][2 * hh] = fma(a, bq0, acc[t][2 * hh]);
+                acc[t][2 * hh + 1] = fma(a, bq1, acc[t][2 * hh + 1]);
+            }
+        }
+        if (tq == 0) pe = fma(kcol[2 * (AR - 1)], krow[warp * 8 + gq], pe);
+    }
+    if constexpr (EDGE) {
+        pe += __shfl_xor_sync(0xffffffffu, pe, 1);
+        pe += __shfl_xor_sync(0xffffffffu, pe, 2);
+        acc[NTL - 1][0] = __shfl_sync(0xffffffffu, pe, (2 * tq) * 4);
+        acc[NTL - 1][1] = __shfl_sync(0xffffffffu, pe, (2 * tq + 1) * 4);
+    }
 
     double* __restrict__ out = (f < 4 && g.outf[f]) ? g.outf[f] : g.out + f * g.out_fstride;
     const double* __restrict__ aux = g.aux ? g.aux + f * g.out_fstride : nullptr;
-    const long long cb = c0 + warp * 8 + tq * 2;
     // per column of this thread: k^2 for the epilogues that need it, the boundary planes
     double ew2[2] = {0.0, 0.0}, eb[2] = {0.0, 0.0}, et[2] = {0.0, 0.0};
 #pragma unroll
@@ -194,7 +249,7 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
             const double wx = g.wavx[(int)((unsigned)cb % (unsigned)g.nx)];
             const double wy = g.wavy[(int)((unsigned)cb / (unsigned)g.nx)];
 #pragma unroll
-            for (int t = 0; t < MT; ++t) {
+            for (int t = 0; t < NTL; ++t) {
                 double2 nv[2], xv[2], yv[2];
 #pragma unroll
                 for (int hh = 0; hh < 2; ++hh) {
@@ -236,7 +291,7 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
             const double dt = g.pp_dt, bdfv = g.pp_bdfv;
             const double dtb = dt * bdfv;
 #pragma unroll
-            for (int t = 0; t < MT; ++t) {
+            for (int t = 0; t < NTL; ++t) {
                 double2 dv[2], uv[2], vv[2];
 #pragma unroll
                 for (int hh = 0; hh < 2; ++hh) {
@@ -265,7 +320,7 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
             }
         } else {
 #pragma unroll
-        for (int t = 0; t < MT; ++t) {
+        for (int t = 0; t < NTL; ++t) {
             // the field values this tile's epilogue reads, loaded together before its stores
             double old[4] = {0.0, 0.0, 0.0, 0.0};
             if (RD && (E == EPI_POISSON_RHS || g.beta != 0.0)) {
@@ -294,7 +349,7 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
                 } else if constexpr (E == EPI_POISSON_RHS) {
                     v = -v - ew2[e] * old[q];
                 } else if constexpr (E == EPI_LIFT_ADD) {  // acc + hb*bcb + ht*bct
-                    if (bcb != nullptr) v = v + erow[r] * eb[e] + erow[MT * 16 + r] * et[e];
+                    if (bcb != nullptr) v = v + erow[r] * eb[e] + erow[ER + r] * et[e];
                 }
                 out[(long long)(r + g.roff) * g.C + c] = v;
             }
@@ -312,25 +367,29 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
     }
 }
 
-template <int MT, int NW>
+template <int MT, int NW, bool EDGE>
 size_t gemm_smem(int Kp) {
-    return (size_t)(GSTAGES * (MT * 16 * LDA_S + GBK * (NW * 8 + 4)) + 4 * Kp + 2 * MT * 16) * sizeof(double);
+    constexpr int AR = MT * 16 + (EDGE ? 1 : 0), ER = (MT + (EDGE ? 1 : 0)) * 16;
+    return (size_t)(GSTAGES * (AR * LDA_S + GBK * (NW * 8 + 4)) + 4 * Kp + 2 * ER + (EDGE ? 2 * AR + NW * 8 : 0)) *
+           sizeof(double);
 }
 
-template <int MT, int NW>
+template <int MT, int NW, bool EDGE>
 void gemm_launch_t(const GemmArgs& g, cudaStream_t s) {
-    const size_t sm = gemm_smem<MT, NW>(g.Kp);
-    allow_smem((const void*)k_gemm<MT, NW>, sm);
+    const size_t sm = gemm_smem<MT, NW, EDGE>(g.Kp);
+    allow_smem((const void*)k_gemm<MT, NW, EDGE>, sm);
     dim3 grid((unsigned)((g.C + NW * 8 - 1) / (NW * 8)), g.nfields);
     lsb::note_launch();
-    k_gemm<MT, NW><<<grid, NW * 32, sm, s>>>(g);
+    k_gemm<MT, NW, EDGE><<<grid, NW * 32, sm, s>>>(g);
 }
 
 // fraction of the last wave's slots that are busy, averaged over the waves
-template <int MT, int NW>
+template <int MT, int NW, bool EDGE>
 double gemm_wave_eff(const GemmArgs& g) {
     const long long tiles = (g.C + NW * 8 - 1) / (NW * 8) * g.nfields;
-    const long long slots = (long long)resident_blocks((const void*)k_gemm<MT, NW>, NW * 32, gemm_smem<MT, NW>(g.Kp)) * sm_count();
+    const long long slots =
+        (long long)resident_blocks((const void*)k_gemm<MT, NW, EDGE>, NW * 32, gemm_smem<MT, NW, EDGE>(g.Kp)) *
+        sm_count();
     if (slots <= 0) return 0.0;
     const long long waves = (tiles + slots - 1) / slots;
     return (double)tiles / (double)(waves * slots);
@@ -338,10 +397,11 @@ double gemm_wave_eff(const GemmArgs& g) {
 
 // 4..8 warps (32..64 columns) per CTA, whichever leaves the least idle in the last wave
 // (ties to the wider CTA, which re-reads the matrix less)
-template <int MT>
+template <int MT, bool EDGE>
 void gemm_pick(const GemmArgs& g, cudaStream_t s) {
-    const double e8 = gemm_wave_eff<MT, 8>(g), e7 = gemm_wave_eff<MT, 7>(g), e6 = gemm_wave_eff<MT, 6>(g),
-                 e5 = gemm_wave_eff<MT, 5>(g), e4 = gemm_wave_eff<MT, 4>(g);
+    const double e8 = gemm_wave_eff<MT, 8, EDGE>(g), e7 = gemm_wave_eff<MT, 7, EDGE>(g),
+                 e6 = gemm_wave_eff<MT, 6, EDGE>(g), e5 = gemm_wave_eff<MT, 5, EDGE>(g),
+                 e4 = gemm_wave_eff<MT, 4, EDGE>(g);
     double best = e8;
     int nw = 8;
     if (e7 > best + 0.02) best = e7, nw = 7;
@@ -350,21 +410,319 @@ void gemm_pick(const GemmArgs& g, cudaStream_t s) {
     if (e4 > best + 0.02) best = e4, nw = 4;
     if (g.nw >= 4 && g.nw <= 8) nw = g.nw;  // a tuned schedule overrides the model
     switch (nw) {
-        case 8: gemm_launch_t<MT, 8>(g, s); break;
-        case 7: gemm_launch_t<MT, 7>(g, s); break;
-        case 6: gemm_launch_t<MT, 6>(g, s); break;
-        case 5: gemm_launch_t<MT, 5>(g, s); break;
-        default: gemm_launch_t<MT, 4>(g, s); break;
+        case 8: gemm_launch_t<MT, 8, EDGE>(g, s); break;
+        case 7: gemm_launch_t<MT, 7, EDGE>(g, s); break;
+        case 6: gemm_launch_t<MT, 6, EDGE>(g, s); break;
+        case 5: gemm_launch_t<MT, 5, EDGE>(g, s); break;
+        default: gemm_launch_t<MT, 4, EDGE>(g, s); break;
     }
 }
 
 void launch_gemm(const GemmArgs& g, cudaStream_t s) {
+    // M = 16 MT + 1 (nzp = 2^n + 1): MT tiles and the edge row, not a mostly-zero last tile
+    // (not under the divergence epilogue: measured slower there, 112 -> 116 us at 256x64x129)
+    const int mt = g.Mp / 16 - 1;
+    if (g.M == mt * 16 + 1 && g.epi != EPI_NLDIV) {
+        switch (mt) {
+            case 1: gemm_pick<1, true>(g, s); return;
+            case 2: gemm_pick<2, true>(g, s); return;
+            case 4: gemm_pick<4, true>(g, s); return;
+            case 8: gemm_pick<8, true>(g, s); return;
+            default: break;
+        }
+    }
     switch (g.Mp / 16) {
 #define LSB_MT(n) \
-    case n: gemm_pick<n>(g, s); break;
+    case n: gemm_pick<n, false>(g, s); break;
         LSB_MT(1) LSB_MT(2) LSB_MT(3) LSB_MT(4) LSB_MT(5) LSB_MT(6) LSB_MT(7) LSB_MT(8) LSB_MT(9)
 #undef LSB_MT
         default: break;
+    }
+}
+
+// The Helmholtz solve in one launch (src/helmholtz.f90:130-208 with the lifting of :324-353):
+// Y = E^-1 (rhs - lift) scaled by 1/(lam_r - k^2 - sigma), then out = E_ext Y + hb bcb + ht bct.
+// The CTA's Y block (all MT1*16 rows x its 8 NW columns) stays in the accumulator registers
+// of the first contraction and feeds the second as its B operand through warp shuffles, so
+// the intermediate is neither written nor re-read and the solve pays one launch tail instead
+// of two.  The second contraction runs in two row passes (registers: Y plus half of the
+// output tiles); its A chunks continue the first contraction's cp.async ring.  E_ext's one
+// row past 16 MT1 (nzp = 16 MT1 + 1: the wall row, zero in E_ext) is the edge row of
+// k_gemm, summed on the FP64 pipe in the last pass.  Every product and sum is the one the
+// two separate contractions make, in the same order.
+//
+// B regrouping: the second contraction's fragment b0 = Y[k = 16 ch + 8 k8 + tq][n = gq] of
+// lane (gq, tq) sits in accumulator acc[ch][2 k8 + (gq & 1)] of lane 4 tq + gq / 2 (the
+// accumulator holds D[8 (q / 2) + gq'][2 tq' + (q & 1)]); b1 is the row 4 further on, in lane
+// 4 (tq + 4) + gq / 2.
+template <int MT1, int NW>
+__global__ void __launch_bounds__(NW * 32, 2) k_helm(GemmArgs g1, GemmArgs g2) {
+    constexpr int NT = NW * 32, GBN = NW * 8, LDB_S = GBN + 4;
+    constexpr int P2A = (MT1 + 1) / 2, P2B = MT1 - P2A;  // output row tiles of the two passes
+    constexpr int NCH = MT1;                             // k chunks per contraction (Kp = 16 MT1)
+    constexpr int NTOT = NCH * (P2B > 0 ? 3 : 2);
+    constexpr int KP = MT1 * 16, AR = KP + 1, ER = KP + 16;
+    extern __shared__ double gsm[];
+    double (*As)[AR][LDA_S] = reinterpret_cast<double (*)[AR][LDA_S]>(gsm);
+    double (*Bs)[GBK][LDB_S] = reinterpret_cast<double (*)[GBK][LDB_S]>(gsm + GSTAGES * AR * LDA_S);
+    double* lrow = gsm + GSTAGES * (AR * LDA_S + GBK * LDB_S);  // [4][KP]: d2hb, hb, d2ht, ht
+    double* elam = lrow + 4 * KP;                               // [KP]
+    double* ehb = elam + KP;                                    // [ER]
+    double* eht = ehb + ER;                                     // [ER]
+    const bool edge = g2.M > KP;  // the launcher guarantees M <= KP + 1
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int gq = lane >> 2, tq = lane & 3;
+    const int f = blockIdx.y;
+    const long long C = g1.C;
+    const long long c0 = (long long)blockIdx.x * GBN;
+    const double* in = (f < 4 && g1.inf[f]) ? g1.inf[f] : g1.in + f * g1.in_fstride;
+    const double* bcb = g1.bcb ? g1.bcb + f * g1.bc_fstride : nullptr;
+    const double* bct = g1.bct ? g1.bct + f * g1.bc_fstride : nullptr;
+    const bool lift = bcb != nullptr;
+
+    const long long lc = c0 + warp * 8 + gq;
+    double lbcb = 0.0, lbct = 0.0, lfac = 0.0;
+    if (lift) {
+        for (int k = tid; k < KP; k += NT) {
+            const bool ok = k < g1.K;
+            const int kin = k + g1.koff;
+            lrow[k] = ok ? g1.d2hb[kin] : 0.0;
+            lrow[KP + k] = ok ? g1.hb[kin] : 0.0;
+            lrow[2 * KP + k] = ok ? g1.d2ht[kin] : 0.0;
+            lrow[3 * KP + k] = ok ? g1.ht[kin] : 0.0;
+        }
+        if (lc < C) {
+            lbcb = bcb[lc];
+            lbct = bct[lc];
+            lfac = (-w2_of(g1, lc)) - g1.lift_sigma;
+        }
+    }
+    for (int r = tid; r < KP; r += NT) elam[r] = r < g1.M ? g1.lam[r] : 0.0;
+    for (int r = tid; r < ER; r += NT) {
+        const bool ok = r < g2.M;
+        ehb[r] = ok ? g2.hb[r + g2.roff] : 0.0;
+        eht[r] = ok ? g2.ht[r + g2.roff] : 0.0;
+    }
+
+    // chunk gc of the ring: E^-1 with the right-hand side for gc < NCH, then E_ext's rows of
+    // pass 0 and of pass 1
+    auto issue = [&](int gc) {
+        const int buf = gc % GSTAGES;
+        if (gc < NCH) {
+            const int kc = gc * GBK;
+            for (int idx = tid; idx < MT1 * 16 * (GBK / 2); idx += NT) {
+                const int r = idx / (GBK / 2), cp = idx % (GBK / 2);
+                cp_async16(&As[buf][r][2 * cp], &g1.A[(long long)r * KP + kc + 2 * cp], 16);
+            }
+            for (int idx = tid; idx < GBK * (GBN / 2); idx += NT) {
+                const int kk = idx / (GBN / 2), n2 = idx % (GBN / 2);
+                const int k = kc + kk;
+                const long long c = c0 + 2 * n2;
+                const bool ok = (k < g1.K && c < C);
+                cp_async16(&Bs[buf][kk][2 * n2], ok ? (const void*)&in[(long long)(k + g1.koff) * C + c] : (const void*)in,
+                           ok ? 16 : 0);
+            }
+        } else {
+            const int p = (gc - NCH) / NCH;
+            const int kc = ((gc - NCH) % NCH) * GBK;
+            const int r0 = p ? P2A * 16 : 0;
+            // the last pass also stages the edge row (global row KP, local row 16 P)
+            const bool last = (P2B > 0) ? p == 1 : true;
+            const int nr = (p ? P2B * 16 : P2A * 16) + (last && edge ? 1 : 0);
+            for (int idx = tid; idx < nr * (GBK / 2); idx += NT) {
+                const int r = idx / (GBK / 2), cp = idx % (GBK / 2);
+                cp_async16(&As[buf][r][2 * cp], &g2.A[(long long)(r0 + r) * KP + kc + 2 * cp], 16);
+            }
+        }
+    };
+    // the slot refilled here was read in iteration gc - 1, before the barrier
+    auto advance = [&](int gc) {
+        cp_async_wait<GSTAGES - 2>();
+        __syncthreads();
+        if (gc + GSTAGES - 1 < NTOT) issue(gc + GSTAGES - 1);
+        cp_async_commit();
+    };
+    auto bval = [&](int buf, int kk, int k) {
+        double v = Bs[buf][kk][warp * 8 + gq];
+        if (lift) {
+            const double abot = lrow[k] + lfac * lrow[KP + k];
+            v = v - abot * lbcb;
+            const double atop = lrow[2 * KP + k] + lfac * lrow[3 * KP + k];
+            v = v - atop * lbct;
+        }
+        return v;
+    };
+
+    double acc[MT1][4];
+#pragma unroll
+    for (int t = 0; t < MT1; ++t) acc[t][0] = acc[t][1] = acc[t][2] = acc[t][3] = 0.0;
+#pragma unroll
+    for (int st = 0; st < GSTAGES - 1; ++st) {
+        issue(st);
+        cp_async_commit();
+    }
+    for (int ch = 0; ch < NCH; ++ch) {
+        advance(ch);
+        const int buf = ch % GSTAGES;
+#pragma unroll
+        for (int k8 = 0; k8 < GBK / 8; ++k8) {
+            const int kk = k8 * 8 + tq;
+            const double b0 = bval(buf, kk, ch * GBK + kk);
+            const double b1 = bval(buf, kk + 4, ch * GBK + kk + 4);
+#pragma unroll
+            for (int t = 0; t < MT1; ++t) {
+                const double a0 = As[buf][t * 16 + gq][k8 * 8 + tq];
+                const double a1 = As[buf][t * 16 + gq + 8][k8 * 8 + tq];
+                const double a2 = As[buf][t * 16 + gq][k8 * 8 + tq + 4];
+                const double a3 = As[buf][t * 16 + gq + 8][k8 * 8 + tq + 4];
+                dmma16(acc[t], a0, a1, a2, a3, b0, b1);
+            }
+        }
+    }
+
+    // Y = acc / (lam_r - k^2 - sigma); the padded rows and columns are zero, as the second
+    // contraction's zero-filled loads of the stored intermediate would be
+    const long long cb = c0 + warp * 8 + tq * 2;
+    double ew2[2] = {0.0, 0.0};
+#pragma unroll
+    for (int e = 0; e < 2; ++e)
+        if (cb + e < C) ew2[e] = w2_of(g1, cb + e);
+#pragma unroll
+    for (int t = 0; t < MT1; ++t) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int r = t * 16 + (q >> 1) * 8 + gq;
+            const int e = q & 1;
+            const double dfac = (-ew2[e]) - g1.sigma;
+            acc[t][q] = (r < g1.M && cb + e < C) ? acc[t][q] / (elam[r] + dfac) : 0.0;
+        }
+    }
+
+    double* __restrict__ out = (f < 4 && g2.outf[f]) ? g2.outf[f] : g2.out + f * g2.out_fstride;
+    const double* bcb2 = g2.bcb ? g2.bcb + f * g2.bc_fstride : nullptr;
+    const double* bct2 = g2.bct ? g2.bct + f * g2.bc_fstride : nullptr;
+    double eb[2] = {0.0, 0.0}, et[2] = {0.0, 0.0};
+    if (bcb2 != nullptr && cb < C) {
+        eb[0] = bcb2[cb];
+        eb[1] = bcb2[cb + 1];
+        et[0] = bct2[cb];
+        et[1] = bct2[cb + 1];
+    }
+    const int src0 = tq * 4 + (gq >> 1), src1 = (tq + 4) * 4 + (gq >> 1);
+    const bool odd = (gq & 1) != 0;
+    // one pass over output row tiles TB .. TB + P - 1 of E_ext Y, then its store
+    auto pass = [&](auto tb_c, auto p_c) {
+        constexpr int TB = decltype(tb_c)::value, P = decltype(p_c)::value;
+        constexpr bool LAST = TB + P == MT1;
+        constexpr int PT = P + (LAST ? 1 : 0);  // tile P of the last pass: the edge row
+        double acc2[PT][4];
+#pragma unroll
+        for (int t = 0; t < PT; ++t) acc2[t][0] = acc2[t][1] = acc2[t][2] = acc2[t][3] = 0.0;
+        double pe = 0.0;
+        constexpr int G0 = NCH * (TB == 0 ? 1 : 2);
+#pragma unroll
+        for (int ch = 0; ch < NCH; ++ch) {
+            advance(G0 + ch);
+            const int buf = (G0 + ch) % GSTAGES;
+#pragma unroll
+            for (int k8 = 0; k8 < GBK / 8; ++k8) {
+                const double l0 = __shfl_sync(0xffffffffu, acc[ch][2 * k8], src0);
+                const double h0 = __shfl_sync(0xffffffffu, acc[ch][2 * k8 + 1], src0);
+                const double l1 = __shfl_sync(0xffffffffu, acc[ch][2 * k8], src1);
+                const double h1 = __shfl_sync(0xffffffffu, acc[ch][2 * k8 + 1], src1);
+                const double b0 = odd ? h0 : l0, b1 = odd ? h1 : l1;
+#pragma unroll
+                for (int t = 0; t < P; ++t) {
+                    const double a0 = As[buf][t * 16 + gq][k8 * 8 + tq];
+                    const double a1 = As[buf][t * 16 + gq + 8][k8 * 8 + tq];
+                    const double a2 = As[buf][t * 16 + gq][k8 * 8 + tq + 4];
+                    const double a3 = As[buf][t * 16 + gq + 8][k8 * 8 + tq + 4];
+                    dmma16(acc2[t], a0, a1, a2, a3, b0, b1);
+                }
+                if (LAST && edge) {
+                    pe = fma(As[buf][P * 16][k8 * 8 + tq], b0, pe);
+                    pe = fma(As[buf][P * 16][k8 * 8 + tq + 4], b1, pe);
+                }
+            }
+        }
+        if (LAST && edge) {
+            pe += __shfl_xor_sync(0xffffffffu, pe, 1);
+            pe += __shfl_xor_sync(0xffffffffu, pe, 2);
+            acc2[PT - 1][0] = __shfl_sync(0xffffffffu, pe, (2 * tq) * 4);
+            acc2[PT - 1][1] = __shfl_sync(0xffffffffu, pe, (2 * tq + 1) * 4);
+        }
+        if (cb >= C) return;  // C and cb are even: cb < C covers both columns
+#pragma unroll
+        for (int t = 0; t < PT; ++t) {
+#pragma unroll
+            for (int hh = 0; hh < 2; ++hh) {
+                const int r = (TB + t) * 16 + hh * 8 + gq;
+                if (r >= g2.M) continue;
+                double v0 = acc2[t][2 * hh], v1 = acc2[t][2 * hh + 1];
+                if (bcb2 != nullptr) {
+                    v0 = v0 + ehb[r] * eb[0] + eht[r] * et[0];
+                    v1 = v1 + ehb[r] * eb[1] + eht[r] * et[1];
+                }
+                *reinterpret_cast<double2*>(out + (long long)(r + g2.roff) * C + cb) = make_double2(v0, v1);
+            }
+        }
+    };
+    pass(std::integral_constant<int, 0>{}, std::integral_constant<int, P2A>{});
+    if constexpr (P2B > 0) pass(std::integral_constant<int, P2A>{}, std::integral_constant<int, P2B>{});
+    cp_async_wait<0>();
+}
+
+template <int MT1, int NW>
+size_t helm_smem() {
+    return (size_t)(GSTAGES * ((MT1 * 16 + 1) * LDA_S + GBK * (NW * 8 + 4)) + 5 * MT1 * 16 + 2 * (MT1 + 1) * 16) *
+           sizeof(double);
+}
+
+template <int MT1, int NW>
+double helm_wave_eff(const GemmArgs& g) {
+    const long long tiles = (g.C + NW * 8 - 1) / (NW * 8) * g.nfields;
+    const long long slots =
+        (long long)resident_blocks((const void*)k_helm<MT1, NW>, NW * 32, helm_smem<MT1, NW>()) * sm_count();
+    if (slots <= 0) return 0.0;
+    const long long waves = (tiles + slots - 1) / slots;
+    return (double)tiles / (double)(waves * slots);
+}
+
+template <int MT1, int NW>
+bool helm_launch_t(const GemmArgs& g1, const GemmArgs& g2, cudaStream_t s) {
+    const size_t sm = helm_smem<MT1, NW>();
+    if (!allow_smem((const void*)k_helm<MT1, NW>, sm)) return false;
+    dim3 grid((unsigned)((g1.C + NW * 8 - 1) / (NW * 8)), g1.nfields);
+    lsb::note_launch();
+    k_helm<MT1, NW><<<grid, NW * 32, sm, s>>>(g1, g2);
+    return true;
+}
+
+// 4 or 6 warps (registers: the intermediate block and half the output tiles stay live at two
+// CTAs per SM), whichever leaves less idle in the last wave; a tuned width other than these
+// keeps the two separate contractions
+template <int MT1>
+bool helm_pick(const GemmArgs& g1, const GemmArgs& g2, cudaStream_t s) {
+    int nw = helm_wave_eff<MT1, 4>(g1) > helm_wave_eff<MT1, 6>(g1) + 0.02 ? 4 : 6;
+    if (g1.nw != 0) nw = g1.nw;
+    if (nw == 4) return helm_launch_t<MT1, 4>(g1, g2, s);
+    if (nw == 6) return helm_launch_t<MT1, 6>(g1, g2, s);
+    return false;
+}
+
+bool launch_helm_fused(const GemmArgs& g1, const GemmArgs& g2, cudaStream_t s) {
+    // the shapes the kernel assumes: E^-1 square on the padded grid, E_ext over the same k
+    // range with at most one row past it, the intermediate exactly the second contraction's
+    // input
+    if (g1.epi != EPI_HELM_SCALE || g2.epi != EPI_LIFT_ADD) return false;
+    if (g1.Kp != g1.Mp || g2.Kp != g1.Mp || g2.M > g1.Mp + 1 || g2.K != g1.M || g2.koff != 0) return false;
+    if (g1.C != g2.C || g1.nfields != g2.nfields || g2.in != g1.out || g2.inf[0] != nullptr) return false;
+    switch (g1.Mp / 16) {
+        case 1: return helm_pick<1>(g1, g2, s);
+        case 2: return helm_pick<2>(g1, g2, s);
+        case 4: return helm_pick<4>(g1, g2, s);
+        case 8: return helm_pick<8>(g1, g2, s);
+        default: return false;
     }
 }
 

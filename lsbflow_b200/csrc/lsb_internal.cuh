@@ -239,6 +239,11 @@ struct GemmArgs {
     double pp_dt, pp_bdfv;
 };
 void launch_gemm(const GemmArgs& g, cudaStream_t s);
+// the FP64 Helmholtz solve in one launch: g1 = E^-1 with the lifted right-hand side and the
+// Helmholtz scale (EPI_HELM_SCALE), g2 = E with the boundary rows and the lift (EPI_LIFT_ADD,
+// its input is g1's output); the intermediate stays in registers.  false when the shapes
+// have no fused form (the caller then launches the two contractions)
+bool launch_helm_fused(const GemmArgs& g1, const GemmArgs& g2, cudaStream_t s);
 void launch_spanwise_stats(const double* ph, double* mean, double* rms, int nf, int nx, int ny, int nzp, long long P,
                            cudaStream_t s);
 

@@ -259,7 +259,6 @@ void helmholtz(lsb_handle* h, const double* rhs, double* out, int nf, double sig
         g1.bc_fstride = 2 * C;
         g1.lift_sigma = sigma;
     }
-    contract(h, g1, tc ? h->oz_ei : OzMat{});
     GemmArgs g2 = gemm_base(h, h->m_eext);
     g2.in = h->T;
     g2.out = out;
@@ -270,6 +269,10 @@ void helmholtz(lsb_handle* h, const double* rhs, double* out, int nf, double sig
         g2.bct = bc;
         g2.bc_fstride = 2 * C;
     }
+    // both contractions on the FP64 tensor cores: one launch, the intermediate in registers
+    const bool fp64 = !(h->cfg.precision == 1 && tc);
+    if (fp64 && launch_helm_fused(g1, g2, h->stream)) return;
+    contract(h, g1, tc ? h->oz_ei : OzMat{});
     contract(h, g2, tc ? h->oz_eext : OzMat{});
 }
 

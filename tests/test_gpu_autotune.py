@@ -81,6 +81,24 @@ def test_tune_and_store(tmp_path):
 
 
 @pytest.mark.parametrize("grid", [dict(nx=256, ny=64, nz=128), dict(nx=64, ny=16, nz=64, sgsflag=0),
+                                  dict(nx=32, ny=8, nz=16, sgsflag=0), dict(nx=128, ny=24, nz=32, precision=1)],
+                         ids=["les256", "nz64", "nz16", "mixed"])
+def test_fused_helmholtz_solves_are_bit_identical(grid):
+    # the velocity and Poisson solves as one launch each (the models' widths, 4 or 6 warps:
+    # E^-1 and E_ext with the intermediate in registers, E_ext's wall row as the edge row)
+    # against the two separate contractions (gemm_warps 5): the same products and sums in
+    # the same order, with the lifted right-hand side of the non-homogeneous solves; in the
+    # mixed form only the Poisson solve has FP64 contractions to fuse
+    cfg = workload("les256", **grid)
+    st = hs.make_setup(cfg)
+    u, v, w = ic.seeded_noise(st, 13, 5e-3)
+    ref = run(st, u, v, w, {"gemm_warps": 5}, n=6)
+    got = run(st, u, v, w, {}, n=6)
+    for k in KEYS:
+        assert np.array_equal(got[k], ref[k]), k
+
+
+@pytest.mark.parametrize("grid", [dict(nx=256, ny=64, nz=128), dict(nx=64, ny=16, nz=64, sgsflag=0),
                                   dict(nx=64, ny=16, nz=16, dealias_layout="ref"), dict(nx=64, ny=16, nz=32, dealiasflag=0)],
                          ids=["les256", "dns64", "ref-layout", "no-dealias"])
 def test_tma_staged_spanwise_passes_are_bit_identical(grid):
