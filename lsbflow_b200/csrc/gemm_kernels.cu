@@ -420,9 +420,10 @@ void gemm_pick(const GemmArgs& g, cudaStream_t s) {
 
 void launch_gemm(const GemmArgs& g, cudaStream_t s) {
     // M = 16 MT + 1 (nzp = 2^n + 1): MT tiles and the edge row, not a mostly-zero last tile
-    // (not under the divergence epilogue: measured slower there, 112 -> 116 us at 256x64x129)
+    // (at 256x64x129: dz of u, v, w 90.6 -> 78.4 us, dz of h_l3 with the divergence 111 ->
+    // 102.8 us)
     const int mt = g.Mp / 16 - 1;
-    if (g.M == mt * 16 + 1 && g.epi != EPI_NLDIV) {
+    if (g.M == mt * 16 + 1) {
         switch (mt) {
             case 1: gemm_pick<1, true>(g, s); return;
             case 2: gemm_pick<2, true>(g, s); return;
