@@ -300,6 +300,9 @@ struct alignas(64) YTmaMaps {
 // [nyl][WKC] is staged double-buffered -- by cp.async (TMA = false) or by TMA tile loads that
 // complete on an mbarrier per buffer (TMA = true, 2 or 4 box loads issued by one thread) --,
 // each column is transformed by a lane group, and the tile is written back in coalesced rows.
+// (A three-buffer ring measured slower at 256 x 64 x 129: on the unpadded grid, where it keeps
+// 4 blocks per SM, 5-8 us per pass -- the larger shared-memory carve-out leaves less L1 --,
+// and on the padded grid it costs a block per SM.)
 // GC: the lane-group width as a compile-time constant (0: the plan's, at run time), so that
 // the transform's cross-lane stages unroll and their twiddle loads are issued up front;
 // 64 registers (4 blocks per SM) fit the unrolled FP64 form without spills
@@ -311,7 +314,7 @@ __global__ void __launch_bounds__(256, 4) k_ywarp(YInvJobList ij, YFwdJobList fj
     double2* smem = reinterpret_cast<double2*>(
         ysm_raw + ((1024u - (unsigned)(__cvta_generic_to_shared(ysm_raw) & 1023u)) & 1023u));
     const int ny = a.ny, nyl = a.nyl, G = GC ? GC : a.plan.g, lgg = GC ? ilog2c(GC) : a.plan.lgg;
-    double2* Buf[2] = {smem, smem + nyl * WKC};
+    auto Buf = [&](int b) { return smem + b * (nyl * WKC); };
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * nyl * WKC);  // [2] (TMA)
     int* sabort = reinterpret_cast<int*>(bar + 2);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -325,8 +328,9 @@ __global__ void __launch_bounds__(256, 4) k_ywarp(YInvJobList ij, YFwdJobList fj
     const bool split = INV && a.layout != 0 && nyl != ny;
     const int h0 = split ? ny / 2 : (INV ? ny : nyl);
     const uint32_t tile_bytes = 2u * (uint32_t)(INV ? ny : nyl) * 128u;
-    uint32_t ph[2] = {0u, 0u};
-    bool inflight[2] = {false, false};
+    // per buffer b: bit b of phm is the mbarrier phase to wait for, bit b of infm marks a load
+    // in flight (bits of a register: indexed arrays of these went to local memory)
+    uint32_t phm = 0u, infm = 0u;
     if (TMA) {
         if (tid == 0) {
             tma::mbar_init(&bar[0], 1);
@@ -337,7 +341,7 @@ __global__ void __launch_bounds__(256, 4) k_ywarp(YInvJobList ij, YFwdJobList fj
         __syncthreads();
     }
     auto issue = [&](int item, int b) {
-        double2* T = Buf[b];
+        double2* T = Buf(b);
         const int ch = item % nch, rest = item / nch, z = rest % a.nzp, jb = rest / a.nzp;
         const int c0 = ch * WKC;
         if (TMA) {
@@ -360,7 +364,7 @@ __global__ void __launch_bounds__(256, 4) k_ywarp(YInvJobList ij, YFwdJobList fj
                     if (split) tma::load_3d(dst + (nyl - (ny - h0)) * 8, map, 2 * c0 + 16 * hf, h0, z, &bar[b]);
                 }
             }
-            inflight[b] = true;
+            infm |= 1u << b;
             return;
         }
         if (INV) {
@@ -394,11 +398,11 @@ __global__ void __launch_bounds__(256, 4) k_ywarp(YInvJobList ij, YFwdJobList fj
     for (; item < nitems; item += gridDim.x) {
         const int ch = item % nch, rest = item / nch, z = rest % a.nzp, jb = rest / a.nzp;
         const int c0 = ch * WKC;
-        double2* T = Buf[cur];
+        double2* T = Buf(cur);
         if (TMA) {
-            if (tma::mbar_wait(&bar[cur], ph[cur])) {
-                ph[cur] ^= 1u;
-                inflight[cur] = false;
+            if (tma::mbar_wait(&bar[cur], (phm >> cur) & 1u)) {
+                phm ^= 1u << cur;
+                infm &= ~(1u << cur);
             } else {
                 *sabort = 1;  // the buffer stays in flight for the clean-up at the end
             }
@@ -518,7 +522,7 @@ __global__ void __launch_bounds__(256, 4) k_ywarp(YInvJobList ij, YFwdJobList fj
         // bounded wait again), and the launch's error word is raised
         if (*sabort != 0) {
             for (int b = 0; b < 2; ++b)
-                if (inflight[b]) tma::mbar_wait(&bar[b], ph[b]);
+                if ((infm >> b) & 1u) tma::mbar_wait(&bar[b], (phm >> b) & 1u);
             if (tid == 0 && a.err) atomicExch(a.err, 1);
         }
     } else {
@@ -1577,18 +1581,18 @@ void ylaunch(const YInvJobList& ij, const YFwdJobList& fj, const YPassArgs& a, c
         const uint32_t box_rows = split ? (uint32_t)(a.ny / 2) : (uint32_t)rows;
         use_tma = tmap_f64_3d(&tm.m[jb], in, (uint64_t)a.nx, rows, (uint64_t)a.nzp, 16, box_rows);
     }
-    const size_t base = (size_t)2 * a.nyl * (WKC + 1) * sizeof(double2);
-    const size_t smt = (size_t)2 * a.nyl * WKC * sizeof(double2) + 64 + 1024;
+    // the two buffers (TMA: 1024-byte alignment slack and the barriers)
+    const size_t sm = use_tma ? (size_t)2 * a.nyl * WKC * sizeof(double2) + 64 + 1024
+                              : (size_t)2 * a.nyl * (WKC + 1) * sizeof(double2);
     lsb::note_launch();
+    auto go = [&](auto kern) { kern<<<persistent_grid_w(kern, sm, nitems), 256, sm, s>>>(ij, fj, a, nch, tm); };
     if (use_tma) {
-        if (a.plan.g == 16)
-            k_ywarp<R, INV, 16, true><<<persistent_grid_w(k_ywarp<R, INV, 16, true>, smt, nitems), 256, smt, s>>>(ij, fj, a, nch, tm);
-        else
-            k_ywarp<R, INV, 0, true><<<persistent_grid_w(k_ywarp<R, INV, 0, true>, smt, nitems), 256, smt, s>>>(ij, fj, a, nch, tm);
+        if (a.plan.g == 16) go(k_ywarp<R, INV, 16, true>);
+        else go(k_ywarp<R, INV, 0, true>);
         return;
     }
-    if (a.plan.g == 16) k_ywarp<R, INV, 16><<<persistent_grid_w(k_ywarp<R, INV, 16>, base, nitems), 256, base, s>>>(ij, fj, a, nch, tm);
-    else k_ywarp<R, INV><<<persistent_grid_w(k_ywarp<R, INV>, base, nitems), 256, base, s>>>(ij, fj, a, nch, tm);
+    if (a.plan.g == 16) go(k_ywarp<R, INV, 16>);
+    else go(k_ywarp<R, INV>);
 }
 
 template <bool INV>

@@ -174,8 +174,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_filter3p(FieldL
     const int nld_v = (rows + 2) << lgrv;
     const long long plane = (long long)ny * nx;
     const int bx = nx < 256 ? nx : 256;        // TMA box width
-    uint32_t ph[RT_ST] = {0u, 0u, 0u};
-    bool inflight[RT_ST] = {false, false, false};
+    // per ring slot i: bit i of phm is the mbarrier phase to wait for, bit i of infm marks a
+    // load in flight (bits of a register: indexed arrays of these went to local memory)
+    uint32_t phm = 0u, infm = 0u;
     if (TMA) {
         if (tid == 0) {
             for (int i = 0; i < RT_ST; ++i) tma::mbar_init(&bar[i], 1);
@@ -204,7 +205,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_filter3p(FieldL
                     tma::load_2d(dst + (r << lgx) + x0, &tm.m[f], x0, kk * ny + j, &bar[sl]);
                 }
             }
-            inflight[sl] = true;
+            infm |= 1u << sl;
             return;
         }
         if (kk <= ke) {
@@ -227,9 +228,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_filter3p(FieldL
     for (int kk = ks; kk <= ke; ++kk) {
         if (TMA) {
             const int sl = kk % RT_ST;
-            if (tma::mbar_wait(&bar[sl], ph[sl])) {
-                ph[sl] ^= 1u;
-                inflight[sl] = false;
+            if (tma::mbar_wait(&bar[sl], (phm >> sl) & 1u)) {
+                phm ^= 1u << sl;
+                infm &= ~(1u << sl);
             } else {
                 *sabort = 1;  // the slot stays in flight for the clean-up below
             }
@@ -289,7 +290,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_filter3p(FieldL
         // waits again), and the launch's error word is raised
         if (*sabort != 0) {
             for (int i = 0; i < RT_ST; ++i)
-                if (inflight[i]) tma::mbar_wait(&bar[i], ph[i]);
+                if ((infm >> i) & 1u) tma::mbar_wait(&bar[i], (phm >> i) & 1u);
             if (tid == 0 && err) atomicExch(err, 1);
         }
     } else {
