@@ -74,7 +74,7 @@ struct lsb_handle {
     double *Y = nullptr;     // 18 y-intermediates on the (padded) transform grid
     double *Yu = nullptr;    // 12 y-intermediates on the unpadded grid
     double *phys = nullptr;  // physical scratch (unpadded grid), kPhys fields
-    double *bc = nullptr, *bcp = nullptr, *d2w = nullptr, *bshape = nullptr;
+    double *bc = nullptr, *bcp = nullptr, *bshape = nullptr;
     double *io = nullptr;    // host-transfer staging, 12 S
     double *red = nullptr;   // reduction scratch
     lsb::SgsWork sgs;

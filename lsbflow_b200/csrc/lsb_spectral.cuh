@@ -35,7 +35,9 @@ struct BcArgs {
     const double* pwall;      // wall plane of p^n
     const double* pnwall;     // wall plane of p^(n-1)
     int top_free;             // 1: u' = v = 0 on the ceiling (bctype 3, bc3_top = 1)
-    const double* d2w;        // [2][C] rows 1 and nzp of d2fdz2(w^n)
+    const double* w;          // w^n ([nzp][C]): rows 1 and nzp of its d2fdz2 are formed in the kernel
+    const double* d2rows;     // the two rows of the Chebyshev second derivative, row stride d2ld
+    int d2ld, nzp;
     const double* btop;       // spectral shape planes of bound(), or null
     const double* bwa;
     const double* bwb;

@@ -757,13 +757,6 @@ void step_one(lsb_handle* h) {
     double pfac0 = 2.0, pfac1 = -1.0;
     if (h->istep == 1) { pfac0 = 0.0; pfac1 = 0.0; }
     else if (h->istep == 2) { pfac0 = 1.0; pfac1 = 0.0; }
-    {
-        TimerScope ts(h, "bc_planes");
-        GemmArgs g = gemm_base(h, h->m_dz2rows);  // rows 1 and nzp of d2fdz2(w^n)
-        g.in = h->veln + 2 * S;
-        g.out = h->d2w;
-        launch_gemm(g, st);
-    }
     const bool active = c.bctype > 0 && h->t >= c.istartbound;
     BcArgs ba{};
     for (int l = 0; l < 3; ++l) {
@@ -774,7 +767,10 @@ void step_one(lsb_handle* h) {
     ba.pwall = h->p + (long long)(d.nzp - 1) * C;
     ba.pnwall = h->pn + (long long)(d.nzp - 1) * C;
     ba.top_free = (c.bctype == 3 && c.bc3_top == 1) ? 1 : 0;
-    ba.d2w = h->d2w;
+    ba.w = h->veln + 2 * S;  // rows 1 and nzp of d2fdz2(w^n), formed by the kernel
+    ba.d2rows = h->m_dz2rows.p;
+    ba.d2ld = h->m_dz2rows.Kp;
+    ba.nzp = d.nzp;
     ba.btop = h->bshape;
     ba.bwa = h->bshape + C;
     ba.bwb = h->bshape + 2 * C;
@@ -1342,7 +1338,6 @@ int lsb_create(const lsb_config* cfg, const lsb_setup* su, lsb_handle** out) {
         h->phys = h->alloc((long long)lsb_handle::kPhys * h->P);
         h->bc = h->alloc(6 * C);
         h->bcp = h->alloc(2 * C);
-        h->d2w = h->alloc(2 * C);
         h->bshape = h->alloc(3 * C);
         h->io = h->alloc(12 * S);
         h->red = h->alloc(512);

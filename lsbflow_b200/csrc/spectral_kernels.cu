@@ -63,9 +63,41 @@ __global__ void k_rhs(RhsArgs a) {
 // ---------------------------------------------------------------- boundary planes
 // Zang-Hussaini BCs of src/navierstokes.f90:1320-1373; bc[f][0] = ceiling (k=1),
 // bc[f][1] = wall (k=nzp).  Bound planes = c_top*btop, c_wa*bwa + c_wb*bwb.
-__global__ void k_bc_planes(BcArgs a) {
+// The ceiling and wall rows of d2fdz2(w^n) (src/navierstokes.f90:1340-1345) are formed here:
+// a block owns BC_MODES (kx, ky) modes, warp s sums the z points k = s, s + 8, ... of both rows
+// for its lane's mode (each z row of the field read as contiguous 16-byte modes), the eight
+// partial sums meet in shared memory and warp 0 writes the planes.
+constexpr int BC_MODES = 32, BC_SLICES = 8;
+__global__ void __launch_bounds__(BC_MODES * BC_SLICES) k_bc_planes(BcArgs a) {
+    __shared__ double2 part[BC_SLICES][2][BC_MODES];
+    const int lane = threadIdx.x & (BC_MODES - 1), sl = threadIdx.x / BC_MODES;
     const long long n2 = a.C / 2;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n2; e += (long long)gridDim.x * blockDim.x) {
+    const long long e = (long long)blockIdx.x * BC_MODES + lane;
+    double2 p0 = make_double2(0.0, 0.0), p1 = make_double2(0.0, 0.0);
+    if (e < n2) {
+        const double2* w = reinterpret_cast<const double2*>(a.w);
+#pragma unroll 4
+        for (int k = sl; k < a.nzp; k += BC_SLICES) {
+            const double2 wk = w[(long long)k * n2 + e];
+            const double d0 = a.d2rows[k], d1 = a.d2rows[a.d2ld + k];
+            p0.x = fma(d0, wk.x, p0.x);
+            p0.y = fma(d0, wk.y, p0.y);
+            p1.x = fma(d1, wk.x, p1.x);
+            p1.y = fma(d1, wk.y, p1.y);
+        }
+    }
+    part[sl][0][lane] = p0;
+    part[sl][1][lane] = p1;
+    __syncthreads();
+    if (sl == 0 && e < n2) {
+        double2 d2t = part[0][0][lane], d2b = part[0][1][lane];  // ceiling and wall rows
+#pragma unroll
+        for (int t = 1; t < BC_SLICES; ++t) {
+            d2t.x += part[t][0][lane].x;
+            d2t.y += part[t][0][lane].y;
+            d2b.x += part[t][1][lane].x;
+            d2b.y += part[t][1][lane].y;
+        }
         int i, j;
         ij_of(e, a.nx, i, j);
         const double wx = a.wavx[i], wy = a.wavy[j];
@@ -97,8 +129,8 @@ __global__ void k_bc_planes(BcArgs a) {
             if (a.btop) { tr = a.ctop * a.btop[re]; ti = a.ctop * a.btop[im]; }
             if (a.bwa) { wr = a.cwa * a.bwa[re]; wi = a.cwa * a.bwa[im]; }
             if (a.bwb) { wr += a.cwb * a.bwb[re]; wi += a.cwb * a.bwb[im]; }
-            a.bc[2][re] = tr + zh * a.d2w[re];
-            a.bc[2][im] = ti + zh * a.d2w[im];
+            a.bc[2][re] = tr + zh * d2t.x;
+            a.bc[2][im] = ti + zh * d2t.y;
             a.bc[2][a.C + re] = wr;
             a.bc[2][a.C + im] = wi;
             // the pressure step's w BC (bound() again, src/navierstokes.f90:1432-1433)
@@ -107,10 +139,10 @@ __global__ void k_bc_planes(BcArgs a) {
             a.bcp[a.C + re] = wr;
             a.bcp[a.C + im] = wi;
         } else {
-            a.bc[2][re] = zh * a.d2w[re];
-            a.bc[2][im] = zh * a.d2w[im];
-            a.bc[2][a.C + re] = zh * a.d2w[a.C + re];
-            a.bc[2][a.C + im] = zh * a.d2w[a.C + im];
+            a.bc[2][re] = zh * d2t.x;
+            a.bc[2][im] = zh * d2t.y;
+            a.bc[2][a.C + re] = zh * d2b.x;
+            a.bc[2][a.C + im] = zh * d2b.y;
             a.bcp[re] = 0.0;
             a.bcp[im] = 0.0;
             a.bcp[a.C + re] = 0.0;
@@ -230,7 +262,10 @@ static inline int nblk(long long n) {
 
 void launch_specfilter(const SpecFilterArgs& a, cudaStream_t s) { lsb::note_launch(); k_specfilter<<<nblk(3 * a.S / 2), 256, 0, s>>>(a); }
 void launch_rhs(const RhsArgs& a, cudaStream_t s) { lsb::note_launch(); k_rhs<<<nblk(3 * a.S), 256, 0, s>>>(a); }
-void launch_bc_planes(const BcArgs& a, cudaStream_t s) { lsb::note_launch(); k_bc_planes<<<nblk(a.C / 2), 256, 0, s>>>(a); }
+void launch_bc_planes(const BcArgs& a, cudaStream_t s) {
+    lsb::note_launch();
+    k_bc_planes<<<(unsigned)((a.C / 2 + BC_MODES - 1) / BC_MODES), BC_MODES * BC_SLICES, 0, s>>>(a);
+}
 void launch_divuv(const double* u, const double* v, double* out, const double* wavx, const double* wavy, int nx,
                   long long S, long long C, cudaStream_t s) {
     { lsb::note_launch(); k_divuv<<<nblk(S / 2), 256, 0, s>>>(u, v, out, wavx, wavy, nx, S, C); }
