@@ -1313,18 +1313,29 @@ __global__ void __launch_bounds__(128, (R <= 6 ? NLR_MINB : 3)) k_row_nl_r(NlRow
 // FP32 variants for the mixed-precision step: y-intermediates are FP32, the transforms run
 // in FP32 with FP32 twiddles; the spectral fields on either side stay FP64 (converted on
 // load and store).  Same work items and layouts as k_ywarp.
+__device__ __forceinline__ void cpa8(void* sdst, const void* gsrc) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gsrc));
+}
+
+// The tile is the FP64 pass's: [nyl][WKC] 16-byte slots under its row swizzle, double-buffered
+// by cp.async -- the inverse stages its FP64 spectral input as it is (converted to FP32 when
+// the transform reads it), the forward its FP32 input in the first half of each slot --, and
+// the transform's FP32 results go to the first half of the slots.  (The single-buffered form
+// that converted on load left each item's load latency exposed.)
 template <int R, bool INV, int GC = 0>
-__global__ void __launch_bounds__(256) k_ywarp_f(YInvJobList ij, YFwdJobList fj, YPassArgs a, int nch) {
-    extern __shared__ float2 fsm[];
+__global__ void __launch_bounds__(256, 4) k_ywarp_f(YInvJobList ij, YFwdJobList fj, YPassArgs a, int nch) {
+    extern __shared__ __align__(16) double2 fsm2[];
     const int ny = a.ny, nyl = a.nyl, G = GC ? GC : a.plan.g, lgg = GC ? ilog2c(GC) : a.plan.lgg;
-    constexpr int TS = WKC + 1;
-    float2* T = fsm;
+    auto Buf = [&](int b) { return fsm2 + b * (nyl * WKC); };
+    auto SL = [&](double2* T, int row, int col) { return reinterpret_cast<float2*>(T + ytix<R>(row, col)); };
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int njobs = INV ? ij.n : fj.n;
     const int nitems = njobs * a.nzp * nch;
     const int lpw = 32 / G;
     const int q = lane / G, g = lane - q * G;
-    for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+    auto issue = [&](int item, int b) {
+        double2* T = Buf(b);
         const int ch = item % nch, rest = item / nch, z = rest % a.nzp, jb = rest / a.nzp;
         const int c0 = ch * WKC;
         if (INV) {
@@ -1332,23 +1343,31 @@ __global__ void __launch_bounds__(256) k_ywarp_f(YInvJobList ij, YFwdJobList fj,
             for (int idx = tid; idx < nyl * WKC; idx += 256) {
                 const int jl = idx / WKC, cc = idx - jl * WKC, c = c0 + cc;
                 const int j = unpad_row(jl, ny, nyl, a.layout);
-                float2 v = make_float2(0.f, 0.f);
-                if (j >= 0 && c < a.kxc) {
-                    const double2 d = __ldg(reinterpret_cast<const double2*>(in + ((long long)z * ny + j) * a.nx) + c);
-                    v = make_float2((float)d.x, (float)d.y);
-                }
-                T[jl * TS + cc] = v;
+                double2* d = T + ytix<R>(jl, cc);
+                if (j >= 0 && c < a.kxc) cpa16(d, in + ((long long)z * ny + j) * a.nx + 2 * c);
+                else *d = make_double2(0.0, 0.0);
             }
         } else {
             const float* in = reinterpret_cast<const float*>(fj.j[jb].in);
             for (int idx = tid; idx < nyl * WKC; idx += 256) {
                 const int jl = idx / WKC, cc = idx - jl * WKC, c = c0 + cc;
-                T[jl * TS + cc] = (c < a.kxc)
-                    ? __ldg(reinterpret_cast<const float2*>(in + ((long long)z * nyl + jl) * a.nx) + c)
-                    : make_float2(0.f, 0.f);
+                float2* d = SL(T, jl, cc);
+                if (c < a.kxc) cpa8(d, in + ((long long)z * nyl + jl) * a.nx + 2 * c);
+                else *d = make_float2(0.f, 0.f);
             }
         }
-        __syncthreads();
+        cpa_commit();
+    };
+    int cur = 0;
+    int item = blockIdx.x;
+    if (item < nitems) issue(item, 0);
+    for (; item < nitems; item += gridDim.x) {
+        const int ch = item % nch, rest = item / nch, z = rest % a.nzp, jb = rest / a.nzp;
+        const int c0 = ch * WKC;
+        double2* T = Buf(cur);
+        cpa_wait_all();
+        __syncthreads();  // this item's tile has landed; every thread is done with the other buffer
+        if (item + (int)gridDim.x < nitems) issue(item + gridDim.x, cur ^ 1);
         const int mode = INV ? ij.j[jb].mode : YM_COPY;
         for (int L0 = warp * lpw; L0 < WKC; L0 += 8 * lpw) {
             const int L = L0 + q;
@@ -1358,7 +1377,13 @@ __global__ void __launch_bounds__(256) k_ywarp_f(YInvJobList ij, YFwdJobList fj,
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 const int n = g + G * r;
-                float2 x = T[n * TS + Lc];
+                float2 x;
+                if (INV) {
+                    const double2 d = T[ytix<R>(n, Lc)];
+                    x = make_float2((float)d.x, (float)d.y);
+                } else {
+                    x = *SL(T, n, Lc);
+                }
                 if (INV && mode != YM_COPY) {
                     float k = 0.f;
                     if (mode == YM_IKY) {
@@ -1377,7 +1402,7 @@ __global__ void __launch_bounds__(256) k_ywarp_f(YInvJobList ij, YFwdJobList fj,
                 __syncwarp();
                 if (act) {
 #pragma unroll
-                    for (int k1 = 0; k1 < R; ++k1) T[xslot<R, 16>(g, k1) * TS + L] = v[k1];
+                    for (int k1 = 0; k1 < R; ++k1) *SL(T, xslot<R, 16>(g, k1), L) = v[k1];
                 }
             } else {
                 wfft<R, INV ? +1 : -1>(v, G, g, a.plan.twf);
@@ -1385,7 +1410,7 @@ __global__ void __launch_bounds__(256) k_ywarp_f(YInvJobList ij, YFwdJobList fj,
                 __syncwarp();
                 if (act) {
 #pragma unroll
-                    for (int k1 = 0; k1 < R; ++k1) T[(R * g + k1) * TS + L] = v[k1];
+                    for (int k1 = 0; k1 < R; ++k1) *SL(T, R * g + k1, L) = v[k1];
                 }
             }
         }
@@ -1395,7 +1420,7 @@ __global__ void __launch_bounds__(256) k_ywarp_f(YInvJobList ij, YFwdJobList fj,
             for (int idx = tid; idx < nyl * WKC; idx += 256) {
                 const int jl = idx / WKC, cc = idx - jl * WKC, c = c0 + cc;
                 if (c >= a.kxc) continue;
-                *reinterpret_cast<float2*>(out + ((long long)z * nyl + jl) * a.nx + 2 * c) = T[jl * TS + cc];
+                *reinterpret_cast<float2*>(out + ((long long)z * nyl + jl) * a.nx + 2 * c) = *SL(T, jl, cc);
             }
         } else {
             const YFwdJob job = fj.j[jb];
@@ -1403,11 +1428,11 @@ __global__ void __launch_bounds__(256) k_ywarp_f(YInvJobList ij, YFwdJobList fj,
                 for (int idx = tid; idx < ny * WKC; idx += 256) {
                     const int j = idx / WKC, cc = idx - j * WKC, c = c0 + cc;
                     if (c >= a.kxc) continue;
-                    const float2 vf = T[pad_row_w(j, ny, nyl, a.layout) * TS + cc];
+                    const float2 vf = *SL(T, pad_row_w(j, ny, nyl, a.layout), cc);
                     double2 v = make_double2((double)vf.x, (double)vf.y);
                     if (job.sym && c == 0) {
                         const int jm = (ny - j) % ny;
-                        const float2 wf = T[pad_row_w(jm, ny, nyl, a.layout) * TS + cc];
+                        const float2 wf = *SL(T, pad_row_w(jm, ny, nyl, a.layout), cc);
                         v = make_double2(0.5 * (v.x + (double)wf.x), 0.5 * (v.y - (double)wf.y));
                     }
                     v.x *= a.scale;
@@ -1432,11 +1457,11 @@ __global__ void __launch_bounds__(256) k_ywarp_f(YInvJobList ij, YFwdJobList fj,
                     const int idx = i0 + e * 256;
                     const int j = idx / WKC, cc = idx - j * WKC, c = c0 + cc;
                     if (idx >= ny * WKC || c >= a.kxc) continue;
-                    const float2 vf = T[pad_row_w(j, ny, nyl, a.layout) * TS + cc];
+                    const float2 vf = *SL(T, pad_row_w(j, ny, nyl, a.layout), cc);
                     double2 v = make_double2((double)vf.x, (double)vf.y);
                     if (job.sym && c == 0) {
                         const int jm = (ny - j) % ny;
-                        const float2 wf = T[pad_row_w(jm, ny, nyl, a.layout) * TS + cc];
+                        const float2 wf = *SL(T, pad_row_w(jm, ny, nyl, a.layout), cc);
                         v = make_double2(0.5 * (v.x + (double)wf.x), 0.5 * (v.y - (double)wf.y));
                     }
                     v.x *= a.scale;
@@ -1453,7 +1478,9 @@ __global__ void __launch_bounds__(256) k_ywarp_f(YInvJobList ij, YFwdJobList fj,
             }
         }
         __syncthreads();
+        cur ^= 1;
     }
+    cpa_wait_all();
 }
 
 // k_row_nl_r in FP32: FP32 rows in and out, same slot layout.  The streamwise velocity is
@@ -1558,7 +1585,7 @@ void ylaunch(const YInvJobList& ij, const YFwdJobList& fj, const YPassArgs& a, c
     const int nch = (a.kxc + WKC - 1) / WKC;
     const int nitems = (INV ? ij.n : fj.n) * a.nzp * nch;
     if (a.f32) {
-        const size_t smf = (size_t)a.nyl * (WKC + 1) * sizeof(float2);
+        const size_t smf = (size_t)2 * a.nyl * WKC * sizeof(double2);
         lsb::note_launch();
         if (a.plan.g == 16) k_ywarp_f<R, INV, 16><<<persistent_grid_w(k_ywarp_f<R, INV, 16>, smf, nitems), 256, smf, s>>>(ij, fj, a, nch);
         else k_ywarp_f<R, INV><<<persistent_grid_w(k_ywarp_f<R, INV>, smf, nitems), 256, smf, s>>>(ij, fj, a, nch);
