@@ -64,10 +64,10 @@ __global__ void k_rhs(RhsArgs a) {
 // Zang-Hussaini BCs of src/navierstokes.f90:1320-1373; bc[f][0] = ceiling (k=1),
 // bc[f][1] = wall (k=nzp).  Bound planes = c_top*btop, c_wa*bwa + c_wb*bwb.
 // The ceiling and wall rows of d2fdz2(w^n) (src/navierstokes.f90:1340-1345) are formed here:
-// a block owns BC_MODES (kx, ky) modes, warp s sums the z points k = s, s + 8, ... of both rows
-// for its lane's mode (each z row of the field read as contiguous 16-byte modes), the eight
-// partial sums meet in shared memory and warp 0 writes the planes.
-constexpr int BC_MODES = 32, BC_SLICES = 8;
+// a block owns BC_MODES (kx, ky) modes, warp s sums the z points k = s, s + 16, ... of both
+// rows for its lane's mode (each z row of the field read as contiguous 16-byte modes), the
+// sixteen partial sums meet in shared memory and warp 0 writes the planes.
+constexpr int BC_MODES = 32, BC_SLICES = 16;
 __global__ void __launch_bounds__(BC_MODES * BC_SLICES) k_bc_planes(BcArgs a) {
     __shared__ double2 part[BC_SLICES][2][BC_MODES];
     const int lane = threadIdx.x & (BC_MODES - 1), sl = threadIdx.x / BC_MODES;
@@ -76,7 +76,7 @@ __global__ void __launch_bounds__(BC_MODES * BC_SLICES) k_bc_planes(BcArgs a) {
     double2 p0 = make_double2(0.0, 0.0), p1 = make_double2(0.0, 0.0);
     if (e < n2) {
         const double2* w = reinterpret_cast<const double2*>(a.w);
-#pragma unroll 4
+#pragma unroll 8
         for (int k = sl; k < a.nzp; k += BC_SLICES) {
             const double2 wk = w[(long long)k * n2 + e];
             const double d0 = a.d2rows[k], d1 = a.d2rows[a.d2ld + k];
