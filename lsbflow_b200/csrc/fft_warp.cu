@@ -1313,6 +1313,14 @@ __global__ void __launch_bounds__(128, (R <= 6 ? NLR_MINB : 3)) k_row_nl_r(NlRow
 // FP32 variants for the mixed-precision step: y-intermediates are FP32, the transforms run
 // in FP32 with FP32 twiddles; the spectral fields on either side stay FP64 (converted on
 // load and store).  Same work items and layouts as k_ywarp.
+// column swizzle of the FP32 compact spanwise tile (16 columns of 8 bytes per row): conflict-free
+// for the natural-order reads (rows g + 16 r) and the exchange network's slot-order writes
+// (rows xslot(g, k)) of 16-lane groups, checked for every column and R = 2, 4, 6, 8
+template <int R>
+__device__ __forceinline__ int fsw(int row) {
+    return R == 6 ? (row & 15) : ((row ^ (row >> 4)) & 15);
+}
+
 __device__ __forceinline__ void cpa8(void* sdst, const void* gsrc) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gsrc));
@@ -1329,6 +1337,14 @@ __global__ void __launch_bounds__(256, 4) k_ywarp_f(YInvJobList ij, YFwdJobList 
     const int ny = a.ny, nyl = a.nyl, G = GC ? GC : a.plan.g, lgg = GC ? ilog2c(GC) : a.plan.lgg;
     auto Buf = [&](int b) { return fsm2 + b * (nyl * WKC); };
     auto SL = [&](double2* T, int row, int col) { return reinterpret_cast<float2*>(T + ytix<R>(row, col)); };
+    // the exchange-network form keeps its FP32 values in a compact tile of 128-byte rows (column
+    // c of row r at r * WKC + (c ^ fsw<R>(r))): 16 lanes then reach 16 distinct 8-byte
+    // positions of a line in the natural-order reads, the slot-order write-back and the row
+    // stores (8-byte values in 16-byte slots reach half of a line's banks: 2-way conflicts)
+    constexpr bool CMP = (GC == 16 && R % 2 == 0);
+    auto OUT = [&](double2* T, int row, int col) {
+        return CMP ? reinterpret_cast<float2*>(T) + row * WKC + (col ^ fsw<R>(row)) : SL(T, row, col);
+    };
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int njobs = INV ? ij.n : fj.n;
     const int nitems = njobs * a.nzp * nch;
@@ -1351,7 +1367,7 @@ __global__ void __launch_bounds__(256, 4) k_ywarp_f(YInvJobList ij, YFwdJobList 
             const float* in = reinterpret_cast<const float*>(fj.j[jb].in);
             for (int idx = tid; idx < nyl * WKC; idx += 256) {
                 const int jl = idx / WKC, cc = idx - jl * WKC, c = c0 + cc;
-                float2* d = SL(T, jl, cc);
+                float2* d = OUT(T, jl, cc);
                 if (c < a.kxc) cpa8(d, in + ((long long)z * nyl + jl) * a.nx + 2 * c);
                 else *d = make_float2(0.f, 0.f);
             }
@@ -1382,7 +1398,7 @@ __global__ void __launch_bounds__(256, 4) k_ywarp_f(YInvJobList ij, YFwdJobList 
                     const double2 d = T[ytix<R>(n, Lc)];
                     x = make_float2((float)d.x, (float)d.y);
                 } else {
-                    x = *SL(T, n, Lc);
+                    x = *OUT(T, n, Lc);
                 }
                 if (INV && mode != YM_COPY) {
                     float k = 0.f;
@@ -1399,10 +1415,13 @@ __global__ void __launch_bounds__(256, 4) k_ywarp_f(YInvJobList ij, YFwdJobList 
             }
             if constexpr (GC == 16 && R % 2 == 0) {
                 wfft_x<R, INV ? +1 : -1, 16>(v, g, a.plan.twf);
-                __syncwarp();
+                // the inverse's compact results overlay FP64 input slots of other columns: every
+                // warp has read its columns first (this loop runs once per warp at 16-lane groups)
+                if (INV) __syncthreads();
+                else __syncwarp();
                 if (act) {
 #pragma unroll
-                    for (int k1 = 0; k1 < R; ++k1) *SL(T, xslot<R, 16>(g, k1), L) = v[k1];
+                    for (int k1 = 0; k1 < R; ++k1) *OUT(T, xslot<R, 16>(g, k1), L) = v[k1];
                 }
             } else {
                 wfft<R, INV ? +1 : -1>(v, G, g, a.plan.twf);
@@ -1420,7 +1439,7 @@ __global__ void __launch_bounds__(256, 4) k_ywarp_f(YInvJobList ij, YFwdJobList 
             for (int idx = tid; idx < nyl * WKC; idx += 256) {
                 const int jl = idx / WKC, cc = idx - jl * WKC, c = c0 + cc;
                 if (c >= a.kxc) continue;
-                *reinterpret_cast<float2*>(out + ((long long)z * nyl + jl) * a.nx + 2 * c) = *SL(T, jl, cc);
+                *reinterpret_cast<float2*>(out + ((long long)z * nyl + jl) * a.nx + 2 * c) = *OUT(T, jl, cc);
             }
         } else {
             const YFwdJob job = fj.j[jb];
@@ -1428,11 +1447,11 @@ __global__ void __launch_bounds__(256, 4) k_ywarp_f(YInvJobList ij, YFwdJobList 
                 for (int idx = tid; idx < ny * WKC; idx += 256) {
                     const int j = idx / WKC, cc = idx - j * WKC, c = c0 + cc;
                     if (c >= a.kxc) continue;
-                    const float2 vf = *SL(T, pad_row_w(j, ny, nyl, a.layout), cc);
+                    const float2 vf = *OUT(T, pad_row_w(j, ny, nyl, a.layout), cc);
                     double2 v = make_double2((double)vf.x, (double)vf.y);
                     if (job.sym && c == 0) {
                         const int jm = (ny - j) % ny;
-                        const float2 wf = *SL(T, pad_row_w(jm, ny, nyl, a.layout), cc);
+                        const float2 wf = *OUT(T, pad_row_w(jm, ny, nyl, a.layout), cc);
                         v = make_double2(0.5 * (v.x + (double)wf.x), 0.5 * (v.y - (double)wf.y));
                     }
                     v.x *= a.scale;
@@ -1457,11 +1476,11 @@ __global__ void __launch_bounds__(256, 4) k_ywarp_f(YInvJobList ij, YFwdJobList 
                     const int idx = i0 + e * 256;
                     const int j = idx / WKC, cc = idx - j * WKC, c = c0 + cc;
                     if (idx >= ny * WKC || c >= a.kxc) continue;
-                    const float2 vf = *SL(T, pad_row_w(j, ny, nyl, a.layout), cc);
+                    const float2 vf = *OUT(T, pad_row_w(j, ny, nyl, a.layout), cc);
                     double2 v = make_double2((double)vf.x, (double)vf.y);
                     if (job.sym && c == 0) {
                         const int jm = (ny - j) % ny;
-                        const float2 wf = *SL(T, pad_row_w(jm, ny, nyl, a.layout), cc);
+                        const float2 wf = *OUT(T, pad_row_w(jm, ny, nyl, a.layout), cc);
                         v = make_double2(0.5 * (v.x + (double)wf.x), 0.5 * (v.y - (double)wf.y));
                     }
                     v.x *= a.scale;
