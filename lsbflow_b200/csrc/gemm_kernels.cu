@@ -456,17 +456,20 @@ void launch_gemm(const GemmArgs& g, cudaStream_t s) {
 // lane (gq, tq) sits in accumulator acc[ch][2 k8 + (gq & 1)] of lane 4 tq + gq / 2 (the
 // accumulator holds D[8 (q / 2) + gq'][2 tq' + (q & 1)]); b1 is the row 4 further on, in lane
 // 4 (tq + 4) + gq / 2.
-template <int MT1, int NW>
+template <int MT1, int NW, int KC>
 __global__ void __launch_bounds__(NW * 32, 2) k_helm(GemmArgs g1, GemmArgs g2) {
     constexpr int NT = NW * 32, GBN = NW * 8, LDB_S = GBN + 4;
     constexpr int P2A = (MT1 + 1) / 2, P2B = MT1 - P2A;  // output row tiles of the two passes
-    constexpr int NCH = MT1;                             // k chunks per contraction (Kp = 16 MT1)
+    // k chunks of KC columns: 16 in a 3-stage ring, or 32 in a double buffer (half the
+    // barriers per contraction)
+    constexpr int HK = KC, HST = (KC == 32 ? 2 : GSTAGES), HLDA = (KC == 32 ? 36 : LDA_S);
+    constexpr int NCH = MT1 * 16 / KC;                   // k chunks per contraction (Kp = 16 MT1)
     constexpr int NTOT = NCH * (P2B > 0 ? 3 : 2);
     constexpr int KP = MT1 * 16, AR = KP + 1, ER = KP + 16;
     extern __shared__ double gsm[];
-    double (*As)[AR][LDA_S] = reinterpret_cast<double (*)[AR][LDA_S]>(gsm);
-    double (*Bs)[GBK][LDB_S] = reinterpret_cast<double (*)[GBK][LDB_S]>(gsm + GSTAGES * AR * LDA_S);
-    double* lrow = gsm + GSTAGES * (AR * LDA_S + GBK * LDB_S);  // [4][KP]: d2hb, hb, d2ht, ht
+    double (*As)[AR][HLDA] = reinterpret_cast<double (*)[AR][HLDA]>(gsm);
+    double (*Bs)[HK][LDB_S] = reinterpret_cast<double (*)[HK][LDB_S]>(gsm + HST * AR * HLDA);
+    double* lrow = gsm + HST * (AR * HLDA + HK * LDB_S);  // [4][KP]: d2hb, hb, d2ht, ht
     double* elam = lrow + 4 * KP;                               // [KP]
     double* ehb = elam + KP;                                    // [ER]
     double* eht = ehb + ER;                                     // [ER]
@@ -508,14 +511,14 @@ __global__ void __launch_bounds__(NW * 32, 2) k_helm(GemmArgs g1, GemmArgs g2) {
     // chunk gc of the ring: E^-1 with the right-hand side for gc < NCH, then E_ext's rows of
     // pass 0 and of pass 1
     auto issue = [&](int gc) {
-        const int buf = gc % GSTAGES;
+        const int buf = gc % HST;
         if (gc < NCH) {
-            const int kc = gc * GBK;
-            for (int idx = tid; idx < MT1 * 16 * (GBK / 2); idx += NT) {
-                const int r = idx / (GBK / 2), cp = idx % (GBK / 2);
+            const int kc = gc * HK;
+            for (int idx = tid; idx < MT1 * 16 * (HK / 2); idx += NT) {
+                const int r = idx / (HK / 2), cp = idx % (HK / 2);
                 cp_async16(&As[buf][r][2 * cp], &g1.A[(long long)r * KP + kc + 2 * cp], 16);
             }
-            for (int idx = tid; idx < GBK * (GBN / 2); idx += NT) {
+            for (int idx = tid; idx < HK * (GBN / 2); idx += NT) {
                 const int kk = idx / (GBN / 2), n2 = idx % (GBN / 2);
                 const int k = kc + kk;
                 const long long c = c0 + 2 * n2;
@@ -525,22 +528,22 @@ __global__ void __launch_bounds__(NW * 32, 2) k_helm(GemmArgs g1, GemmArgs g2) {
             }
         } else {
             const int p = (gc - NCH) / NCH;
-            const int kc = ((gc - NCH) % NCH) * GBK;
+            const int kc = ((gc - NCH) % NCH) * HK;
             const int r0 = p ? P2A * 16 : 0;
             // the last pass also stages the edge row (global row KP, local row 16 P)
             const bool last = (P2B > 0) ? p == 1 : true;
             const int nr = (p ? P2B * 16 : P2A * 16) + (last && edge ? 1 : 0);
-            for (int idx = tid; idx < nr * (GBK / 2); idx += NT) {
-                const int r = idx / (GBK / 2), cp = idx % (GBK / 2);
+            for (int idx = tid; idx < nr * (HK / 2); idx += NT) {
+                const int r = idx / (HK / 2), cp = idx % (HK / 2);
                 cp_async16(&As[buf][r][2 * cp], &g2.A[(long long)(r0 + r) * KP + kc + 2 * cp], 16);
             }
         }
     };
     // the slot refilled here was read in iteration gc - 1, before the barrier
     auto advance = [&](int gc) {
-        cp_async_wait<GSTAGES - 2>();
+        cp_async_wait<HST - 2>();
         __syncthreads();
-        if (gc + GSTAGES - 1 < NTOT) issue(gc + GSTAGES - 1);
+        if (gc + HST - 1 < NTOT) issue(gc + HST - 1);
         cp_async_commit();
     };
     auto bval = [&](int buf, int kk, int k) {
@@ -558,18 +561,18 @@ __global__ void __launch_bounds__(NW * 32, 2) k_helm(GemmArgs g1, GemmArgs g2) {
 #pragma unroll
     for (int t = 0; t < MT1; ++t) acc[t][0] = acc[t][1] = acc[t][2] = acc[t][3] = 0.0;
 #pragma unroll
-    for (int st = 0; st < GSTAGES - 1; ++st) {
+    for (int st = 0; st < HST - 1; ++st) {
         issue(st);
         cp_async_commit();
     }
     for (int ch = 0; ch < NCH; ++ch) {
         advance(ch);
-        const int buf = ch % GSTAGES;
+        const int buf = ch % HST;
 #pragma unroll
-        for (int k8 = 0; k8 < GBK / 8; ++k8) {
+        for (int k8 = 0; k8 < HK / 8; ++k8) {
             const int kk = k8 * 8 + tq;
-            const double b0 = bval(buf, kk, ch * GBK + kk);
-            const double b1 = bval(buf, kk + 4, ch * GBK + kk + 4);
+            const double b0 = bval(buf, kk, ch * HK + kk);
+            const double b1 = bval(buf, kk + 4, ch * HK + kk + 4);
 #pragma unroll
             for (int t = 0; t < MT1; ++t) {
                 const double a0 = As[buf][t * 16 + gq][k8 * 8 + tq];
@@ -624,13 +627,15 @@ __global__ void __launch_bounds__(NW * 32, 2) k_helm(GemmArgs g1, GemmArgs g2) {
 #pragma unroll
         for (int ch = 0; ch < NCH; ++ch) {
             advance(G0 + ch);
-            const int buf = (G0 + ch) % GSTAGES;
+            const int buf = (G0 + ch) % HST;
 #pragma unroll
-            for (int k8 = 0; k8 < GBK / 8; ++k8) {
-                const double l0 = __shfl_sync(0xffffffffu, acc[ch][2 * k8], src0);
-                const double h0 = __shfl_sync(0xffffffffu, acc[ch][2 * k8 + 1], src0);
-                const double l1 = __shfl_sync(0xffffffffu, acc[ch][2 * k8], src1);
-                const double h1 = __shfl_sync(0xffffffffu, acc[ch][2 * k8 + 1], src1);
+            for (int k8 = 0; k8 < HK / 8; ++k8) {
+                // rows 8 k8 .. of chunk ch are rows 8 (k8 % 2) .. of Y tile ch * KC / 16 + k8 / 2
+                const int yt = ch * (HK / 16) + (k8 >> 1), yk = k8 & 1;
+                const double l0 = __shfl_sync(0xffffffffu, acc[yt][2 * yk], src0);
+                const double h0 = __shfl_sync(0xffffffffu, acc[yt][2 * yk + 1], src0);
+                const double l1 = __shfl_sync(0xffffffffu, acc[yt][2 * yk], src1);
+                const double h1 = __shfl_sync(0xffffffffu, acc[yt][2 * yk + 1], src1);
                 const double b0 = odd ? h0 : l0, b1 = odd ? h1 : l1;
 #pragma unroll
                 for (int t = 0; t < P; ++t) {
@@ -673,41 +678,43 @@ __global__ void __launch_bounds__(NW * 32, 2) k_helm(GemmArgs g1, GemmArgs g2) {
     cp_async_wait<0>();
 }
 
-template <int MT1, int NW>
+template <int MT1, int NW, int KC>
 size_t helm_smem() {
-    return (size_t)(GSTAGES * ((MT1 * 16 + 1) * LDA_S + GBK * (NW * 8 + 4)) + 5 * MT1 * 16 + 2 * (MT1 + 1) * 16) *
+    constexpr int HST = (KC == 32 ? 2 : GSTAGES), HLDA = (KC == 32 ? 36 : LDA_S);
+    return (size_t)(HST * ((MT1 * 16 + 1) * HLDA + KC * (NW * 8 + 4)) + 5 * MT1 * 16 + 2 * (MT1 + 1) * 16) *
            sizeof(double);
 }
 
-template <int MT1, int NW>
+template <int MT1, int NW, int KC>
 double helm_wave_eff(const GemmArgs& g) {
     const long long tiles = (g.C + NW * 8 - 1) / (NW * 8) * g.nfields;
     const long long slots =
-        (long long)resident_blocks((const void*)k_helm<MT1, NW>, NW * 32, helm_smem<MT1, NW>()) * sm_count();
+        (long long)resident_blocks((const void*)k_helm<MT1, NW, KC>, NW * 32, helm_smem<MT1, NW, KC>()) * sm_count();
     if (slots <= 0) return 0.0;
     const long long waves = (tiles + slots - 1) / slots;
     return (double)tiles / (double)(waves * slots);
 }
 
-template <int MT1, int NW>
+template <int MT1, int NW, int KC>
 bool helm_launch_t(const GemmArgs& g1, const GemmArgs& g2, cudaStream_t s) {
-    const size_t sm = helm_smem<MT1, NW>();
-    if (!allow_smem((const void*)k_helm<MT1, NW>, sm)) return false;
+    const size_t sm = helm_smem<MT1, NW, KC>();
+    if (!allow_smem((const void*)k_helm<MT1, NW, KC>, sm)) return false;
     dim3 grid((unsigned)((g1.C + NW * 8 - 1) / (NW * 8)), g1.nfields);
     lsb::note_launch();
-    k_helm<MT1, NW><<<grid, NW * 32, sm, s>>>(g1, g2);
+    k_helm<MT1, NW, KC><<<grid, NW * 32, sm, s>>>(g1, g2);
     return true;
 }
 
 // 4 or 6 warps (registers: the intermediate block and half the output tiles stay live at two
 // CTAs per SM), whichever leaves less idle in the last wave; a tuned width other than these
-// keeps the two separate contractions
+// keeps the two separate contractions.  k chunks of 32 where Kp allows
 template <int MT1>
 bool helm_pick(const GemmArgs& g1, const GemmArgs& g2, cudaStream_t s) {
-    int nw = helm_wave_eff<MT1, 4>(g1) > helm_wave_eff<MT1, 6>(g1) + 0.02 ? 4 : 6;
+    constexpr int KC = (MT1 % 2 == 0) ? 32 : 16;
+    int nw = helm_wave_eff<MT1, 4, KC>(g1) > helm_wave_eff<MT1, 6, KC>(g1) + 0.02 ? 4 : 6;
     if (g1.nw != 0) nw = g1.nw;
-    if (nw == 4) return helm_launch_t<MT1, 4>(g1, g2, s);
-    if (nw == 6) return helm_launch_t<MT1, 6>(g1, g2, s);
+    if (nw == 4) return helm_launch_t<MT1, 4, KC>(g1, g2, s);
+    if (nw == 6) return helm_launch_t<MT1, 6, KC>(g1, g2, s);
     return false;
 }
 
