@@ -11,16 +11,16 @@
 //
 // tcgen05 has no FP64 kind, so the FP64 form uses the FP64 tensor-core MMA
 // (mma.sync m16n8k8 f64: 1024 FMAs per instruction).  One CTA owns all Mp rows of a block
-// of 32..64 columns (8 per warp), A and B staged through shared memory in k-chunks of 16 with
-// conflict-free strides.
+// of 32..64 columns (8 per warp), A and B staged through shared memory in k-chunks of 16 (a
+// 3-stage ring) or 32 (a double buffer) with conflict-free strides.
 #include <type_traits>
 
 #include "lsb_internal.cuh"
 
 namespace lsb {
 
-constexpr int GBK = 16;
-constexpr int LDA_S = 20;  // doubles; 8r mod 32 distinct for r = 0..3 -> no bank conflicts
+constexpr int LDA_S = 20;  // doubles; 8r mod 32 distinct for r = 0..3 -> no bank conflicts (36 for
+                           // the 32-column chunks: the same residues)
 
 // D (16x8) += A (16x8) B (8x8).  Fragments (g = lane / 4, t = lane % 4): a = A[g][t],
 // A[g+8][t], A[g][t+4], A[g+8][t+4]; b = B[t][g], B[t+4][g]; c = D[g][2t], D[g][2t+1],
@@ -63,15 +63,18 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // EDGE instantiations (M = 16 MT + 1); the others compile without them.
 constexpr int GSTAGES = 3;
 
-template <int MT, int NW, bool EDGE>
+template <int MT, int NW, bool EDGE, int KC = 16>
 __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
     constexpr int NT = NW * 32, GBN = NW * 8, LDB_S = GBN + 4;  // GBN + 4 = 4 or 12 mod 16: conflict-free
+    // k chunks of KC columns: 16 in a 3-stage ring, or 32 in a double buffer (half the barriers;
+    // the launcher takes it where the chunks end exactly at Kp or at the rank-1 column)
+    constexpr int HK = KC, HST = (KC == 32 ? 2 : GSTAGES), HLDA = (KC == 32 ? 36 : LDA_S);
     constexpr int NTL = MT + (EDGE ? 1 : 0);                     // accumulator tiles (+ the edge row)
     constexpr int AR = MT * 16 + (EDGE ? 1 : 0), ER = NTL * 16;  // A rows staged, epilogue row stride
     extern __shared__ double gsm[];
-    double (*As)[AR][LDA_S] = reinterpret_cast<double (*)[AR][LDA_S]>(gsm);
-    double (*Bs)[GBK][LDB_S] = reinterpret_cast<double (*)[GBK][LDB_S]>(gsm + GSTAGES * AR * LDA_S);
-    double* lrow = gsm + GSTAGES * (AR * LDA_S + GBK * LDB_S);  // [4][Kp]: d2hb, hb, d2ht, ht
+    double (*As)[AR][HLDA] = reinterpret_cast<double (*)[AR][HLDA]>(gsm);
+    double (*Bs)[HK][LDB_S] = reinterpret_cast<double (*)[HK][LDB_S]>(gsm + HST * AR * HLDA);
+    double* lrow = gsm + HST * (AR * HLDA + HK * LDB_S);  // [4][Kp]: d2hb, hb, d2ht, ht
     double* erow = lrow + 4 * g.Kp;  // [2][ER]: the epilogue's row factors (lam, or hb and ht)
     double* kcol = erow + 2 * ER;    // [AR][2]: A[r][K-1], A[r][K] of the rank-1 update
     double* krow = kcol + 2 * AR;    // [GBN]: B[K-1][c0 ..] of the rank-1 update
@@ -83,8 +86,8 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
     const double* bcb = g.bcb ? g.bcb + f * g.bc_fstride : nullptr;
     const double* bct = g.bct ? g.bct + f * g.bc_fstride : nullptr;
     const bool lift = (g.epi != 5) && (bcb != nullptr);
-    const int nchunks = g.Kp / GBK;
-    const bool edge_k = EDGE && !lift && nchunks > 1 && g.K == (nchunks - 1) * GBK + 1;
+    const int nchunks = (g.Kp + HK - 1) / HK;
+    const bool edge_k = EDGE && !lift && nchunks > 1 && g.K == (nchunks - 1) * HK + 1;
     const int nmma = edge_k ? nchunks - 1 : nchunks;
     // tile MT of the EDGE form (the launcher guarantees M == 16 MT + 1): the edge row, row
     // MT*16 in its first two entries
@@ -128,12 +131,12 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
     constexpr int arows = AR;
     auto load_chunk = [&](int buf, int kc) {
         // A: 16-byte copies (Kp and the chunk start are multiples of 16 doubles)
-        for (int idx = tid; idx < arows * (GBK / 2); idx += NT) {
-            const int r = idx / (GBK / 2), cp = idx % (GBK / 2);
+        for (int idx = tid; idx < arows * (HK / 2); idx += NT) {
+            const int r = idx / (HK / 2), cp = idx % (HK / 2);
             cp_async16(&As[buf][r][2 * cp], &g.A[(long long)r * g.Kp + kc + 2 * cp], 16);
         }
         // B: 16-byte copies of column pairs (C and the field stride are even)
-        for (int idx = tid; idx < GBK * (GBN / 2); idx += NT) {
+        for (int idx = tid; idx < HK * (GBN / 2); idx += NT) {
             const int kk = idx / (GBN / 2), n2 = idx % (GBN / 2);
             const int k = kc + kk;
             const long long c = c0 + 2 * n2;
@@ -167,22 +170,22 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
         }
     }
 #pragma unroll
-    for (int st = 0; st < GSTAGES - 1; ++st) {
-        if (st < nmma) load_chunk(st, st * GBK);
+    for (int st = 0; st < HST - 1; ++st) {
+        if (st < nmma) load_chunk(st, st * HK);
         cp_async_commit();
     }
     for (int ch = 0; ch < nmma; ++ch) {
-        const int buf = ch % GSTAGES;
-        cp_async_wait<GSTAGES - 2>();
+        const int buf = ch % HST;
+        cp_async_wait<HST - 2>();
         __syncthreads();
         // the ring slot refilled here was read in iteration ch - 1, before the barrier
-        if (ch + GSTAGES - 1 < nmma) load_chunk((ch + GSTAGES - 1) % GSTAGES, (ch + GSTAGES - 1) * GBK);
+        if (ch + HST - 1 < nmma) load_chunk((ch + HST - 1) % HST, (ch + HST - 1) * HK);
         cp_async_commit();
 #pragma unroll
-        for (int k8 = 0; k8 < GBK / 8; ++k8) {
+        for (int k8 = 0; k8 < HK / 8; ++k8) {
             const int kk = k8 * 8 + tq;
-            const double b0 = bval(buf, kk, ch * GBK + kk);
-            const double b1 = bval(buf, kk + 4, ch * GBK + kk + 4);
+            const double b0 = bval(buf, kk, ch * HK + kk);
+            const double b1 = bval(buf, kk + 4, ch * HK + kk + 4);
 #pragma unroll
             for (int t = 0; t < MT; ++t) {
                 const double a0 = As[buf][t * 16 + gq][k8 * 8 + tq];
@@ -367,28 +370,29 @@ __global__ void __launch_bounds__(NW * 32) k_gemm(GemmArgs g) {
     }
 }
 
-template <int MT, int NW, bool EDGE>
+template <int MT, int NW, bool EDGE, int KC = 16>
 size_t gemm_smem(int Kp) {
     constexpr int AR = MT * 16 + (EDGE ? 1 : 0), ER = (MT + (EDGE ? 1 : 0)) * 16;
-    return (size_t)(GSTAGES * (AR * LDA_S + GBK * (NW * 8 + 4)) + 4 * Kp + 2 * ER + (EDGE ? 2 * AR + NW * 8 : 0)) *
+    constexpr int HST = (KC == 32 ? 2 : GSTAGES), HLDA = (KC == 32 ? 36 : LDA_S);
+    return (size_t)(HST * (AR * HLDA + KC * (NW * 8 + 4)) + 4 * Kp + 2 * ER + (EDGE ? 2 * AR + NW * 8 : 0)) *
            sizeof(double);
 }
 
-template <int MT, int NW, bool EDGE>
+template <int MT, int NW, bool EDGE, int KC = 16>
 void gemm_launch_t(const GemmArgs& g, cudaStream_t s) {
-    const size_t sm = gemm_smem<MT, NW, EDGE>(g.Kp);
-    allow_smem((const void*)k_gemm<MT, NW, EDGE>, sm);
+    const size_t sm = gemm_smem<MT, NW, EDGE, KC>(g.Kp);
+    allow_smem((const void*)k_gemm<MT, NW, EDGE, KC>, sm);
     dim3 grid((unsigned)((g.C + NW * 8 - 1) / (NW * 8)), g.nfields);
     lsb::note_launch();
-    k_gemm<MT, NW, EDGE><<<grid, NW * 32, sm, s>>>(g);
+    k_gemm<MT, NW, EDGE, KC><<<grid, NW * 32, sm, s>>>(g);
 }
 
 // fraction of the last wave's slots that are busy, averaged over the waves
-template <int MT, int NW, bool EDGE>
+template <int MT, int NW, bool EDGE, int KC = 16>
 double gemm_wave_eff(const GemmArgs& g) {
     const long long tiles = (g.C + NW * 8 - 1) / (NW * 8) * g.nfields;
     const long long slots =
-        (long long)resident_blocks((const void*)k_gemm<MT, NW, EDGE>, NW * 32, gemm_smem<MT, NW, EDGE>(g.Kp)) *
+        (long long)resident_blocks((const void*)k_gemm<MT, NW, EDGE, KC>, NW * 32, gemm_smem<MT, NW, EDGE, KC>(g.Kp)) *
         sm_count();
     if (slots <= 0) return 0.0;
     const long long waves = (tiles + slots - 1) / slots;
@@ -397,11 +401,11 @@ double gemm_wave_eff(const GemmArgs& g) {
 
 // 4..8 warps (32..64 columns) per CTA, whichever leaves the least idle in the last wave
 // (ties to the wider CTA, which re-reads the matrix less)
-template <int MT, bool EDGE>
+template <int MT, bool EDGE, int KC = 16>
 void gemm_pick(const GemmArgs& g, cudaStream_t s) {
-    const double e8 = gemm_wave_eff<MT, 8, EDGE>(g), e7 = gemm_wave_eff<MT, 7, EDGE>(g),
-                 e6 = gemm_wave_eff<MT, 6, EDGE>(g), e5 = gemm_wave_eff<MT, 5, EDGE>(g),
-                 e4 = gemm_wave_eff<MT, 4, EDGE>(g);
+    const double e8 = gemm_wave_eff<MT, 8, EDGE, KC>(g), e7 = gemm_wave_eff<MT, 7, EDGE, KC>(g),
+                 e6 = gemm_wave_eff<MT, 6, EDGE, KC>(g), e5 = gemm_wave_eff<MT, 5, EDGE, KC>(g),
+                 e4 = gemm_wave_eff<MT, 4, EDGE, KC>(g);
     double best = e8;
     int nw = 8;
     if (e7 > best + 0.02) best = e7, nw = 7;
@@ -410,11 +414,11 @@ void gemm_pick(const GemmArgs& g, cudaStream_t s) {
     if (e4 > best + 0.02) best = e4, nw = 4;
     if (g.nw >= 4 && g.nw <= 8) nw = g.nw;  // a tuned schedule overrides the model
     switch (nw) {
-        case 8: gemm_launch_t<MT, 8, EDGE>(g, s); break;
-        case 7: gemm_launch_t<MT, 7, EDGE>(g, s); break;
-        case 6: gemm_launch_t<MT, 6, EDGE>(g, s); break;
-        case 5: gemm_launch_t<MT, 5, EDGE>(g, s); break;
-        default: gemm_launch_t<MT, 4, EDGE>(g, s); break;
+        case 8: gemm_launch_t<MT, 8, EDGE, KC>(g, s); break;
+        case 7: gemm_launch_t<MT, 7, EDGE, KC>(g, s); break;
+        case 6: gemm_launch_t<MT, 6, EDGE, KC>(g, s); break;
+        case 5: gemm_launch_t<MT, 5, EDGE, KC>(g, s); break;
+        default: gemm_launch_t<MT, 4, EDGE, KC>(g, s); break;
     }
 }
 
@@ -424,11 +428,18 @@ void launch_gemm(const GemmArgs& g, cudaStream_t s) {
     // 102.8 us)
     const int mt = g.Mp / 16 - 1;
     if (g.M == mt * 16 + 1) {
+        // k chunks of 32 where they end exactly at Kp, or at the rank-1 column, for the light
+        // epilogues (at 256x64x129: dz of u, v, w 80.3 -> 77.4 us, the Poisson right-hand side
+        // -1.8 us; the divergence and pressure epilogues, which read three fields per element,
+        // measured slower with them, 103 -> 121 and 47 -> 52 us)
+        const bool lift = g.epi != EPI_LIFT_ADD && g.bcb != nullptr;
+        const bool k32 = (g.epi == EPI_STORE || g.epi == EPI_POISSON_RHS) &&
+                         (g.Kp % 32 == 0 || (!lift && g.K == g.Kp - 15 && (g.Kp - 16) % 32 == 0));
         switch (mt) {
             case 1: gemm_pick<1, true>(g, s); return;
             case 2: gemm_pick<2, true>(g, s); return;
-            case 4: gemm_pick<4, true>(g, s); return;
-            case 8: gemm_pick<8, true>(g, s); return;
+            case 4: k32 ? gemm_pick<4, true, 32>(g, s) : gemm_pick<4, true>(g, s); return;
+            case 8: k32 ? gemm_pick<8, true, 32>(g, s) : gemm_pick<8, true>(g, s); return;
             default: break;
         }
     }
